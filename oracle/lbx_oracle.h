@@ -1,0 +1,39 @@
+/*
+ * lbx_oracle.h -- parameters of the CPU restatement in lbx_oracle.c.
+ * TEST INFRASTRUCTURE ONLY (see lbx_oracle.c).
+ *
+ * Field meanings follow the reference's params.in (src/params.h:40-660) and
+ * the __constant__ block its kernels read (src/lattice.c:2224-2268).
+ */
+#ifndef LBX_ORACLE_H
+#define LBX_ORACLE_H
+#include <stdint.h>
+
+typedef struct {
+  int dims;                 /* 2 (D2Q9) or 3 (D3Q19) */
+  int LX, LY, LZ;           /* LZ == 1 for dims == 2 */
+  int nsubs;                /* 1 = flow; 2 = flow + solute (Inamuro sigma) */
+  int accurate;             /* 1 = shifted populations d = f - w rho_A */
+  int compressible;         /* 0 = He-Luo incompressible */
+  double tau[2], rho_A[2], gaccel[6], sink;
+  int sigma_t_on, sigma_t_off;
+  /* 2D Zou-He / zero-gradient faces (src/bcs.c GPU branches) */
+  int pressure_n_in[2], pressure_s_in[2], pressure_n_out[2], pressure_s_out[2];
+  int zeroconcgrad_n, zeroconcgrad_s;
+  double rho_in, rho_out, pfadd, pfmul;
+  int bc_ramp_start, bc_ramp_stop;
+  const double* pressure_n_table; int pressure_n_len;
+  const double* pressure_s_table; int pressure_s_len;
+} orc_params;
+
+int orc_run_f64(const orc_params*, double* f, const uint8_t* solids,
+                double* mv, int t0, int nsteps, int frame_rate,
+                int nthreads);
+int orc_run_f32(const orc_params*, float* f, const uint8_t* solids,
+                float* mv, int t0, int nsteps, int frame_rate,
+                int nthreads);
+int orc_init_feq_f64(const orc_params*, const double* rho, const double* ux,
+                     const double* uy, const double* uz, double* f);
+int orc_init_feq_f32(const orc_params*, const float* rho, const float* ux,
+                     const float* uy, const float* uz, float* f);
+#endif

@@ -1,0 +1,235 @@
+"""ctypes access to the CPU oracle and to the reference-kernel harness.
+
+TEST INFRASTRUCTURE ONLY.  Imported by tests/, __graft_entry__.smoke() and the
+CPU-baseline leg of bench.py, never by the product package.
+
+* ``run_oracle`` -- oracle/liblbx_oracle.so, the C restatement of the
+  reference's GPU path (oracle/lbx_oracle.c).
+* ``run_reference`` -- oracle/_ref/librefk_<variant>.so, the reference's own
+  kernel sources compiled for the CPU (oracle/refk_harness.c).  Present only
+  where the reference tree was available at build time.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass, field
+from typing import Optional
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "liblbx_oracle.so")
+REF_DIR = os.path.join(HERE, "_ref")
+
+
+@dataclass
+class Params:
+    """Run parameters, named as in the reference's params.in."""
+    dims: int = 3
+    LX: int = 8
+    LY: int = 8
+    LZ: int = 8
+    nsubs: int = 1
+    accurate: int = 1
+    compressible: int = 0
+    tau: tuple = (1.0, 1.0)
+    rho_A: tuple = (1.0, 1.0)
+    gaccel: tuple = (0.0,) * 6
+    sink: float = 0.0
+    sigma_t_on: int = 0
+    sigma_t_off: int = 1 << 30
+    pressure_n_in: tuple = (0, 0)
+    pressure_s_in: tuple = (0, 0)
+    pressure_n_out: tuple = (0, 0)
+    pressure_s_out: tuple = (0, 0)
+    zeroconcgrad_n: int = 0
+    zeroconcgrad_s: int = 0
+    rho_in: float = 1.0
+    rho_out: float = 1.0
+    pfadd: float = 1.0
+    pfmul: float = 0.1
+    bc_ramp_start: int = -1
+    bc_ramp_stop: int = -1
+    pressure_n_table: Optional[np.ndarray] = None
+    pressure_s_table: Optional[np.ndarray] = None
+
+    @property
+    def Q(self) -> int:
+        return 9 if self.dims == 2 else 19
+
+    @property
+    def NN(self) -> int:
+        return self.LX * self.LY * self.LZ
+
+
+_D2 = C.c_double * 2
+_D6 = C.c_double * 6
+_I2 = C.c_int * 2
+
+
+class _OrcParams(C.Structure):
+    _fields_ = [
+        ("dims", C.c_int), ("LX", C.c_int), ("LY", C.c_int), ("LZ", C.c_int),
+        ("nsubs", C.c_int), ("accurate", C.c_int), ("compressible", C.c_int),
+        ("tau", _D2), ("rho_A", _D2), ("gaccel", _D6), ("sink", C.c_double),
+        ("sigma_t_on", C.c_int), ("sigma_t_off", C.c_int),
+        ("pressure_n_in", _I2), ("pressure_s_in", _I2),
+        ("pressure_n_out", _I2), ("pressure_s_out", _I2),
+        ("zeroconcgrad_n", C.c_int), ("zeroconcgrad_s", C.c_int),
+        ("rho_in", C.c_double), ("rho_out", C.c_double),
+        ("pfadd", C.c_double), ("pfmul", C.c_double),
+        ("bc_ramp_start", C.c_int), ("bc_ramp_stop", C.c_int),
+        ("pressure_n_table", C.POINTER(C.c_double)), ("pressure_n_len", C.c_int),
+        ("pressure_s_table", C.POINTER(C.c_double)), ("pressure_s_len", C.c_int),
+    ]
+
+
+class _RefParams(C.Structure):
+    _fields_ = [
+        ("LX", C.c_int), ("LY", C.c_int), ("LZ", C.c_int),
+        ("tau", _D2), ("rho_A", _D2), ("gaccel", _D6), ("sink", C.c_double),
+        ("sigma_t_on", C.c_int), ("sigma_t_off", C.c_int),
+        ("pressure_n_in", _I2), ("pressure_s_in", _I2),
+        ("pressure_n_out", _I2), ("pressure_s_out", _I2),
+        ("zeroconcgrad_n", C.c_int), ("zeroconcgrad_s", C.c_int),
+        ("rho_in", C.c_double), ("rho_out", C.c_double),
+        ("pfadd", C.c_double), ("pfmul", C.c_double),
+        ("bc_ramp_start", C.c_int), ("bc_ramp_stop", C.c_int),
+        ("pressure_n_table", C.POINTER(C.c_double)), ("pressure_n_len", C.c_int),
+        ("pressure_s_table", C.POINTER(C.c_double)), ("pressure_s_len", C.c_int),
+    ]
+
+
+def _fill(st, p: Params, keep):
+    for name, _ in st._fields_:
+        if name.endswith("_table"):
+            tab = getattr(p, name)
+            if tab is not None:
+                arr = np.ascontiguousarray(tab, dtype=np.float64)
+                keep.append(arr)
+                setattr(st, name, arr.ctypes.data_as(C.POINTER(C.c_double)))
+                setattr(st, name.replace("_table", "_len"), len(arr))
+            continue
+        if name.endswith("_len"):
+            continue
+        v = getattr(p, name)
+        if isinstance(v, tuple):
+            fld = getattr(st, name)
+            for i, x in enumerate(v):
+                fld[i] = x
+        else:
+            setattr(st, name, v)
+
+
+_oracle = None
+
+
+def _lib():
+    global _oracle
+    if _oracle is None:
+        if not os.path.exists(ORACLE_SO):
+            raise RuntimeError("oracle not built: run `make -C oracle`")
+        lib = C.CDLL(ORACLE_SO)
+        for sfx, ct in (("f64", C.c_double), ("f32", C.c_float)):
+            fn = getattr(lib, "orc_run_" + sfx)
+            fn.argtypes = [C.POINTER(_OrcParams), C.POINTER(ct), C.c_void_p,
+                           C.POINTER(ct), C.c_int, C.c_int, C.c_int, C.c_int]
+            fn.restype = C.c_int
+            fn = getattr(lib, "orc_init_feq_" + sfx)
+            fn.argtypes = [C.POINTER(_OrcParams)] + [C.POINTER(ct)] * 4 + [C.POINTER(ct)]
+            fn.restype = C.c_int
+        _oracle = lib
+    return _oracle
+
+
+def _ct(dtype):
+    return C.c_double if np.dtype(dtype) == np.float64 else C.c_float
+
+
+def _sfx(dtype):
+    return "f64" if np.dtype(dtype) == np.float64 else "f32"
+
+
+def run_oracle(p: Params, f: np.ndarray, solids: np.ndarray, t0: int,
+               nsteps: int, frame_rate: int = 0, mv: Optional[np.ndarray] = None,
+               threads: int = 0):
+    """Advance f ([nsubs, Q, N], float64 or float32) in place; returns (f, mv)."""
+    dtype = f.dtype
+    assert f.flags.c_contiguous and f.size == p.nsubs * p.Q * p.NN
+    sol = np.ascontiguousarray(solids, dtype=np.uint8).reshape(-1)
+    assert sol.size == p.NN
+    if mv is None:
+        mv = np.zeros((p.nsubs, 1 + p.dims, p.NN), dtype=dtype)
+    keep = []
+    st = _OrcParams()
+    _fill(st, p, keep)
+    nt = threads or min(os.cpu_count() or 1, 64)
+    rc = getattr(_lib(), "orc_run_" + _sfx(dtype))(
+        C.byref(st), f.ctypes.data_as(C.POINTER(_ct(dtype))),
+        sol.ctypes.data, mv.ctypes.data_as(C.POINTER(_ct(dtype))),
+        t0, nsteps, frame_rate, nt)
+    if rc != 0:
+        raise ValueError("orc_run rejected the parameters")
+    return f, mv
+
+
+def init_feq(p: Params, rho: np.ndarray, ux: np.ndarray, uy: np.ndarray,
+             uz: Optional[np.ndarray], dtype=np.float64) -> np.ndarray:
+    """Equilibrium initial state; rho/u are [nsubs, N]."""
+    f = np.zeros((p.nsubs, p.Q, p.NN), dtype=dtype)
+    arrs = [np.ascontiguousarray(x, dtype=dtype).reshape(p.nsubs, p.NN)
+            for x in (rho, ux, uy, uz if uz is not None else np.zeros_like(rho))]
+    st = _OrcParams()
+    _fill(st, p, [])
+    ct = C.POINTER(_ct(dtype))
+    getattr(_lib(), "orc_init_feq_" + _sfx(dtype))(
+        C.byref(st), *[a.ctypes.data_as(ct) for a in arrs], f.ctypes.data_as(ct))
+    return f
+
+
+_refs = {}
+
+
+def reference_available(variant: str) -> bool:
+    return os.path.exists(os.path.join(REF_DIR, "librefk_%s.so" % variant))
+
+
+def run_reference(variant: str, p: Params, f: np.ndarray, solids: np.ndarray,
+                  t0: int, nsteps: int, frame_rate: int = 0,
+                  mv: Optional[np.ndarray] = None):
+    """Same contract as run_oracle, through the reference's own kernels."""
+    if variant not in _refs:
+        lib = C.CDLL(os.path.join(REF_DIR, "librefk_%s.so" % variant))
+        lib.refk_run.restype = C.c_int
+        lib.refk_real_size.restype = C.c_int
+        _refs[variant] = lib
+    lib = _refs[variant]
+    rs = lib.refk_real_size()
+    assert f.dtype.itemsize == rs, "variant precision mismatch"
+    assert lib.refk_num_dims() == p.dims and lib.refk_num_subs() == p.nsubs
+    assert lib.refk_accurate() == p.accurate
+    assert lib.refk_compressible() == p.compressible
+    sol = np.ascontiguousarray(solids, dtype=np.uint8).reshape(-1)
+    if mv is None:
+        mv = np.zeros((p.nsubs, 1 + p.dims, p.NN), dtype=f.dtype)
+    keep = []
+    st = _RefParams()
+    _fill(st, p, keep)
+    rc = lib.refk_run(C.byref(st), f.ctypes.data_as(C.c_void_p),
+                      sol.ctypes.data_as(C.c_void_p),
+                      mv.ctypes.data_as(C.c_void_p), t0, nsteps, frame_rate)
+    if rc != 0:
+        raise ValueError("refk_run rejected the parameters")
+    return f, mv
+
+
+def variant_name(p: Params, dtype) -> str:
+    base = "d2q9" if p.dims == 2 else "d3q19"
+    if p.nsubs == 2:
+        base += "s"
+    elif not p.accurate:
+        base += "p"
+    elif p.compressible:
+        base += "c"
+    return base + "_" + _sfx(dtype)

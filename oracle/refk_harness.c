@@ -1,0 +1,280 @@
+/*
+ * refk_harness.c -- runs the reference's own CUDA kernel sources on the CPU.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This file is the checker's checker: it pins the
+ * C restatement in oracle/lbx_oracle.c against the reference's own kernel
+ * code.  Nothing in the product path links or calls it.
+ *
+ * Built by oracle/ref_build.py, which force-includes a variant of the
+ * reference's src/flags.h and puts the reference's src/ on the include path.
+ * The reference files are compiled where they lie; nothing is copied.
+ *
+ * How a launch is emulated: every kernel is launched with one-thread blocks
+ * (BX=BY=BZ=1), so the per-thread shared-memory scratch `fptr` is one
+ * (Q+D+1)-entry array, and the grid is walked block by block.  The reference
+ * kernels are data-parallel with a disjoint read/write slot set per node
+ * (src/k_stream_collide_stream.c:46-67 pulls and :401-423 pushes the same
+ * slots; src/k_collide.c:53-77 and :408-416 touch only the node's own slots),
+ * so the sequential walk computes what the GPU launch computes.
+ *
+ * The host orchestration that cannot be compiled here (src/bcs.c uses <<<>>>
+ * launch syntax; src/lbgpu_prime.cu is the CUDA main) is restated below with
+ * file:line citations: the per-step order of src/lbgpu_prime.cu:369-915 and
+ * the density schedule of src/bcs.c:278-558 / :1231-1506.
+ */
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <math.h>
+#include <assert.h>
+#include <time.h>
+
+#if DP_ON
+typedef double real;
+#else
+typedef float real;
+#endif
+
+/* CUDA keywords and built-ins for a host build. */
+#define __global__
+#define __device__
+#define __constant__
+#define __shared__
+#define __CUDACC__ 1
+#define __CUDA_ARCH__ 1000
+typedef struct { unsigned int x, y, z; } refk_dim3;
+static refk_dim3 threadIdx, blockIdx, blockDim;
+
+/* CUDA runtime names referenced by host code in src/lattice.c (never run). */
+typedef int cudaError_t;
+#define cudaSuccess 0
+enum { cudaMemcpyHostToDevice = 1, cudaMemcpyDeviceToHost = 2,
+       cudaMemcpyDeviceToDevice = 3 };
+static int cudaGetLastError(void) { return 0; }
+static const char* cudaGetErrorString(int e) { (void)e; return ""; }
+static int cudaThreadSynchronize(void) { return 0; }
+static int cudaMemcpy(void* d, const void* s, size_t n, int k)
+{ (void)k; memcpy(d, s, n); return 0; }
+
+/* Velocity table in the reference's order (src/lbgpu_prime.h:82-84):
+   opposite directions adjacent (a odd <-> a+1), D2Q9 = the first nine. */
+int vx[19] = { 0, 1,-1, 0, 0, 1,-1,-1, 1, 0, 0, 1,-1,-1, 1, 0, 0, 0, 0};
+int vy[19] = { 0, 0, 0, 1,-1, 1,-1, 1,-1, 0, 0, 0, 0, 0, 0, 1,-1,-1, 1};
+int vz[19] = { 0, 0, 0, 0, 0, 0, 0, 0, 0, 1,-1, 1,-1, 1,-1, 1,-1, 1,-1};
+real wt[19];
+int cumul_stride[20];
+/* Direction names used by the boundary kernels (src/lbgpu_prime.h:91-109). */
+#define C  0
+#define E  1
+#define W  2
+#define N  3
+#define S  4
+#define NE 5
+#define SW 6
+#define NW 7
+#define SE 8
+#define T  9
+#define B  10
+#define TE 11
+#define BW 12
+#define TW 13
+#define BE 14
+#define TN 15
+#define BS 16
+#define TS 17
+#define BN 18
+
+#include "process.h"
+#include "lattice.h"
+#include "forward_declarations.h"
+#include "lattice.c"
+#include "system_boundary_kernels.c"
+#include "k_stream_collide_stream.c"
+#include "k_collide.c"
+
+/* The dynamic shared-memory scratch of one one-thread block. */
+real fptr[32];
+
+#define EXPORT __attribute__((visibility("default")))
+
+typedef struct {
+  int LX, LY, LZ;
+  double tau[2], rho_A[2], gaccel[6], sink;
+  int sigma_t_on, sigma_t_off;
+  /* 2D system boundaries (src/bcs.c GPU branches) */
+  int pressure_n_in[2], pressure_s_in[2], pressure_n_out[2], pressure_s_out[2];
+  int zeroconcgrad_n, zeroconcgrad_s;
+  double rho_in, rho_out, pfadd, pfmul;
+  int bc_ramp_start, bc_ramp_stop;
+  const double* pressure_n_table; int pressure_n_len;   /* subs 0 */
+  const double* pressure_s_table; int pressure_s_len;
+} refk_params;
+
+EXPORT int refk_real_size(void) { return (int)sizeof(real); }
+EXPORT int refk_num_dims(void) { return NUM_DIMENSIONS; }
+EXPORT int refk_num_subs(void) { return NUM_FLUID_COMPONENTS; }
+EXPORT int refk_accurate(void) { return ACCURATE; }
+EXPORT int refk_compressible(void) { return COMPRESSIBLE; }
+
+/* Constant upload, as construct_lattice does it (src/latman.c:147-376) for
+   a serial run: EndBoundSize = 0, so cumul_stride[a] = a*NumNodes. */
+static void upload_constants(const refk_params* p)
+{
+  int a, s;
+  int D = NUM_DIMENSIONS, Qd = 2 * D * D + 1, NS = NUM_FLUID_COMPONENTS;
+  int NN = p->LX * p->LY * p->LZ;
+  memcpy(vx_c, vx, sizeof vx); memcpy(vy_c, vy, sizeof vy);
+  memcpy(vz_c, vz, sizeof vz);
+  if (D == 2) {
+    real W0 = 4./9., W1 = 1./9., W2 = 1./36.;
+    wt[0] = W0;
+    for (a = 1; a < 5; a++) wt[a] = W1;
+    for (; a < 9; a++) wt[a] = W2;
+    for (; a < 19; a++) wt[a] = 0.;
+  } else {
+    real W0 = 1./3., W1 = 1./18., W2 = 1./36.;
+    wt[0] = W0;
+    for (a = 1; a < 5; a++) wt[a] = W1;
+    for (; a < 9; a++) wt[a] = W2;
+    for (; a < 11; a++) wt[a] = W1;
+    for (; a < 19; a++) wt[a] = W2;
+  }
+  for (a = 0; a <= Qd; a++) cumul_stride[a] = a * NN;
+  memcpy(wt_c, wt, sizeof wt);
+  memcpy(cumul_stride_c, cumul_stride, sizeof cumul_stride);
+  for (s = 0; s < NS; s++) {
+    tau_c[s] = (real)p->tau[s];
+    inv_tau_c[s] = 1. / (real)p->tau[s];     /* src/latman.c:232-235 */
+    rho_A_c[s] = (real)p->rho_A[s];
+    for (a = 0; a < D; a++) gaccel_c[s * 3 + a] = (real)p->gaccel[s * 3 + a];
+  }
+  numsubs_c = NS; numdims_c = D; numdirs_c = Qd;
+  numbounddirs_c = (D == 2) ? 6 : 10; numunbounddirs_c = Qd - numbounddirs_c;
+  end_bound_c = 0; proc_id_c = 0; num_procs_c = 1;
+  ni_c = p->LX; nj_c = p->LY; nk_c = p->LZ;
+  kloop_c = 1; bixbj_c = 1; bixbk_c = 1; bjxbk_c = 1;
+  nixnj_c = p->LX * p->LY; blocksize_c = 1; numnodes_c = NN;
+  sink_c = (real)p->sink; pfmul_c = (real)p->pfmul; pfadd_c = (real)p->pfadd;
+#if INAMURO_SIGMA_COMPONENT
+  sigma_t_on_c = p->sigma_t_on; sigma_t_off_c = p->sigma_t_off;
+#endif
+  is_end_of_frame_mem_c = 0; pest_output_flag_c = 0;
+}
+
+typedef void (*refk_kernel)(real*, real*, unsigned char*, real*);
+typedef void (*refk_bc_kernel)(real*, unsigned char*, real*);
+
+static void launch_grid(refk_kernel k, int gx, int gy, int gz,
+                        real* f, real* mv, unsigned char* sol)
+{
+  unsigned x, y, z;
+  blockDim.x = blockDim.y = blockDim.z = 1;
+  threadIdx.x = threadIdx.y = threadIdx.z = 0;
+  for (z = 0; z < (unsigned)gz; z++)
+    for (y = 0; y < (unsigned)gy; y++)
+      for (x = 0; x < (unsigned)gx; x++) {
+        blockIdx.x = x; blockIdx.y = y; blockIdx.z = z;
+        k(f, mv, sol, NULL);
+      }
+}
+
+static void launch_row(refk_bc_kernel k, int gx, real* f, unsigned char* sol)
+{
+  unsigned x;
+  blockDim.x = blockDim.y = blockDim.z = 1;
+  threadIdx.x = threadIdx.y = threadIdx.z = 0;
+  blockIdx.y = blockIdx.z = 0;
+  for (x = 0; x < (unsigned)gx; x++) { blockIdx.x = x; k(f, sol, NULL); }
+}
+
+/* Density for one pressure face at `time`: src/bcs.c:286-322 (north in),
+   :345-371 (north out), :396-431 (south in), :458-484 (south out). */
+static real face_rho(const refk_params* p, int subs, int time, int in_flag,
+                     int is_in, const double* table, int len)
+{
+  real rho, ramp_factor;
+  if (is_in && in_flag == 2)
+    rho = (real)p->pfadd + (real)p->pfmul * (real)table[time % len];
+  else
+    rho = is_in ? (real)p->rho_in : (real)p->rho_out;
+  if (p->bc_ramp_start >= 0 && p->bc_ramp_stop >= 0) {
+    if (time < p->bc_ramp_start) {
+      rho = (real)p->rho_A[subs];
+    } else if (time < p->bc_ramp_stop) {
+      ramp_factor = ((real)(time - p->bc_ramp_start))
+                  / ((real)(p->bc_ramp_stop - p->bc_ramp_start));
+      rho *= ramp_factor;
+      rho += (1. - ramp_factor) * (real)p->rho_A[subs];
+    }
+  }
+  return rho;
+}
+
+/* bcs_1 / bcs_2 (src/bcs.c:226-558, :1179-1506): per substance, north in,
+   north out, south in, south out, then (solute only) zero-gradient N, S. */
+static void bcs(const refk_params* p, int time, int second,
+                real* f, unsigned char* sol)
+{
+  int subs;
+  refk_bc_kernel pn = second ? k_sysbound_pressure_n_2 : k_sysbound_pressure_n_1;
+  refk_bc_kernel ps = second ? k_sysbound_pressure_s_2 : k_sysbound_pressure_s_1;
+  for (subs = 0; subs < NUM_FLUID_COMPONENTS; subs++) {
+    subs_c = subs;
+    if (p->pressure_n_in[subs]) {
+      fixed_bound_var_c = face_rho(p, subs, time, p->pressure_n_in[subs], 1,
+                                   p->pressure_n_table, p->pressure_n_len);
+      launch_row(pn, p->LX, f, sol);
+    }
+    if (p->pressure_n_out[subs]) {
+      fixed_bound_var_c = face_rho(p, subs, time, 0, 0, NULL, 0);
+      launch_row(pn, p->LX, f, sol);
+    }
+    if (p->pressure_s_in[subs]) {
+      fixed_bound_var_c = face_rho(p, subs, time, p->pressure_s_in[subs], 1,
+                                   p->pressure_s_table, p->pressure_s_len);
+      launch_row(ps, p->LX, f, sol);
+    }
+    if (p->pressure_s_out[subs]) {
+      fixed_bound_var_c = face_rho(p, subs, time, 0, 0, NULL, 0);
+      launch_row(ps, p->LX, f, sol);
+    }
+#if INAMURO_SIGMA_COMPONENT
+    if (subs == 1 && p->zeroconcgrad_n)
+      launch_row(second ? k_sysbound_zeroconcgrad_n_2
+                        : k_sysbound_zeroconcgrad_n_1, p->LX, f, sol);
+    if (subs == 1 && p->zeroconcgrad_s)
+      launch_row(second ? k_sysbound_zeroconcgrad_s_2
+                        : k_sysbound_zeroconcgrad_s_1, p->LX, f, sol);
+#endif
+  }
+}
+
+/*
+ * Run lattice times t0+1 .. t0+nsteps (t0 even: an AA pair starts on an odd
+ * time).  f is [NumSubs][Q][N] in the reference's serial layout, mv is
+ * [NumSubs][1+D][N].  mv is written at the steps where t % frame_rate == 0
+ * (frame_rate <= 0: never), exactly as is_end_of_frame_mem_c gates it.
+ * Per step, src/lbgpu_prime.cu:369-915: set time_c; 2D only: bcs_1 (odd) or
+ * bcs_2 (even); then k_stream_collide_stream (odd) or k_collide (even).
+ */
+EXPORT int refk_run(const refk_params* p, real* f, const unsigned char* solids,
+                    real* mv, int t0, int nsteps, int frame_rate)
+{
+  int t;
+  unsigned char* sol = (unsigned char*)solids;
+  if (t0 % 2) return -1;
+  upload_constants(p);
+  for (t = t0 + 1; t <= t0 + nsteps; t++) {
+#if INAMURO_SIGMA_COMPONENT
+    time_c = t;
+#endif
+    if (NUM_DIMENSIONS == 2) bcs(p, t, !(t % 2 == 1), f, sol);
+    is_end_of_frame_mem_c = (frame_rate > 0 && t % frame_rate == 0);
+    if (t % 2 == 1)
+      launch_grid(k_stream_collide_stream, p->LX, p->LY, p->LZ, f, mv, sol);
+    else
+      launch_grid(k_collide, p->LX, p->LY, p->LZ, f, mv, sol);
+    is_end_of_frame_mem_c = 0;
+  }
+  return 0;
+}
