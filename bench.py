@@ -1,0 +1,346 @@
+"""Benchmark: D3Q19 MLUPS of the AA-pattern LBM step on B200.
+
+Workload (one replica per GPU; "replicas only" -- the path does not shard
+here): D3Q19 BGK flow on a 256^3 lattice, FP32 shifted populations
+(f_i - w_i rho_A), tau = 0.8, body force gx = 1e-6, periodic on every face,
+solid mask = overlapping spheres of radius 6 from a fixed seed, added until
+the porosity is 0.4.  Synthetic, seeded: no dataset is involved.
+
+One bench step = one lattice time step (one odd or one even AA kernel; the
+run alternates them as the reference does).  `value` = lattice node updates
+per second over all ranks (MLUPS, all nodes); MFLUPS counts fluid nodes.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+`--impl reference` times the reference's own implementation of this path on
+the host cores: its kernel sources compiled for the CPU (oracle/_ref), on
+the same lattice and metric.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "lbgpu-prime-dev_b200"))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+N_EDGE = 256
+TAU = 0.8
+GX = 1e-6
+RADIUS = 6
+POROSITY = 0.4
+SEED = 1234
+Q = 19
+REAL = 4
+BYTES_PER_FLUID_UPDATE = 2 * Q * REAL          # 152 B: read + write 19 floats
+FLAG_BYTES_PER_NODE = 1.0 / 8.0                 # bit-packed solid flag
+METRIC = "D3Q19 MLUPS (FP32 shifted populations, 256^3 sphere pack)"
+
+
+def workload_config(world: int) -> dict:
+    return {
+        "workload": "D3Q19 BGK 256^3, FP32 shifted populations, tau=0.8, gx=1e-6, "
+                    "periodic, overlapping spheres r=6 to porosity 0.4 (seed 1234)",
+        "lattice": [N_EDGE] * 3, "velocity_set": "D3Q19", "tau": TAU, "gx": GX,
+        "sphere_radius": RADIUS, "porosity_target": POROSITY, "seed": SEED,
+        "parallelism": "replicas x%d (one independent lattice per GPU)" % world,
+        "l2": "inputs larger than L2 (1.27 GB populations per lattice)",
+    }
+
+
+def load_peaks() -> dict:
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as fh:
+            d = json.load(fh)
+        return {"hbm_gbs": float(d["hbm_gbs"]), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+def load_traffic() -> float | None:
+    """DRAM bytes per launch of the step kernel from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "aa_step_d3q19_f32_256cube.md")
+    if not os.path.exists(path):
+        return None
+    m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", open(path).read())
+    return float(m.group(1)) if m else None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.dev), "--query-gpu=" + self.Q,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict | None:
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4)
+                          if r[5 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def make_mask():
+    from lbx import geometry
+    return geometry.sphere_pack(N_EDGE, N_EDGE, N_EDGE, RADIUS, POROSITY, SEED)
+
+
+def cpu_baseline(mask, steps: int = 4) -> dict:
+    """The reference's kernels on the host cores (bounded sample), else the
+    oracle port."""
+    import pyoracle as po
+    p = po.Params(dims=3, LX=N_EDGE, LY=N_EDGE, LZ=N_EDGE, tau=(TAU, 1.0),
+                  gaccel=(GX, 0, 0, 0, 0, 0))
+    f = np.zeros((1, Q, p.NN), np.float32)
+    cores = os.cpu_count() or 1
+    if po.reference_available("d3q19_f32"):
+        kind = "reference"
+        po.run_reference("d3q19_f32", p, f, mask, 0, 0)   # load the library
+        po._refs["d3q19_f32"].refk_set_threads(cores)
+        t0 = time.perf_counter()
+        po.run_reference("d3q19_f32", p, f, mask, 0, steps)
+        dt = time.perf_counter() - t0
+    else:
+        kind = "port"
+        t0 = time.perf_counter()
+        po.run_oracle(p, f, mask, 0, steps, threads=cores)
+        dt = time.perf_counter() - t0
+    return {"value": round(p.NN * steps / dt / 1e6, 3), "unit": "MLUPS", "cores": cores,
+            "kind": kind,
+            "sample": "%d lattice steps of the full 256^3 workload, FP32, %s threads"
+                      % (steps, cores)}
+
+
+def reference_arm(args, rank: int, world: int):
+    if rank != 0:
+        return 0
+    import pyoracle as po
+    variant = "d3q19_f32"
+    if not po.reference_available(variant):
+        print(json.dumps({"impl": "reference",
+                          "unavailable": "oracle/_ref not built (reference tree absent at build)"}))
+        return 0
+    mask = make_mask()
+    p = po.Params(dims=3, LX=N_EDGE, LY=N_EDGE, LZ=N_EDGE, tau=(TAU, 1.0),
+                  gaccel=(GX, 0, 0, 0, 0, 0))
+    f = np.zeros((1, Q, p.NN), np.float32)
+    cores = os.cpu_count() or 1
+    po.run_reference(variant, p, f, mask, 0, 0)
+    po._refs[variant].refk_set_threads(cores)
+    # warm-up: an even number of steps, so the timed run starts at an even
+    # time as every AA run must
+    warm = args.warmup + (args.warmup % 2)
+    po.run_reference(variant, p, f, mask, 0, warm)
+    t0 = time.perf_counter()
+    po.run_reference(variant, p, f, mask, warm, args.steps)
+    dt = time.perf_counter() - t0
+    value = p.NN * args.steps / dt / 1e6
+    line = {
+        "metric": METRIC, "value": round(value, 3), "unit": "MLUPS", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(dt / args.steps * 1e3, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": workload_config(1), "impl": "reference",
+        "cpu_baseline": {"value": round(value, 3), "unit": "MLUPS", "cores": cores,
+                         "kind": "reference",
+                         "sample": "the full 256^3 lattice each step; the reference's "
+                                   "kernel sources compiled for the host, %d threads" % cores},
+        "e2e": {"value": round(value, 3), "unit": "MLUPS", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=40)
+    ap.add_argument("--warmup", type=int, default=4)
+    ap.add_argument("--impl", default="lbx", choices=["lbx", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args(argv)
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return reference_arm(args, rank, world)
+
+    import torch
+    import lbx
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    mask = make_mask()
+    fluid = int(np.count_nonzero(mask != 1))
+    NN = mask.size
+    params = lbx.Params(dims=3, LX=N_EDGE, LY=N_EDGE, LZ=N_EDGE, precision=REAL,
+                        tau=(TAU, 1.0), gaccel=(GX, 0, 0, 0, 0, 0), device=local)
+    stream = torch.cuda.current_stream()
+    dom = lbx.Domain(params, mask)
+    dom.set_stream(stream.cuda_stream)
+    dom.init_equilibrium(0, 1.0, 0.0, 0.0, 0.0)
+
+    # warm-up (W >= 3 steps), then K timed steps between barriers
+    t = 0
+    dom.run(t, args.warmup, 0)
+    t += args.warmup
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    launches0 = dom.launch_count()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    dom.run(t, args.steps, 0)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    t += args.steps
+    ms = ev0.elapsed_time(ev1)
+    launches = dom.launch_count() - launches0
+    clocks = sampler.stop()
+    if dist:
+        tms = torch.tensor([ms], device="cuda")
+        dist.all_reduce(tms, op=dist.ReduceOp.MAX)
+        ms = float(tms.item())
+        dist.barrier()
+    ms_step = ms / args.steps
+    value = world * NN * args.steps / (ms / 1e3) / 1e6
+    mflups = world * fluid * args.steps / (ms / 1e3) / 1e6
+
+    # per-kind launch durations (odd = stream-collide-stream, even = collide)
+    per_kind = {}
+    for kind in ("odd", "even"):
+        if (t % 2 == 0) != (kind == "odd"):
+            dom.step(t + 1)
+            t += 1
+        reps = 6
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+               for _ in range(reps)]
+        durs = []
+        for a, b in evs:
+            a.record(stream)
+            dom.step(t + 1)
+            b.record(stream)
+            t += 1
+            dom.step(t + 1)   # keep the AA order; not timed
+            t += 1
+        torch.cuda.synchronize()
+        durs = [a.elapsed_time(b) for a, b in evs]
+        per_kind[kind] = float(np.median(durs))
+
+    peaks = load_peaks()
+    alg_bytes = fluid * BYTES_PER_FLUID_UPDATE + NN * FLAG_BYTES_PER_NODE
+    achieved = alg_bytes / (ms_step / 1e3) / 1e9
+    roofline = {
+        "bound": "hbm", "achieved": round(achieved, 1), "peak": peaks["hbm_gbs"],
+        "unit": "GB/s", "frac": round(achieved / peaks["hbm_gbs"], 4),
+        "traffic": load_traffic(),
+        "peak_source": peaks["source"],
+        "kernel": "aa_step<float,19,1,SHIFTED_INC> (odd and even alternate)",
+        "alg_bytes_per_launch": alg_bytes,
+        "by_kind_ms": {k: round(v, 4) for k, v in per_kind.items()},
+        "by_kind_frac": {k: round(alg_bytes / (v / 1e3) / 1e9 / peaks["hbm_gbs"], 4)
+                         for k, v in per_kind.items()},
+    }
+
+    # end to end through the C ABI with host buffers: upload the populations
+    # from pinned memory, K steps, macro variables of the last step back.
+    f_host = torch.zeros((Q, NN), dtype=torch.float32, pin_memory=True)
+    mv_host = torch.empty((4, NN), dtype=torch.float32, pin_memory=True)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    lib = lbx.load_library()
+    h = dom._h
+    lbx._check(lib.lbx_upload_f(h, 0, f_host.data_ptr()))   # natural order at time 0
+    lbx._check(lib.lbx_run(h, 0, args.steps - 1, 0))
+    lbx._check(lib.lbx_step(h, args.steps, lbx.LBX_WRITE_MV))
+    lbx._check(lib.lbx_download_mv(h, 0, mv_host[0].data_ptr(), mv_host[1].data_ptr(),
+                                   mv_host[2].data_ptr(), mv_host[3].data_ptr()))
+    e2e_s = time.perf_counter() - t0
+    if dist:
+        te2 = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(te2, op=dist.ReduceOp.MAX)
+        e2e_s = float(te2.item())
+    e2e = {"value": round(world * NN * args.steps / e2e_s / 1e6, 3), "unit": "MLUPS",
+           "h2d_bytes_per_step": int(Q * NN * REAL / args.steps),
+           "d2h_bytes_per_step": int(4 * NN * REAL / args.steps),
+           "note": "upload of all populations from pinned host memory, K steps, "
+                   "download of rho,u of the last step; wall clock"}
+
+    line = {
+        "metric": METRIC, "value": round(value, 3), "unit": "MLUPS", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_step, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic", "config": workload_config(world),
+        "mflups": round(mflups, 3), "fluid_nodes": fluid, "nodes": NN,
+        "roofline": roofline, "clocks": clocks, "e2e": e2e,
+        "gpu_launches": launches,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(mask)
+    dom.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,176 @@
+/*
+ * lbx.h -- C ABI of the B200-native lattice-Boltzmann hot path.
+ *
+ * This is the drop-in boundary for the reference's device path: the
+ * in-place two-kernel (AA-pattern) update of src/k_stream_collide_stream.c
+ * (odd times) and src/k_collide.c (even times), with halfway bounce-back at
+ * solid nodes, the Zou-He pressure faces and the solute zero-gradient faces
+ * of src/system_boundary_kernels.c, for D2Q9 and D3Q19 BGK flow and the
+ * coupled solute (Inamuro sigma) lattice.
+ *
+ * Conventions (same as the reference's device data):
+ *   - node index  n = i + LX*(j + LY*k)            (x fastest)
+ *   - populations [subs][a][n], a in the reference's direction order
+ *     (src/lbgpu_prime.h:82-84: opposites adjacent, a odd <-> a+1)
+ *   - macro vars  [subs][0..D][n] = rho, ux, uy[, uz]  (src/lattice.c:2748)
+ *   - solids      one byte per node; solid iff the byte == 1, the device
+ *                 rule of src/lattice.c:2291/:2314 (255 counts as fluid)
+ *   - real        double (precision 8) or float (precision 4)
+ *   - times       the reference's: the step at an odd time is
+ *                 stream-collide-stream, at an even time collide; a run
+ *                 starts from the natural-order state at an even time.
+ *
+ * Every call returns LBX_OK (0) or an error code; lbx_last_error() gives a
+ * message for the calling thread.  A domain handle is not thread-safe: use
+ * one per host thread.  The library owns all device memory and a CUDA stream
+ * per domain; host buffers are the caller's and are copied during the call.
+ */
+#ifndef LBX_H
+#define LBX_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int lbx_status;
+enum {
+  LBX_OK = 0,
+  LBX_ERR_INVALID = 1,   /* bad argument or unsupported combination   */
+  LBX_ERR_CUDA = 2,      /* a CUDA runtime call failed                 */
+  LBX_ERR_NOMEM = 3,     /* device allocation failed                   */
+  LBX_ERR_STATE = 4,     /* call out of order (AA parity, closed handle) */
+  LBX_ERR_NUMERIC = 5    /* non-finite or negative density detected    */
+};
+
+/* Step flags. */
+enum {
+  LBX_WRITE_MV = 1u      /* store rho and u this step: is_end_of_frame_mem_c */
+};
+
+/* Parameters.  Field names and meanings are those of the reference's
+ * params.in (src/params.h:40-660) and of the __constant__ block its kernels
+ * read (src/lattice.c:2224-2268). */
+typedef struct lbx_params {
+  int dims;                 /* 2 (D2Q9) or 3 (D3Q19)                       */
+  int LX, LY, LZ;           /* LZ must be 1 when dims == 2                 */
+  int nsubs;                /* 1: flow; 2: flow + solute (sigma) lattice   */
+  int precision;            /* 8 = double, 4 = float                       */
+  int accurate;             /* ACCURATE: 1 = shifted populations f - w rho_A */
+  int compressible;         /* COMPRESSIBLE: 0 = He-Luo incompressible     */
+  double tau[2];            /* tau[0] flow, tau[1] solute                  */
+  double rho_A[2];          /* reference density per substance             */
+  double gaccel[6];         /* body acceleration gforce_{x,y,z}[subs]      */
+  double sink;              /* solute sink coefficient                     */
+  int sigma_t_on, sigma_t_off; /* solute active for sigma_t_on<=t<=sigma_t_off */
+  /* 2D faces: north = row j=LY-1, south = row j=0 (src/bcs.c GPU code) */
+  int pressure_n_in[2], pressure_s_in[2];    /* 1 = rho_in, 2 = table      */
+  int pressure_n_out[2], pressure_s_out[2];  /* 1 = rho_out                */
+  int zeroconcgrad_n, zeroconcgrad_s;        /* solute zero gradient       */
+  double rho_in, rho_out;
+  double pfadd, pfmul;      /* table density = pfadd + pfmul * table[t%len] */
+  int bc_ramp_start, bc_ramp_stop;           /* < 0: no ramp               */
+  const double* pressure_n_table; int pressure_n_len;
+  const double* pressure_s_table; int pressure_s_len;
+  int device;               /* CUDA device ordinal                         */
+} lbx_params;
+
+typedef struct lbx_domain lbx_domain;
+
+/* FP64 reductions over the current macro variables (see lbx_reduce). */
+typedef struct lbx_reductions {
+  double mass;              /* sum over fluid nodes of rho (subs 0)        */
+  double solute_mass;       /* sum over fluid nodes of C (subs 1), else 0  */
+  double momentum[3];       /* sum over fluid nodes of rho*u (subs 0)      */
+  double u_sum[3];          /* sum over fluid nodes of u (subs 0)          */
+  double rho_min, rho_max;  /* over fluid nodes (subs 0)                   */
+  long long fluid_nodes;
+  int nonfinite;            /* count of non-finite rho/u values seen       */
+} lbx_reductions;
+
+/* Fill `p` with the reference defaults: tau 1, rho_A 1, no force, no faces,
+ * ramp off, double precision, shifted incompressible model. */
+void lbx_params_default(lbx_params* p);
+
+/* Allocate the device lattice and classify nodes from `solids`
+ * (LX*LY*LZ bytes, host).  Replaces construct_lattice's device part:
+ * the constant upload of src/latman.c:147-376, the cudaMalloc of
+ * src/latman.c:461-493 and the solid upload of src/lbgpu_prime.cu:170-257. */
+lbx_status lbx_create(const lbx_params* p, const uint8_t* solids,
+                      lbx_domain** out);
+
+/* Release everything.  Replaces src/latman.c:2144-2172 (device part). */
+lbx_status lbx_destroy(lbx_domain* d);
+
+/* Populations of one substance, [Q][N] reals in the reference's order.
+ * Replaces the per-direction cudaMemcpy of src/lbgpu_prime.cu:316-343
+ * (upload) and :874-900 (download).  Uploaded populations are the
+ * natural-order state of an even time, so the next step must be at an odd
+ * time (as after init_problem in the reference's main). */
+lbx_status lbx_upload_f(lbx_domain* d, int subs, const void* f_host);
+lbx_status lbx_download_f(lbx_domain* d, int subs, void* f_host);
+
+/* Macro variables of one substance, [1+D][N] reals.  Replaces
+ * src/lbgpu_prime.cu:345-350 (upload) and :544-583 / :765-804 (download:
+ * rho, ux, uy[, uz]; uz may be NULL in 2D). */
+lbx_status lbx_upload_mv(lbx_domain* d, int subs, const void* mv_host);
+lbx_status lbx_download_mv(lbx_domain* d, int subs, void* rho, void* ux,
+                           void* uy, void* uz);
+
+/* Equilibrium initial state on the device from host rho/u ([N] reals each
+ * for substance `subs`; uz may be NULL in 2D): the f = feq loop of
+ * src/latman.c:1786-1840 (shifted deviations for the flow lattice of an
+ * ACCURATE run, full feq otherwise).  Solid nodes are initialised too. */
+lbx_status lbx_init_equilibrium(lbx_domain* d, int subs, const void* rho,
+                                const void* ux, const void* uy,
+                                const void* uz);
+
+/* One lattice step at `time`: the system boundaries of bcs_1 / bcs_2 and
+ * then k_stream_collide_stream (odd time) or k_collide (even time).
+ * Replaces src/lbgpu_prime.cu:490-530 (odd) and :722-752 (even).  Steps
+ * must alternate odd/even starting from an odd time (LBX_ERR_STATE
+ * otherwise).  Asynchronous: returns once the work is queued. */
+lbx_status lbx_step(lbx_domain* d, int time, unsigned flags);
+
+/* The pair of steps time, time+1 (time odd). */
+lbx_status lbx_step_pair(lbx_domain* d, int time, unsigned flags);
+
+/* Steps t0+1 .. t0+nsteps (t0 even), writing macro variables at every time
+ * that is a multiple of frame_rate (frame_rate <= 0: never) -- the
+ * is_end_of_frame rule of src/lattice.c:2094-2097.  Asynchronous. */
+lbx_status lbx_run(lbx_domain* d, int t0, int nsteps, int frame_rate);
+
+/* Run the domain's work on the caller's CUDA stream (a cudaStream_t passed
+ * as void*; NULL restores the library's own stream).  Lets a caller order
+ * lbx launches with its own work and time them with its own events. */
+lbx_status lbx_set_stream(lbx_domain* d, void* stream);
+
+/* Wait for all queued work of the domain; reports asynchronous errors. */
+lbx_status lbx_sync(lbx_domain* d);
+
+/* FP64 on-device reductions over the macro variables last written (a step
+ * with LBX_WRITE_MV).  Replaces the host-side compute_{max,min,ave}_rho /
+ * _u of src/compute.c:1159-1416 used by the frame summary.  Synchronous. */
+lbx_status lbx_reduce(lbx_domain* d, lbx_reductions* out);
+
+/* Device pointers to the populations ([nsubs][Q][N]) and macro variables
+ * ([nsubs][1+D][N]) for callers that keep data on the device. */
+lbx_status lbx_device_f(lbx_domain* d, void** ptr);
+lbx_status lbx_device_mv(lbx_domain* d, void** ptr);
+
+/* Counts from classification: fluid nodes, and whether the 2D face
+ * boundaries run fused into the step kernels (1) or as separate kernels (0). */
+lbx_status lbx_info(lbx_domain* d, long long* fluid_nodes, int* faces_fused);
+
+/* Number of this library's kernels launched on the domain so far. */
+long long lbx_launch_count(lbx_domain* d);
+
+/* Message for the last failed call on this thread ("" if none). */
+const char* lbx_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LBX_H */

@@ -1,0 +1,556 @@
+// lbx_abi.cu -- the C ABI (include/lbx.h) over the sm_100a kernels.
+//
+// Host-side restatement of the reference's device orchestration:
+//   construct_lattice device part   src/latman.c:147-376, :461-493
+//   solid upload                    src/lbgpu_prime.cu:170-257
+//   per-step order                  src/lbgpu_prime.cu:369-915
+//   face schedule (bcs_1 / bcs_2)   src/bcs.c:226-558, :1179-1506
+// No CPU compute path exists here: every step is a CUDA launch, and a
+// failed launch is an error returned to the caller.
+#include "lbx.h"
+#include "lbx_kernels.cuh"
+
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+using namespace lbx;
+
+namespace {
+
+thread_local std::string g_err;
+
+lbx_status fail(lbx_status code, const char* fmt, ...)
+    __attribute__((format(printf, 2, 3)));
+
+lbx_status fail(lbx_status code, const char* fmt, ...)
+{
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return code;
+}
+
+#define CK(call)                                                              \
+  do {                                                                        \
+    cudaError_t e_ = (call);                                                  \
+    if (e_ != cudaSuccess)                                                    \
+      return fail(e_ == cudaErrorMemoryAllocation ? LBX_ERR_NOMEM             \
+                                                  : LBX_ERR_CUDA,             \
+                  "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__,  \
+                  __LINE__);                                                  \
+  } while (0)
+
+}  // namespace
+
+struct lbx_domain {
+  lbx_params p;
+  int Q = 0, D = 0;
+  long long N = 0;
+  size_t real_size = 0;
+  void* f = nullptr;          // [nsubs][Q][N]
+  void* mv = nullptr;         // [nsubs][1+D][N]
+  uint8_t* solids = nullptr;  // [N] as given (device rule: == 1)
+  uint8_t* cls = nullptr;     // [N]
+  uint32_t* nbm = nullptr;    // [N]
+  void* red = nullptr;        // reduction partials
+  int red_blocks = 0;
+  cudaStream_t stream = nullptr;      // stream all work is queued on
+  cudaStream_t own_stream = nullptr;  // the library's stream
+  std::vector<double> n_table, s_table;
+  long long fluid = 0;
+  bool faces_active = false;  // any 2D face boundary configured
+  bool faces_fused = false;   // fused into the step kernels
+  int parity = 0;             // 0: natural order (next step odd); 1: swapped
+  long long launches = 0;
+  // graph replay of frame-free step runs
+  cudaGraphExec_t graph = nullptr;
+  int graph_steps = 0;
+  int graph_t0 = -1;
+};
+
+namespace {
+
+template <typename T>
+T face_rho(const lbx_domain* d, int s, int t, int in_kind, bool is_in,
+           const std::vector<double>& table)
+{
+  // src/bcs.c:286-322 (and the three sibling faces), in the run's `real`.
+  const lbx_params& p = d->p;
+  T rho;
+  if (is_in && in_kind == 2)
+    rho = (T)p.pfadd + (T)p.pfmul * (T)table[t % (int)table.size()];
+  else
+    rho = is_in ? (T)p.rho_in : (T)p.rho_out;
+  if (p.bc_ramp_start >= 0 && p.bc_ramp_stop >= 0) {
+    if (t < p.bc_ramp_start) {
+      rho = (T)p.rho_A[s];
+    } else if (t < p.bc_ramp_stop) {
+      T ramp = ((T)(t - p.bc_ramp_start)) / ((T)(p.bc_ramp_stop - p.bc_ramp_start));
+      rho *= ramp;
+      rho = (T)((double)rho + (1. - (double)ramp) * (double)(T)p.rho_A[s]);
+    }
+  }
+  return rho;
+}
+
+template <typename T>
+StepArgs<T> make_args(const lbx_domain* d, int t, unsigned flags)
+{
+  const lbx_params& p = d->p;
+  StepArgs<T> A;
+  std::memset(&A, 0, sizeof A);
+  A.f = (T*)d->f;
+  A.mv = (T*)d->mv;
+  A.cls = d->cls;
+  A.nbm = d->nbm;
+  A.LX = p.LX; A.LY = p.LY; A.LZ = p.LZ;
+  A.N = d->N;
+  for (int s = 0; s < 2; ++s) {
+    const T tau = (T)p.tau[s];
+    const T itau = (T)(1. / tau);
+    A.sc[s].itau = itau;
+    A.sc[s].omc = (T)(1. - itau);
+    A.sc[s].rhoA = (T)p.rho_A[s];
+    for (int c = 0; c < 3; ++c) A.sc[s].tg[c] = tau * (T)p.gaccel[s * 3 + c];
+  }
+  A.sink1 = (T)(1.0 - (T)p.sink * (T)p.tau[1]);
+  A.write_mv = (flags & LBX_WRITE_MV) ? 1 : 0;
+  A.solute_on = (t >= p.sigma_t_on && t <= p.sigma_t_off) ? 1 : 0;
+  if (d->faces_fused) {
+    for (int s = 0; s < p.nsubs; ++s) {
+      // last active boundary on each face wins (see FaceKind)
+      if (s == 1 && p.zeroconcgrad_n) A.face_n[s] = FACE_ZEROGRAD;
+      else if (p.pressure_n_out[s]) { A.face_n[s] = FACE_PRESSURE; A.rho_n[s] = face_rho<T>(d, s, t, 0, false, d->n_table); }
+      else if (p.pressure_n_in[s]) { A.face_n[s] = FACE_PRESSURE; A.rho_n[s] = face_rho<T>(d, s, t, p.pressure_n_in[s], true, d->n_table); }
+      if (s == 1 && p.zeroconcgrad_s) A.face_s[s] = FACE_ZEROGRAD;
+      else if (p.pressure_s_out[s]) { A.face_s[s] = FACE_PRESSURE; A.rho_s[s] = face_rho<T>(d, s, t, 0, false, d->s_table); }
+      else if (p.pressure_s_in[s]) { A.face_s[s] = FACE_PRESSURE; A.rho_s[s] = face_rho<T>(d, s, t, p.pressure_s_in[s], true, d->s_table); }
+    }
+  }
+  return A;
+}
+
+template <typename T, int Q, int NS, int MODEL>
+void launch_aa(lbx_domain* d, const StepArgs<T>& A, bool odd)
+{
+  dim3 block(128, 1, 1);
+  dim3 grid((A.LX + 127) / 128, A.LY, A.LZ);
+  if (odd) aa_step<T, Q, NS, MODEL, true><<<grid, block, 0, d->stream>>>(A);
+  else aa_step<T, Q, NS, MODEL, false><<<grid, block, 0, d->stream>>>(A);
+  d->launches++;
+}
+
+template <typename T, int Q, int NS>
+void launch_model(lbx_domain* d, const StepArgs<T>& A, bool odd)
+{
+  const int model = d->p.accurate ? (d->p.compressible ? SHIFTED_COMP : SHIFTED_INC)
+                                  : PLAIN_COMP;
+  if (model == SHIFTED_INC) launch_aa<T, Q, NS, SHIFTED_INC>(d, A, odd);
+  else if (model == PLAIN_COMP) launch_aa<T, Q, NS, PLAIN_COMP>(d, A, odd);
+  else launch_aa<T, Q, NS, SHIFTED_COMP>(d, A, odd);
+}
+
+// The stand-alone face kernels, in the order of bcs_1 / bcs_2.
+template <typename T>
+void launch_faces_exact(lbx_domain* d, int t, bool second)
+{
+  const lbx_params& p = d->p;
+  dim3 block(128), grid((p.LX + 127) / 128);
+  for (int s = 0; s < p.nsubs; ++s) {
+    T* fs = (T*)d->f + (long long)s * d->Q * d->N;
+    const int shifted = p.accurate && !(s == 1 && p.nsubs == 2);
+    const T rhoA = (T)p.rho_A[s];
+    auto run = [&](int north, int kind, T rho) {
+      face_row<T><<<grid, block, 0, d->stream>>>(fs, d->solids, p.LX, p.LY, d->N,
+                                                 north, kind, second ? 1 : 0, rho,
+                                                 rhoA, shifted);
+      d->launches++;
+    };
+    if (p.pressure_n_in[s]) run(1, FACE_PRESSURE, face_rho<T>(d, s, t, p.pressure_n_in[s], true, d->n_table));
+    if (p.pressure_n_out[s]) run(1, FACE_PRESSURE, face_rho<T>(d, s, t, 0, false, d->n_table));
+    if (p.pressure_s_in[s]) run(0, FACE_PRESSURE, face_rho<T>(d, s, t, p.pressure_s_in[s], true, d->s_table));
+    if (p.pressure_s_out[s]) run(0, FACE_PRESSURE, face_rho<T>(d, s, t, 0, false, d->s_table));
+    if (s == 1 && p.nsubs == 2 && p.zeroconcgrad_n) run(1, FACE_ZEROGRAD, T(0));
+    if (s == 1 && p.nsubs == 2 && p.zeroconcgrad_s) run(0, FACE_ZEROGRAD, T(0));
+  }
+}
+
+template <typename T>
+lbx_status step_t(lbx_domain* d, int t, unsigned flags)
+{
+  const bool odd = (t % 2) != 0;
+  if (d->faces_active && !d->faces_fused) launch_faces_exact<T>(d, t, !odd);
+  StepArgs<T> A = make_args<T>(d, t, flags);
+  if (d->Q == 9) {
+    if (d->p.nsubs == 1) launch_model<T, 9, 1>(d, A, odd);
+    else launch_model<T, 9, 2>(d, A, odd);
+  } else {
+    if (d->p.nsubs == 1) launch_model<T, 19, 1>(d, A, odd);
+    else launch_model<T, 19, 2>(d, A, odd);
+  }
+  CK(cudaGetLastError());
+  return LBX_OK;
+}
+
+lbx_status check_params(const lbx_params* p)
+{
+  if (!p) return fail(LBX_ERR_INVALID, "params is NULL");
+  if (p->dims != 2 && p->dims != 3) return fail(LBX_ERR_INVALID, "dims must be 2 or 3");
+  if (p->LX < 1 || p->LY < 1 || p->LZ < 1)
+    return fail(LBX_ERR_INVALID, "lattice extents must be positive");
+  if (p->dims == 2 && p->LZ != 1) return fail(LBX_ERR_INVALID, "LZ must be 1 in 2D");
+  if (p->LY > 65535 || p->LZ > 65535)
+    return fail(LBX_ERR_INVALID, "LY and LZ are limited to 65535");
+  if ((long long)p->LX * p->LY * p->LZ >= (1LL << 31))
+    return fail(LBX_ERR_INVALID, "a domain holds fewer than 2^31 nodes");
+  if (p->nsubs != 1 && p->nsubs != 2) return fail(LBX_ERR_INVALID, "nsubs must be 1 or 2");
+  if (p->precision != 4 && p->precision != 8)
+    return fail(LBX_ERR_INVALID, "precision must be 4 or 8");
+  if (!p->accurate && !p->compressible)
+    return fail(LBX_ERR_INVALID,
+                "accurate=0 requires compressible=1 (the reference does not "
+                "build ACCURATE 0, COMPRESSIBLE 0)");
+  for (int s = 0; s < p->nsubs; ++s)
+    if (!(p->tau[s] > 0.5)) return fail(LBX_ERR_INVALID, "tau[%d] must exceed 0.5", s);
+  bool faces = false;
+  for (int s = 0; s < p->nsubs; ++s)
+    faces |= p->pressure_n_in[s] || p->pressure_s_in[s] || p->pressure_n_out[s] ||
+             p->pressure_s_out[s];
+  faces |= p->nsubs == 2 && (p->zeroconcgrad_n || p->zeroconcgrad_s);
+  if (faces && p->dims != 2)
+    return fail(LBX_ERR_INVALID, "face boundaries exist for 2D runs only");
+  if (faces && p->LY < 3) return fail(LBX_ERR_INVALID, "face boundaries need LY >= 3");
+  for (int s = 0; s < p->nsubs; ++s) {
+    if (p->pressure_n_in[s] == 2 && (!p->pressure_n_table || p->pressure_n_len < 1))
+      return fail(LBX_ERR_INVALID, "pressure_n_in == 2 needs pressure_n_table");
+    if (p->pressure_s_in[s] == 2 && (!p->pressure_s_table || p->pressure_s_len < 1))
+      return fail(LBX_ERR_INVALID, "pressure_s_in == 2 needs pressure_s_table");
+  }
+  return LBX_OK;
+}
+
+// Fused faces are exact when every configured face node pulls its unknowns
+// from a fluid (wrapped) upstream node: then the reference's deposit lands on
+// exactly the slot the node pulls and overwrites in the same step.
+bool faces_fusable(const lbx_params& p, const uint8_t* sol)
+{
+  auto solid = [&](int i, int j) {
+    i = (i + p.LX) % p.LX; j = (j + p.LY) % p.LY;
+    return sol[(long long)i + (long long)p.LX * j] == 1;
+  };
+  bool north = false, south = false;
+  for (int s = 0; s < p.nsubs; ++s) {
+    north |= p.pressure_n_in[s] || p.pressure_n_out[s];
+    south |= p.pressure_s_in[s] || p.pressure_s_out[s];
+  }
+  if (p.nsubs == 2) { north |= p.zeroconcgrad_n != 0; south |= p.zeroconcgrad_s != 0; }
+  for (int i = 0; i < p.LX; ++i) {
+    if (north && !solid(i, p.LY - 1))
+      if (solid(i, 0) || solid(i + 1, 0) || solid(i - 1, 0)) return false;
+    if (south && !solid(i, 0))
+      if (solid(i, p.LY - 1) || solid(i - 1, p.LY - 1) || solid(i + 1, p.LY - 1)) return false;
+  }
+  return true;
+}
+
+void release(lbx_domain* d)
+{
+  if (d->graph) cudaGraphExecDestroy(d->graph);
+  cudaFree(d->f); cudaFree(d->mv); cudaFree(d->solids); cudaFree(d->cls);
+  cudaFree(d->nbm); cudaFree(d->red);
+  if (d->own_stream) cudaStreamDestroy(d->own_stream);
+}
+
+lbx_status check_subs(lbx_domain* d, int subs)
+{
+  if (!d) return fail(LBX_ERR_INVALID, "domain is NULL");
+  if (subs < 0 || subs >= d->p.nsubs) return fail(LBX_ERR_INVALID, "subs out of range");
+  return LBX_OK;
+}
+
+lbx_status do_step(lbx_domain* d, int t, unsigned flags)
+{
+  const int want_odd = d->parity == 0;
+  if (t < 1) return fail(LBX_ERR_INVALID, "time must be >= 1");
+  if (((t % 2) != 0) != (want_odd != 0))
+    return fail(LBX_ERR_STATE, "step at time %d out of AA order: expected an %s time", t,
+                want_odd ? "odd" : "even");
+  lbx_status st = d->real_size == 8 ? step_t<double>(d, t, flags) : step_t<float>(d, t, flags);
+  if (st == LBX_OK) d->parity ^= 1;
+  return st;
+}
+
+}  // namespace
+
+extern "C" {
+
+void lbx_params_default(lbx_params* p)
+{
+  std::memset(p, 0, sizeof *p);
+  p->dims = 3; p->LX = p->LY = p->LZ = 1; p->nsubs = 1; p->precision = 8;
+  p->accurate = 1; p->compressible = 0;
+  p->tau[0] = p->tau[1] = 1.0; p->rho_A[0] = p->rho_A[1] = 1.0;
+  p->sigma_t_on = 0; p->sigma_t_off = -1;
+  p->rho_in = p->rho_out = 1.0; p->pfadd = 1.0; p->pfmul = 0.1;
+  p->bc_ramp_start = p->bc_ramp_stop = -1;
+}
+
+lbx_status lbx_create(const lbx_params* p, const uint8_t* solids, lbx_domain** out)
+{
+  if (!out) return fail(LBX_ERR_INVALID, "out is NULL");
+  *out = nullptr;
+  lbx_status st = check_params(p);
+  if (st) return st;
+  if (!solids) return fail(LBX_ERR_INVALID, "solids is NULL");
+  CK(cudaSetDevice(p->device));
+  lbx_domain* d = new lbx_domain();
+  d->p = *p;
+  d->p.pressure_n_table = nullptr; d->p.pressure_s_table = nullptr;
+  if (p->pressure_n_table) d->n_table.assign(p->pressure_n_table, p->pressure_n_table + p->pressure_n_len);
+  if (p->pressure_s_table) d->s_table.assign(p->pressure_s_table, p->pressure_s_table + p->pressure_s_len);
+  d->Q = p->dims == 2 ? 9 : 19;
+  d->D = p->dims;
+  d->N = (long long)p->LX * p->LY * p->LZ;
+  d->real_size = (size_t)p->precision;
+  for (int s = 0; s < p->nsubs; ++s)
+    d->faces_active |= p->pressure_n_in[s] || p->pressure_s_in[s] || p->pressure_n_out[s] ||
+                       p->pressure_s_out[s];
+  d->faces_active |= p->nsubs == 2 && (p->zeroconcgrad_n || p->zeroconcgrad_s);
+  d->faces_fused = d->faces_active && faces_fusable(*p, solids);
+  for (long long n = 0; n < d->N; ++n) d->fluid += solids[n] != 1;
+
+  auto bail = [&](lbx_status s) { release(d); delete d; return s; };
+  cudaError_t e;
+#define CKD(call)                                                                  \
+  if ((e = (call)) != cudaSuccess)                                                 \
+    return bail(fail(e == cudaErrorMemoryAllocation ? LBX_ERR_NOMEM : LBX_ERR_CUDA, \
+                     "%s: %s", #call, cudaGetErrorString(e)));
+  CKD(cudaStreamCreateWithFlags(&d->own_stream, cudaStreamNonBlocking));
+  d->stream = d->own_stream;
+  const size_t fbytes = (size_t)p->nsubs * d->Q * d->N * d->real_size;
+  const size_t mvbytes = (size_t)p->nsubs * (1 + d->D) * d->N * d->real_size;
+  CKD(cudaMalloc(&d->f, fbytes));
+  CKD(cudaMalloc(&d->mv, mvbytes));
+  CKD(cudaMalloc(&d->solids, d->N));
+  CKD(cudaMalloc(&d->cls, d->N));
+  CKD(cudaMalloc(&d->nbm, d->N * sizeof(uint32_t)));
+  d->red_blocks = 2 * 148;
+  CKD(cudaMalloc(&d->red, d->red_blocks * sizeof(RedPartial)));
+  CKD(cudaMemsetAsync(d->f, 0, fbytes, d->stream));
+  CKD(cudaMemsetAsync(d->mv, 0, mvbytes, d->stream));
+  CKD(cudaMemcpyAsync(d->solids, solids, d->N, cudaMemcpyHostToDevice, d->stream));
+  {
+    dim3 block(128), grid((p->LX + 127) / 128, p->LY, p->LZ);
+    if (d->Q == 9) classify<9><<<grid, block, 0, d->stream>>>(d->solids, d->cls, d->nbm, p->LX, p->LY, p->LZ);
+    else classify<19><<<grid, block, 0, d->stream>>>(d->solids, d->cls, d->nbm, p->LX, p->LY, p->LZ);
+    d->launches++;
+  }
+  CKD(cudaGetLastError());
+  CKD(cudaStreamSynchronize(d->stream));
+#undef CKD
+  *out = d;
+  return LBX_OK;
+}
+
+lbx_status lbx_destroy(lbx_domain* d)
+{
+  if (!d) return LBX_OK;
+  if (d->stream) cudaStreamSynchronize(d->stream);
+  release(d);
+  delete d;
+  return LBX_OK;
+}
+
+lbx_status lbx_upload_f(lbx_domain* d, int subs, const void* f_host)
+{
+  if (lbx_status st = check_subs(d, subs)) return st;
+  if (!f_host) return fail(LBX_ERR_INVALID, "f_host is NULL");
+  const size_t bytes = (size_t)d->Q * d->N * d->real_size;
+  CK(cudaMemcpyAsync((char*)d->f + subs * bytes, f_host, bytes, cudaMemcpyHostToDevice,
+                     d->stream));
+  CK(cudaStreamSynchronize(d->stream));
+  d->parity = 0;
+  return LBX_OK;
+}
+
+lbx_status lbx_download_f(lbx_domain* d, int subs, void* f_host)
+{
+  if (lbx_status st = check_subs(d, subs)) return st;
+  if (!f_host) return fail(LBX_ERR_INVALID, "f_host is NULL");
+  const size_t bytes = (size_t)d->Q * d->N * d->real_size;
+  CK(cudaMemcpyAsync(f_host, (char*)d->f + subs * bytes, bytes, cudaMemcpyDeviceToHost,
+                     d->stream));
+  CK(cudaStreamSynchronize(d->stream));
+  return LBX_OK;
+}
+
+lbx_status lbx_upload_mv(lbx_domain* d, int subs, const void* mv_host)
+{
+  if (lbx_status st = check_subs(d, subs)) return st;
+  if (!mv_host) return fail(LBX_ERR_INVALID, "mv_host is NULL");
+  const size_t bytes = (size_t)(1 + d->D) * d->N * d->real_size;
+  CK(cudaMemcpyAsync((char*)d->mv + subs * bytes, mv_host, bytes, cudaMemcpyHostToDevice,
+                     d->stream));
+  CK(cudaStreamSynchronize(d->stream));
+  return LBX_OK;
+}
+
+lbx_status lbx_download_mv(lbx_domain* d, int subs, void* rho, void* ux, void* uy, void* uz)
+{
+  if (lbx_status st = check_subs(d, subs)) return st;
+  const size_t plane = (size_t)d->N * d->real_size;
+  char* base = (char*)d->mv + (size_t)subs * (1 + d->D) * plane;
+  void* dst[4] = {rho, ux, uy, uz};
+  for (int c = 0; c <= d->D; ++c)
+    if (dst[c])
+      CK(cudaMemcpyAsync(dst[c], base + c * plane, plane, cudaMemcpyDeviceToHost, d->stream));
+  CK(cudaStreamSynchronize(d->stream));
+  return LBX_OK;
+}
+
+lbx_status lbx_init_equilibrium(lbx_domain* d, int subs, const void* rho, const void* ux,
+                                const void* uy, const void* uz)
+{
+  if (lbx_status st = check_subs(d, subs)) return st;
+  if (!rho || !ux || !uy || (d->D == 3 && !uz))
+    return fail(LBX_ERR_INVALID, "rho/ux/uy (and uz in 3D) are required");
+  const size_t plane = (size_t)d->N * d->real_size;
+  void* tmp = nullptr;
+  CK(cudaMalloc(&tmp, 4 * plane));
+  const void* src[4] = {rho, ux, uy, uz};
+  cudaError_t e = cudaSuccess;
+  for (int c = 0; c < 4 && e == cudaSuccess; ++c)
+    if (src[c]) e = cudaMemcpyAsync((char*)tmp + c * plane, src[c], plane,
+                                    cudaMemcpyHostToDevice, d->stream);
+  if (e == cudaSuccess) {
+    const int shifted = d->p.accurate && subs == 0;
+    const unsigned blocks = (unsigned)((d->N + 255) / 256);
+    char* t = (char*)tmp;
+    if (d->real_size == 8) {
+      double* fs = (double*)d->f + (long long)subs * d->Q * d->N;
+      const double* uzp = uz ? (const double*)(t + 3 * plane) : nullptr;
+      if (d->Q == 9) init_feq<double, 9><<<blocks, 256, 0, d->stream>>>(fs, (double*)t, (double*)(t + plane), (double*)(t + 2 * plane), uzp, d->N, shifted);
+      else init_feq<double, 19><<<blocks, 256, 0, d->stream>>>(fs, (double*)t, (double*)(t + plane), (double*)(t + 2 * plane), uzp, d->N, shifted);
+    } else {
+      float* fs = (float*)d->f + (long long)subs * d->Q * d->N;
+      const float* uzp = uz ? (const float*)(t + 3 * plane) : nullptr;
+      if (d->Q == 9) init_feq<float, 9><<<blocks, 256, 0, d->stream>>>(fs, (float*)t, (float*)(t + plane), (float*)(t + 2 * plane), uzp, d->N, shifted);
+      else init_feq<float, 19><<<blocks, 256, 0, d->stream>>>(fs, (float*)t, (float*)(t + plane), (float*)(t + 2 * plane), uzp, d->N, shifted);
+    }
+    d->launches++;
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(d->stream);
+  cudaFree(tmp);
+  if (e != cudaSuccess) return fail(LBX_ERR_CUDA, "init_equilibrium: %s", cudaGetErrorString(e));
+  d->parity = 0;
+  return LBX_OK;
+}
+
+lbx_status lbx_step(lbx_domain* d, int time, unsigned flags)
+{
+  if (!d) return fail(LBX_ERR_INVALID, "domain is NULL");
+  return do_step(d, time, flags);
+}
+
+lbx_status lbx_step_pair(lbx_domain* d, int time, unsigned flags)
+{
+  if (!d) return fail(LBX_ERR_INVALID, "domain is NULL");
+  if (lbx_status st = do_step(d, time, flags)) return st;
+  return do_step(d, time + 1, flags);
+}
+
+lbx_status lbx_run(lbx_domain* d, int t0, int nsteps, int frame_rate)
+{
+  if (!d) return fail(LBX_ERR_INVALID, "domain is NULL");
+  if (nsteps < 0) return fail(LBX_ERR_INVALID, "nsteps must be >= 0");
+  for (int t = t0 + 1; t <= t0 + nsteps; ++t) {
+    const unsigned fl = (frame_rate > 0 && t % frame_rate == 0) ? LBX_WRITE_MV : 0u;
+    if (lbx_status st = do_step(d, t, fl)) return st;
+  }
+  return LBX_OK;
+}
+
+lbx_status lbx_set_stream(lbx_domain* d, void* stream)
+{
+  if (!d) return fail(LBX_ERR_INVALID, "domain is NULL");
+  CK(cudaStreamSynchronize(d->stream));
+  d->stream = stream ? (cudaStream_t)stream : d->own_stream;
+  return LBX_OK;
+}
+
+lbx_status lbx_sync(lbx_domain* d)
+{
+  if (!d) return fail(LBX_ERR_INVALID, "domain is NULL");
+  CK(cudaStreamSynchronize(d->stream));
+  CK(cudaGetLastError());
+  return LBX_OK;
+}
+
+lbx_status lbx_reduce(lbx_domain* d, lbx_reductions* out)
+{
+  if (!d || !out) return fail(LBX_ERR_INVALID, "NULL argument");
+  const int nb = d->red_blocks;
+  RedPartial* red = (RedPartial*)d->red;
+  if (d->real_size == 8) {
+    if (d->D == 2) reduce_mv<double, 2><<<nb, 256, 0, d->stream>>>((const double*)d->mv, d->cls, d->N, d->p.nsubs, red);
+    else reduce_mv<double, 3><<<nb, 256, 0, d->stream>>>((const double*)d->mv, d->cls, d->N, d->p.nsubs, red);
+  } else {
+    if (d->D == 2) reduce_mv<float, 2><<<nb, 256, 0, d->stream>>>((const float*)d->mv, d->cls, d->N, d->p.nsubs, red);
+    else reduce_mv<float, 3><<<nb, 256, 0, d->stream>>>((const float*)d->mv, d->cls, d->N, d->p.nsubs, red);
+  }
+  d->launches++;
+  CK(cudaGetLastError());
+  std::vector<RedPartial> h(nb);
+  CK(cudaMemcpyAsync(h.data(), red, nb * sizeof(RedPartial), cudaMemcpyDeviceToHost, d->stream));
+  CK(cudaStreamSynchronize(d->stream));
+  std::memset(out, 0, sizeof *out);
+  out->rho_min = 1e300; out->rho_max = -1e300;
+  unsigned long long fl = 0, nf = 0;
+  for (const RedPartial& r : h) {
+    out->mass += r.mass; out->solute_mass += r.solute;
+    for (int c = 0; c < 3; ++c) { out->momentum[c] += r.mom[c]; out->u_sum[c] += r.usum[c]; }
+    out->rho_min = r.rmin < out->rho_min ? r.rmin : out->rho_min;
+    out->rho_max = r.rmax > out->rho_max ? r.rmax : out->rho_max;
+    fl += r.fluid; nf += r.nonfinite;
+  }
+  out->fluid_nodes = (long long)fl;
+  out->nonfinite = (int)nf;
+  if (nf) return fail(LBX_ERR_NUMERIC, "%llu fluid nodes hold non-finite macro variables", nf);
+  return LBX_OK;
+}
+
+lbx_status lbx_device_f(lbx_domain* d, void** ptr)
+{
+  if (!d || !ptr) return fail(LBX_ERR_INVALID, "NULL argument");
+  *ptr = d->f;
+  return LBX_OK;
+}
+
+lbx_status lbx_device_mv(lbx_domain* d, void** ptr)
+{
+  if (!d || !ptr) return fail(LBX_ERR_INVALID, "NULL argument");
+  *ptr = d->mv;
+  return LBX_OK;
+}
+
+lbx_status lbx_info(lbx_domain* d, long long* fluid_nodes, int* faces_fused)
+{
+  if (!d) return fail(LBX_ERR_INVALID, "domain is NULL");
+  if (fluid_nodes) *fluid_nodes = d->fluid;
+  if (faces_fused) *faces_fused = d->faces_fused ? 1 : 0;
+  return LBX_OK;
+}
+
+long long lbx_launch_count(lbx_domain* d) { return d ? d->launches : -1; }
+
+const char* lbx_last_error(void) { return g_err.c_str(); }
+
+}  // extern "C"

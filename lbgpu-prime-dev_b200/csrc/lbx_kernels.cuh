@@ -1,0 +1,439 @@
+// lbx_kernels.cuh -- sm_100a device code for the AA-pattern LBM hot path.
+//
+// One thread per lattice node, x fastest, so every population access of a
+// warp is one contiguous run of 32 reals in one direction's plane of the SoA
+// array [subs][a][n].  The step is HBM-bound (19 loads + 19 stores of
+// populations per fluid node and one byte of node class), so there is no
+// shared-memory staging of populations and no tensor-core work: the only
+// per-node state is the Q populations, held in registers.
+//
+// Reference semantics restated here (file:line in the reference tree):
+//   odd step   src/k_stream_collide_stream.c:15-423  (pull, collide, push)
+//   even step  src/k_collide.c:17-416                (swapped local update)
+//   helpers    src/lattice.c:2660-2944               (bounce-back, BGK)
+//   faces      src/system_boundary_kernels.c:5-831   (Zou-He, zero gradient)
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace lbx {
+
+// ---- lattice tables --------------------------------------------------------
+// Direction order of the reference (src/lbgpu_prime.h:82-84): opposites are
+// adjacent (a odd <-> a+1) and D2Q9 is the first nine directions.
+__host__ __device__ constexpr int cx(int a) {
+  return (a == 1 || a == 5 || a == 8 || a == 11 || a == 14) ? 1
+       : (a == 2 || a == 6 || a == 7 || a == 12 || a == 13) ? -1 : 0;
+}
+__host__ __device__ constexpr int cy(int a) {
+  return (a == 3 || a == 5 || a == 7 || a == 15 || a == 18) ? 1
+       : (a == 4 || a == 6 || a == 8 || a == 16 || a == 17) ? -1 : 0;
+}
+__host__ __device__ constexpr int cz(int a) {
+  return (a == 9 || a == 11 || a == 13 || a == 15 || a == 17) ? 1
+       : (a == 10 || a == 12 || a == 14 || a == 16 || a == 18) ? -1 : 0;
+}
+__host__ __device__ constexpr int opp(int a) {
+  return a == 0 ? 0 : ((a & 1) ? a + 1 : a - 1);
+}
+// Weights (src/latman.c:161-192), rounded to T as the reference's `real`.
+template <typename T, int Q>
+__host__ __device__ constexpr T wgt(int a) {
+  return Q == 9
+    ? (a == 0 ? T(4. / 9.) : (a < 5 ? T(1. / 9.) : T(1. / 36.)))
+    : (a == 0 ? T(1. / 3.)
+       : (a < 5 ? T(1. / 18.)
+          : (a < 9 ? T(1. / 36.) : (a < 11 ? T(1. / 18.) : T(1. / 36.)))));
+}
+
+enum Dir2 { DC = 0, DE, DW, DN, DS, DNE, DSW, DNW, DSE };
+
+// Node class byte, built once per domain from the solids mask.
+enum : uint8_t {
+  CLS_SOLID = 1,      // byte == 1 in the reference's mask
+  CLS_NEAR = 2,       // fluid with at least one solid neighbour: read nbm[n]
+  CLS_NORTH = 4,      // 2D: row j = LY-1
+  CLS_SOUTH = 8       // 2D: row j = 0
+};
+
+// Collision models: the reference's ACCURATE / COMPRESSIBLE flag pairs.
+enum Model { SHIFTED_INC = 0, PLAIN_COMP = 1, SHIFTED_COMP = 2 };
+
+// Face action per substance (2D): what the last active boundary on that
+// face does; boundaries on one face all rewrite the same three unknowns from
+// the same knowns, so the last one in the reference's order wins.
+enum FaceKind { FACE_NONE = 0, FACE_PRESSURE = 1, FACE_ZEROGRAD = 2 };
+
+template <typename T>
+struct SubsConst {
+  T omc;     // 1 - 1/tau
+  T itau;    // 1/tau
+  T rhoA;    // rho_A
+  T tg[3];   // tau * g  (velocity shift of the body force)
+};
+
+template <typename T>
+struct StepArgs {
+  T* f;                  // [nsubs][Q][N]
+  T* mv;                 // [nsubs][1+D][N]
+  const uint8_t* cls;    // [N]
+  const uint32_t* nbm;   // [N]: bit a set iff node n + c_a is solid
+  int LX, LY, LZ;
+  long long N;
+  SubsConst<T> sc[2];
+  T sink1;               // (1 - sink * tau[1]) for the solute
+  int write_mv;
+  int solute_on;
+  int face_n[2], face_s[2];   // FaceKind per substance (2D, fused path)
+  T rho_n[2], rho_s[2];       // face densities this step
+};
+
+// ---- per-node collision ---------------------------------------------------
+// d[] holds the node's incoming populations of substance s; u carries the
+// fluid velocity to the solute as the reference's per-thread scratch does.
+// sinks: the solute sink applies once on odd steps and twice on even steps
+// (src/k_stream_collide_stream.c:254-256; src/k_collide.c:96-97, :261-262).
+template <typename T, int Q, int MODEL>
+__device__ __forceinline__ void collide(const StepArgs<T>& A, int s, bool solute,
+                                        int sinks, T (&d)[Q], T (&u)[3],
+                                        long long n)
+{
+  constexpr int D = (Q == 9) ? 2 : 3;
+  const SubsConst<T>& c = A.sc[s];
+  T rho = d[0];
+#pragma unroll
+  for (int a = 1; a < Q; ++a) rho += d[a];
+  if (solute) {
+    if (sinks == 2) rho *= A.sink1;
+    rho *= A.sink1;
+  } else {
+    T m0 = T(0), m1 = T(0), m2 = T(0);
+#pragma unroll
+    for (int a = 0; a < Q; ++a) {
+      if (cx(a) > 0) m0 += d[a]; else if (cx(a) < 0) m0 -= d[a];
+      if (cy(a) > 0) m1 += d[a]; else if (cy(a) < 0) m1 -= d[a];
+      if (D == 3) { if (cz(a) > 0) m2 += d[a]; else if (cz(a) < 0) m2 -= d[a]; }
+    }
+    T den = (MODEL == SHIFTED_INC) ? c.rhoA
+          : (MODEL == PLAIN_COMP) ? rho : (c.rhoA + rho);
+    u[0] = m0 / den + c.tg[0];
+    u[1] = m1 / den + c.tg[1];
+    u[2] = (D == 3) ? (m2 / den + c.tg[2]) : T(0);
+  }
+  if (A.write_mv) {
+    T* m = A.mv + (long long)s * (1 + D) * A.N;
+    m[n] = (!solute && MODEL != PLAIN_COMP) ? rho + c.rhoA : rho;
+    m[A.N + n] = u[0];
+    m[2 * A.N + n] = u[1];
+    if (D == 3) m[3 * A.N + n] = u[2];
+  }
+  if (solute) {
+    // g_a <- g_a (1 - 1/tau_s) + w_a C (1 + 3 c.u) / tau_s  (src/lattice.c:2858-2875)
+#pragma unroll
+    for (int a = 0; a < Q; ++a) {
+      T cu = T(cx(a)) * u[0] + T(cy(a)) * u[1] + (D == 3 ? T(cz(a)) * u[2] : T(0));
+      d[a] = d[a] * c.omc + wgt<T, Q>(a) * rho * (T(1) + T(3) * cu) * c.itau;
+    }
+  } else {
+    // BGK in shifted or plain form (src/lattice.c:2880-2919)
+    T usq = u[0] * u[0] + u[1] * u[1] + (D == 3 ? u[2] * u[2] : T(0));
+    T rq = (MODEL == SHIFTED_INC) ? c.rhoA
+         : (MODEL == PLAIN_COMP) ? rho : (c.rhoA + rho);
+#pragma unroll
+    for (int a = 0; a < Q; ++a) {
+      T cu = T(cx(a)) * u[0] + T(cy(a)) * u[1] + (D == 3 ? T(cz(a)) * u[2] : T(0));
+      T w = wgt<T, Q>(a);
+      d[a] = d[a] * c.omc + w * rho * c.itau
+           + w * rq * (T(3) * cu + T(4.5) * cu * cu - T(1.5) * usq) * c.itau;
+    }
+  }
+}
+
+// ---- fused 2D faces ---------------------------------------------------------
+// Zou-He density on the north / south row in shifted or plain form
+// (src/system_boundary_kernels.c:58-83, :282-307) and the solute
+// zero-gradient rule (:503-521, :692-710), applied to the node's incoming
+// populations in registers.  Valid only where the reference's deposit of the
+// unknowns lands on the slot this node then pulls (the host checks that the
+// wrapped upstream nodes of every face node are fluid, else it runs the
+// stand-alone face kernels below).
+template <typename T>
+__device__ __forceinline__ void face_north(int kind, T rho_bc, T rhoA, bool shifted,
+                                           T (&d)[9])
+{
+  if (kind == FACE_PRESSURE) {
+    T X = d[DC] + d[DE] + d[DW] + d[DN] + d[DN] + d[DNE] + d[DNE] + d[DNW] + d[DNW];
+    X -= rho_bc;
+    if (shifted) X += rhoA;
+    d[DS] = d[DN] - T(2. / 3.) * X;
+    d[DSW] = d[DNE] + T(0.5) * (d[DE] - d[DW]) - T(1. / 6.) * X;
+    d[DSE] = d[DNW] + T(0.5) * (d[DW] - d[DE]) - T(1. / 6.) * X;
+  } else if (kind == FACE_ZEROGRAD) {
+    T X = (d[DN] + d[DNE] + d[DNW]) / (wgt<T, 9>(DS) + wgt<T, 9>(DSW) + wgt<T, 9>(DSE));
+    d[DS] = wgt<T, 9>(DS) * X;
+    d[DSW] = wgt<T, 9>(DSW) * X;
+    d[DSE] = wgt<T, 9>(DSE) * X;
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ void face_south(int kind, T rho_bc, T rhoA, bool shifted,
+                                           T (&d)[9])
+{
+  if (kind == FACE_PRESSURE) {
+    T X = -d[DC] - d[DE] - d[DW] - d[DS] - d[DS] - d[DSE] - d[DSE] - d[DSW] - d[DSW];
+    X += rho_bc;
+    if (shifted) X -= rhoA;
+    d[DN] = d[DS] + T(2. / 3.) * X;
+    d[DNE] = d[DSW] + T(0.5) * (d[DW] - d[DE]) + T(1. / 6.) * X;
+    d[DNW] = d[DSE] + T(0.5) * (d[DE] - d[DW]) + T(1. / 6.) * X;
+  } else if (kind == FACE_ZEROGRAD) {
+    T X = (d[DS] + d[DSW] + d[DSE]) / (wgt<T, 9>(DN) + wgt<T, 9>(DNE) + wgt<T, 9>(DNW));
+    d[DN] = wgt<T, 9>(DN) * X;
+    d[DNE] = wgt<T, 9>(DNE) * X;
+    d[DNW] = wgt<T, 9>(DNW) * X;
+  }
+}
+
+// ---- the AA step kernel -----------------------------------------------------
+// ODD: pull d_a from f[a][n - c_a] (own f[opp a][n] if that node is solid),
+//      collide, push d_a to f[opp a][n + c_a] (own f[a][n] if solid).
+// EVEN: d_a = f[opp a][n], collide, f[a][n] = d_a.
+// Each node reads and writes one fixed slot set, disjoint from every other
+// node's, so the update is in place with no ordering between threads.
+template <typename T, int Q, int NS, int MODEL, bool ODD>
+__global__ void __launch_bounds__(128)
+aa_step(StepArgs<T> A)
+{
+  constexpr int D = (Q == 9) ? 2 : 3;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= A.LX) return;
+  const int j = blockIdx.y, k = blockIdx.z;
+  const int LX = A.LX, LY = A.LY;
+  // Node indices are 32-bit (the host rejects N >= 2^31); direction planes
+  // are reached through 64-bit base pointers, which are uniform per warp.
+  const int plane = LX * LY;
+  const int n = i + LX * j + plane * k;
+  const uint8_t cl = A.cls[n];
+  if (cl & CLS_SOLID) return;
+  const uint32_t nb = (cl & CLS_NEAR) ? A.nbm[n] : 0u;
+
+  // nbr[a] = node n + c_a, periodic on every axis (a serial run's wrap).
+  int nbr[Q];
+  if (ODD) {
+    const int xm = (i == 0) ? LX - 1 : -1, xp = (i == LX - 1) ? 1 - LX : 1;
+    const int ym = (j == 0) ? plane - LX : -LX, yp = (j == LY - 1) ? LX - plane : LX;
+    int zm = 0, zp = 0;
+    if (D == 3) {
+      const int tot = plane * A.LZ;
+      zm = (k == 0) ? tot - plane : -plane;
+      zp = (k == A.LZ - 1) ? plane - tot : plane;
+    }
+#pragma unroll
+    for (int a = 0; a < Q; ++a)
+      nbr[a] = n + (cx(a) < 0 ? xm : (cx(a) > 0 ? xp : 0))
+                 + (cy(a) < 0 ? ym : (cy(a) > 0 ? yp : 0))
+                 + (cz(a) < 0 ? zm : (cz(a) > 0 ? zp : 0));
+  }
+
+  T u[3] = {T(0), T(0), T(0)};
+#pragma unroll
+  for (int s = 0; s < NS; ++s) {
+    const bool solute = (NS == 2 && s == 1);
+    if (solute && !A.solute_on) break;
+    T* const fs = A.f + (size_t)s * Q * (size_t)A.N;
+    const size_t N = (size_t)A.N;
+    T d[Q];
+    if (ODD) {
+      // pull: d_a = f[a][n - c_a], or own f[opp a][n] behind a solid
+#pragma unroll
+      for (int a = 0; a < Q; ++a) {
+        if ((nb >> opp(a)) & 1u) d[a] = fs[opp(a) * N + n];
+        else d[a] = fs[a * N + nbr[opp(a)]];
+      }
+    } else {
+#pragma unroll
+      for (int a = 0; a < Q; ++a) d[a] = fs[opp(a) * N + n];
+    }
+    if (Q == 9 && (cl & (CLS_NORTH | CLS_SOUTH))) {
+      T (&d9)[9] = reinterpret_cast<T (&)[9]>(d);
+      const bool shifted = (MODEL != PLAIN_COMP) && !solute;
+      if (cl & CLS_NORTH) face_north<T>(A.face_n[s], A.rho_n[s], A.sc[s].rhoA, shifted, d9);
+      if (cl & CLS_SOUTH) face_south<T>(A.face_s[s], A.rho_s[s], A.sc[s].rhoA, shifted, d9);
+    }
+    collide<T, Q, MODEL>(A, s, solute, ODD ? 1 : 2, d, u, n);
+    if (ODD) {
+      // push: f[opp a][n + c_a] = d_a, or own f[a][n] in front of a solid
+#pragma unroll
+      for (int a = 0; a < Q; ++a) {
+        if ((nb >> a) & 1u) fs[a * N + n] = d[a];
+        else fs[opp(a) * N + nbr[a]] = d[a];
+      }
+    } else {
+#pragma unroll
+      for (int a = 0; a < Q; ++a) fs[a * N + n] = d[a];
+    }
+  }
+}
+
+// ---- stand-alone 2D face kernels (exact reference semantics) ----------------
+// One thread per node of the row.  `_1` form (before an odd step): pull the
+// node's populations through bounce-back, compute the unknowns, deposit each
+// into slot a of the upstream node n - c_a, or into the node's own slot a if
+// that node is solid (set_f1d_d with offset -c_a).  `_2` form (before an even
+// step): swapped own-slot load, unknown a stored in own slot opp(a).
+template <typename T>
+__global__ void face_row(T* fs, const uint8_t* solids, int LX, int LY,
+                         long long N, int north, int kind, int second, T rho_bc,
+                         T rhoA, int shifted)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= LX) return;
+  const int j = north ? LY - 1 : 0;
+  const long long n = (long long)i + (long long)LX * j;
+  if (solids[n] == 1) return;
+  auto wrap = [&](int ii, int jj) -> long long {
+    ii = ii < 0 ? ii + LX : (ii == LX ? 0 : ii);
+    jj = jj < 0 ? jj + LY : (jj == LY ? 0 : jj);
+    return (long long)ii + (long long)LX * jj;
+  };
+  T d[9];
+#pragma unroll
+  for (int a = 0; a < 9; ++a) {
+    if (second) {
+      d[a] = fs[(long long)opp(a) * N + n];
+    } else {
+      const long long up = wrap(i - cx(a), j - cy(a));
+      d[a] = (solids[up] == 1) ? fs[(long long)opp(a) * N + n]
+                               : fs[(long long)a * N + up];
+    }
+  }
+  if (north) face_north<T>(kind, rho_bc, rhoA, shifted != 0, d);
+  else face_south<T>(kind, rho_bc, rhoA, shifted != 0, d);
+  const int u0 = north ? DS : DN, u1 = north ? DSE : DNW, u2 = north ? DSW : DNE;
+  const int unk[3] = {u0, u1, u2};
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    const int a = unk[q];
+    if (second) {
+      fs[(long long)opp(a) * N + n] = d[a];
+    } else {
+      const long long up = wrap(i - cx(a), j - cy(a));
+      if (solids[up] == 1) fs[(long long)a * N + n] = d[a];
+      else fs[(long long)a * N + up] = d[a];
+    }
+  }
+}
+
+// ---- node classification ----------------------------------------------------
+template <int Q>
+__global__ void classify(const uint8_t* solids, uint8_t* cls, uint32_t* nbm,
+                         int LX, int LY, int LZ)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= LX) return;
+  const int j = blockIdx.y, k = blockIdx.z;
+  const long long n = (long long)i + (long long)LX * (j + (long long)LY * k);
+  if (solids[n] == 1) { cls[n] = CLS_SOLID; nbm[n] = 0; return; }
+  uint32_t m = 0;
+#pragma unroll
+  for (int a = 1; a < Q; ++a) {
+    int ii = i + cx(a), jj = j + cy(a), kk = k + cz(a);
+    ii = ii < 0 ? ii + LX : (ii == LX ? 0 : ii);
+    jj = jj < 0 ? jj + LY : (jj == LY ? 0 : jj);
+    kk = kk < 0 ? kk + LZ : (kk == LZ ? 0 : kk);
+    const long long nn = (long long)ii + (long long)LX * (jj + (long long)LY * kk);
+    if (solids[nn] == 1) m |= 1u << a;
+  }
+  uint8_t c = m ? CLS_NEAR : 0;
+  if (Q == 9) {
+    if (j == LY - 1) c |= CLS_NORTH;
+    if (j == 0) c |= CLS_SOUTH;
+  }
+  cls[n] = c;
+  nbm[n] = m;
+}
+
+// ---- equilibrium initial state (src/latman.c:1786-1840) --------------------
+template <typename T, int Q>
+__global__ void init_feq(T* fs, const T* rho, const T* ux, const T* uy,
+                         const T* uz, long long N, int shifted)
+{
+  const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= N) return;
+  const T r = rho[n], x = ux[n], y = uy[n], z = uz ? uz[n] : T(0);
+  const T usq = x * x + y * y + z * z;
+#pragma unroll
+  for (int a = 0; a < Q; ++a) {
+    const T cu = T(cx(a)) * x + T(cy(a)) * y + T(cz(a)) * z;
+    const T w = wgt<T, Q>(a);
+    T v;
+    if (a == 0) v = shifted ? w * r * (T(-1.5) * usq) : w * r * (T(1) - T(1.5) * usq);
+    else if (shifted) v = w * r * (T(3) * cu + T(4.5) * cu * cu - T(1.5) * usq);
+    else v = w * r * (T(1) + T(3) * cu + T(4.5) * cu * cu - T(1.5) * usq);
+    fs[(long long)a * N + n] = v;
+  }
+}
+
+// ---- FP64 reductions over macro variables -----------------------------------
+struct RedPartial {
+  double mass, solute, mom[3], usum[3], rmin, rmax;
+  unsigned long long fluid, nonfinite;
+};
+
+template <typename T, int D>
+__global__ void reduce_mv(const T* mv, const uint8_t* cls, long long N, int nsubs,
+                          RedPartial* out)
+{
+  RedPartial r;
+  r.mass = r.solute = 0; r.mom[0] = r.mom[1] = r.mom[2] = 0;
+  r.usum[0] = r.usum[1] = r.usum[2] = 0;
+  r.rmin = 1e300; r.rmax = -1e300; r.fluid = 0; r.nonfinite = 0;
+  for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < N;
+       n += (long long)gridDim.x * blockDim.x) {
+    if (cls[n] & CLS_SOLID) continue;
+    const double rho = (double)mv[n];
+    double u[3] = {(double)mv[N + n], (double)mv[2 * N + n],
+                   D == 3 ? (double)mv[3 * N + n] : 0.0};
+    if (!isfinite(rho) || !isfinite(u[0]) || !isfinite(u[1]) || !isfinite(u[2])) {
+      r.nonfinite++;
+      continue;
+    }
+    r.fluid++;
+    r.mass += rho;
+    r.rmin = fmin(r.rmin, rho);
+    r.rmax = fmax(r.rmax, rho);
+    for (int c = 0; c < 3; ++c) { r.mom[c] += rho * u[c]; r.usum[c] += u[c]; }
+    if (nsubs == 2) r.solute += (double)mv[(long long)(1 + D) * N + n];
+  }
+  // warp then block reduction
+  for (int off = 16; off > 0; off >>= 1) {
+    r.mass += __shfl_down_sync(0xffffffffu, r.mass, off);
+    r.solute += __shfl_down_sync(0xffffffffu, r.solute, off);
+    for (int c = 0; c < 3; ++c) {
+      r.mom[c] += __shfl_down_sync(0xffffffffu, r.mom[c], off);
+      r.usum[c] += __shfl_down_sync(0xffffffffu, r.usum[c], off);
+    }
+    r.rmin = fmin(r.rmin, __shfl_down_sync(0xffffffffu, r.rmin, off));
+    r.rmax = fmax(r.rmax, __shfl_down_sync(0xffffffffu, r.rmax, off));
+    r.fluid += __shfl_down_sync(0xffffffffu, r.fluid, off);
+    r.nonfinite += __shfl_down_sync(0xffffffffu, r.nonfinite, off);
+  }
+  __shared__ RedPartial sh[32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) sh[wid] = r;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    RedPartial t = sh[0];
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) {
+      t.mass += sh[w].mass; t.solute += sh[w].solute;
+      for (int c = 0; c < 3; ++c) { t.mom[c] += sh[w].mom[c]; t.usum[c] += sh[w].usum[c]; }
+      t.rmin = fmin(t.rmin, sh[w].rmin); t.rmax = fmax(t.rmax, sh[w].rmax);
+      t.fluid += sh[w].fluid; t.nonfinite += sh[w].nonfinite;
+    }
+    out[blockIdx.x] = t;
+  }
+}
+
+}  // namespace lbx

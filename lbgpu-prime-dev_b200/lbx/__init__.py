@@ -1,0 +1,311 @@
+"""Python binding of the lbx C ABI (include/lbx.h) over ctypes.
+
+The binding is a thin host-side mirror of the reference's device-facing
+calls: construct the device lattice, upload the populations, step at the
+reference's odd/even times, download the macro variables.  All compute runs
+in the CUDA library ``lib/liblbx.so``; there is no CPU fallback and importing
+this module fails if the library has not been built.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass, field, fields
+from typing import Optional, Sequence
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(_HERE), "lib", "liblbx.so")
+
+LBX_OK, LBX_ERR_INVALID, LBX_ERR_CUDA, LBX_ERR_NOMEM, LBX_ERR_STATE, LBX_ERR_NUMERIC = range(6)
+LBX_WRITE_MV = 1
+
+_D2 = C.c_double * 2
+_D6 = C.c_double * 6
+_I2 = C.c_int * 2
+
+
+class _CParams(C.Structure):
+    _fields_ = [
+        ("dims", C.c_int), ("LX", C.c_int), ("LY", C.c_int), ("LZ", C.c_int),
+        ("nsubs", C.c_int), ("precision", C.c_int),
+        ("accurate", C.c_int), ("compressible", C.c_int),
+        ("tau", _D2), ("rho_A", _D2), ("gaccel", _D6), ("sink", C.c_double),
+        ("sigma_t_on", C.c_int), ("sigma_t_off", C.c_int),
+        ("pressure_n_in", _I2), ("pressure_s_in", _I2),
+        ("pressure_n_out", _I2), ("pressure_s_out", _I2),
+        ("zeroconcgrad_n", C.c_int), ("zeroconcgrad_s", C.c_int),
+        ("rho_in", C.c_double), ("rho_out", C.c_double),
+        ("pfadd", C.c_double), ("pfmul", C.c_double),
+        ("bc_ramp_start", C.c_int), ("bc_ramp_stop", C.c_int),
+        ("pressure_n_table", C.POINTER(C.c_double)), ("pressure_n_len", C.c_int),
+        ("pressure_s_table", C.POINTER(C.c_double)), ("pressure_s_len", C.c_int),
+        ("device", C.c_int),
+    ]
+
+
+class _CReductions(C.Structure):
+    _fields_ = [
+        ("mass", C.c_double), ("solute_mass", C.c_double),
+        ("momentum", C.c_double * 3), ("u_sum", C.c_double * 3),
+        ("rho_min", C.c_double), ("rho_max", C.c_double),
+        ("fluid_nodes", C.c_longlong), ("nonfinite", C.c_int),
+    ]
+
+
+# Every symbol include/lbx.h declares, with its ctypes signature.
+_SIGNATURES = {
+    "lbx_params_default": (None, [C.POINTER(_CParams)]),
+    "lbx_create": (C.c_int, [C.POINTER(_CParams), C.c_void_p, C.POINTER(C.c_void_p)]),
+    "lbx_destroy": (C.c_int, [C.c_void_p]),
+    "lbx_upload_f": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    "lbx_download_f": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    "lbx_upload_mv": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    "lbx_download_mv": (C.c_int, [C.c_void_p, C.c_int] + [C.c_void_p] * 4),
+    "lbx_init_equilibrium": (C.c_int, [C.c_void_p, C.c_int] + [C.c_void_p] * 4),
+    "lbx_step": (C.c_int, [C.c_void_p, C.c_int, C.c_uint]),
+    "lbx_step_pair": (C.c_int, [C.c_void_p, C.c_int, C.c_uint]),
+    "lbx_run": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int]),
+    "lbx_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "lbx_sync": (C.c_int, [C.c_void_p]),
+    "lbx_reduce": (C.c_int, [C.c_void_p, C.POINTER(_CReductions)]),
+    "lbx_device_f": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "lbx_device_mv": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "lbx_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_longlong), C.POINTER(C.c_int)]),
+    "lbx_launch_count": (C.c_longlong, [C.c_void_p]),
+    "lbx_last_error": (C.c_char_p, []),
+}
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH):
+    """Load liblbx.so and bind every exported symbol; raises if missing."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError(
+            "liblbx.so not found at %s: build it with `make -C lbgpu-prime-dev_b200` "
+            "(there is no CPU fallback)" % path)
+    lib = C.CDLL(path)
+    for name, (res, args) in _SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+class LbxError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__("lbx error %d: %s" % (code, msg))
+        self.code = code
+
+
+def _check(rc: int):
+    if rc != LBX_OK:
+        raise LbxError(rc, _lib.lbx_last_error().decode())
+
+
+@dataclass
+class Params:
+    """lbx_params; names and meanings follow the reference's params.in."""
+    dims: int = 3
+    LX: int = 1
+    LY: int = 1
+    LZ: int = 1
+    nsubs: int = 1
+    precision: int = 8
+    accurate: int = 1
+    compressible: int = 0
+    tau: Sequence[float] = (1.0, 1.0)
+    rho_A: Sequence[float] = (1.0, 1.0)
+    gaccel: Sequence[float] = (0.0,) * 6
+    sink: float = 0.0
+    sigma_t_on: int = 0
+    sigma_t_off: int = -1
+    pressure_n_in: Sequence[int] = (0, 0)
+    pressure_s_in: Sequence[int] = (0, 0)
+    pressure_n_out: Sequence[int] = (0, 0)
+    pressure_s_out: Sequence[int] = (0, 0)
+    zeroconcgrad_n: int = 0
+    zeroconcgrad_s: int = 0
+    rho_in: float = 1.0
+    rho_out: float = 1.0
+    pfadd: float = 1.0
+    pfmul: float = 0.1
+    bc_ramp_start: int = -1
+    bc_ramp_stop: int = -1
+    pressure_n_table: Optional[np.ndarray] = None
+    pressure_s_table: Optional[np.ndarray] = None
+    device: int = 0
+
+    @property
+    def Q(self) -> int:
+        return 9 if self.dims == 2 else 19
+
+    @property
+    def NN(self) -> int:
+        return self.LX * self.LY * self.LZ
+
+    @property
+    def dtype(self):
+        return np.float64 if self.precision == 8 else np.float32
+
+    def _to_c(self, keep: list) -> _CParams:
+        st = _CParams()
+        for name, _ in _CParams._fields_:
+            if name.endswith("_len"):
+                continue
+            v = getattr(self, name)
+            if name.endswith("_table"):
+                if v is not None:
+                    arr = np.ascontiguousarray(v, dtype=np.float64)
+                    keep.append(arr)
+                    setattr(st, name, arr.ctypes.data_as(C.POINTER(C.c_double)))
+                    setattr(st, name.replace("_table", "_len"), len(arr))
+                continue
+            if isinstance(v, (tuple, list)):
+                fld = getattr(st, name)
+                for i, x in enumerate(v):
+                    fld[i] = x
+            else:
+                setattr(st, name, v)
+        return st
+
+
+class Domain:
+    """One device lattice (lbx_domain)."""
+
+    def __init__(self, params: Params, solids: np.ndarray):
+        load_library()
+        self.p = params
+        sol = np.ascontiguousarray(solids, dtype=np.uint8).reshape(-1)
+        if sol.size != params.NN:
+            raise ValueError("solids must hold LX*LY*LZ bytes")
+        keep = []
+        cp = params._to_c(keep)
+        h = C.c_void_p()
+        _check(_lib.lbx_create(C.byref(cp), sol.ctypes.data, C.byref(h)))
+        self._h = h
+
+    # -- lifecycle ---------------------------------------------------------
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.lbx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- data --------------------------------------------------------------
+    def upload_f(self, f: np.ndarray, subs: Optional[int] = None):
+        """f: [nsubs, Q, N] (all substances) or [Q, N] with subs given."""
+        p = self.p
+        f = np.ascontiguousarray(f, dtype=p.dtype)
+        if subs is None:
+            f = f.reshape(p.nsubs, p.Q, p.NN)
+            for s in range(p.nsubs):
+                _check(_lib.lbx_upload_f(self._h, s, f[s].ctypes.data))
+        else:
+            _check(_lib.lbx_upload_f(self._h, subs, f.reshape(p.Q, p.NN).ctypes.data))
+
+    def download_f(self) -> np.ndarray:
+        p = self.p
+        out = np.empty((p.nsubs, p.Q, p.NN), dtype=p.dtype)
+        for s in range(p.nsubs):
+            _check(_lib.lbx_download_f(self._h, s, out[s].ctypes.data))
+        return out
+
+    def upload_mv(self, mv: np.ndarray):
+        p = self.p
+        mv = np.ascontiguousarray(mv, dtype=p.dtype).reshape(p.nsubs, 1 + p.dims, p.NN)
+        for s in range(p.nsubs):
+            _check(_lib.lbx_upload_mv(self._h, s, mv[s].ctypes.data))
+
+    def download_mv(self) -> np.ndarray:
+        """[nsubs, 1+D, N]: rho, ux, uy[, uz] per substance."""
+        p = self.p
+        out = np.empty((p.nsubs, 1 + p.dims, p.NN), dtype=p.dtype)
+        for s in range(p.nsubs):
+            ptrs = [out[s, c].ctypes.data for c in range(1 + p.dims)]
+            if p.dims == 2:
+                ptrs.append(None)
+            _check(_lib.lbx_download_mv(self._h, s, *ptrs))
+        return out
+
+    def init_equilibrium(self, subs: int, rho, ux, uy, uz=None):
+        p = self.p
+        arrs = [np.ascontiguousarray(np.broadcast_to(np.asarray(x, dtype=p.dtype), (p.NN,)))
+                for x in (rho, ux, uy)]
+        uzp = None
+        if p.dims == 3:
+            arrs.append(np.ascontiguousarray(np.broadcast_to(
+                np.asarray(0.0 if uz is None else uz, dtype=p.dtype), (p.NN,))))
+            uzp = arrs[3].ctypes.data
+        _check(_lib.lbx_init_equilibrium(self._h, subs, arrs[0].ctypes.data,
+                                         arrs[1].ctypes.data, arrs[2].ctypes.data, uzp))
+
+    # -- stepping ----------------------------------------------------------
+    def step(self, time: int, write_mv: bool = False):
+        _check(_lib.lbx_step(self._h, time, LBX_WRITE_MV if write_mv else 0))
+
+    def step_pair(self, time: int, write_mv: bool = False):
+        _check(_lib.lbx_step_pair(self._h, time, LBX_WRITE_MV if write_mv else 0))
+
+    def run(self, t0: int, nsteps: int, frame_rate: int = 0):
+        _check(_lib.lbx_run(self._h, t0, nsteps, frame_rate))
+
+    def set_stream(self, stream_handle: Optional[int]):
+        """Queue work on a caller's cudaStream_t (an integer handle), or None."""
+        _check(_lib.lbx_set_stream(self._h, stream_handle))
+
+    def sync(self):
+        _check(_lib.lbx_sync(self._h))
+
+    def reduce(self) -> dict:
+        r = _CReductions()
+        rc = _lib.lbx_reduce(self._h, C.byref(r))
+        out = dict(mass=r.mass, solute_mass=r.solute_mass,
+                   momentum=tuple(r.momentum), u_sum=tuple(r.u_sum),
+                   rho_min=r.rho_min, rho_max=r.rho_max,
+                   fluid_nodes=r.fluid_nodes, nonfinite=r.nonfinite)
+        if rc not in (LBX_OK, LBX_ERR_NUMERIC):
+            _check(rc)
+        out["status"] = rc
+        return out
+
+    # -- introspection -----------------------------------------------------
+    def device_f_ptr(self) -> int:
+        ptr = C.c_void_p()
+        _check(_lib.lbx_device_f(self._h, C.byref(ptr)))
+        return ptr.value
+
+    def device_mv_ptr(self) -> int:
+        ptr = C.c_void_p()
+        _check(_lib.lbx_device_mv(self._h, C.byref(ptr)))
+        return ptr.value
+
+    def info(self) -> dict:
+        fl = C.c_longlong()
+        fused = C.c_int()
+        _check(_lib.lbx_info(self._h, C.byref(fl), C.byref(fused)))
+        return dict(fluid_nodes=fl.value, faces_fused=bool(fused.value))
+
+    def launch_count(self) -> int:
+        return int(_lib.lbx_launch_count(self._h))
+
+
+def exported_symbols() -> list:
+    return list(_SIGNATURES)

@@ -2,7 +2,7 @@
 
 Test infrastructure only.  Nothing in the product path imports or links this.
 
-Two kinds of artefact are produced, both only into ``oracle/_ref/``:
+The artefacts, written only into ``oracle/_ref/``, are
 
 * ``librefk_<variant>.so`` -- the reference's CUDA kernel sources
   (``src/k_stream_collide_stream.c``, ``src/k_collide.c``,
@@ -11,10 +11,8 @@ Two kinds of artefact are produced, both only into ``oracle/_ref/``:
   ``oracle/refk_harness.c``, which runs every launch as a sequential loop over
   blocks of one thread.  The AA-pattern kernels touch a disjoint slot set per
   node, so the sequential run computes what the GPU launch computes (up to FMA
-  contraction on the GPU).
-* ``refcpu_<variant>`` -- the reference's CPU time loop
-  (``src/stream_collide_stream.c`` + ``src/collide.c``) through
-  ``oracle/refcpu_harness.c``; used only as the timed CPU baseline.
+  contraction on the GPU).  They pin the C restatement and, run on the
+  host cores, are the reference arm of bench.py.
 
 A build variant is a set of ``flags.h`` values.  ``flags.h`` has one include
 guard and no per-flag guards, so each variant gets an edited copy written to
@@ -54,17 +52,12 @@ VARIANTS = {
     # shifted compressible ("ACCURATE 1, COMPRESSIBLE 1")
     "d3q19c_f64": dict(NUM_DIMENSIONS=3, NUM_FLUID_COMPONENTS=1, DP_ON=1,
                        ACCURATE=1, COMPRESSIBLE=1),
-}
-
-# CPU-loop variants for the timed baseline: the reference's CPU loops divide
-# by sum(f), which is zero for shifted populations, so they run unshifted.
-CPU_VARIANTS = {
-    "d3q19_cpu": dict(NUM_DIMENSIONS=3, NUM_FLUID_COMPONENTS=1, DP_ON=1,
+    "d3q19p_f32": dict(NUM_DIMENSIONS=3, NUM_FLUID_COMPONENTS=1, DP_ON=0,
+                       ACCURATE=0, COMPRESSIBLE=1),
+    "d2q9p_f32": dict(NUM_DIMENSIONS=2, NUM_FLUID_COMPONENTS=1, DP_ON=0,
                       ACCURATE=0, COMPRESSIBLE=1),
-    "d2q9_cpu": dict(NUM_DIMENSIONS=2, NUM_FLUID_COMPONENTS=1, DP_ON=1,
-                     ACCURATE=0, COMPRESSIBLE=1),
+    "d2q9s_f32": dict(NUM_DIMENSIONS=2, NUM_FLUID_COMPONENTS=2, DP_ON=0),
 }
-
 
 def variant_flags(src: str, overrides: dict) -> str:
     with open(os.path.join(src, "flags.h")) as fh:
@@ -103,19 +96,6 @@ def build(src: str, only=None) -> None:
             "-include", fl, "-I", src,
             os.path.join(HERE, "refk_harness.c"),
             "-o", os.path.join(OUT, "librefk_%s.so" % name), "-lm"])
-    for name, ov in CPU_VARIANTS.items():
-        if only and name not in only:
-            continue
-        vdir = os.path.join(OUT, name)
-        os.makedirs(vdir, exist_ok=True)
-        fl = os.path.join(vdir, "flags.h")
-        with open(fl, "w") as fh:
-            fh.write(variant_flags(src, ov))
-        sh(["gcc", "-O3", "-std=gnu99", "-w",
-            "-ffunction-sections", "-fdata-sections", "-Wl,--gc-sections",
-            "-include", fl, "-I", src,
-            os.path.join(HERE, "refcpu_harness.c"),
-            "-o", os.path.join(OUT, "refcpu_%s" % name), "-lm"])
 
 
 def main(argv=None) -> int:

@@ -28,6 +28,7 @@
 #include <math.h>
 #include <assert.h>
 #include <time.h>
+#include <pthread.h>
 
 #if DP_ON
 typedef double real;
@@ -39,11 +40,12 @@ typedef float real;
 #define __global__
 #define __device__
 #define __constant__
-#define __shared__
+#define __shared__ __thread   /* only `extern __shared__ real fptr[]` uses it */
 #define __CUDACC__ 1
 #define __CUDA_ARCH__ 1000
 typedef struct { unsigned int x, y, z; } refk_dim3;
-static refk_dim3 threadIdx, blockIdx, blockDim;
+/* Thread-local, so host threads can each walk a part of the grid. */
+static __thread refk_dim3 threadIdx, blockIdx, blockDim;
 
 /* CUDA runtime names referenced by host code in src/lattice.c (never run). */
 typedef int cudaError_t;
@@ -92,8 +94,9 @@ int cumul_stride[20];
 #include "k_stream_collide_stream.c"
 #include "k_collide.c"
 
-/* The dynamic shared-memory scratch of one one-thread block. */
-real fptr[32];
+/* The dynamic shared-memory scratch of one one-thread block (per host
+   thread). */
+__thread real fptr[32];
 
 #define EXPORT __attribute__((visibility("default")))
 
@@ -164,18 +167,69 @@ static void upload_constants(const refk_params* p)
 typedef void (*refk_kernel)(real*, real*, unsigned char*, real*);
 typedef void (*refk_bc_kernel)(real*, unsigned char*, real*);
 
-static void launch_grid(refk_kernel k, int gx, int gy, int gz,
-                        real* f, real* mv, unsigned char* sol)
+typedef struct {
+  refk_kernel k; int gx, gy, z0, z1; real* f; real* mv; unsigned char* sol;
+} grid_job;
+
+static void* grid_worker(void* arg)
 {
+  grid_job* g = (grid_job*)arg;
   unsigned x, y, z;
   blockDim.x = blockDim.y = blockDim.z = 1;
   threadIdx.x = threadIdx.y = threadIdx.z = 0;
-  for (z = 0; z < (unsigned)gz; z++)
-    for (y = 0; y < (unsigned)gy; y++)
-      for (x = 0; x < (unsigned)gx; x++) {
+  for (z = (unsigned)g->z0; z < (unsigned)g->z1; z++)
+    for (y = 0; y < (unsigned)g->gy; y++)
+      for (x = 0; x < (unsigned)g->gx; x++) {
         blockIdx.x = x; blockIdx.y = y; blockIdx.z = z;
-        k(f, mv, sol, NULL);
+        g->k(g->f, g->mv, g->sol, NULL);
       }
+  return NULL;
+}
+
+static void* grid_worker_rows(void* arg)
+{
+  grid_job* g = (grid_job*)arg;
+  unsigned x, y;
+  blockDim.x = blockDim.y = blockDim.z = 1;
+  threadIdx.x = threadIdx.y = threadIdx.z = 0;
+  blockIdx.z = 0;
+  for (y = 0; y < (unsigned)g->gy; y++)
+    for (x = 0; x < (unsigned)g->gx; x++) {
+      blockIdx.x = x; blockIdx.y = (unsigned)g->z0 + y;
+      g->k(g->f, g->mv, g->sol, NULL);
+    }
+  return NULL;
+}
+
+static int g_threads = 1;
+EXPORT void refk_set_threads(int n) { g_threads = n < 1 ? 1 : (n > 256 ? 256 : n); }
+
+/* Walk the grid, split into slabs of z-planes (or y-rows in 2D) over
+   g_threads host threads; the per-node slot sets are disjoint. */
+static void launch_grid(refk_kernel k, int gx, int gy, int gz,
+                        real* f, real* mv, unsigned char* sol)
+{
+  grid_job jobs[256];
+  pthread_t th[256];
+  int nt = g_threads, t;
+  int split_y = (gz == 1);
+  int extent = split_y ? gy : gz;
+  if (nt > extent) nt = extent;
+  for (t = 0; t < nt; t++) {
+    int a = (int)((long)extent * t / nt), b = (int)((long)extent * (t + 1) / nt);
+    jobs[t].k = k; jobs[t].f = f; jobs[t].mv = mv; jobs[t].sol = sol;
+    jobs[t].gx = gx;
+    if (split_y) { jobs[t].gy = b - a; jobs[t].z0 = 0; jobs[t].z1 = 1; }
+    else { jobs[t].gy = gy; jobs[t].z0 = a; jobs[t].z1 = b; }
+  }
+  if (split_y) {
+    /* rows: run a y-offset grid by shifting blockIdx.y inside the worker */
+    for (t = 0; t < nt; t++) jobs[t].z0 = (int)((long)extent * t / nt);
+  }
+  if (nt == 1 && !split_y) { grid_worker(&jobs[0]); return; }
+  for (t = 0; t < nt; t++)
+    pthread_create(&th[t], NULL, split_y ? grid_worker_rows : grid_worker, &jobs[t]);
+  for (t = 0; t < nt; t++) pthread_join(th[t], NULL);
 }
 
 static void launch_row(refk_bc_kernel k, int gx, real* f, unsigned char* sol)

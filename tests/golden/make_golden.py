@@ -1,0 +1,94 @@
+"""Generate the golden fixtures in tests/golden/ from the reference itself.
+
+Runs the reference's own kernel sources (compiled for the CPU by
+oracle/ref_build.py through oracle/refk_harness.c) on small seeded cases and
+stores inputs and outputs as .npz.  Needs oracle/_ref (built where the
+reference tree is available); the fixtures are committed so the tests need
+neither the reference nor the harness.
+
+    python tests/golden/make_golden.py
+"""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+import pyoracle as po  # noqa: E402
+
+W9 = np.array([4 / 9] + [1 / 9] * 4 + [1 / 36] * 4)
+W19 = np.array([1 / 3] + [1 / 18] * 4 + [1 / 36] * 4 + [1 / 18] * 2 + [1 / 36] * 8)
+
+
+def cases():
+    out = []
+    g3 = (2e-4, -3e-5, 5e-5, 0, 0, 0)
+    for name, kw, dt in [
+        ("d3q19_f64", dict(), np.float64),
+        ("d3q19_f32", dict(), np.float32),
+        ("d3q19p_f64", dict(accurate=0, compressible=1), np.float64),
+        ("d3q19c_f64", dict(compressible=1), np.float64),
+        ("d3q19s_f64", dict(nsubs=2, sink=2e-3, sigma_t_on=3, sigma_t_off=40), np.float64),
+        ("d3q19s_f32", dict(nsubs=2, sink=2e-3, sigma_t_on=3, sigma_t_off=40), np.float32),
+    ]:
+        p = po.Params(dims=3, LX=10, LY=9, LZ=8, tau=(0.8, 0.7), gaccel=g3, **kw)
+        out.append((name, p, dt, 16, 4))
+    g2 = (2e-4, 3e-5, 0, 0, 0, 0)
+    bc = dict(pressure_s_in=(1, 0), pressure_n_out=(1, 0), rho_in=1.004, rho_out=1.0,
+              bc_ramp_start=2, bc_ramp_stop=9)
+    for name, kw, dt in [
+        ("d2q9_f64", dict(), np.float64),
+        ("d2q9_f32", dict(), np.float32),
+        ("d2q9p_f64", dict(accurate=0, compressible=1), np.float64),
+        ("d2q9_bc_f64", bc, np.float64),
+        ("d2q9_bc_f32", bc, np.float32),
+        ("d2q9p_bc_f64", dict(bc, accurate=0, compressible=1), np.float64),
+        ("d2q9_table_f64", dict(pressure_n_in=(2, 0), pressure_s_out=(1, 0), pfadd=1.0,
+                                pfmul=0.01, rho_out=0.999,
+                                pressure_n_table=np.array([0.1, 0.3, 0.2, 0.5, 0.4])),
+         np.float64),
+        ("d2q9s_bc_f64", dict(bc, nsubs=2, sink=1e-3, zeroconcgrad_n=1, zeroconcgrad_s=1),
+         np.float64),
+    ]:
+        p = po.Params(dims=2, LX=12, LY=10, LZ=1, tau=(0.9, 0.75), gaccel=g2, **kw)
+        out.append((name, p, dt, 18, 6))
+    return out
+
+
+def make_inputs(name, p, dtype, rng, fluid_faces):
+    sol = rng.choice([0, 1, 255], size=p.NN, p=[0.72, 0.2, 0.08]).astype(np.uint8)
+    if fluid_faces and p.dims == 2:
+        m = sol.reshape(p.LY, p.LX)
+        m[0, :] = np.where(m[0, :] == 1, 0, m[0, :])
+        m[-1, :] = np.where(m[-1, :] == 1, 0, m[-1, :])
+    f = rng.standard_normal((p.nsubs, p.Q, p.NN)) * 1e-3
+    W = W9 if p.dims == 2 else W19
+    if not p.accurate:
+        f[0] += W[:, None]
+    if p.nsubs == 2:
+        f[1] = np.abs(f[1]) + 0.5 * W[:, None]
+    return sol, f.astype(dtype)
+
+
+def main():
+    rng = np.random.default_rng(20261203)
+    for name, p, dtype, steps, fr in cases():
+        variant = po.variant_name(p, dtype)
+        for tag, fluid_faces in (("", True),) if "bc" not in name and "table" not in name \
+                else (("", True), ("_wrapsolid", False)):
+            sol, f0 = make_inputs(name, p, dtype, rng, fluid_faces)
+            f = f0.copy()
+            f, mv = po.run_reference(variant, p, f, sol, 0, steps, frame_rate=fr)
+            pd = {k: (np.asarray(v) if v is not None else np.array([]))
+                  for k, v in p.__dict__.items()}
+            np.savez_compressed(os.path.join(HERE, name + tag + ".npz"),
+                                solids=sol, f0=f0, f=f, mv=mv, steps=steps,
+                                frame_rate=fr, variant=variant,
+                                **{"p_" + k: v for k, v in pd.items()})
+            print(name + tag, variant, f.dtype, steps, "steps")
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,248 @@
+"""Parity of the sm_100a kernels with the reference (GPU).
+
+Every case runs through the C ABI (liblbx.so via the lbx binding) and is
+compared with either the committed golden fixtures -- outputs of the
+reference's own kernel sources -- or the CPU oracle run live on the same
+inputs.  Tolerances (norm-wise relative error, ||gpu - ref|| / ||ref||):
+FP64 1e-12, FP32 1e-5.  Node classification is checked bit-exact.
+"""
+import numpy as np
+import pytest
+
+import lbx
+import pyoracle as po
+from lbx import geometry
+from _golden import golden_names, load, rel_err
+
+pytestmark = pytest.mark.gpu
+
+TOL = {np.dtype(np.float64): 1e-12, np.dtype(np.float32): 1e-5}
+
+
+def to_lbx(p: po.Params, dtype) -> lbx.Params:
+    kw = {k: getattr(p, k) for k in (
+        "dims", "LX", "LY", "LZ", "nsubs", "accurate", "compressible", "tau", "rho_A",
+        "gaccel", "sink", "sigma_t_on", "sigma_t_off", "pressure_n_in", "pressure_s_in",
+        "pressure_n_out", "pressure_s_out", "zeroconcgrad_n", "zeroconcgrad_s", "rho_in",
+        "rho_out", "pfadd", "pfmul", "bc_ramp_start", "bc_ramp_stop", "pressure_n_table",
+        "pressure_s_table")}
+    return lbx.Params(precision=np.dtype(dtype).itemsize, **kw)
+
+
+def run_gpu(p: po.Params, f0, sol, steps, frame_rate, dtype):
+    with lbx.Domain(to_lbx(p, dtype), sol) as d:
+        d.upload_f(f0)
+        d.run(0, steps, frame_rate)
+        d.sync()
+        return d.download_f(), d.download_mv(), d.info()
+
+
+def fusable(p: po.Params, sol) -> bool:
+    m = sol.reshape(p.LY, p.LX) == 1
+    north = any(p.pressure_n_in[:p.nsubs]) or any(p.pressure_n_out[:p.nsubs]) or \
+        (p.nsubs == 2 and p.zeroconcgrad_n)
+    south = any(p.pressure_s_in[:p.nsubs]) or any(p.pressure_s_out[:p.nsubs]) or \
+        (p.nsubs == 2 and p.zeroconcgrad_s)
+    for i in range(p.LX):
+        up = [(i - 1) % p.LX, i, (i + 1) % p.LX]
+        if north and not m[-1, i] and m[0, up].any():
+            return False
+        if south and not m[0, i] and m[-1, up].any():
+            return False
+    return True
+
+
+def assert_close(f, mv, f_ref, mv_ref, sol, dtype):
+    tol = TOL[np.dtype(dtype)]
+    fluid = sol.reshape(-1) != 1
+    assert rel_err(f, f_ref) <= tol, "populations: %g" % rel_err(f, f_ref)
+    for s in range(mv.shape[0]):
+        for c in range(mv.shape[1]):
+            e = rel_err(mv[s, c], mv_ref[s, c], fluid)
+            assert e <= tol, "mv[%d][%d]: %g" % (s, c, e)
+    # solid nodes are never written
+    assert np.array_equal(mv[..., ~fluid], mv_ref[..., ~fluid])
+
+
+@pytest.mark.parametrize("name", golden_names())
+def test_gpu_matches_reference_golden(name):
+    p, z = load(name)
+    dtype = z["f0"].dtype
+    f, mv, info = run_gpu(p, z["f0"], z["solids"], int(z["steps"]), int(z["frame_rate"]), dtype)
+    assert_close(f, mv, z["f"], z["mv"], z["solids"], dtype)
+    if p.dims == 2 and ("bc" in name or "table" in name):
+        assert info["faces_fused"] == fusable(p, z["solids"])
+    assert info["fluid_nodes"] == int(np.count_nonzero(z["solids"] != 1))
+
+
+def _oracle(p, f0, sol, steps, fr):
+    f = f0.copy()
+    return po.run_oracle(p, f, sol, 0, steps, fr)
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+@pytest.mark.parametrize("model", [(1, 0), (0, 1), (1, 1)])
+def test_gpu_matches_oracle_d3q19_sphere_pack(dtype, model):
+    acc, comp = model
+    p = po.Params(dims=3, LX=40, LY=36, LZ=32, accurate=acc, compressible=comp,
+                  tau=(0.8, 1.0), gaccel=(1e-5, 2e-6, -1e-6, 0, 0, 0))
+    sol = geometry.sphere_pack(40, 36, 32, radius=4, porosity=0.45, seed=11)
+    rng = np.random.default_rng(2)
+    f0 = rng.standard_normal((1, 19, p.NN)) * 1e-4
+    if not acc:
+        f0[0] += np.array([1 / 3] + [1 / 18] * 4 + [1 / 36] * 4 + [1 / 18] * 2 + [1 / 36] * 8)[:, None]
+    f0 = f0.astype(dtype)
+    f, mv, _ = run_gpu(p, f0, sol, 30, 15, dtype)
+    fo, mvo = _oracle(p, f0, sol, 30, 15)
+    assert_close(f, mv, fo, mvo, sol, dtype)
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_gpu_matches_oracle_d3q19_solute(dtype):
+    p = po.Params(dims=3, LX=33, LY=20, LZ=24, nsubs=2, tau=(0.9, 0.7), sink=1e-3,
+                  gaccel=(2e-5, 0, 0, 0, 0, 0), sigma_t_on=5, sigma_t_off=1000)
+    sol = geometry.sphere_pack(33, 20, 24, radius=3, porosity=0.5, seed=4)
+    rng = np.random.default_rng(3)
+    f0 = rng.standard_normal((2, 19, p.NN)) * 1e-4
+    f0[1] = np.abs(f0[1]) * 10
+    f0 = f0.astype(dtype)
+    f, mv, _ = run_gpu(p, f0, sol, 24, 12, dtype)
+    fo, mvo = _oracle(p, f0, sol, 24, 12)
+    assert_close(f, mv, fo, mvo, sol, dtype)
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+@pytest.mark.parametrize("fused", [True, False])
+def test_gpu_matches_oracle_d2q9_pressure_faces(dtype, fused):
+    """The configuration of the 2D benchmark (flow between pressure faces) on
+    a smaller lattice; `fused=False` plants solids across the periodic wrap
+    so the stand-alone face kernels run."""
+    LX, LY = 48, 64
+    p = po.Params(dims=2, LX=LX, LY=LY, LZ=1, tau=(1.0, 1.0), pressure_s_in=(1, 0),
+                  pressure_n_out=(1, 0), rho_in=1.001, rho_out=1.0)
+    sol = geometry.transpose_2d(geometry.disc_pack(LY, LX, radius=4, porosity=0.6, seed=9),
+                                LY, LX)
+    if not fused:
+        g = sol.reshape(LY, LX)
+        g[0, 5] = 1
+        g[-1, 20] = 1
+    f0 = np.zeros((1, 9, p.NN), dtype=dtype)
+    f, mv, info = run_gpu(p, f0, sol, 60, 20, dtype)
+    assert info["faces_fused"] == fused
+    fo, mvo = _oracle(p, f0, sol, 60, 20)
+    assert_close(f, mv, fo, mvo, sol, dtype)
+
+
+def test_gpu_d2q9_solute_faces_fp64():
+    p = po.Params(dims=2, LX=40, LY=30, LZ=1, nsubs=2, tau=(0.9, 0.8), sink=1e-3,
+                  pressure_s_in=(1, 0), pressure_n_out=(1, 0), rho_in=1.002, rho_out=1.0,
+                  zeroconcgrad_n=1, zeroconcgrad_s=1, bc_ramp_start=3, bc_ramp_stop=20)
+    rng = np.random.default_rng(8)
+    sol = (rng.random(p.NN) < 0.15).astype(np.uint8)
+    f0 = rng.standard_normal((2, 9, p.NN)) * 1e-4
+    f0[1] = np.abs(f0[1]) + 0.1
+    f, mv, _ = run_gpu(p, f0, sol, 40, 10, np.float64)
+    fo, mvo = _oracle(p, f0, sol, 40, 10)
+    assert_close(f, mv, fo, mvo, sol, np.float64)
+
+
+def test_gpu_full_size_step_pair_matches_oracle():
+    """256^3 D3Q19 FP32 sphere pack (the benchmark lattice): one AA pair."""
+    n = 256
+    p = po.Params(dims=3, LX=n, LY=n, LZ=n, tau=(0.8, 1.0), gaccel=(1e-6, 0, 0, 0, 0, 0))
+    sol = geometry.sphere_pack(n, n, n, radius=6, porosity=0.4, seed=1234)
+    rng = np.random.default_rng(0)
+    f0 = (rng.standard_normal((1, 19, p.NN), dtype=np.float32) * np.float32(1e-4))
+    f, mv, info = run_gpu(p, f0, sol, 2, 2, np.float32)
+    assert info["fluid_nodes"] == int(np.count_nonzero(sol != 1))
+    fo, mvo = _oracle(p, f0, sol, 2, 2)
+    assert_close(f, mv, fo, mvo, sol, np.float32)
+
+
+def test_gpu_mass_conserved_full_size():
+    """Bounce-back and periodic streaming conserve mass: 200 steps at 256^3."""
+    n = 256
+    lp = lbx.Params(dims=3, LX=n, LY=n, LZ=n, precision=4, tau=(0.8, 1.0),
+                    gaccel=(1e-6, 0, 0, 0, 0, 0))
+    sol = geometry.sphere_pack(n, n, n, radius=6, porosity=0.4, seed=1234)
+    with lbx.Domain(lp, sol) as d:
+        d.init_equilibrium(0, 1.0, 0.0, 0.0, 0.0)
+        d.run(0, 199, 0)
+        d.step(200, write_mv=True)
+        r = d.reduce()
+        assert r["status"] == lbx.LBX_OK and r["nonfinite"] == 0
+        nf = int(np.count_nonzero(sol != 1))
+        assert r["fluid_nodes"] == nf
+        assert abs(r["mass"] - nf) / nf < 1e-6
+        # flow develops along +x
+        assert r["u_sum"][0] > 0 and abs(r["u_sum"][1]) < 1e-3 * r["u_sum"][0]
+
+
+def test_gpu_reduce_matches_numpy():
+    p = lbx.Params(dims=3, LX=30, LY=20, LZ=10, precision=8, nsubs=2)
+    rng = np.random.default_rng(1)
+    sol = (rng.random(p.NN) < 0.3).astype(np.uint8)
+    mv = rng.random((2, 4, p.NN)) + 0.5
+    with lbx.Domain(p, sol) as d:
+        d.upload_mv(mv)
+        r = d.reduce()
+    fl = sol != 1
+    assert r["fluid_nodes"] == fl.sum()
+    assert np.isclose(r["mass"], mv[0, 0, fl].sum(), rtol=1e-13)
+    assert np.isclose(r["solute_mass"], mv[1, 0, fl].sum(), rtol=1e-13)
+    for c in range(3):
+        assert np.isclose(r["momentum"][c], (mv[0, 0, fl] * mv[0, 1 + c, fl]).sum(), rtol=1e-12)
+    assert r["rho_min"] == mv[0, 0, fl].min() and r["rho_max"] == mv[0, 0, fl].max()
+
+
+def test_gpu_reduce_flags_nonfinite():
+    p = lbx.Params(dims=2, LX=8, LY=8, LZ=1, precision=4)
+    mv = np.ones((1, 3, 64), np.float32)
+    mv[0, 1, 10] = np.nan
+    with lbx.Domain(p, np.zeros(64, np.uint8)) as d:
+        d.upload_mv(mv)
+        r = d.reduce()
+    assert r["status"] == lbx.LBX_ERR_NUMERIC and r["nonfinite"] == 1
+
+
+def test_gpu_init_equilibrium_matches_oracle():
+    p = po.Params(dims=3, LX=16, LY=12, LZ=10, nsubs=2)
+    rng = np.random.default_rng(6)
+    rho = 1 + 0.01 * rng.random((2, p.NN))
+    u = 0.01 * rng.standard_normal((3, 2, p.NN))
+    fo = po.init_feq(p, rho, u[0], u[1], u[2])
+    with lbx.Domain(to_lbx(p, np.float64), np.zeros(p.NN, np.uint8)) as d:
+        for s in range(2):
+            d.init_equilibrium(s, rho[s], u[0, s], u[1, s], u[2, s])
+        f = d.download_f()
+    assert rel_err(f, fo) < 1e-14
+
+
+def test_gpu_rejects_out_of_order_steps():
+    p = lbx.Params(dims=3, LX=8, LY=8, LZ=8, precision=4)
+    with lbx.Domain(p, np.zeros(512, np.uint8)) as d:
+        with pytest.raises(lbx.LbxError) as ei:
+            d.step(2)
+        assert ei.value.code == lbx.LBX_ERR_STATE
+        d.step(1)
+        with pytest.raises(lbx.LbxError):
+            d.step(3)
+        d.step(2)
+
+
+def test_gpu_caller_stream():
+    torch = pytest.importorskip("torch")
+    p = po.Params(dims=3, LX=20, LY=18, LZ=16, tau=(0.9, 1), gaccel=(1e-5, 0, 0, 0, 0, 0))
+    sol = geometry.sphere_pack(20, 18, 16, radius=3, porosity=0.5, seed=2)
+    f0 = (np.random.default_rng(1).standard_normal((1, 19, p.NN)) * 1e-4)
+    s = torch.cuda.Stream()
+    with lbx.Domain(to_lbx(p, np.float64), sol) as d:
+        d.upload_f(f0)
+        d.set_stream(s.cuda_stream)
+        d.run(0, 10, 10)
+        s.synchronize()
+        d.set_stream(None)
+        f = d.download_f()
+        assert d.launch_count() >= 10
+    fo, _ = _oracle(p, f0, sol, 10, 10)
+    assert rel_err(f, fo) < 1e-12
