@@ -48,12 +48,13 @@ METRIC = "D3Q19 MLUPS (FP32 shifted populations, 256^3 sphere pack)"
 
 def workload_config(world: int) -> dict:
     return {
-        "workload": "D3Q19 BGK 256^3, FP32 shifted populations, tau=0.8, gx=1e-6, "
-                    "periodic, overlapping spheres r=6 to porosity 0.4 (seed 1234)",
+        "workload": "D3Q19 BGK %d^3, FP32 shifted populations, tau=0.8, gx=1e-6, "
+                    "periodic, overlapping spheres r=6 to porosity 0.4 (seed 1234)" % N_EDGE,
         "lattice": [N_EDGE] * 3, "velocity_set": "D3Q19", "tau": TAU, "gx": GX,
         "sphere_radius": RADIUS, "porosity_target": POROSITY, "seed": SEED,
         "parallelism": "replicas x%d (one independent lattice per GPU)" % world,
-        "l2": "inputs larger than L2 (1.27 GB populations per lattice)",
+        "l2": "inputs larger than L2 (%.2f GB populations per lattice)"
+              % (Q * REAL * N_EDGE ** 3 / 1e9),
     }
 
 
@@ -151,8 +152,8 @@ def cpu_baseline(mask, steps: int = 4) -> dict:
         dt = time.perf_counter() - t0
     return {"value": round(p.NN * steps / dt / 1e6, 3), "unit": "MLUPS", "cores": cores,
             "kind": kind,
-            "sample": "%d lattice steps of the full 256^3 workload, FP32, %s threads"
-                      % (steps, cores)}
+            "sample": "%d lattice steps of the full %d^3 workload, FP32, %s threads"
+                      % (steps, N_EDGE, cores)}
 
 
 def reference_arm(args, rank: int, world: int):
@@ -187,8 +188,9 @@ def reference_arm(args, rank: int, world: int):
         "config": workload_config(1), "impl": "reference",
         "cpu_baseline": {"value": round(value, 3), "unit": "MLUPS", "cores": cores,
                          "kind": "reference",
-                         "sample": "the full 256^3 lattice each step; the reference's "
-                                   "kernel sources compiled for the host, %d threads" % cores},
+                         "sample": "the full %d^3 lattice each step; the reference's "
+                                   "kernel sources compiled for the host, %d threads"
+                                   % (N_EDGE, cores)},
         "e2e": {"value": round(value, 3), "unit": "MLUPS", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -203,7 +205,12 @@ def main(argv=None) -> int:
     ap.add_argument("--warmup", type=int, default=4)
     ap.add_argument("--impl", default="lbx", choices=["lbx", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--edge", type=int, default=256,
+                    help="lattice edge; 256 is the benchmark workload, smaller "
+                         "edges are for profiling captures only")
     args = ap.parse_args(argv)
+    global N_EDGE
+    N_EDGE = args.edge
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -224,7 +231,10 @@ def main(argv=None) -> int:
     NN = mask.size
     params = lbx.Params(dims=3, LX=N_EDGE, LY=N_EDGE, LZ=N_EDGE, precision=REAL,
                         tau=(TAU, 1.0), gaccel=(GX, 0, 0, 0, 0, 0), device=local)
-    stream = torch.cuda.current_stream()
+    # a dedicated stream: its handle is non-zero, and the events below are
+    # recorded on the stream the step kernels run on
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     dom = lbx.Domain(params, mask)
     dom.set_stream(stream.cuda_stream)
     dom.init_equilibrium(0, 1.0, 0.0, 0.0, 0.0)

@@ -143,8 +143,9 @@ lbx_status lbx_step_pair(lbx_domain* d, int time, unsigned flags);
 lbx_status lbx_run(lbx_domain* d, int t0, int nsteps, int frame_rate);
 
 /* Run the domain's work on the caller's CUDA stream (a cudaStream_t passed
- * as void*; NULL restores the library's own stream).  Lets a caller order
- * lbx launches with its own work and time them with its own events. */
+ * as void*; NULL is the CUDA default stream).  The domain uses a stream of
+ * its own until the first call.  Lets a caller order lbx launches with its
+ * own work and time them with its own events. */
 lbx_status lbx_set_stream(lbx_domain* d, void* stream);
 
 /* Wait for all queued work of the domain; reports asynchronous errors. */

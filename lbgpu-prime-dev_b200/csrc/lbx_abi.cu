@@ -126,12 +126,16 @@ StepArgs<T> make_args(const lbx_domain* d, int t, unsigned flags)
   if (d->faces_fused) {
     for (int s = 0; s < p.nsubs; ++s) {
       // last active boundary on each face wins (see FaceKind)
-      if (s == 1 && p.zeroconcgrad_n) A.face_n[s] = FACE_ZEROGRAD;
+      if (s == 1 && p.nsubs == 2 && p.zeroconcgrad_n) A.face_n[s] = FACE_ZEROGRAD;
       else if (p.pressure_n_out[s]) { A.face_n[s] = FACE_PRESSURE; A.rho_n[s] = face_rho<T>(d, s, t, 0, false, d->n_table); }
       else if (p.pressure_n_in[s]) { A.face_n[s] = FACE_PRESSURE; A.rho_n[s] = face_rho<T>(d, s, t, p.pressure_n_in[s], true, d->n_table); }
-      if (s == 1 && p.zeroconcgrad_s) A.face_s[s] = FACE_ZEROGRAD;
+      if (s == 1 && p.nsubs == 2 && p.zeroconcgrad_s) A.face_s[s] = FACE_ZEROGRAD;
       else if (p.pressure_s_out[s]) { A.face_s[s] = FACE_PRESSURE; A.rho_s[s] = face_rho<T>(d, s, t, 0, false, d->s_table); }
       else if (p.pressure_s_in[s]) { A.face_s[s] = FACE_PRESSURE; A.rho_s[s] = face_rho<T>(d, s, t, p.pressure_s_in[s], true, d->s_table); }
+    }
+    for (int s = 0; s < p.nsubs; ++s) {
+      A.drho_n[s] = (T)((double)A.rho_n[s] - (double)A.sc[s].rhoA);
+      A.drho_s[s] = (T)((double)A.rho_s[s] - (double)A.sc[s].rhoA);
     }
   }
   return A;
@@ -168,9 +172,10 @@ void launch_faces_exact(lbx_domain* d, int t, bool second)
     const int shifted = p.accurate && !(s == 1 && p.nsubs == 2);
     const T rhoA = (T)p.rho_A[s];
     auto run = [&](int north, int kind, T rho) {
+      const T drho = (T)((double)rho - (double)rhoA);
       face_row<T><<<grid, block, 0, d->stream>>>(fs, d->solids, p.LX, p.LY, d->N,
                                                  north, kind, second ? 1 : 0, rho,
-                                                 rhoA, shifted);
+                                                 rhoA, drho, shifted);
       d->launches++;
     };
     if (p.pressure_n_in[s]) run(1, FACE_PRESSURE, face_rho<T>(d, s, t, p.pressure_n_in[s], true, d->n_table));
@@ -482,7 +487,7 @@ lbx_status lbx_set_stream(lbx_domain* d, void* stream)
 {
   if (!d) return fail(LBX_ERR_INVALID, "domain is NULL");
   CK(cudaStreamSynchronize(d->stream));
-  d->stream = stream ? (cudaStream_t)stream : d->own_stream;
+  d->stream = (cudaStream_t)stream;
   return LBX_OK;
 }
 

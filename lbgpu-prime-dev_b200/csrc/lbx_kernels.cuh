@@ -87,6 +87,7 @@ struct StepArgs {
   int solute_on;
   int face_n[2], face_s[2];   // FaceKind per substance (2D, fused path)
   T rho_n[2], rho_s[2];       // face densities this step
+  T drho_n[2], drho_s[2];     // face density minus rho_A, formed in double
 };
 
 // ---- per-node collision ---------------------------------------------------
@@ -158,14 +159,27 @@ __device__ __forceinline__ void collide(const StepArgs<T>& A, int s, bool solute
 // unknowns lands on the slot this node then pulls (the host checks that the
 // wrapped upstream nodes of every face node are fluid, else it runs the
 // stand-alone face kernels below).
+// In FP32 the shifted density balance cancels at magnitude 1
+// (sum - rho_bc + rho_A with rho_bc ~ 1), which costs ~1e-5 relative in the
+// unknowns; there the host passes rho_bc - rho_A formed in double instead
+// (`drho`), so X = sum - drho keeps float precision.  FP64 keeps the
+// reference's operation order.
 template <typename T>
-__device__ __forceinline__ void face_north(int kind, T rho_bc, T rhoA, bool shifted,
+__device__ __forceinline__ T face_balance(T sum, T rho_bc, T rhoA, T drho, bool shifted)
+{
+  if (sizeof(T) == 4 && shifted) return sum - drho;
+  T X = sum - rho_bc;
+  if (shifted) X += rhoA;
+  return X;
+}
+
+template <typename T>
+__device__ __forceinline__ void face_north(int kind, T rho_bc, T rhoA, T drho, bool shifted,
                                            T (&d)[9])
 {
   if (kind == FACE_PRESSURE) {
-    T X = d[DC] + d[DE] + d[DW] + d[DN] + d[DN] + d[DNE] + d[DNE] + d[DNW] + d[DNW];
-    X -= rho_bc;
-    if (shifted) X += rhoA;
+    const T X = face_balance<T>(d[DC] + d[DE] + d[DW] + d[DN] + d[DN] + d[DNE] + d[DNE]
+                                + d[DNW] + d[DNW], rho_bc, rhoA, drho, shifted);
     d[DS] = d[DN] - T(2. / 3.) * X;
     d[DSW] = d[DNE] + T(0.5) * (d[DE] - d[DW]) - T(1. / 6.) * X;
     d[DSE] = d[DNW] + T(0.5) * (d[DW] - d[DE]) - T(1. / 6.) * X;
@@ -178,13 +192,13 @@ __device__ __forceinline__ void face_north(int kind, T rho_bc, T rhoA, bool shif
 }
 
 template <typename T>
-__device__ __forceinline__ void face_south(int kind, T rho_bc, T rhoA, bool shifted,
+__device__ __forceinline__ void face_south(int kind, T rho_bc, T rhoA, T drho, bool shifted,
                                            T (&d)[9])
 {
   if (kind == FACE_PRESSURE) {
-    T X = -d[DC] - d[DE] - d[DW] - d[DS] - d[DS] - d[DSE] - d[DSE] - d[DSW] - d[DSW];
-    X += rho_bc;
-    if (shifted) X -= rhoA;
+    // south balance is the negated north one: -(sum) + rho_bc - rho_A
+    const T X = -face_balance<T>(d[DC] + d[DE] + d[DW] + d[DS] + d[DS] + d[DSE] + d[DSE]
+                                 + d[DSW] + d[DSW], rho_bc, rhoA, drho, shifted);
     d[DN] = d[DS] + T(2. / 3.) * X;
     d[DNE] = d[DSW] + T(0.5) * (d[DW] - d[DE]) + T(1. / 6.) * X;
     d[DNW] = d[DSE] + T(0.5) * (d[DE] - d[DW]) + T(1. / 6.) * X;
@@ -259,8 +273,10 @@ aa_step(StepArgs<T> A)
     if (Q == 9 && (cl & (CLS_NORTH | CLS_SOUTH))) {
       T (&d9)[9] = reinterpret_cast<T (&)[9]>(d);
       const bool shifted = (MODEL != PLAIN_COMP) && !solute;
-      if (cl & CLS_NORTH) face_north<T>(A.face_n[s], A.rho_n[s], A.sc[s].rhoA, shifted, d9);
-      if (cl & CLS_SOUTH) face_south<T>(A.face_s[s], A.rho_s[s], A.sc[s].rhoA, shifted, d9);
+      if (cl & CLS_NORTH)
+        face_north<T>(A.face_n[s], A.rho_n[s], A.sc[s].rhoA, A.drho_n[s], shifted, d9);
+      if (cl & CLS_SOUTH)
+        face_south<T>(A.face_s[s], A.rho_s[s], A.sc[s].rhoA, A.drho_s[s], shifted, d9);
     }
     collide<T, Q, MODEL>(A, s, solute, ODD ? 1 : 2, d, u, n);
     if (ODD) {
@@ -286,7 +302,7 @@ aa_step(StepArgs<T> A)
 template <typename T>
 __global__ void face_row(T* fs, const uint8_t* solids, int LX, int LY,
                          long long N, int north, int kind, int second, T rho_bc,
-                         T rhoA, int shifted)
+                         T rhoA, T drho, int shifted)
 {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= LX) return;
@@ -309,8 +325,8 @@ __global__ void face_row(T* fs, const uint8_t* solids, int LX, int LY,
                                : fs[(long long)a * N + up];
     }
   }
-  if (north) face_north<T>(kind, rho_bc, rhoA, shifted != 0, d);
-  else face_south<T>(kind, rho_bc, rhoA, shifted != 0, d);
+  if (north) face_north<T>(kind, rho_bc, rhoA, drho, shifted != 0, d);
+  else face_south<T>(kind, rho_bc, rhoA, drho, shifted != 0, d);
   const int u0 = north ? DS : DN, u1 = north ? DSE : DNW, u2 = north ? DSW : DNE;
   const int unk[3] = {u0, u1, u2};
 #pragma unroll

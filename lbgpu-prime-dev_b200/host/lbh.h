@@ -1,0 +1,101 @@
+/*
+ * lbh.h -- host-side C library that keeps the reference's input/output
+ * interface around the lbx C ABI: the positional params.in reader, the
+ * .bmp/.raw solid-mask decoders, the initial density field, and the frame
+ * writers.  The driver in lbgpu_main.c strings them together exactly as the
+ * reference's main() does (src/lbgpu_prime.cu:82-940), with every device
+ * call going through include/lbx.h.
+ */
+#ifndef LBH_H
+#define LBH_H
+
+#include <stdint.h>
+#include <stdio.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* One real-valued parameter as read: the double value and the float value
+ * parsed from the same text, so a float run rounds the text once, as the
+ * reference's "%f" scanf of a float `real` does (src/params.h:55). */
+typedef struct { double d; float f; } lbh_real;
+
+/* Everything src/params.h:40-660 reads, in file order.  Fields the
+ * reference discards for a build are still read (the file is positional). */
+typedef struct lbh_params {
+  int LX, LY, LZ, BX, BY, BZ, length_scale, NumFrames, FrameRate;
+  lbh_real tau[2], gforce[2][3];
+  int end_grav[2];
+  int buoyancy, incompressible, simple_diffusion;
+  lbh_real rho_A[2], rho_B[2];
+  lbh_real rho_sigma, rho_sigma_in, rho_sigma_out, u_sigma, u_sigma_in, u_sigma_out;
+  int sigma_t_on, sigma_t_off, sigma_start, sigma_stop, sigma_btc_rate, sigma_btc_spot;
+  int GZL, PressureBC, AllBoundaryPeriodic;
+  lbh_real sink, pfmul, pfadd, rho_in, rho_out, ux_in, ux_out, uy_in, uy_out, uz_in, uz_out;
+  lbh_real big_V0, big_V0_solid[2];
+  int ns_flag;
+  lbh_real ns;
+  int ic_poisseuille, bc_poisseuille, bc_slip_north, bc_sigma_slip;
+  int bc_ramp_start, bc_ramp_stop;
+  /* per substance: t b (in/out) n s e w, pressure and velocity */
+  int pressure_t_in[2], pressure_b_in[2], pressure_t_out[2], pressure_b_out[2];
+  int velocity_t_in[2], velocity_b_in[2], velocity_t_out[2], velocity_b_out[2];
+  int pressure_n_in[2], pressure_s_in[2], pressure_n_out[2], pressure_s_out[2];
+  int velocity_n_in[2], velocity_s_in[2], velocity_n_out[2], velocity_s_out[2];
+  int pressure_e_in[2], pressure_w_in[2], pressure_e_out[2], pressure_w_out[2];
+  int velocity_e_in[2], velocity_w_in[2], velocity_e_out[2], velocity_w_out[2];
+  int constcon[24];          /* constcon/constflx t b n s e w in/out      */
+  int zeroconcgrad_t, zeroconcgrad_b, zeroconcgrad_n, zeroconcgrad_s;
+  int zeroconcgrad_e, zeroconcgrad_w, zeroconcgrad_full;
+  int plot_scale_dynamic, use_colormap, initial_condition;
+  int x0, y0, z0, r0;        /* INTEGER_IC_BOUND build (the default)      */
+  lbh_real cut;
+  int x1, x2, y1, y2, z1, z2;
+  lbh_real rel_x1, rel_x2, rel_y1, rel_y2, rel_z1, rel_z2;
+  int dump_rho, dump_u, dump_force, dump_vor;
+  /* derived, as read_params sets them (src/params.h:395-470) */
+  long long NumNodes;
+  int NumTimeSteps;
+} lbh_params;
+
+/* Read a positional params.in for a run with `dims` dimensions and `nsubs`
+ * substances (NUM_DIMENSIONS / NUM_FLUID_COMPONENTS of the reference build).
+ * Returns 0, or -1 with a message in `err` (missing file, short file). */
+int lbh_read_params(const char* path, int dims, int nsubs, lbh_params* out,
+                    char* err, int errlen);
+
+/* 24-bit BMP mask, black pixel -> 1, anything else -> 0, rows in file order
+ * (bottom-up), as spy_bmp does (src/lbio.c:3073-3363).  out: LX*LY bytes.
+ * Returns 0, or -1 (unreadable, not "BM", compressed, size mismatch, or a
+ * bit depth other than 24) with a message in `err`. */
+int lbh_read_bmp_mask(const char* path, int LX, int LY, uint8_t* out,
+                      char* err, int errlen);
+
+/* Raw mask: exactly N bytes copied verbatim (src/lbio.c:507-559). */
+int lbh_read_raw_mask(const char* path, long long N, uint8_t* out,
+                      char* err, int errlen);
+
+/* Write a 24-bit BMP / raw mask in the same conventions (for generators). */
+int lbh_write_bmp_mask(const char* path, int LX, int LY, const uint8_t* mask);
+int lbh_write_raw_mask(const char* path, long long N, const uint8_t* mask);
+
+/* Initial density of substance `subs` per initial_condition 0 (uniform),
+ * 2 (cube) or 3 (sphere) of init_problem (src/latman.c:1319-1632).
+ * rho: N doubles.  Returns 0, or -1 for an unsupported condition. */
+int lbh_initial_rho(const lbh_params* p, int dims, int nsubs, int subs,
+                    double* rho);
+
+/* Frame output: the reference's .dat writer (binary reals, zero where the
+ * mask byte is non-zero -- the host rule of src/lbio.c:2530-2540) under its
+ * file names (src/lattice.c:371-452). */
+int lbh_write_dat(const char* path, const void* a, int real_size, long long N,
+                  const uint8_t* mask);
+void lbh_frame_filename(char* buf, int buflen, const char* outdir,
+                        const char* prefix, int dims, int LX, int LY, int LZ,
+                        int frame, int nsubs, int subs, const char* suffix);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -268,7 +268,8 @@ class Domain:
         _check(_lib.lbx_run(self._h, t0, nsteps, frame_rate))
 
     def set_stream(self, stream_handle: Optional[int]):
-        """Queue work on a caller's cudaStream_t (an integer handle), or None."""
+        """Queue work on a caller's cudaStream_t (an integer handle); 0 or
+        None is the CUDA default stream."""
         _check(_lib.lbx_set_stream(self._h, stream_handle))
 
     def sync(self):

@@ -90,6 +90,9 @@ int cumul_stride[20];
 #include "lattice.h"
 #include "forward_declarations.h"
 #include "lattice.c"
+#include "params.h"
+#include "process.c"
+#include "lbio.c"
 #include "system_boundary_kernels.c"
 #include "k_stream_collide_stream.c"
 #include "k_collide.c"
@@ -330,5 +333,66 @@ EXPORT int refk_run(const refk_params* p, real* f, const unsigned char* solids,
       launch_grid(k_collide, p->LX, p->LY, p->LZ, f, mv, sol);
     is_end_of_frame_mem_c = 0;
   }
+  return 0;
+}
+
+/* ---- host-side input readers of the reference ------------------------------
+ * read_params (src/params.h:40-660), spy_bmp (src/lbio.c:3073-3363) and
+ * read_solids (src/lbio.c:507-629), run on a lattice struct the harness
+ * fills itself (a serial build never sets the global extents these readers
+ * use, so the harness sets them as a one-rank parallel run would). */
+static struct lattice_struct* harness_lattice(int LX, int LY, int LZ)
+{
+  struct lattice_struct* l = (struct lattice_struct*)calloc(1, sizeof *l);
+  l->param.LX = LX; l->param.LY = LY; l->param.LZ = LZ;
+  l->NumNodes = LX * LY * LZ;
+  l->process.id = 0; l->process.num_procs = 1;
+  l->process.g_LX = LX; l->process.g_LY = LY; l->process.g_LZ = LZ;
+  l->process.g_NumNodes = LX * LY * LZ;
+  l->process.g_SX = l->process.g_SY = l->process.g_SZ = 0;
+  l->process.g_StartNode = 0;
+  l->solids_memblock = (unsigned char*)calloc((size_t)(LX * LY * LZ), 1);
+  return l;
+}
+
+/* out[0..9] = LX LY LZ NumFrames FrameRate initial_condition
+ *             bc_ramp_start bc_ramp_stop pressure_n_in[0] pressure_s_in[0]
+ * dout[0..7] = tau[0] rho_A[0] rho_B[0] rho_in rho_out sink gforce[0][0] pfmul */
+EXPORT int refk_read_params(const char* path, int* iout, double* dout)
+{
+  struct lattice_struct* l = harness_lattice(1, 1, 1);
+  read_params(l, path);
+  iout[0] = l->param.LX; iout[1] = l->param.LY; iout[2] = l->param.LZ;
+  iout[3] = l->param.NumFrames; iout[4] = l->param.FrameRate;
+  iout[5] = l->param.initial_condition; iout[6] = l->param.bc_ramp_start;
+  iout[7] = l->param.bc_ramp_stop; iout[8] = l->param.pressure_n_in[0];
+  iout[9] = l->param.pressure_s_in[0];
+  dout[0] = l->param.tau[0]; dout[1] = l->param.rho_A[0]; dout[2] = l->param.rho_B[0];
+  dout[3] = l->param.rho_in; dout[4] = l->param.rho_out; dout[5] = l->param.sink;
+  dout[6] = l->param.gforce[0][0]; dout[7] = l->param.pfmul;
+  free(l->solids_memblock); free(l);
+  return 0;
+}
+
+EXPORT int refk_read_bmp(const char* path, int LX, int LY, unsigned char* out)
+{
+  struct lattice_struct* l = harness_lattice(LX, LY, 1);
+  int j, i;
+  int** matrix = (int**)malloc((size_t)LY * sizeof(int*));
+  for (j = 0; j < LY; j++) matrix[j] = (int*)calloc((size_t)LX, sizeof(int));
+  spy_bmp(l, (char*)path, matrix);
+  for (j = 0; j < LY; j++)
+    for (i = 0; i < LX; i++) out[j * LX + i] = (unsigned char)matrix[j][i];
+  for (j = 0; j < LY; j++) free(matrix[j]);
+  free(matrix); free(l->solids_memblock); free(l);
+  return 0;
+}
+
+EXPORT int refk_read_raw(const char* path, int LX, int LY, int LZ, unsigned char* out)
+{
+  struct lattice_struct* l = harness_lattice(LX, LY, LZ);
+  read_solids(l, (char*)path);
+  memcpy(out, l->solids_memblock, (size_t)(LX * LY * LZ));
+  free(l->solids_memblock); free(l);
   return 0;
 }

@@ -19,6 +19,15 @@ pytestmark = pytest.mark.gpu
 TOL = {np.dtype(np.float64): 1e-12, np.dtype(np.float32): 1e-5}
 
 
+def _pairs(f, mv, sol):
+    """(name, array, mask) for populations and each macro variable plane."""
+    fluid = sol.reshape(-1) != 1
+    yield "f", f, None
+    for s in range(mv.shape[0]):
+        for c in range(mv.shape[1]):
+            yield "mv[%d][%d]" % (s, c), mv[s, c], fluid
+
+
 def to_lbx(p: po.Params, dtype) -> lbx.Params:
     kw = {k: getattr(p, k) for k in (
         "dims", "LX", "LY", "LZ", "nsubs", "accurate", "compressible", "tau", "rho_A",
@@ -52,24 +61,45 @@ def fusable(p: po.Params, sol) -> bool:
     return True
 
 
-def assert_close(f, mv, f_ref, mv_ref, sol, dtype):
+def assert_close(f, mv, f_ref, mv_ref, sol, dtype, truth=None):
+    """FP64: within 1e-12 of the reference.  FP32: within 1e-5 of the
+    reference's FP32 result, or -- where that result itself is more than
+    1e-5 from the FP64 result `truth` (the shifted pressure faces cancel at
+    magnitude 1 in FP32) -- at least as close to the FP64 result as the
+    reference's FP32 result is."""
     tol = TOL[np.dtype(dtype)]
     fluid = sol.reshape(-1) != 1
-    assert rel_err(f, f_ref) <= tol, "populations: %g" % rel_err(f, f_ref)
-    for s in range(mv.shape[0]):
-        for c in range(mv.shape[1]):
-            e = rel_err(mv[s, c], mv_ref[s, c], fluid)
-            assert e <= tol, "mv[%d][%d]: %g" % (s, c, e)
+    ours = dict((k, (a, m)) for k, a, m in _pairs(f, mv, sol))
+    tp = dict((k, a) for k, a, _ in _pairs(*truth, sol)) if truth is not None else None
+    for k, a_ref, m in _pairs(f_ref, mv_ref, sol):
+        a, _ = ours[k]
+        e = rel_err(a, a_ref, m)
+        if e <= tol:
+            continue
+        assert tp is not None, "%s: %g" % (k, e)
+        e_ref = rel_err(a_ref, tp[k], m)
+        e_ours = rel_err(a, tp[k], m)
+        assert e_ref > tol and e_ours <= e_ref, \
+            "%s: %g from the reference; vs FP64 ours %g, reference %g" % (k, e, e_ours, e_ref)
     # solid nodes are never written
     assert np.array_equal(mv[..., ~fluid], mv_ref[..., ~fluid])
+
+
+def fp64_truth(p, f0, sol, steps, fr):
+    """The same run in FP64 (the oracle), for judging FP32 results."""
+    f = f0.astype(np.float64)
+    f, mv = po.run_oracle(p, f, sol, 0, steps, fr)
+    return f, mv
 
 
 @pytest.mark.parametrize("name", golden_names())
 def test_gpu_matches_reference_golden(name):
     p, z = load(name)
     dtype = z["f0"].dtype
-    f, mv, info = run_gpu(p, z["f0"], z["solids"], int(z["steps"]), int(z["frame_rate"]), dtype)
-    assert_close(f, mv, z["f"], z["mv"], z["solids"], dtype)
+    steps, fr = int(z["steps"]), int(z["frame_rate"])
+    f, mv, info = run_gpu(p, z["f0"], z["solids"], steps, fr, dtype)
+    truth = fp64_truth(p, z["f0"], z["solids"], steps, fr) if dtype == np.float32 else None
+    assert_close(f, mv, z["f"], z["mv"], z["solids"], dtype, truth)
     if p.dims == 2 and ("bc" in name or "table" in name):
         assert info["faces_fused"] == fusable(p, z["solids"])
     assert info["fluid_nodes"] == int(np.count_nonzero(z["solids"] != 1))
@@ -94,7 +124,8 @@ def test_gpu_matches_oracle_d3q19_sphere_pack(dtype, model):
     f0 = f0.astype(dtype)
     f, mv, _ = run_gpu(p, f0, sol, 30, 15, dtype)
     fo, mvo = _oracle(p, f0, sol, 30, 15)
-    assert_close(f, mv, fo, mvo, sol, dtype)
+    assert_close(f, mv, fo, mvo, sol, dtype,
+                 fp64_truth(p, f0, sol, 30, 15) if dtype == np.float32 else None)
 
 
 @pytest.mark.parametrize("dtype", [np.float64, np.float32])
@@ -108,7 +139,8 @@ def test_gpu_matches_oracle_d3q19_solute(dtype):
     f0 = f0.astype(dtype)
     f, mv, _ = run_gpu(p, f0, sol, 24, 12, dtype)
     fo, mvo = _oracle(p, f0, sol, 24, 12)
-    assert_close(f, mv, fo, mvo, sol, dtype)
+    assert_close(f, mv, fo, mvo, sol, dtype,
+                 fp64_truth(p, f0, sol, 24, 12) if dtype == np.float32 else None)
 
 
 @pytest.mark.parametrize("dtype", [np.float64, np.float32])
@@ -130,7 +162,8 @@ def test_gpu_matches_oracle_d2q9_pressure_faces(dtype, fused):
     f, mv, info = run_gpu(p, f0, sol, 60, 20, dtype)
     assert info["faces_fused"] == fused
     fo, mvo = _oracle(p, f0, sol, 60, 20)
-    assert_close(f, mv, fo, mvo, sol, dtype)
+    assert_close(f, mv, fo, mvo, sol, dtype,
+                 fp64_truth(p, f0, sol, 60, 20) if dtype == np.float32 else None)
 
 
 def test_gpu_d2q9_solute_faces_fp64():
@@ -156,7 +189,7 @@ def test_gpu_full_size_step_pair_matches_oracle():
     f, mv, info = run_gpu(p, f0, sol, 2, 2, np.float32)
     assert info["fluid_nodes"] == int(np.count_nonzero(sol != 1))
     fo, mvo = _oracle(p, f0, sol, 2, 2)
-    assert_close(f, mv, fo, mvo, sol, np.float32)
+    assert_close(f, mv, fo, mvo, sol, np.float32, fp64_truth(p, f0, sol, 2, 2))
 
 
 def test_gpu_mass_conserved_full_size():
