@@ -238,6 +238,7 @@ def main(argv=None) -> int:
     dom = lbx.Domain(params, mask)
     dom.set_stream(stream.cuda_stream)
     dom.init_equilibrium(0, 1.0, 0.0, 0.0, 0.0)
+    layout = dom.info()["layout"]
 
     # warm-up (W >= 3 steps), then K timed steps between barriers
     t = 0
@@ -299,7 +300,8 @@ def main(argv=None) -> int:
         "unit": "GB/s", "frac": round(achieved / peaks["hbm_gbs"], 4),
         "traffic": load_traffic(),
         "peak_source": peaks["source"],
-        "kernel": "aa_step<float,19,1,SHIFTED_INC> (odd and even alternate)",
+        "kernel": "%s<float,19,1,SHIFTED_INC> (odd and even alternate)"
+                  % ("aa_step_compact" if layout == "compact" else "aa_step"),
         "alg_bytes_per_launch": alg_bytes,
         "by_kind_ms": {k: round(v, 4) for k, v in per_kind.items()},
         "by_kind_frac": {k: round(alg_bytes / (v / 1e3) / 1e9 / peaks["hbm_gbs"], 4)
@@ -337,7 +339,7 @@ def main(argv=None) -> int:
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_step, 4),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic", "config": workload_config(world),
-        "mflups": round(mflups, 3), "fluid_nodes": fluid, "nodes": NN,
+        "mflups": round(mflups, 3), "fluid_nodes": fluid, "nodes": NN, "layout": layout,
         "roofline": roofline, "clocks": clocks, "e2e": e2e,
         "gpu_launches": launches,
     }

@@ -75,7 +75,16 @@ typedef struct lbx_params {
   const double* pressure_n_table; int pressure_n_len;
   const double* pressure_s_table; int pressure_s_len;
   int device;               /* CUDA device ordinal                         */
+  int layout;               /* LBX_LAYOUT_*: device storage of populations */
 } lbx_params;
+
+/* Device storage of the populations.  DENSE keeps the reference's
+ * [subs][a][N] array; COMPACT stores fluid nodes only ([subs][a][F], dense
+ * node order) and moves only the bytes of fluid nodes each step.  Both
+ * compute the same results; uploads and downloads always use the dense
+ * exchange format.  AUTO picks COMPACT when solids are at least 5% of the
+ * nodes, DENSE otherwise. */
+enum { LBX_LAYOUT_AUTO = 0, LBX_LAYOUT_DENSE = 1, LBX_LAYOUT_COMPACT = 2 };
 
 typedef struct lbx_domain lbx_domain;
 
@@ -156,14 +165,18 @@ lbx_status lbx_sync(lbx_domain* d);
  * _u of src/compute.c:1159-1416 used by the frame summary.  Synchronous. */
 lbx_status lbx_reduce(lbx_domain* d, lbx_reductions* out);
 
-/* Device pointers to the populations ([nsubs][Q][N]) and macro variables
+/* Device pointers to the populations ([nsubs][Q][N], the dense exchange
+ * format; with the compact layout this first writes the current state into
+ * it, and the pointer is valid until the next step) and macro variables
  * ([nsubs][1+D][N]) for callers that keep data on the device. */
 lbx_status lbx_device_f(lbx_domain* d, void** ptr);
 lbx_status lbx_device_mv(lbx_domain* d, void** ptr);
 
-/* Counts from classification: fluid nodes, and whether the 2D face
- * boundaries run fused into the step kernels (1) or as separate kernels (0). */
-lbx_status lbx_info(lbx_domain* d, long long* fluid_nodes, int* faces_fused);
+/* Counts from classification: fluid nodes, whether the 2D face boundaries
+ * run fused into the step kernels (1) or as separate kernels (0), and the
+ * layout in use (LBX_LAYOUT_DENSE or LBX_LAYOUT_COMPACT). */
+lbx_status lbx_info(lbx_domain* d, long long* fluid_nodes, int* faces_fused,
+                    int* layout);
 
 /* Number of this library's kernels launched on the domain so far. */
 long long lbx_launch_count(lbx_domain* d);

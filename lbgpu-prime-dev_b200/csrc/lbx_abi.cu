@@ -13,6 +13,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
+#include <algorithm>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -54,7 +55,12 @@ struct lbx_domain {
   int Q = 0, D = 0;
   long long N = 0;
   size_t real_size = 0;
-  void* f = nullptr;          // [nsubs][Q][N]
+  void* f = nullptr;          // [nsubs][Q][N] dense (the exchange format)
+  void* fc = nullptr;         // [nsubs][Q][F] compact layout
+  int* fidx = nullptr;        // [N] dense -> compact (-1 solid)
+  int* fnode = nullptr;       // [F] compact -> dense
+  int layout = LBX_LAYOUT_DENSE;
+  bool dense_stale = false;   // compact state newer than the dense array
   void* mv = nullptr;         // [nsubs][1+D][N]
   uint8_t* solids = nullptr;  // [N] as given (device rule: == 1)
   uint8_t* cls = nullptr;     // [N]
@@ -106,7 +112,7 @@ StepArgs<T> make_args(const lbx_domain* d, int t, unsigned flags)
   const lbx_params& p = d->p;
   StepArgs<T> A;
   std::memset(&A, 0, sizeof A);
-  A.f = (T*)d->f;
+  A.f = (T*)(d->layout == LBX_LAYOUT_COMPACT ? d->fc : d->f);
   A.mv = (T*)d->mv;
   A.cls = d->cls;
   A.nbm = d->nbm;
@@ -144,6 +150,20 @@ StepArgs<T> make_args(const lbx_domain* d, int t, unsigned flags)
 template <typename T, int Q, int NS, int MODEL>
 void launch_aa(lbx_domain* d, const StepArgs<T>& A, bool odd)
 {
+  if (d->layout == LBX_LAYOUT_COMPACT) {
+    CompactArgs<T> C;
+    C.s = A;
+    C.fidx = d->fidx;
+    C.fnode = d->fnode;
+    C.F = (int)d->fluid;
+    C.faces = d->faces_fused ? 1 : 0;
+    const unsigned blocks = (unsigned)((d->fluid + 255) / 256);
+    if (blocks == 0) return;
+    if (odd) aa_step_compact<T, Q, NS, MODEL, true><<<blocks, 256, 0, d->stream>>>(C);
+    else aa_step_compact<T, Q, NS, MODEL, false><<<blocks, 256, 0, d->stream>>>(C);
+    d->launches++;
+    return;
+  }
   dim3 block(128, 1, 1);
   dim3 grid((A.LX + 127) / 128, A.LY, A.LZ);
   if (odd) aa_step<T, Q, NS, MODEL, true><<<grid, block, 0, d->stream>>>(A);
@@ -168,14 +188,22 @@ void launch_faces_exact(lbx_domain* d, int t, bool second)
   const lbx_params& p = d->p;
   dim3 block(128), grid((p.LX + 127) / 128);
   for (int s = 0; s < p.nsubs; ++s) {
-    T* fs = (T*)d->f + (long long)s * d->Q * d->N;
+    const bool compact = d->layout == LBX_LAYOUT_COMPACT;
+    T* fs = compact ? (T*)d->fc + (long long)s * d->Q * d->fluid
+                    : (T*)d->f + (long long)s * d->Q * d->N;
     const int shifted = p.accurate && !(s == 1 && p.nsubs == 2);
     const T rhoA = (T)p.rho_A[s];
     auto run = [&](int north, int kind, T rho) {
       const T drho = (T)((double)rho - (double)rhoA);
-      face_row<T><<<grid, block, 0, d->stream>>>(fs, d->solids, p.LX, p.LY, d->N,
-                                                 north, kind, second ? 1 : 0, rho,
-                                                 rhoA, drho, shifted);
+      if (compact)
+        face_row_compact<T><<<grid, block, 0, d->stream>>>(fs, d->fidx, p.LX, p.LY,
+                                                           (int)d->fluid, north, kind,
+                                                           second ? 1 : 0, rho, rhoA,
+                                                           drho, shifted);
+      else
+        face_row<T><<<grid, block, 0, d->stream>>>(fs, d->solids, p.LX, p.LY, d->N,
+                                                   north, kind, second ? 1 : 0, rho,
+                                                   rhoA, drho, shifted);
       d->launches++;
     };
     if (p.pressure_n_in[s]) run(1, FACE_PRESSURE, face_rho<T>(d, s, t, p.pressure_n_in[s], true, d->n_table));
@@ -218,6 +246,8 @@ lbx_status check_params(const lbx_params* p)
   if (p->nsubs != 1 && p->nsubs != 2) return fail(LBX_ERR_INVALID, "nsubs must be 1 or 2");
   if (p->precision != 4 && p->precision != 8)
     return fail(LBX_ERR_INVALID, "precision must be 4 or 8");
+  if (p->layout < LBX_LAYOUT_AUTO || p->layout > LBX_LAYOUT_COMPACT)
+    return fail(LBX_ERR_INVALID, "layout must be one of LBX_LAYOUT_*");
   if (!p->accurate && !p->compressible)
     return fail(LBX_ERR_INVALID,
                 "accurate=0 requires compressible=1 (the reference does not "
@@ -268,6 +298,7 @@ bool faces_fusable(const lbx_params& p, const uint8_t* sol)
 void release(lbx_domain* d)
 {
   if (d->graph) cudaGraphExecDestroy(d->graph);
+  cudaFree(d->fc); cudaFree(d->fidx); cudaFree(d->fnode);
   cudaFree(d->f); cudaFree(d->mv); cudaFree(d->solids); cudaFree(d->cls);
   cudaFree(d->nbm); cudaFree(d->red);
   if (d->own_stream) cudaStreamDestroy(d->own_stream);
@@ -288,8 +319,31 @@ lbx_status do_step(lbx_domain* d, int t, unsigned flags)
     return fail(LBX_ERR_STATE, "step at time %d out of AA order: expected an %s time", t,
                 want_odd ? "odd" : "even");
   lbx_status st = d->real_size == 8 ? step_t<double>(d, t, flags) : step_t<float>(d, t, flags);
-  if (st == LBX_OK) d->parity ^= 1;
+  if (st == LBX_OK) {
+    d->parity ^= 1;
+    if (d->layout == LBX_LAYOUT_COMPACT) d->dense_stale = true;
+  }
   return st;
+}
+
+// Dense exchange array <-> compact populations.
+lbx_status exchange(lbx_domain* d, bool to_compact)
+{
+  if (d->layout != LBX_LAYOUT_COMPACT || d->fluid == 0) return LBX_OK;
+  const int planes = d->p.nsubs * d->Q;
+  const long long total = d->fluid * planes;
+  const unsigned blocks = (unsigned)((total + 255) / 256);
+  if (d->real_size == 8) {
+    if (to_compact) gather_compact<double><<<blocks, 256, 0, d->stream>>>((double*)d->fc, (const double*)d->f, d->fnode, (int)d->fluid, d->N, planes);
+    else scatter_compact<double><<<blocks, 256, 0, d->stream>>>((double*)d->f, (const double*)d->fc, d->fnode, (int)d->fluid, d->N, planes);
+  } else {
+    if (to_compact) gather_compact<float><<<blocks, 256, 0, d->stream>>>((float*)d->fc, (const float*)d->f, d->fnode, (int)d->fluid, d->N, planes);
+    else scatter_compact<float><<<blocks, 256, 0, d->stream>>>((float*)d->f, (const float*)d->fc, d->fnode, (int)d->fluid, d->N, planes);
+  }
+  d->launches++;
+  CK(cudaGetLastError());
+  if (!to_compact) d->dense_stale = false;
+  return LBX_OK;
 }
 
 }  // namespace
@@ -330,6 +384,9 @@ lbx_status lbx_create(const lbx_params* p, const uint8_t* solids, lbx_domain** o
   d->faces_active |= p->nsubs == 2 && (p->zeroconcgrad_n || p->zeroconcgrad_s);
   d->faces_fused = d->faces_active && faces_fusable(*p, solids);
   for (long long n = 0; n < d->N; ++n) d->fluid += solids[n] != 1;
+  d->layout = p->layout == LBX_LAYOUT_AUTO
+                  ? ((d->N - d->fluid) * 20 >= d->N ? LBX_LAYOUT_COMPACT : LBX_LAYOUT_DENSE)
+                  : p->layout;
 
   auto bail = [&](lbx_status s) { release(d); delete d; return s; };
   cudaError_t e;
@@ -348,6 +405,20 @@ lbx_status lbx_create(const lbx_params* p, const uint8_t* solids, lbx_domain** o
   CKD(cudaMalloc(&d->nbm, d->N * sizeof(uint32_t)));
   d->red_blocks = 2 * 148;
   CKD(cudaMalloc(&d->red, d->red_blocks * sizeof(RedPartial)));
+  if (d->layout == LBX_LAYOUT_COMPACT) {
+    std::vector<int> fidx(d->N), fnode(d->fluid > 0 ? d->fluid : 1);
+    int m = 0;
+    for (long long n = 0; n < d->N; ++n) {
+      if (solids[n] == 1) fidx[n] = -1;
+      else { fidx[n] = m; fnode[m++] = (int)n; }
+    }
+    CKD(cudaMalloc(&d->fc, std::max<size_t>(1, (size_t)p->nsubs * d->Q * d->fluid * d->real_size)));
+    CKD(cudaMalloc(&d->fidx, d->N * sizeof(int)));
+    CKD(cudaMalloc(&d->fnode, fnode.size() * sizeof(int)));
+    CKD(cudaMemcpy(d->fidx, fidx.data(), d->N * sizeof(int), cudaMemcpyHostToDevice));
+    CKD(cudaMemcpy(d->fnode, fnode.data(), fnode.size() * sizeof(int), cudaMemcpyHostToDevice));
+    CKD(cudaMemsetAsync(d->fc, 0, (size_t)p->nsubs * d->Q * d->fluid * d->real_size, d->stream));
+  }
   CKD(cudaMemsetAsync(d->f, 0, fbytes, d->stream));
   CKD(cudaMemsetAsync(d->mv, 0, mvbytes, d->stream));
   CKD(cudaMemcpyAsync(d->solids, solids, d->N, cudaMemcpyHostToDevice, d->stream));
@@ -378,8 +449,10 @@ lbx_status lbx_upload_f(lbx_domain* d, int subs, const void* f_host)
   if (lbx_status st = check_subs(d, subs)) return st;
   if (!f_host) return fail(LBX_ERR_INVALID, "f_host is NULL");
   const size_t bytes = (size_t)d->Q * d->N * d->real_size;
+  if (d->dense_stale) { if (lbx_status st = exchange(d, false)) return st; }
   CK(cudaMemcpyAsync((char*)d->f + subs * bytes, f_host, bytes, cudaMemcpyHostToDevice,
                      d->stream));
+  if (lbx_status st = exchange(d, true)) return st;
   CK(cudaStreamSynchronize(d->stream));
   d->parity = 0;
   return LBX_OK;
@@ -390,6 +463,7 @@ lbx_status lbx_download_f(lbx_domain* d, int subs, void* f_host)
   if (lbx_status st = check_subs(d, subs)) return st;
   if (!f_host) return fail(LBX_ERR_INVALID, "f_host is NULL");
   const size_t bytes = (size_t)d->Q * d->N * d->real_size;
+  if (d->dense_stale) { if (lbx_status st = exchange(d, false)) return st; }
   CK(cudaMemcpyAsync(f_host, (char*)d->f + subs * bytes, bytes, cudaMemcpyDeviceToHost,
                      d->stream));
   CK(cudaStreamSynchronize(d->stream));
@@ -424,6 +498,7 @@ lbx_status lbx_init_equilibrium(lbx_domain* d, int subs, const void* rho, const 
                                 const void* uy, const void* uz)
 {
   if (lbx_status st = check_subs(d, subs)) return st;
+  if (d->dense_stale) { if (lbx_status st = exchange(d, false)) return st; }
   if (!rho || !ux || !uy || (d->D == 3 && !uz))
     return fail(LBX_ERR_INVALID, "rho/ux/uy (and uz in 3D) are required");
   const size_t plane = (size_t)d->N * d->real_size;
@@ -451,6 +526,9 @@ lbx_status lbx_init_equilibrium(lbx_domain* d, int subs, const void* rho, const 
     }
     d->launches++;
     e = cudaGetLastError();
+  }
+  if (e == cudaSuccess && d->layout == LBX_LAYOUT_COMPACT) {
+    if (exchange(d, true) != LBX_OK) e = cudaErrorUnknown;
   }
   if (e == cudaSuccess) e = cudaStreamSynchronize(d->stream);
   cudaFree(tmp);
@@ -505,11 +583,11 @@ lbx_status lbx_reduce(lbx_domain* d, lbx_reductions* out)
   const int nb = d->red_blocks;
   RedPartial* red = (RedPartial*)d->red;
   if (d->real_size == 8) {
-    if (d->D == 2) reduce_mv<double, 2><<<nb, 256, 0, d->stream>>>((const double*)d->mv, d->cls, d->N, d->p.nsubs, red);
-    else reduce_mv<double, 3><<<nb, 256, 0, d->stream>>>((const double*)d->mv, d->cls, d->N, d->p.nsubs, red);
+    if (d->D == 2) reduce_mv<double, 2><<<nb, 256, 0, d->stream>>>((const double*)d->mv, d->solids, d->N, d->p.nsubs, red);
+    else reduce_mv<double, 3><<<nb, 256, 0, d->stream>>>((const double*)d->mv, d->solids, d->N, d->p.nsubs, red);
   } else {
-    if (d->D == 2) reduce_mv<float, 2><<<nb, 256, 0, d->stream>>>((const float*)d->mv, d->cls, d->N, d->p.nsubs, red);
-    else reduce_mv<float, 3><<<nb, 256, 0, d->stream>>>((const float*)d->mv, d->cls, d->N, d->p.nsubs, red);
+    if (d->D == 2) reduce_mv<float, 2><<<nb, 256, 0, d->stream>>>((const float*)d->mv, d->solids, d->N, d->p.nsubs, red);
+    else reduce_mv<float, 3><<<nb, 256, 0, d->stream>>>((const float*)d->mv, d->solids, d->N, d->p.nsubs, red);
   }
   d->launches++;
   CK(cudaGetLastError());
@@ -535,6 +613,8 @@ lbx_status lbx_reduce(lbx_domain* d, lbx_reductions* out)
 lbx_status lbx_device_f(lbx_domain* d, void** ptr)
 {
   if (!d || !ptr) return fail(LBX_ERR_INVALID, "NULL argument");
+  if (d->dense_stale) { if (lbx_status st = exchange(d, false)) return st; }
+  CK(cudaStreamSynchronize(d->stream));
   *ptr = d->f;
   return LBX_OK;
 }
@@ -546,11 +626,12 @@ lbx_status lbx_device_mv(lbx_domain* d, void** ptr)
   return LBX_OK;
 }
 
-lbx_status lbx_info(lbx_domain* d, long long* fluid_nodes, int* faces_fused)
+lbx_status lbx_info(lbx_domain* d, long long* fluid_nodes, int* faces_fused, int* layout)
 {
   if (!d) return fail(LBX_ERR_INVALID, "domain is NULL");
   if (fluid_nodes) *fluid_nodes = d->fluid;
   if (faces_fused) *faces_fused = d->faces_fused ? 1 : 0;
+  if (layout) *layout = d->layout;
   return LBX_OK;
 }
 

@@ -49,6 +49,25 @@ __host__ __device__ constexpr T wgt(int a) {
 
 enum Dir2 { DC = 0, DE, DW, DN, DS, DNE, DSW, DNW, DSE };
 
+// A load the compiler may neither merge with an earlier load of the same
+// address nor hoist: used to re-read small index arrays (L1 hits) instead of
+// holding them in registers across the collision.
+__device__ __forceinline__ int ld_reload(const int* p)
+{
+  int v;
+  asm volatile("ld.global.nc.b32 %0, [%1];" : "=r"(v) : "l"(p));
+  return v;
+}
+
+// An opaque copy: stops the compiler from proving two address expressions
+// equal and keeping the first set of addresses live in registers.
+__device__ __forceinline__ int opaque(int x)
+{
+  int v;
+  asm volatile("mov.b32 %0, %1;" : "=r"(v) : "r"(x));
+  return v;
+}
+
 // Node class byte, built once per domain from the solids mask.
 enum : uint8_t {
   CLS_SOLID = 1,      // byte == 1 in the reference's mask
@@ -233,23 +252,20 @@ aa_step(StepArgs<T> A)
   if (cl & CLS_SOLID) return;
   const uint32_t nb = (cl & CLS_NEAR) ? A.nbm[n] : 0u;
 
-  // nbr[a] = node n + c_a, periodic on every axis (a serial run's wrap).
-  int nbr[Q];
-  if (ODD) {
-    const int xm = (i == 0) ? LX - 1 : -1, xp = (i == LX - 1) ? 1 - LX : 1;
-    const int ym = (j == 0) ? plane - LX : -LX, yp = (j == LY - 1) ? LX - plane : LX;
-    int zm = 0, zp = 0;
-    if (D == 3) {
-      const int tot = plane * A.LZ;
-      zm = (k == 0) ? tot - plane : -plane;
-      zp = (k == A.LZ - 1) ? plane - tot : plane;
-    }
-#pragma unroll
-    for (int a = 0; a < Q; ++a)
-      nbr[a] = n + (cx(a) < 0 ? xm : (cx(a) > 0 ? xp : 0))
-                 + (cy(a) < 0 ? ym : (cy(a) > 0 ? yp : 0))
-                 + (cz(a) < 0 ? zm : (cz(a) > 0 ? zp : 0));
+  // dense offsets to the neighbours along each axis (periodic on every
+  // axis, a serial run's wrap); neighbour n + c_a = n + off(a)
+  int xm = (i == 0) ? LX - 1 : -1, xp = (i == LX - 1) ? 1 - LX : 1;
+  int ym = (j == 0) ? plane - LX : -LX, yp = (j == LY - 1) ? LX - plane : LX;
+  int zm = 0, zp = 0;
+  if (D == 3) {
+    const int tot = plane * A.LZ;
+    zm = (k == 0) ? tot - plane : -plane;
+    zp = (k == A.LZ - 1) ? plane - tot : plane;
   }
+  auto off = [&](int a) -> int {
+    return (cx(a) < 0 ? xm : (cx(a) > 0 ? xp : 0)) + (cy(a) < 0 ? ym : (cy(a) > 0 ? yp : 0))
+         + (cz(a) < 0 ? zm : (cz(a) > 0 ? zp : 0));
+  };
 
   T u[3] = {T(0), T(0), T(0)};
 #pragma unroll
@@ -264,7 +280,7 @@ aa_step(StepArgs<T> A)
 #pragma unroll
       for (int a = 0; a < Q; ++a) {
         if ((nb >> opp(a)) & 1u) d[a] = fs[opp(a) * N + n];
-        else d[a] = fs[a * N + nbr[opp(a)]];
+        else d[a] = fs[a * N + (n + off(opp(a)))];
       }
     } else {
 #pragma unroll
@@ -281,14 +297,181 @@ aa_step(StepArgs<T> A)
     collide<T, Q, MODEL>(A, s, solute, ODD ? 1 : 2, d, u, n);
     if (ODD) {
       // push: f[opp a][n + c_a] = d_a, or own f[a][n] in front of a solid
+      // (offsets laundered so the pull addresses are not kept live)
+      xm = opaque(xm); xp = opaque(xp); ym = opaque(ym); yp = opaque(yp);
+      if (D == 3) { zm = opaque(zm); zp = opaque(zp); }
 #pragma unroll
       for (int a = 0; a < Q; ++a) {
         if ((nb >> a) & 1u) fs[a * N + n] = d[a];
-        else fs[opp(a) * N + nbr[a]] = d[a];
+        else fs[opp(a) * N + (n + off(a))] = d[a];
+      }
+    } else {
+      const int n2 = opaque(n);   // do not keep the load addresses live
+#pragma unroll
+      for (int a = 0; a < Q; ++a) fs[a * N + n2] = d[a];
+    }
+  }
+}
+
+// ---- the AA step on the compact fluid-only layout ---------------------------
+// Populations are stored for fluid nodes only, [subs][a][F] in dense node
+// order, so a warp's accesses in every direction plane cover only fluid
+// data (with 60% solids a dense layout fetches ~2x the useful bytes at
+// sector granularity).  fidx[n] maps a dense node to its compact index
+// (-1: solid); fnode[m] maps back.  One thread per fluid node.
+template <typename T>
+struct CompactArgs {
+  StepArgs<T> s;          // f = compact populations; N = dense node count
+  const int* fidx;        // [N]
+  const int* fnode;       // [F]
+  int F;
+  int faces;              // 2D: fused face boundaries configured
+};
+
+template <typename T, int Q, int NS, int MODEL, bool ODD>
+__global__ void __launch_bounds__(256)
+aa_step_compact(CompactArgs<T> C)
+{
+  constexpr int D = (Q == 9) ? 2 : 3;
+  const StepArgs<T>& A = C.s;
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= C.F) return;
+  const size_t F = (size_t)C.F;
+  const int LX = A.LX, LY = A.LY;
+  const int plane = LX * LY;
+  const bool faces = (Q == 9) && C.faces;
+  int n = 0, j = 0;
+  // dense offsets to the neighbours along each axis (odd step only)
+  int xm = 0, xp = 0, ym = 0, yp = 0, zm = 0, zp = 0;
+  if (ODD || A.write_mv || faces) {
+    n = C.fnode[m];
+    const int k = n / plane;
+    const int r = n - k * plane;
+    j = r / LX;
+    const int i = r - j * LX;
+    if (ODD) {
+      xm = (i == 0) ? LX - 1 : -1; xp = (i == LX - 1) ? 1 - LX : 1;
+      ym = (j == 0) ? plane - LX : -LX; yp = (j == LY - 1) ? LX - plane : LX;
+      if (D == 3) {
+        const int tot = plane * A.LZ;
+        zm = (k == 0) ? tot - plane : -plane;
+        zp = (k == A.LZ - 1) ? plane - tot : plane;
+      }
+    }
+  }
+  // dense offset of neighbour n + c_a
+  auto off = [&](int a) -> int {
+    return (cx(a) < 0 ? xm : (cx(a) > 0 ? xp : 0)) + (cy(a) < 0 ? ym : (cy(a) > 0 ? yp : 0))
+         + (cz(a) < 0 ? zm : (cz(a) > 0 ? zp : 0));
+  };
+  const int* const fidx_n = C.fidx + n;
+  T u[3] = {T(0), T(0), T(0)};
+#pragma unroll
+  for (int s = 0; s < NS; ++s) {
+    const bool solute = (NS == 2 && s == 1);
+    if (solute && !A.solute_on) break;
+    T* const fs = A.f + (size_t)s * Q * F;
+    T d[Q];
+    if (ODD) {
+      // pull: d_a = f[a][idx(n - c_a)], or own f[opp a] behind a solid
+#pragma unroll
+      for (int a = 0; a < Q; ++a) {
+        const int up = (a == 0) ? m : fidx_n[off(opp(a))];
+        d[a] = (up >= 0) ? fs[a * F + up] : fs[opp(a) * F + m];
       }
     } else {
 #pragma unroll
-      for (int a = 0; a < Q; ++a) fs[a * N + n] = d[a];
+      for (int a = 0; a < Q; ++a) d[a] = fs[opp(a) * F + m];
+    }
+    if (faces && (j == 0 || j == LY - 1)) {
+      T (&d9)[9] = reinterpret_cast<T (&)[9]>(d);
+      const bool shifted = (MODEL != PLAIN_COMP) && !solute;
+      if (j == LY - 1)
+        face_north<T>(A.face_n[s], A.rho_n[s], A.sc[s].rhoA, A.drho_n[s], shifted, d9);
+      if (j == 0)
+        face_south<T>(A.face_s[s], A.rho_s[s], A.sc[s].rhoA, A.drho_s[s], shifted, d9);
+    }
+    collide<T, Q, MODEL>(A, s, solute, ODD ? 1 : 2, d, u, n);
+    if (ODD) {
+      // push: f[opp a][idx(n + c_a)] = d_a, or own f[a] in front of a solid;
+      // the neighbour indices are re-read rather than kept in registers
+      xm = opaque(xm); xp = opaque(xp); ym = opaque(ym); yp = opaque(yp);
+      if (D == 3) { zm = opaque(zm); zp = opaque(zp); }
+#pragma unroll
+      for (int a = 0; a < Q; ++a) {
+        const int dn = (a == 0) ? m : ld_reload(fidx_n + off(a));
+        if (dn >= 0) fs[opp(a) * F + dn] = d[a];
+        else fs[a * F + m] = d[a];
+      }
+    } else {
+      const int m2 = opaque(m);   // do not keep the load addresses live
+#pragma unroll
+      for (int a = 0; a < Q; ++a) fs[a * F + m2] = d[a];
+    }
+  }
+}
+
+// Dense <-> compact exchange of all substances' populations.
+template <typename T>
+__global__ void gather_compact(T* fc, const T* fdense, const int* fnode, int F,
+                               long long N, int planes)
+{
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)F * planes) return;
+  const int pl = (int)(t / F), m = (int)(t - (long long)pl * F);
+  fc[t] = fdense[(long long)pl * N + fnode[m]];
+}
+
+template <typename T>
+__global__ void scatter_compact(T* fdense, const T* fc, const int* fnode, int F,
+                                long long N, int planes)
+{
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)F * planes) return;
+  const int pl = (int)(t / F), m = (int)(t - (long long)pl * F);
+  fdense[(long long)pl * N + fnode[m]] = fc[t];
+}
+
+// Stand-alone face kernel on the compact layout: the same deposits as
+// face_row, with each fluid node's slot reached through fidx.
+template <typename T>
+__global__ void face_row_compact(T* fs, const int* fidx, int LX, int LY, int F,
+                                 int north, int kind, int second, T rho_bc, T rhoA,
+                                 T drho, int shifted)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= LX) return;
+  const int j = north ? LY - 1 : 0;
+  const int m = fidx[i + LX * j];
+  if (m < 0) return;
+  auto cidx = [&](int ii, int jj) -> int {
+    ii = ii < 0 ? ii + LX : (ii == LX ? 0 : ii);
+    jj = jj < 0 ? jj + LY : (jj == LY ? 0 : jj);
+    return fidx[ii + LX * jj];
+  };
+  const size_t P = (size_t)F;
+  T d[9];
+#pragma unroll
+  for (int a = 0; a < 9; ++a) {
+    if (second) {
+      d[a] = fs[opp(a) * P + m];
+    } else {
+      const int up = cidx(i - cx(a), j - cy(a));
+      d[a] = (up < 0) ? fs[opp(a) * P + m] : fs[a * P + up];
+    }
+  }
+  if (north) face_north<T>(kind, rho_bc, rhoA, drho, shifted != 0, d);
+  else face_south<T>(kind, rho_bc, rhoA, drho, shifted != 0, d);
+  const int unk[3] = {north ? DS : DN, north ? DSE : DNW, north ? DSW : DNE};
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    const int a = unk[q];
+    if (second) {
+      fs[opp(a) * P + m] = d[a];
+    } else {
+      const int up = cidx(i - cx(a), j - cy(a));
+      if (up < 0) fs[a * P + m] = d[a];
+      else fs[a * P + up] = d[a];
     }
   }
 }
@@ -399,7 +582,7 @@ struct RedPartial {
 };
 
 template <typename T, int D>
-__global__ void reduce_mv(const T* mv, const uint8_t* cls, long long N, int nsubs,
+__global__ void reduce_mv(const T* mv, const uint8_t* solids, long long N, int nsubs,
                           RedPartial* out)
 {
   RedPartial r;
@@ -408,7 +591,7 @@ __global__ void reduce_mv(const T* mv, const uint8_t* cls, long long N, int nsub
   r.rmin = 1e300; r.rmax = -1e300; r.fluid = 0; r.nonfinite = 0;
   for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < N;
        n += (long long)gridDim.x * blockDim.x) {
-    if (cls[n] & CLS_SOLID) continue;
+    if (solids[n] == 1) continue;
     const double rho = (double)mv[n];
     double u[3] = {(double)mv[N + n], (double)mv[2 * N + n],
                    D == 3 ? (double)mv[3 * N + n] : 0.0};

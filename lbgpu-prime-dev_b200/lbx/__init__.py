@@ -20,6 +20,7 @@ LIB_PATH = os.path.join(os.path.dirname(_HERE), "lib", "liblbx.so")
 
 LBX_OK, LBX_ERR_INVALID, LBX_ERR_CUDA, LBX_ERR_NOMEM, LBX_ERR_STATE, LBX_ERR_NUMERIC = range(6)
 LBX_WRITE_MV = 1
+LBX_LAYOUT_AUTO, LBX_LAYOUT_DENSE, LBX_LAYOUT_COMPACT = 0, 1, 2
 
 _D2 = C.c_double * 2
 _D6 = C.c_double * 6
@@ -41,7 +42,7 @@ class _CParams(C.Structure):
         ("bc_ramp_start", C.c_int), ("bc_ramp_stop", C.c_int),
         ("pressure_n_table", C.POINTER(C.c_double)), ("pressure_n_len", C.c_int),
         ("pressure_s_table", C.POINTER(C.c_double)), ("pressure_s_len", C.c_int),
-        ("device", C.c_int),
+        ("device", C.c_int), ("layout", C.c_int),
     ]
 
 
@@ -72,7 +73,8 @@ _SIGNATURES = {
     "lbx_reduce": (C.c_int, [C.c_void_p, C.POINTER(_CReductions)]),
     "lbx_device_f": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "lbx_device_mv": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
-    "lbx_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_longlong), C.POINTER(C.c_int)]),
+    "lbx_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_longlong), C.POINTER(C.c_int),
+                           C.POINTER(C.c_int)]),
     "lbx_launch_count": (C.c_longlong, [C.c_void_p]),
     "lbx_last_error": (C.c_char_p, []),
 }
@@ -141,6 +143,7 @@ class Params:
     pressure_n_table: Optional[np.ndarray] = None
     pressure_s_table: Optional[np.ndarray] = None
     device: int = 0
+    layout: int = LBX_LAYOUT_AUTO
 
     @property
     def Q(self) -> int:
@@ -301,8 +304,10 @@ class Domain:
     def info(self) -> dict:
         fl = C.c_longlong()
         fused = C.c_int()
-        _check(_lib.lbx_info(self._h, C.byref(fl), C.byref(fused)))
-        return dict(fluid_nodes=fl.value, faces_fused=bool(fused.value))
+        layout = C.c_int()
+        _check(_lib.lbx_info(self._h, C.byref(fl), C.byref(fused), C.byref(layout)))
+        return dict(fluid_nodes=fl.value, faces_fused=bool(fused.value),
+                    layout={LBX_LAYOUT_DENSE: "dense", LBX_LAYOUT_COMPACT: "compact"}[layout.value])
 
     def launch_count(self) -> int:
         return int(_lib.lbx_launch_count(self._h))
