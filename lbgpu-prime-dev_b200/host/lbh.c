@@ -34,11 +34,11 @@ static void skip_label(FILE* in)
 /* F_INTW: read with "%d ", which also eats the whitespace after the value
  * (and so changes where the next skip_label starts). */
 enum { F_INT, F_INTW, F_REAL };
-typedef struct { int kind; size_t off; } field_t;
+typedef struct { int kind; size_t off; const char* name; } field_t;
 
-#define I(member) { F_INT, offsetof(lbh_params, member) }
-#define IW(member) { F_INTW, offsetof(lbh_params, member) }
-#define R(member) { F_REAL, offsetof(lbh_params, member) }
+#define I(member) { F_INT, offsetof(lbh_params, member), #member }
+#define IW(member) { F_INTW, offsetof(lbh_params, member), #member }
+#define R(member) { F_REAL, offsetof(lbh_params, member), #member }
 
 /* File order of src/params.h:40-660 (INTEGER_IC_BOUND build). */
 static const field_t FIELDS[] = {
@@ -79,6 +79,15 @@ static const field_t FIELDS[] = {
 #undef I
 #undef IW
 #undef R
+
+int lbh_params_field_count(void) { return (int)(sizeof FIELDS / sizeof FIELDS[0]); }
+
+const char* lbh_params_field(int k, int* is_real)
+{
+  if (k < 0 || k >= lbh_params_field_count()) return NULL;
+  if (is_real) *is_real = FIELDS[k].kind == F_REAL;
+  return FIELDS[k].name;
+}
 
 static int read_token(FILE* in, char* buf, int len)
 {

@@ -65,6 +65,11 @@ typedef struct lbh_params {
 int lbh_read_params(const char* path, int dims, int nsubs, lbh_params* out,
                     char* err, int errlen);
 
+/* The positional layout itself: the number of fields, and the name (the
+ * lbh_params member, e.g. "tau[1]") and kind of field k in file order. */
+int lbh_params_field_count(void);
+const char* lbh_params_field(int k, int* is_real);
+
 /* 24-bit BMP mask, black pixel -> 1, anything else -> 0, rows in file order
  * (bottom-up), as spy_bmp does (src/lbio.c:3073-3363).  out: LX*LY bytes.
  * Returns 0, or -1 (unreadable, not "BM", compressed, size mismatch, or a

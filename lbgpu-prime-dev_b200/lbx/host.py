@@ -1,0 +1,151 @@
+"""ctypes binding of the host C library lib/liblbh.so (host/lbh.h).
+
+The reference's file interface: the positional params.in reader, the 24-bit
+BMP and raw solid-mask decoders/writers, the initial density field and the
+frame file names.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(_HERE), "lib", "liblbh.so")
+
+
+class Real(C.Structure):
+    _fields_ = [("d", C.c_double), ("f", C.c_float)]
+
+
+def _ints(n):
+    return C.c_int * n
+
+
+class HostParams(C.Structure):
+    """Mirror of lbh_params (host/lbh.h), field for field."""
+    _fields_ = [
+        ("LX", C.c_int), ("LY", C.c_int), ("LZ", C.c_int), ("BX", C.c_int), ("BY", C.c_int),
+        ("BZ", C.c_int), ("length_scale", C.c_int), ("NumFrames", C.c_int),
+        ("FrameRate", C.c_int),
+        ("tau", Real * 2), ("gforce", (Real * 3) * 2), ("end_grav", _ints(2)),
+        ("buoyancy", C.c_int), ("incompressible", C.c_int), ("simple_diffusion", C.c_int),
+        ("rho_A", Real * 2), ("rho_B", Real * 2),
+        ("rho_sigma", Real), ("rho_sigma_in", Real), ("rho_sigma_out", Real),
+        ("u_sigma", Real), ("u_sigma_in", Real), ("u_sigma_out", Real),
+        ("sigma_t_on", C.c_int), ("sigma_t_off", C.c_int), ("sigma_start", C.c_int),
+        ("sigma_stop", C.c_int), ("sigma_btc_rate", C.c_int), ("sigma_btc_spot", C.c_int),
+        ("GZL", C.c_int), ("PressureBC", C.c_int), ("AllBoundaryPeriodic", C.c_int),
+        ("sink", Real), ("pfmul", Real), ("pfadd", Real), ("rho_in", Real), ("rho_out", Real),
+        ("ux_in", Real), ("ux_out", Real), ("uy_in", Real), ("uy_out", Real),
+        ("uz_in", Real), ("uz_out", Real), ("big_V0", Real), ("big_V0_solid", Real * 2),
+        ("ns_flag", C.c_int), ("ns", Real),
+        ("ic_poisseuille", C.c_int), ("bc_poisseuille", C.c_int),
+        ("bc_slip_north", C.c_int), ("bc_sigma_slip", C.c_int),
+        ("bc_ramp_start", C.c_int), ("bc_ramp_stop", C.c_int),
+    ] + [(n, _ints(2)) for n in (
+        "pressure_t_in", "pressure_b_in", "pressure_t_out", "pressure_b_out",
+        "velocity_t_in", "velocity_b_in", "velocity_t_out", "velocity_b_out",
+        "pressure_n_in", "pressure_s_in", "pressure_n_out", "pressure_s_out",
+        "velocity_n_in", "velocity_s_in", "velocity_n_out", "velocity_s_out",
+        "pressure_e_in", "pressure_w_in", "pressure_e_out", "pressure_w_out",
+        "velocity_e_in", "velocity_w_in", "velocity_e_out", "velocity_w_out")] + [
+        ("constcon", _ints(24)),
+        ("zeroconcgrad_t", C.c_int), ("zeroconcgrad_b", C.c_int),
+        ("zeroconcgrad_n", C.c_int), ("zeroconcgrad_s", C.c_int),
+        ("zeroconcgrad_e", C.c_int), ("zeroconcgrad_w", C.c_int),
+        ("zeroconcgrad_full", C.c_int),
+        ("plot_scale_dynamic", C.c_int), ("use_colormap", C.c_int),
+        ("initial_condition", C.c_int),
+        ("x0", C.c_int), ("y0", C.c_int), ("z0", C.c_int), ("r0", C.c_int), ("cut", Real),
+        ("x1", C.c_int), ("x2", C.c_int), ("y1", C.c_int), ("y2", C.c_int),
+        ("z1", C.c_int), ("z2", C.c_int),
+        ("rel_x1", Real), ("rel_x2", Real), ("rel_y1", Real), ("rel_y2", Real),
+        ("rel_z1", Real), ("rel_z2", Real),
+        ("dump_rho", C.c_int), ("dump_u", C.c_int), ("dump_force", C.c_int),
+        ("dump_vor", C.c_int),
+        ("NumNodes", C.c_longlong), ("NumTimeSteps", C.c_int),
+    ]
+
+
+_lib = None
+
+
+def load():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError("liblbh.so missing: make -C lbgpu-prime-dev_b200")
+        lib = C.CDLL(LIB_PATH)
+        lib.lbh_read_params.argtypes = [C.c_char_p, C.c_int, C.c_int, C.POINTER(HostParams),
+                                        C.c_char_p, C.c_int]
+        lib.lbh_read_bmp_mask.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_void_p,
+                                          C.c_char_p, C.c_int]
+        lib.lbh_read_raw_mask.argtypes = [C.c_char_p, C.c_longlong, C.c_void_p,
+                                          C.c_char_p, C.c_int]
+        lib.lbh_write_bmp_mask.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_void_p]
+        lib.lbh_write_raw_mask.argtypes = [C.c_char_p, C.c_longlong, C.c_void_p]
+        lib.lbh_initial_rho.argtypes = [C.POINTER(HostParams), C.c_int, C.c_int, C.c_int,
+                                        C.c_void_p]
+        _lib = lib
+    return _lib
+
+
+class HostError(RuntimeError):
+    pass
+
+
+def read_params(path: str, dims: int = 2, nsubs: int = 1) -> HostParams:
+    p = HostParams()
+    err = C.create_string_buffer(512)
+    if load().lbh_read_params(path.encode(), dims, nsubs, C.byref(p), err, 512):
+        raise HostError(err.value.decode())
+    return p
+
+
+def read_bmp_mask(path: str, LX: int, LY: int) -> np.ndarray:
+    out = np.zeros(LX * LY, np.uint8)
+    err = C.create_string_buffer(512)
+    if load().lbh_read_bmp_mask(path.encode(), LX, LY, out.ctypes.data, err, 512):
+        raise HostError(err.value.decode())
+    return out
+
+
+def read_raw_mask(path: str, N: int) -> np.ndarray:
+    out = np.zeros(N, np.uint8)
+    err = C.create_string_buffer(512)
+    if load().lbh_read_raw_mask(path.encode(), N, out.ctypes.data, err, 512):
+        raise HostError(err.value.decode())
+    return out
+
+
+def write_bmp_mask(path: str, LX: int, LY: int, mask: np.ndarray):
+    m = np.ascontiguousarray(mask, dtype=np.uint8)
+    if load().lbh_write_bmp_mask(path.encode(), LX, LY, m.ctypes.data):
+        raise HostError("cannot write " + path)
+
+
+def write_raw_mask(path: str, mask: np.ndarray):
+    m = np.ascontiguousarray(mask, dtype=np.uint8)
+    if load().lbh_write_raw_mask(path.encode(), m.size, m.ctypes.data):
+        raise HostError("cannot write " + path)
+
+
+def initial_rho(p: HostParams, dims: int, nsubs: int, subs: int) -> np.ndarray:
+    out = np.zeros(p.NumNodes, np.float64)
+    if load().lbh_initial_rho(C.byref(p), dims, nsubs, subs, out.ctypes.data):
+        raise HostError("initial_condition %d is not supported" % p.initial_condition)
+    return out
+
+
+def params_layout():
+    """[(name, is_real)] of params.in fields in file order (src/params.h:40-660)."""
+    lib = load()
+    lib.lbh_params_field.restype = C.c_char_p
+    lib.lbh_params_field.argtypes = [C.c_int, C.POINTER(C.c_int)]
+    out = []
+    for k in range(lib.lbh_params_field_count()):
+        r = C.c_int()
+        out.append((lib.lbh_params_field(k, C.byref(r)).decode(), bool(r.value)))
+    return out

@@ -233,3 +233,54 @@ def variant_name(p: Params, dtype) -> str:
     elif p.compressible:
         base += "c"
     return base + "_" + _sfx(dtype)
+
+
+def _ref_any():
+    """Any built harness variant (the readers are the same in every variant)."""
+    for v in ("d2q9_f64", "d3q19_f64"):
+        if reference_available(v):
+            if v not in _refs:
+                lib = C.CDLL(os.path.join(REF_DIR, "librefk_%s.so" % v))
+                lib.refk_run.restype = C.c_int
+                lib.refk_real_size.restype = C.c_int
+                _refs[v] = lib
+            return _refs[v]
+    return None
+
+
+def reference_read_params(path: str):
+    """The reference's read_params (src/params.h:40-660) on `path`: selected
+    fields as a dict, or None without the harness."""
+    lib = _ref_any()
+    if lib is None:
+        return None
+    iout = (C.c_int * 10)()
+    dout = (C.c_double * 8)()
+    lib.refk_read_params(path.encode(), iout, dout)
+    keys_i = ["LX", "LY", "LZ", "NumFrames", "FrameRate", "initial_condition",
+              "bc_ramp_start", "bc_ramp_stop", "pressure_n_in[0]", "pressure_s_in[0]"]
+    keys_d = ["tau[0]", "rho_A[0]", "rho_B[0]", "rho_in", "rho_out", "sink",
+              "gforce[0][0]", "pfmul"]
+    out = dict(zip(keys_i, list(iout)))
+    out.update(zip(keys_d, list(dout)))
+    return out
+
+
+def reference_read_bmp(path: str, LX: int, LY: int):
+    """The reference's spy_bmp (src/lbio.c:3073-3363) decode, or None."""
+    lib = _ref_any()
+    if lib is None:
+        return None
+    out = np.zeros(LX * LY, np.uint8)
+    lib.refk_read_bmp(path.encode(), LX, LY, out.ctypes.data_as(C.c_void_p))
+    return out
+
+
+def reference_read_raw(path: str, LX: int, LY: int, LZ: int):
+    """The reference's read_solids (src/lbio.c:507-629), or None."""
+    lib = _ref_any()
+    if lib is None:
+        return None
+    out = np.zeros(LX * LY * LZ, np.uint8)
+    lib.refk_read_raw(path.encode(), LX, LY, LZ, out.ctypes.data_as(C.c_void_p))
+    return out

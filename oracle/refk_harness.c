@@ -30,6 +30,10 @@
 #include <time.h>
 #include <pthread.h>
 
+#ifndef CLK_TCK
+#define CLK_TCK CLOCKS_PER_SEC   /* as src/lbgpu_prime.h:18-21 */
+#endif
+
 #if DP_ON
 typedef double real;
 #else
@@ -339,18 +343,14 @@ EXPORT int refk_run(const refk_params* p, real* f, const unsigned char* solids,
 /* ---- host-side input readers of the reference ------------------------------
  * read_params (src/params.h:40-660), spy_bmp (src/lbio.c:3073-3363) and
  * read_solids (src/lbio.c:507-629), run on a lattice struct the harness
- * fills itself (a serial build never sets the global extents these readers
- * use, so the harness sets them as a one-rank parallel run would). */
+ * fills itself (in a serial build the global extents they use are the
+ * local ones, src/process.c:2115-2126). */
 static struct lattice_struct* harness_lattice(int LX, int LY, int LZ)
 {
   struct lattice_struct* l = (struct lattice_struct*)calloc(1, sizeof *l);
   l->param.LX = LX; l->param.LY = LY; l->param.LZ = LZ;
   l->NumNodes = LX * LY * LZ;
   l->process.id = 0; l->process.num_procs = 1;
-  l->process.g_LX = LX; l->process.g_LY = LY; l->process.g_LZ = LZ;
-  l->process.g_NumNodes = LX * LY * LZ;
-  l->process.g_SX = l->process.g_SY = l->process.g_SZ = 0;
-  l->process.g_StartNode = 0;
   l->solids_memblock = (unsigned char*)calloc((size_t)(LX * LY * LZ), 1);
   return l;
 }
