@@ -75,10 +75,11 @@ struct lbx_domain {
   bool faces_fused = false;   // fused into the step kernels
   int parity = 0;             // 0: natural order (next step odd); 1: swapped
   long long launches = 0;
-  // graph replay of frame-free step runs
+  // graph replay of frame-free, time-invariant runs: one captured AA pair
   cudaGraphExec_t graph = nullptr;
-  int graph_steps = 0;
-  int graph_t0 = -1;
+  cudaStream_t graph_stream = nullptr;   // stream the pair was captured on
+  unsigned char graph_key[2 * 512];      // StepArgs bytes of the odd, even step
+  size_t graph_key_len = 0;
 };
 
 namespace {
@@ -107,11 +108,10 @@ T face_rho(const lbx_domain* d, int s, int t, int in_kind, bool is_in,
 }
 
 template <typename T>
-StepArgs<T> make_args(const lbx_domain* d, int t, unsigned flags)
+void fill_args(const lbx_domain* d, int t, unsigned flags, StepArgs<T>& A)
 {
   const lbx_params& p = d->p;
-  StepArgs<T> A;
-  std::memset(&A, 0, sizeof A);
+  std::memset(&A, 0, sizeof A);   // padding included: args are compared as bytes
   A.f = (T*)(d->layout == LBX_LAYOUT_COMPACT ? d->fc : d->f);
   A.mv = (T*)d->mv;
   A.cls = d->cls;
@@ -144,6 +144,13 @@ StepArgs<T> make_args(const lbx_domain* d, int t, unsigned flags)
       A.drho_s[s] = (T)((double)A.rho_s[s] - (double)A.sc[s].rhoA);
     }
   }
+}
+
+template <typename T>
+StepArgs<T> make_args(const lbx_domain* d, int t, unsigned flags)
+{
+  StepArgs<T> A;
+  fill_args<T>(d, t, flags, A);
   return A;
 }
 
@@ -298,6 +305,7 @@ bool faces_fusable(const lbx_params& p, const uint8_t* sol)
 void release(lbx_domain* d)
 {
   if (d->graph) cudaGraphExecDestroy(d->graph);
+  d->graph = nullptr;
   cudaFree(d->fc); cudaFree(d->fidx); cudaFree(d->fnode);
   cudaFree(d->f); cudaFree(d->mv); cudaFree(d->solids); cudaFree(d->cls);
   cudaFree(d->nbm); cudaFree(d->red);
@@ -324,6 +332,69 @@ lbx_status do_step(lbx_domain* d, int t, unsigned flags)
     if (d->layout == LBX_LAYOUT_COMPACT) d->dense_stale = true;
   }
   return st;
+}
+
+// The launch arguments of the step at time t, as bytes (for comparing steps:
+// two steps with equal bytes launch identical work).
+static_assert(sizeof(StepArgs<double>) <= 512 && sizeof(StepArgs<float>) <= 512,
+              "graph keys hold one StepArgs in 512 bytes");
+
+size_t step_key(const lbx_domain* d, int t, unsigned char* out)
+{
+  if (d->real_size == 8) {
+    fill_args<double>(d, t, 0, *reinterpret_cast<StepArgs<double>*>(out));
+    return sizeof(StepArgs<double>);
+  }
+  fill_args<float>(d, t, 0, *reinterpret_cast<StepArgs<float>*>(out));
+  return sizeof(StepArgs<float>);
+}
+
+// Replay `pairs` AA pairs starting at odd time t from one captured pair.
+// Only called when every step of the stretch has the launch arguments of
+// the first pair (checked by the caller) and the stream is capturable.
+lbx_status replay_pairs(lbx_domain* d, int t, int pairs)
+{
+  alignas(16) unsigned char key[2 * 512];
+  const size_t k1 = step_key(d, t, key);
+  const size_t k2 = step_key(d, t + 1, key + 512);
+  std::memmove(key + k1, key + 512, k2);
+  const size_t klen = k1 + k2;
+  if (!d->graph || d->graph_stream != d->stream || d->graph_key_len != klen ||
+      std::memcmp(d->graph_key, key, klen) != 0) {
+    if (d->graph) { cudaGraphExecDestroy(d->graph); d->graph = nullptr; }
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(d->stream, cudaStreamCaptureModeThreadLocal));
+    const long long before = d->launches;
+    lbx_status st = d->real_size == 8 ? step_t<double>(d, t, 0) : step_t<float>(d, t, 0);
+    if (st == LBX_OK)
+      st = d->real_size == 8 ? step_t<double>(d, t + 1, 0) : step_t<float>(d, t + 1, 0);
+    cudaError_t e = cudaStreamEndCapture(d->stream, &g);
+    d->launches = before;
+    if (st != LBX_OK) { if (g) cudaGraphDestroy(g); return st; }
+    if (e != cudaSuccess) return fail(LBX_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
+    e = cudaGraphInstantiate(&d->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) { d->graph = nullptr; return fail(LBX_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e)); }
+    d->graph_stream = d->stream;
+    std::memcpy(d->graph_key, key, klen);
+    d->graph_key_len = klen;
+  }
+  const long long per_pair = (d->faces_active && !d->faces_fused) ? 0 : 2;
+  for (int r = 0; r < pairs; ++r) {
+    CK(cudaGraphLaunch(d->graph, d->stream));
+    d->launches += per_pair;
+  }
+  if (per_pair == 0) {
+    // stand-alone face kernels are inside the graph too: count them
+    long long n = 0;
+    for (int s = 0; s < d->p.nsubs; ++s)
+      n += (d->p.pressure_n_in[s] != 0) + (d->p.pressure_n_out[s] != 0) +
+           (d->p.pressure_s_in[s] != 0) + (d->p.pressure_s_out[s] != 0);
+    if (d->p.nsubs == 2) n += (d->p.zeroconcgrad_n != 0) + (d->p.zeroconcgrad_s != 0);
+    d->launches += (long long)pairs * 2 * (n + 1);
+  }
+  if (d->layout == LBX_LAYOUT_COMPACT) d->dense_stale = true;
+  return LBX_OK;
 }
 
 // Dense exchange array <-> compact populations.
@@ -554,9 +625,31 @@ lbx_status lbx_run(lbx_domain* d, int t0, int nsteps, int frame_rate)
 {
   if (!d) return fail(LBX_ERR_INVALID, "domain is NULL");
   if (nsteps < 0) return fail(LBX_ERR_INVALID, "nsteps must be >= 0");
-  for (int t = t0 + 1; t <= t0 + nsteps; ++t) {
-    const unsigned fl = (frame_rate > 0 && t % frame_rate == 0) ? LBX_WRITE_MV : 0u;
-    if (lbx_status st = do_step(d, t, fl)) return st;
+  const int tend = t0 + nsteps;
+  int t = t0 + 1;
+  alignas(16) unsigned char k_odd[512], k_even[512], k[512];
+  while (t <= tend) {
+    const bool frame = frame_rate > 0 && t % frame_rate == 0;
+    // a stretch of >= 8 frame-free steps starting on an odd time, with the
+    // launch arguments of its first pair throughout, is replayed from a graph
+    if (!frame && (t % 2) == 1 && d->parity == 0 && d->stream != nullptr && tend - t + 1 >= 8) {
+      const size_t ko = step_key(d, t, k_odd), ke = step_key(d, t + 1, k_even);
+      int pairs = 0;
+      for (int u = t; u + 1 <= tend; u += 2) {
+        if (frame_rate > 0 && (u % frame_rate == 0 || (u + 1) % frame_rate == 0)) break;
+        if (pairs > 0 && (step_key(d, u, k) != ko || std::memcmp(k, k_odd, ko) ||
+                          step_key(d, u + 1, k) != ke || std::memcmp(k, k_even, ke)))
+          break;
+        ++pairs;
+      }
+      if (pairs >= 4) {
+        if (lbx_status st = replay_pairs(d, t, pairs)) return st;
+        t += 2 * pairs;
+        continue;
+      }
+    }
+    if (lbx_status st = do_step(d, t, frame ? LBX_WRITE_MV : 0u)) return st;
+    ++t;
   }
   return LBX_OK;
 }

@@ -1,0 +1,139 @@
+"""The benchmark configurations of the LBM path, runnable end to end.
+
+    python -m lbx.configs cfg1 [--steps 2000]
+    python -m lbx.configs cfg2 [--steps 10000]
+
+cfg1: D2Q9 BGK 256x256, FP64, tau = 1.0, non-overlapping discs r = 8 to
+      porosity 0.6 (the inlet/outlet rows kept fluid), Zou-He pressure
+      rho_in = 1.001 / rho_out = 1.0, periodic across, start at rho = 1,
+      u = 0.  The reference has pressure faces on its y faces only (north /
+      south rows), so the flow runs along j; the lattice is the transpose of
+      an x-directed channel.  Reports MLUPS and the Darcy permeability
+      k = nu <u_flow> L / dp with nu = (tau - 1/2)/3, dp = (rho_in - rho_out)/3,
+      L = 255 and <.> over all nodes (superficial).
+cfg2: D3Q19 BGK 256^3, tau = 0.8, overlapping spheres r = 6 to porosity 0.4,
+      gx = 1e-6, periodic.  Runs FP32 shifted, FP64 shifted and FP64 plain
+      (unshifted, compressible) populations; reports MLUPS of each and the
+      permeability k = nu <u_x> / gx of each with the relative error of the
+      FP32 run against the FP64 run.
+
+Each run prints one JSON line.  Times come from CUDA events on the stream
+the kernels run on.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import sys
+
+import numpy as np
+
+from . import Domain, Params, LBX_LAYOUT_AUTO
+from . import geometry
+
+
+def _timed_run(dom: Domain, t0: int, steps: int, frame_at_end: bool = True):
+    import torch
+    s = torch.cuda.Stream()
+    dom.set_stream(s.cuda_stream)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(s)
+    if frame_at_end:
+        dom.run(t0, steps - 1, 0)
+        dom.step(t0 + steps, write_mv=True)
+    else:
+        dom.run(t0, steps, 0)
+    e1.record(s)
+    s.synchronize()
+    return e0.elapsed_time(e1) / 1e3
+
+
+def cfg1_params(precision: int = 8, layout: int = LBX_LAYOUT_AUTO) -> tuple:
+    LX = LY = 256
+    # discs placed along the flow direction x' (= j here) with the first and
+    # last x' columns kept fluid, then transposed so x' runs along j
+    mask = geometry.transpose_2d(geometry.disc_pack(LY, LX, radius=8, porosity=0.6, seed=2026),
+                                 LY, LX)
+    p = Params(dims=2, LX=LX, LY=LY, LZ=1, precision=precision, tau=(1.0, 1.0),
+               pressure_s_in=(1, 0), pressure_n_out=(1, 0), rho_in=1.001, rho_out=1.0,
+               layout=layout)
+    return p, mask
+
+
+def run_cfg1(steps: int = 2000) -> dict:
+    p, mask = cfg1_params()
+    with Domain(p, mask) as dom:
+        dom.init_equilibrium(0, 1.0, 0.0, 0.0)
+        dom.run(0, 20, 0)                         # warm-up
+        dom.init_equilibrium(0, 1.0, 0.0, 0.0)
+        secs = _timed_run(dom, 0, steps)
+        mv = dom.download_mv()
+        info = dom.info()
+    fluid = mask != 1
+    nu = (1.0 - 0.5) / 3.0
+    dp = (1.001 - 1.0) / 3.0
+    u_flow = np.where(fluid, mv[0, 2], 0.0).mean()     # superficial, along j
+    k = nu * u_flow * 255.0 / dp
+    return {"config": "cfg1", "lattice": [256, 256], "dtype": "f64", "steps": steps,
+            "porosity": float(fluid.mean()), "mlups": 256 * 256 * steps / secs / 1e6,
+            "seconds": secs, "permeability": k, "mean_u_flow": float(u_flow),
+            "layout": info["layout"], "faces_fused": info["faces_fused"]}
+
+
+def cfg2_params(precision: int, accurate: int = 1, compressible: int = 0,
+                layout: int = LBX_LAYOUT_AUTO, n: int = 256):
+    mask = geometry.sphere_pack(n, n, n, radius=6, porosity=0.4, seed=1234)
+    p = Params(dims=3, LX=n, LY=n, LZ=n, precision=precision, accurate=accurate,
+               compressible=compressible, tau=(0.8, 1.0), gaccel=(1e-6, 0, 0, 0, 0, 0),
+               layout=layout)
+    return p, mask
+
+
+def run_cfg2(steps: int = 10000, n: int = 256) -> list:
+    out = []
+    nu = (0.8 - 0.5) / 3.0
+    ks = {}
+    for name, prec, acc, comp in (("fp32_shifted", 4, 1, 0), ("fp64_shifted", 8, 1, 0),
+                                  ("fp64_plain", 8, 0, 1)):
+        p, mask = cfg2_params(prec, acc, comp, n=n)
+        fluid = mask != 1
+        with Domain(p, mask) as dom:
+            dom.init_equilibrium(0, 1.0, 0.0, 0.0, 0.0)
+            dom.run(0, 8, 0)
+            dom.init_equilibrium(0, 1.0, 0.0, 0.0, 0.0)
+            secs = _timed_run(dom, 0, steps)
+            r = dom.reduce()
+            info = dom.info()
+        ux_mean = r["u_sum"][0] / mask.size        # superficial: solids hold u = 0
+        k = nu * ux_mean / 1e-6
+        ks[name] = k
+        out.append({"config": "cfg2", "run": name, "lattice": [n] * 3, "steps": steps,
+                    "mlups": n ** 3 * steps / secs / 1e6,
+                    "mflups": int(fluid.sum()) * steps / secs / 1e6, "seconds": secs,
+                    "permeability": k, "mass": r["mass"], "layout": info["layout"]})
+    for o in out:
+        o["perm_rel_err_vs_fp64_shifted"] = abs(o["permeability"] - ks["fp64_shifted"]) / abs(
+            ks["fp64_shifted"])
+    f32 = next(o for o in out if o["run"] == "fp32_shifted")
+    plain = next(o for o in out if o["run"] == "fp64_plain")
+    f32["speedup_vs_fp64_plain"] = f32["mlups"] / plain["mlups"]
+    return out
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("config", choices=["cfg1", "cfg2"])
+    ap.add_argument("--steps", type=int, default=None)
+    ap.add_argument("--edge", type=int, default=256)
+    a = ap.parse_args(argv)
+    if a.config == "cfg1":
+        print(json.dumps(run_cfg1(a.steps or 2000)))
+    else:
+        for line in run_cfg2(a.steps or 10000, a.edge):
+            print(json.dumps(line))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())
