@@ -165,6 +165,23 @@ lbx_status lbx_sync(lbx_domain* d);
  * _u of src/compute.c:1159-1416 used by the frame summary.  Synchronous. */
 lbx_status lbx_reduce(lbx_domain* d, lbx_reductions* out);
 
+/* The reductions of lbx_reduce for callers that cannot allocate device
+ * memory -- a host program whose device memory is handed in full to its own
+ * pool allocator, or one that must not add an allocation (which can
+ * synchronize the device, or fail) to a time-critical loop.  No counterpart
+ * in the reference.  mv ([nsubs][1+dims][N] reals) and solids (N bytes) are
+ * device pointers the caller owns; the work is queued on `stream` (NULL: the
+ * default stream) and the call waits for it.  Scratch lives in a fixed array
+ * inside the library (384 KiB, held on every GPU that loads the library
+ * until exit), so N is limited to 67,108,864 nodes (LBX_ERR_INVALID beyond).
+ * The first call on a device looks up that array's device address; make it
+ * before any stream capture.  Calls share the array: calls that overlap on
+ * the GPU race.  Allocates nothing: no cudaMalloc, cudaFree or allocating
+ * library call. */
+lbx_status lbx_reduce_mv_static(const void* mv, const uint8_t* solids,
+                                long long N, int dims, int nsubs, int precision,
+                                void* stream, lbx_reductions* out);
+
 /* Device pointers to the populations ([nsubs][Q][N], the dense exchange
  * format; with the compact layout this first writes the current state into
  * it, and the pointer is valid until the next step) and macro variables

@@ -38,6 +38,18 @@ lbx_status fail(lbx_status code, const char* fmt, ...)
   return code;
 }
 
+}  // namespace
+
+// For the library's other translation units; hidden, so not an entry point.
+__attribute__((visibility("hidden"))) lbx_status lbx_internal_fail(lbx_status code,
+                                                                    const char* msg)
+{
+  g_err = msg;
+  return code;
+}
+
+namespace {
+
 #define CK(call)                                                              \
   do {                                                                        \
     cudaError_t e_ = (call);                                                  \

@@ -71,6 +71,9 @@ _SIGNATURES = {
     "lbx_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
     "lbx_sync": (C.c_int, [C.c_void_p]),
     "lbx_reduce": (C.c_int, [C.c_void_p, C.POINTER(_CReductions)]),
+    "lbx_reduce_mv_static": (C.c_int, [C.c_void_p, C.c_void_p, C.c_longlong, C.c_int,
+                                       C.c_int, C.c_int, C.c_void_p,
+                                       C.POINTER(_CReductions)]),
     "lbx_device_f": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "lbx_device_mv": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "lbx_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_longlong), C.POINTER(C.c_int),
