@@ -198,6 +198,46 @@ lbx_status lbx_info(lbx_domain* d, long long* fluid_nodes, int* faces_fused,
 /* Number of this library's kernels launched on the domain so far. */
 long long lbx_launch_count(lbx_domain* d);
 
+/* ---- batches of independent lattices ---------------------------------------
+ * Many samples of uneven size (same dims, precision and collision model;
+ * each with its own extents, mask, tau, rho_A and body force; one substance;
+ * no face boundaries) stepped together: the reference runs one lattice per
+ * process, so a study over many samples pays one set of launches per sample
+ * and step.  Populations of all samples share one compact fluid-only array;
+ * lbx_batch_run then advances every sample with one launch per step
+ * (FUSED, graph-replayed), with one cooperative launch per run of steps
+ * (PERSISTENT), or with one launch per sample per step (SEQUENTIAL, the
+ * per-sample baseline).  AUTO uses the mode lbx_batch_autotune chose
+ * (FUSED before any tuning).  Results are per sample identical to running
+ * the sample alone. */
+typedef struct lbx_batch lbx_batch;
+enum { LBX_BATCH_AUTO = 0, LBX_BATCH_FUSED = 1, LBX_BATCH_PERSISTENT = 2,
+       LBX_BATCH_SEQUENTIAL = 3 };
+
+lbx_status lbx_batch_create(int nsamples, const lbx_params* params,
+                            const uint8_t* const* solids, lbx_batch** out);
+lbx_status lbx_batch_destroy(lbx_batch* b);
+/* Per sample, dense [Q][N] populations (the natural-order state of an even
+ * time) and [1+D][N] macro variables, as for a domain. */
+lbx_status lbx_batch_upload_f(lbx_batch* b, int sample, const void* f_host);
+lbx_status lbx_batch_download_f(lbx_batch* b, int sample, void* f_host);
+lbx_status lbx_batch_download_mv(lbx_batch* b, int sample, void* rho, void* ux,
+                                 void* uy, void* uz);
+lbx_status lbx_batch_init_equilibrium(lbx_batch* b, int sample, const void* rho,
+                                      const void* ux, const void* uy,
+                                      const void* uz);
+/* Steps t0+1 .. t0+nsteps of every sample, macro variables at multiples of
+ * frame_rate, in `mode` (LBX_BATCH_*). */
+lbx_status lbx_batch_run(lbx_batch* b, int t0, int nsteps, int frame_rate, int mode);
+/* Times FUSED at block sizes 128/256/512 and PERSISTENT on `steps` trial
+ * steps, restores the populations, and keeps the fastest for AUTO. */
+lbx_status lbx_batch_autotune(lbx_batch* b, int steps, int* mode, int* block);
+lbx_status lbx_batch_set_stream(lbx_batch* b, void* stream);
+lbx_status lbx_batch_sync(lbx_batch* b);
+/* FP64 reductions over one sample's macro variables (as lbx_reduce). */
+lbx_status lbx_batch_reduce(lbx_batch* b, int sample, lbx_reductions* out);
+long long lbx_batch_launch_count(lbx_batch* b);
+
 /* Message for the last failed call on this thread ("" if none). */
 const char* lbx_last_error(void);
 

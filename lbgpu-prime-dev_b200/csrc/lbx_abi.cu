@@ -71,6 +71,7 @@ struct lbx_domain {
   void* fc = nullptr;         // [nsubs][Q][F] compact layout
   int* fidx = nullptr;        // [N] dense -> compact (-1 solid)
   int* fnode = nullptr;       // [F] compact -> dense
+  int16_t* nbd = nullptr;     // [Q-1][F] neighbour deltas, if they fit in 16 bits
   int layout = LBX_LAYOUT_DENSE;
   bool dense_stale = false;   // compact state newer than the dense array
   void* mv = nullptr;         // [nsubs][1+D][N]
@@ -90,7 +91,7 @@ struct lbx_domain {
   // graph replay of frame-free, time-invariant runs: one captured AA pair
   cudaGraphExec_t graph = nullptr;
   cudaStream_t graph_stream = nullptr;   // stream the pair was captured on
-  unsigned char graph_key[2 * 512];      // StepArgs bytes of the odd, even step
+  unsigned char graph_key[2 * 640];      // keys of the odd and the even step
   size_t graph_key_len = 0;
 };
 
@@ -174,12 +175,17 @@ void launch_aa(lbx_domain* d, const StepArgs<T>& A, bool odd)
     C.s = A;
     C.fidx = d->fidx;
     C.fnode = d->fnode;
+    C.nbd = d->nbd;
     C.F = (int)d->fluid;
     C.faces = d->faces_fused ? 1 : 0;
     const unsigned blocks = (unsigned)((d->fluid + 255) / 256);
     if (blocks == 0) return;
-    if (odd) aa_step_compact<T, Q, NS, MODEL, true><<<blocks, 256, 0, d->stream>>>(C);
-    else aa_step_compact<T, Q, NS, MODEL, false><<<blocks, 256, 0, d->stream>>>(C);
+    if (odd) {
+      if (d->nbd) aa_step_compact<T, Q, NS, MODEL, true, 1><<<blocks, 256, 0, d->stream>>>(C);
+      else aa_step_compact<T, Q, NS, MODEL, true, 0><<<blocks, 256, 0, d->stream>>>(C);
+    } else {
+      aa_step_compact<T, Q, NS, MODEL, false, 0><<<blocks, 256, 0, d->stream>>>(C);
+    }
     d->launches++;
     return;
   }
@@ -318,7 +324,7 @@ void release(lbx_domain* d)
 {
   if (d->graph) cudaGraphExecDestroy(d->graph);
   d->graph = nullptr;
-  cudaFree(d->fc); cudaFree(d->fidx); cudaFree(d->fnode);
+  cudaFree(d->fc); cudaFree(d->fidx); cudaFree(d->fnode); cudaFree(d->nbd);
   cudaFree(d->f); cudaFree(d->mv); cudaFree(d->solids); cudaFree(d->cls);
   cudaFree(d->nbm); cudaFree(d->red);
   if (d->own_stream) cudaStreamDestroy(d->own_stream);
@@ -348,17 +354,36 @@ lbx_status do_step(lbx_domain* d, int t, unsigned flags)
 
 // The launch arguments of the step at time t, as bytes (for comparing steps:
 // two steps with equal bytes launch identical work).
-static_assert(sizeof(StepArgs<double>) <= 512 && sizeof(StepArgs<float>) <= 512,
-              "graph keys hold one StepArgs in 512 bytes");
+constexpr size_t kKey = 640;   // one step's key: StepArgs bytes + face densities
+static_assert(sizeof(StepArgs<double>) + 8 * sizeof(double) <= kKey &&
+              sizeof(StepArgs<float>) + 8 * sizeof(double) <= kKey, "step key size");
 
+// The launch arguments of the step at time t, as bytes, followed by the
+// densities of every configured face (the stand-alone face kernels take
+// them as arguments): two steps with equal keys launch identical work.
 size_t step_key(const lbx_domain* d, int t, unsigned char* out)
 {
+  std::memset(out, 0, kKey);
+  size_t len;
   if (d->real_size == 8) {
     fill_args<double>(d, t, 0, *reinterpret_cast<StepArgs<double>*>(out));
-    return sizeof(StepArgs<double>);
+    len = sizeof(StepArgs<double>);
+  } else {
+    fill_args<float>(d, t, 0, *reinterpret_cast<StepArgs<float>*>(out));
+    len = sizeof(StepArgs<float>);
   }
-  fill_args<float>(d, t, 0, *reinterpret_cast<StepArgs<float>*>(out));
-  return sizeof(StepArgs<float>);
+  if (d->faces_active) {
+    const lbx_params& p = d->p;
+    double rho[8] = {0};
+    for (int s = 0; s < p.nsubs; ++s) {
+      if (p.pressure_n_in[s]) rho[4 * s + 0] = face_rho<double>(d, s, t, p.pressure_n_in[s], true, d->n_table);
+      if (p.pressure_n_out[s]) rho[4 * s + 1] = face_rho<double>(d, s, t, 0, false, d->n_table);
+      if (p.pressure_s_in[s]) rho[4 * s + 2] = face_rho<double>(d, s, t, p.pressure_s_in[s], true, d->s_table);
+      if (p.pressure_s_out[s]) rho[4 * s + 3] = face_rho<double>(d, s, t, 0, false, d->s_table);
+    }
+    std::memcpy(out + len, rho, sizeof rho);
+  }
+  return len + 8 * sizeof(double);
 }
 
 // Replay `pairs` AA pairs starting at odd time t from one captured pair.
@@ -366,10 +391,10 @@ size_t step_key(const lbx_domain* d, int t, unsigned char* out)
 // the first pair (checked by the caller) and the stream is capturable.
 lbx_status replay_pairs(lbx_domain* d, int t, int pairs)
 {
-  alignas(16) unsigned char key[2 * 512];
+  alignas(16) unsigned char key[2 * kKey];
   const size_t k1 = step_key(d, t, key);
-  const size_t k2 = step_key(d, t + 1, key + 512);
-  std::memmove(key + k1, key + 512, k2);
+  const size_t k2 = step_key(d, t + 1, key + kKey);
+  std::memmove(key + k1, key + kKey, k2);
   const size_t klen = k1 + k2;
   if (!d->graph || d->graph_stream != d->stream || d->graph_key_len != klen ||
       std::memcmp(d->graph_key, key, klen) != 0) {
@@ -501,6 +526,23 @@ lbx_status lbx_create(const lbx_params* p, const uint8_t* solids, lbx_domain** o
     CKD(cudaMemcpy(d->fidx, fidx.data(), d->N * sizeof(int), cudaMemcpyHostToDevice));
     CKD(cudaMemcpy(d->fnode, fnode.data(), fnode.size() * sizeof(int), cudaMemcpyHostToDevice));
     CKD(cudaMemsetAsync(d->fc, 0, (size_t)p->nsubs * d->Q * d->fluid * d->real_size, d->stream));
+    // neighbour-delta table for the odd step, kept only if every delta fits
+    if (d->fluid > 0) {
+      int* ovf = nullptr;
+      int hovf = 0;
+      CKD(cudaMalloc(&d->nbd, (size_t)(d->Q - 1) * d->fluid * sizeof(int16_t)));
+      CKD(cudaMalloc(&ovf, sizeof(int)));
+      CKD(cudaMemsetAsync(ovf, 0, sizeof(int), d->stream));
+      const unsigned nb = (unsigned)((d->fluid + 255) / 256);
+      if (d->Q == 9) build_nbd<9><<<nb, 256, 0, d->stream>>>(d->nbd, d->fidx, d->fnode, (int)d->fluid, p->LX, p->LY, p->LZ, ovf);
+      else build_nbd<19><<<nb, 256, 0, d->stream>>>(d->nbd, d->fidx, d->fnode, (int)d->fluid, p->LX, p->LY, p->LZ, ovf);
+      d->launches++;
+      CKD(cudaGetLastError());
+      CKD(cudaMemcpyAsync(&hovf, ovf, sizeof(int), cudaMemcpyDeviceToHost, d->stream));
+      CKD(cudaStreamSynchronize(d->stream));
+      cudaFree(ovf);
+      if (hovf) { cudaFree(d->nbd); d->nbd = nullptr; }
+    }
   }
   CKD(cudaMemsetAsync(d->f, 0, fbytes, d->stream));
   CKD(cudaMemsetAsync(d->mv, 0, mvbytes, d->stream));
@@ -639,12 +681,12 @@ lbx_status lbx_run(lbx_domain* d, int t0, int nsteps, int frame_rate)
   if (nsteps < 0) return fail(LBX_ERR_INVALID, "nsteps must be >= 0");
   const int tend = t0 + nsteps;
   int t = t0 + 1;
-  alignas(16) unsigned char k_odd[512], k_even[512], k[512];
+  alignas(16) unsigned char k_odd[kKey], k_even[kKey], k[kKey];
   while (t <= tend) {
     const bool frame = frame_rate > 0 && t % frame_rate == 0;
-    // a stretch of >= 8 frame-free steps starting on an odd time, with the
+    // a stretch of >= 4 frame-free steps starting on an odd time, with the
     // launch arguments of its first pair throughout, is replayed from a graph
-    if (!frame && (t % 2) == 1 && d->parity == 0 && d->stream != nullptr && tend - t + 1 >= 8) {
+    if (!frame && (t % 2) == 1 && d->parity == 0 && d->stream != nullptr && tend - t + 1 >= 4) {
       const size_t ko = step_key(d, t, k_odd), ke = step_key(d, t + 1, k_even);
       int pairs = 0;
       for (int u = t; u + 1 <= tend; u += 2) {
@@ -654,7 +696,7 @@ lbx_status lbx_run(lbx_domain* d, int t0, int nsteps, int frame_rate)
           break;
         ++pairs;
       }
-      if (pairs >= 4) {
+      if (pairs >= 2) {
         if (lbx_status st = replay_pairs(d, t, pairs)) return st;
         t += 2 * pairs;
         continue;

@@ -49,6 +49,17 @@ __host__ __device__ constexpr T wgt(int a) {
 
 enum Dir2 { DC = 0, DE, DW, DN, DS, DNE, DSW, DNW, DSE };
 
+// FP64 arithmetic without contraction: every product and sum is rounded as
+// written (the intrinsics are never fused into FMAs), so the FP64 kernels
+// compute the reference's C arithmetic, in its operation order, bit for bit.
+// FP32 uses plain operators and lets the compiler form FMAs.
+__device__ __forceinline__ double mul_(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double add_(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double sub_(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ float mul_(float a, float b) { return a * b; }
+__device__ __forceinline__ float add_(float a, float b) { return a + b; }
+__device__ __forceinline__ float sub_(float a, float b) { return a - b; }
+
 // A load the compiler may neither merge with an earlier load of the same
 // address nor hoist: used to re-read small index arrays (L1 hits) instead of
 // holding them in registers across the collision.
@@ -137,9 +148,9 @@ __device__ __forceinline__ void collide(const StepArgs<T>& A, int s, bool solute
     }
     T den = (MODEL == SHIFTED_INC) ? c.rhoA
           : (MODEL == PLAIN_COMP) ? rho : (c.rhoA + rho);
-    u[0] = m0 / den + c.tg[0];
-    u[1] = m1 / den + c.tg[1];
-    u[2] = (D == 3) ? (m2 / den + c.tg[2]) : T(0);
+    u[0] = add_(m0 / den, c.tg[0]);
+    u[1] = add_(m1 / den, c.tg[1]);
+    u[2] = (D == 3) ? add_(m2 / den, c.tg[2]) : T(0);
   }
   if (A.write_mv) {
     T* m = A.mv + (long long)s * (1 + D) * A.N;
@@ -153,19 +164,24 @@ __device__ __forceinline__ void collide(const StepArgs<T>& A, int s, bool solute
 #pragma unroll
     for (int a = 0; a < Q; ++a) {
       T cu = T(cx(a)) * u[0] + T(cy(a)) * u[1] + (D == 3 ? T(cz(a)) * u[2] : T(0));
-      d[a] = d[a] * c.omc + wgt<T, Q>(a) * rho * (T(1) + T(3) * cu) * c.itau;
+      d[a] = add_(mul_(d[a], c.omc),
+                  mul_(mul_(mul_(wgt<T, Q>(a), rho), add_(T(1), mul_(T(3), cu))), c.itau));
     }
   } else {
-    // BGK in shifted or plain form (src/lattice.c:2880-2919)
-    T usq = u[0] * u[0] + u[1] * u[1] + (D == 3 ? u[2] * u[2] : T(0));
+    // BGK in shifted or plain form (src/lattice.c:2880-2919):
+    // d (1 - 1/tau) + w drho / tau + w rq (3 cu + 4.5 cu^2 - 1.5 u^2) / tau
+    T usq = add_(mul_(u[0], u[0]), mul_(u[1], u[1]));
+    if (D == 3) usq = add_(usq, mul_(u[2], u[2]));
     T rq = (MODEL == SHIFTED_INC) ? c.rhoA
          : (MODEL == PLAIN_COMP) ? rho : (c.rhoA + rho);
 #pragma unroll
     for (int a = 0; a < Q; ++a) {
+      // c.u: products by -1, 0, 1 are exact, so contraction cannot change it
       T cu = T(cx(a)) * u[0] + T(cy(a)) * u[1] + (D == 3 ? T(cz(a)) * u[2] : T(0));
       T w = wgt<T, Q>(a);
-      d[a] = d[a] * c.omc + w * rho * c.itau
-           + w * rq * (T(3) * cu + T(4.5) * cu * cu - T(1.5) * usq) * c.itau;
+      T poly = sub_(add_(mul_(T(3), cu), mul_(mul_(T(4.5), cu), cu)), mul_(T(1.5), usq));
+      d[a] = add_(add_(mul_(d[a], c.omc), mul_(mul_(w, rho), c.itau)),
+                  mul_(mul_(mul_(w, rq), poly), c.itau));
     }
   }
 }
@@ -199,9 +215,9 @@ __device__ __forceinline__ void face_north(int kind, T rho_bc, T rhoA, T drho, b
   if (kind == FACE_PRESSURE) {
     const T X = face_balance<T>(d[DC] + d[DE] + d[DW] + d[DN] + d[DN] + d[DNE] + d[DNE]
                                 + d[DNW] + d[DNW], rho_bc, rhoA, drho, shifted);
-    d[DS] = d[DN] - T(2. / 3.) * X;
-    d[DSW] = d[DNE] + T(0.5) * (d[DE] - d[DW]) - T(1. / 6.) * X;
-    d[DSE] = d[DNW] + T(0.5) * (d[DW] - d[DE]) - T(1. / 6.) * X;
+    d[DS] = sub_(d[DN], mul_(T(2. / 3.), X));
+    d[DSW] = sub_(add_(d[DNE], mul_(T(0.5), d[DE] - d[DW])), mul_(T(1. / 6.), X));
+    d[DSE] = sub_(add_(d[DNW], mul_(T(0.5), d[DW] - d[DE])), mul_(T(1. / 6.), X));
   } else if (kind == FACE_ZEROGRAD) {
     T X = (d[DN] + d[DNE] + d[DNW]) / (wgt<T, 9>(DS) + wgt<T, 9>(DSW) + wgt<T, 9>(DSE));
     d[DS] = wgt<T, 9>(DS) * X;
@@ -218,9 +234,9 @@ __device__ __forceinline__ void face_south(int kind, T rho_bc, T rhoA, T drho, b
     // south balance is the negated north one: -(sum) + rho_bc - rho_A
     const T X = -face_balance<T>(d[DC] + d[DE] + d[DW] + d[DS] + d[DS] + d[DSE] + d[DSE]
                                  + d[DSW] + d[DSW], rho_bc, rhoA, drho, shifted);
-    d[DN] = d[DS] + T(2. / 3.) * X;
-    d[DNE] = d[DSW] + T(0.5) * (d[DW] - d[DE]) + T(1. / 6.) * X;
-    d[DNW] = d[DSE] + T(0.5) * (d[DE] - d[DW]) + T(1. / 6.) * X;
+    d[DN] = add_(d[DS], mul_(T(2. / 3.), X));
+    d[DNE] = add_(add_(d[DSW], mul_(T(0.5), d[DW] - d[DE])), mul_(T(1. / 6.), X));
+    d[DNW] = add_(add_(d[DSE], mul_(T(0.5), d[DE] - d[DW])), mul_(T(1. / 6.), X));
   } else if (kind == FACE_ZEROGRAD) {
     T X = (d[DS] + d[DSW] + d[DSE]) / (wgt<T, 9>(DN) + wgt<T, 9>(DNE) + wgt<T, 9>(DNW));
     d[DN] = wgt<T, 9>(DN) * X;
@@ -324,11 +340,59 @@ struct CompactArgs {
   StepArgs<T> s;          // f = compact populations; N = dense node count
   const int* fidx;        // [N]
   const int* fnode;       // [F]
+  const int16_t* nbd;     // [Q-1][F] neighbour deltas (NB == 1), see build_nbd
   int F;
   int faces;              // 2D: fused face boundaries configured
 };
 
-template <typename T, int Q, int NS, int MODEL, bool ODD>
+// Neighbour table of the compact layout: for fluid node m and direction
+// a >= 1, nbd[a-1][m] = idx(n + c_a) - m, or kNbdSolid if that node is
+// solid.  Built once per domain when every delta fits in 16 bits; the odd
+// step then streams 36 B of coalesced deltas per node instead of walking
+// fnode -> coordinates -> fidx (three dependent round trips).
+constexpr int16_t kNbdSolid = -32768;
+
+__device__ __forceinline__ int ld_reload16(const int16_t* p)
+{
+  short v;
+  asm volatile("ld.global.nc.s16 %0, [%1];" : "=h"(v) : "l"(p));
+  return (int)v;
+}
+
+template <int Q>
+__global__ void build_nbd(int16_t* nbd, const int* fidx, const int* fnode, int F,
+                          int LX, int LY, int LZ, int* overflow)
+{
+  constexpr int D = (Q == 9) ? 2 : 3;
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= F) return;
+  const int plane = LX * LY;
+  const int n = fnode[m];
+  const int k = n / plane, r = n - k * plane, j = r / LX, i = r - j * LX;
+  const int xm = (i == 0) ? LX - 1 : -1, xp = (i == LX - 1) ? 1 - LX : 1;
+  const int ym = (j == 0) ? plane - LX : -LX, yp = (j == LY - 1) ? LX - plane : LX;
+  int zm = 0, zp = 0;
+  if (D == 3) {
+    const int tot = plane * LZ;
+    zm = (k == 0) ? tot - plane : -plane;
+    zp = (k == LZ - 1) ? plane - tot : plane;
+  }
+#pragma unroll
+  for (int a = 1; a < Q; ++a) {
+    const int o = (cx(a) < 0 ? xm : (cx(a) > 0 ? xp : 0)) + (cy(a) < 0 ? ym : (cy(a) > 0 ? yp : 0))
+                + (cz(a) < 0 ? zm : (cz(a) > 0 ? zp : 0));
+    const int q = fidx[n + o];
+    int16_t v = kNbdSolid;
+    if (q >= 0) {
+      const int dlt = q - m;
+      if (dlt < -32767 || dlt > 32767) atomicOr(overflow, 1);
+      else v = (int16_t)dlt;
+    }
+    nbd[(size_t)(a - 1) * F + m] = v;
+  }
+}
+
+template <typename T, int Q, int NS, int MODEL, bool ODD, int NB>
 __global__ void __launch_bounds__(256)
 aa_step_compact(CompactArgs<T> C)
 {
@@ -341,15 +405,15 @@ aa_step_compact(CompactArgs<T> C)
   const int plane = LX * LY;
   const bool faces = (Q == 9) && C.faces;
   int n = 0, j = 0;
-  // dense offsets to the neighbours along each axis (odd step only)
+  // dense offsets to the neighbours along each axis (odd step, no table)
   int xm = 0, xp = 0, ym = 0, yp = 0, zm = 0, zp = 0;
-  if (ODD || A.write_mv || faces) {
+  if ((ODD && NB == 0) || A.write_mv || faces) {
     n = C.fnode[m];
     const int k = n / plane;
     const int r = n - k * plane;
     j = r / LX;
     const int i = r - j * LX;
-    if (ODD) {
+    if (ODD && NB == 0) {
       xm = (i == 0) ? LX - 1 : -1; xp = (i == LX - 1) ? 1 - LX : 1;
       ym = (j == 0) ? plane - LX : -LX; yp = (j == LY - 1) ? LX - plane : LX;
       if (D == 3) {
@@ -365,6 +429,16 @@ aa_step_compact(CompactArgs<T> C)
          + (cz(a) < 0 ? zm : (cz(a) > 0 ? zp : 0));
   };
   const int* const fidx_n = C.fidx + n;
+  const int16_t* const nbd_m = C.nbd + m;
+  // compact index of neighbour n + c_a (a >= 1), -1 if solid
+  auto nb_pull = [&](int a) -> int {
+    if (NB) { const int v = nbd_m[(size_t)(a - 1) * F]; return v == kNbdSolid ? -1 : m + v; }
+    return fidx_n[off(a)];
+  };
+  auto nb_push = [&](int a) -> int {
+    if (NB) { const int v = ld_reload16(nbd_m + (size_t)(a - 1) * F); return v == kNbdSolid ? -1 : m + v; }
+    return ld_reload(fidx_n + off(a));
+  };
   T u[3] = {T(0), T(0), T(0)};
 #pragma unroll
   for (int s = 0; s < NS; ++s) {
@@ -376,7 +450,7 @@ aa_step_compact(CompactArgs<T> C)
       // pull: d_a = f[a][idx(n - c_a)], or own f[opp a] behind a solid
 #pragma unroll
       for (int a = 0; a < Q; ++a) {
-        const int up = (a == 0) ? m : fidx_n[off(opp(a))];
+        const int up = (a == 0) ? m : nb_pull(opp(a));
         d[a] = (up >= 0) ? fs[a * F + up] : fs[opp(a) * F + m];
       }
     } else {
@@ -399,7 +473,7 @@ aa_step_compact(CompactArgs<T> C)
       if (D == 3) { zm = opaque(zm); zp = opaque(zp); }
 #pragma unroll
       for (int a = 0; a < Q; ++a) {
-        const int dn = (a == 0) ? m : ld_reload(fidx_n + off(a));
+        const int dn = (a == 0) ? m : nb_push(a);
         if (dn >= 0) fs[opp(a) * F + dn] = d[a];
         else fs[a * F + m] = d[a];
       }
@@ -562,15 +636,17 @@ __global__ void init_feq(T* fs, const T* rho, const T* ux, const T* uy,
   const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= N) return;
   const T r = rho[n], x = ux[n], y = uy[n], z = uz ? uz[n] : T(0);
-  const T usq = x * x + y * y + z * z;
+  const T usq = add_(add_(mul_(x, x), mul_(y, y)), mul_(z, z));
 #pragma unroll
   for (int a = 0; a < Q; ++a) {
     const T cu = T(cx(a)) * x + T(cy(a)) * y + T(cz(a)) * z;
-    const T w = wgt<T, Q>(a);
+    const T wr = mul_(wgt<T, Q>(a), r);
+    const T q = add_(mul_(T(3), cu), mul_(mul_(T(4.5), cu), cu));   // 3 cu + 4.5 cu^2
     T v;
-    if (a == 0) v = shifted ? w * r * (T(-1.5) * usq) : w * r * (T(1) - T(1.5) * usq);
-    else if (shifted) v = w * r * (T(3) * cu + T(4.5) * cu * cu - T(1.5) * usq);
-    else v = w * r * (T(1) + T(3) * cu + T(4.5) * cu * cu - T(1.5) * usq);
+    if (a == 0) v = shifted ? mul_(wr, mul_(T(-1.5), usq)) : mul_(wr, sub_(T(1), mul_(T(1.5), usq)));
+    else if (shifted) v = mul_(wr, sub_(q, mul_(T(1.5), usq)));
+    else v = mul_(wr, sub_(add_(add_(T(1), mul_(T(3), cu)), mul_(mul_(T(4.5), cu), cu)),
+                           mul_(T(1.5), usq)));
     fs[(long long)a * N + n] = v;
   }
 }

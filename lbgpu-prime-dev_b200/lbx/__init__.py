@@ -79,6 +79,20 @@ _SIGNATURES = {
     "lbx_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_longlong), C.POINTER(C.c_int),
                            C.POINTER(C.c_int)]),
     "lbx_launch_count": (C.c_longlong, [C.c_void_p]),
+    "lbx_batch_create": (C.c_int, [C.c_int, C.POINTER(_CParams), C.c_void_p,
+                                   C.POINTER(C.c_void_p)]),
+    "lbx_batch_destroy": (C.c_int, [C.c_void_p]),
+    "lbx_batch_upload_f": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    "lbx_batch_download_f": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    "lbx_batch_download_mv": (C.c_int, [C.c_void_p, C.c_int] + [C.c_void_p] * 4),
+    "lbx_batch_init_equilibrium": (C.c_int, [C.c_void_p, C.c_int] + [C.c_void_p] * 4),
+    "lbx_batch_run": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int]),
+    "lbx_batch_autotune": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int),
+                                     C.POINTER(C.c_int)]),
+    "lbx_batch_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "lbx_batch_sync": (C.c_int, [C.c_void_p]),
+    "lbx_batch_reduce": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(_CReductions)]),
+    "lbx_batch_launch_count": (C.c_longlong, [C.c_void_p]),
     "lbx_last_error": (C.c_char_p, []),
 }
 

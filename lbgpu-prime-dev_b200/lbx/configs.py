@@ -17,6 +17,12 @@ cfg2: D3Q19 BGK 256^3, tau = 0.8, overlapping spheres r = 6 to porosity 0.4,
       permeability k = nu <u_x> / gx of each with the relative error of the
       FP32 run against the FP64 run.
 
+cfg4: 512 independent D3Q19 samples, FP32 shifted, cubic edges drawn from
+      U{32..96}, tau ~ U[0.6, 1.2], porosity ~ U[0.3, 0.7], sphere radius
+      ~ U{3..6} (seed base + i), gx = 1e-6, periodic.  One batch; reports the
+      aggregate MLUPS of FUSED, PERSISTENT and SEQUENTIAL runs, the mode the
+      autotuner picks, and the per-sample permeabilities.
+
 Each run prints one JSON line.  Times come from CUDA events on the stream
 the kernels run on.
 """
@@ -121,14 +127,88 @@ def run_cfg2(steps: int = 10000, n: int = 256) -> list:
     return out
 
 
+def cfg4_samples(nsamples: int = 512, seed: int = 4000):
+    rng = np.random.default_rng(seed)
+    params, masks = [], []
+    for i in range(nsamples):
+        n = int(rng.integers(32, 97))
+        tau = float(rng.uniform(0.6, 1.2))
+        por = float(rng.uniform(0.3, 0.7))
+        r = int(rng.integers(3, 7))
+        masks.append(geometry.sphere_pack(n, n, n, r, por, seed + 1 + i))
+        params.append(Params(dims=3, LX=n, LY=n, LZ=n, precision=4, tau=(tau, 1.0),
+                             gaccel=(1e-6, 0, 0, 0, 0, 0)))
+    return params, masks
+
+
+def run_cfg4(nsamples: int = 512, steps: int = 200, perm_steps: int = 0) -> list:
+    import torch
+    from .batch import Batch
+    params, masks = cfg4_samples(nsamples)
+    nodes = sum(m.size for m in masks)
+    fluid = sum(int((m != 1).sum()) for m in masks)
+    out = []
+    with Batch(params, masks) as b:
+        s = torch.cuda.Stream()
+        b.set_stream(s.cuda_stream)
+        times = {}
+        for mode in ("fused", "persistent", "sequential"):
+            for i in range(nsamples):
+                b.init_equilibrium(i, 1.0)
+            b.run(0, 4, 0, mode=mode)                    # warm-up (graph capture)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(s)
+            b.run(4, steps, 0, mode=mode)
+            e1.record(s)
+            s.synchronize()
+            times[mode] = e0.elapsed_time(e1) / 1e3
+        for i in range(nsamples):
+            b.init_equilibrium(i, 1.0)
+        tuned = b.autotune(6)
+        for mode, secs in times.items():
+            out.append({"config": "cfg4", "mode": mode, "samples": nsamples, "steps": steps,
+                        "nodes": nodes, "fluid_nodes": fluid,
+                        "mlups": nodes * steps / secs / 1e6,
+                        "mflups": fluid * steps / secs / 1e6, "seconds": secs,
+                        "speedup_vs_sequential": times["sequential"] / secs})
+        out.append({"config": "cfg4", "autotuned": {"mode": tuned[0], "block": tuned[1]}})
+        if perm_steps:
+            for i in range(nsamples):
+                b.init_equilibrium(i, 1.0)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(s)
+            b.run(0, perm_steps, perm_steps)
+            e1.record(s)
+            s.synchronize()
+            secs = e0.elapsed_time(e1) / 1e3
+            ks = []
+            for i, p in enumerate(params):
+                r = b.reduce(i)
+                nu = (p.tau[0] - 0.5) / 3.0
+                ks.append(nu * (r["u_sum"][0] / p.NN) / 1e-6)
+            ks = np.array(ks)
+            out.append({"config": "cfg4", "run": "permeability", "steps": perm_steps,
+                        "mlups": nodes * perm_steps / secs / 1e6, "seconds": secs,
+                        "k_min": float(ks.min()), "k_median": float(np.median(ks)),
+                        "k_max": float(ks.max()), "k_first8": [float(x) for x in ks[:8]]})
+    return out
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
-    ap.add_argument("config", choices=["cfg1", "cfg2"])
+    ap.add_argument("config", choices=["cfg1", "cfg2", "cfg4"])
     ap.add_argument("--steps", type=int, default=None)
     ap.add_argument("--edge", type=int, default=256)
+    ap.add_argument("--samples", type=int, default=512)
+    ap.add_argument("--perm-steps", type=int, default=0)
     a = ap.parse_args(argv)
     if a.config == "cfg1":
         print(json.dumps(run_cfg1(a.steps or 2000)))
+    elif a.config == "cfg4":
+        for line in run_cfg4(a.samples, a.steps or 200, a.perm_steps):
+            print(json.dumps(line))
     else:
         for line in run_cfg2(a.steps or 10000, a.edge):
             print(json.dumps(line))

@@ -1,0 +1,66 @@
+"""Batched lattices (GPU): every sample of a batch must evolve exactly as the
+same lattice run alone, in every batch mode."""
+import numpy as np
+import pytest
+
+import lbx
+import pyoracle as po
+from lbx import geometry
+from lbx.batch import Batch
+from _golden import rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+def make_samples(n, seed, prec=4, sizes=(12, 30)):
+    rng = np.random.default_rng(seed)
+    params, masks = [], []
+    for i in range(n):
+        L = [int(x) for x in rng.integers(sizes[0], sizes[1], size=3)]
+        tau = float(rng.uniform(0.6, 1.2))
+        por = float(rng.uniform(0.3, 0.7))
+        r = int(rng.integers(2, 5))
+        masks.append(geometry.sphere_pack(L[0], L[1], L[2], r, por, seed * 1000 + i))
+        params.append(lbx.Params(dims=3, LX=L[0], LY=L[1], LZ=L[2], precision=prec,
+                                 tau=(tau, 1.0), gaccel=(1e-5, 0, 0, 0, 0, 0)))
+    return params, masks
+
+
+@pytest.mark.parametrize("mode", ["fused", "persistent", "sequential"])
+@pytest.mark.parametrize("prec", [8, 4])
+def test_batch_matches_oracle_per_sample(mode, prec):
+    params, masks = make_samples(7, seed=3, prec=prec)
+    rng = np.random.default_rng(1)
+    f0 = [(rng.standard_normal((19, p.NN)) * 1e-4).astype(p.dtype) for p in params]
+    with Batch(params, masks) as b:
+        for i in range(len(params)):
+            b.upload_f(i, f0[i])
+        b.run(0, 23, 23, mode=mode)
+        b.sync()
+        out = [(b.download_f(i), b.download_mv(i)) for i in range(len(params))]
+    tol = 1e-12 if prec == 8 else 1e-5
+    for i, p in enumerate(params):
+        q = po.Params(dims=3, LX=p.LX, LY=p.LY, LZ=p.LZ, tau=tuple(p.tau),
+                      gaccel=tuple(p.gaccel))
+        fo, mvo = po.run_oracle(q, f0[i].reshape(1, 19, -1).copy(), masks[i], 0, 23, 23)
+        fl = masks[i] != 1
+        assert rel_err(out[i][0], fo[0]) <= tol, (i, rel_err(out[i][0], fo[0]))
+        for c in range(4):
+            e = rel_err(out[i][1][c], mvo[0, c], fl)
+            assert e <= (tol if prec == 8 else 2e-5), (i, c, e)
+
+
+def test_batch_autotune_keeps_state_and_picks_a_mode():
+    params, masks = make_samples(5, seed=9, prec=4)
+    with Batch(params, masks) as b:
+        for i in range(5):
+            b.init_equilibrium(i, 1.0)
+        before = [b.download_f(i) for i in range(5)]
+        mode, bs = b.autotune(4)
+        assert mode in ("fused", "persistent") and bs in (128, 256, 512)
+        after = [b.download_f(i) for i in range(5)]
+        for x, y in zip(before, after):
+            assert np.array_equal(x, y)
+        b.run(0, 10, 10)
+        r = b.reduce(0)
+        assert r["fluid_nodes"] == int((masks[0] != 1).sum())
