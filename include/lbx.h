@@ -76,6 +76,20 @@ typedef struct lbx_params {
   const double* pressure_s_table; int pressure_s_len;
   int device;               /* CUDA device ordinal                         */
   int layout;               /* LBX_LAYOUT_*: device storage of populations */
+  /* 3D faces: top = plane k=LZ-1, bottom = plane k=0.  The reference reads
+   * these flags (src/params.h:191-198, :282-307) but has no device code for
+   * them; here they are the 2D rules carried to the z faces: Zou-He density
+   * with zero tangential velocity (the D3Q19 reconstruction of the
+   * reference's CPU top/bottom code, src/bcs.c:596-870), the solute's
+   * zero-gradient rule, and a constant solute concentration that sets the
+   * face's unknown populations to w_a X with sum_a g_a = rho_sigma_in.
+   * Applied before each step in the order t_in, t_out, b_in, b_out (per
+   * substance), then constcon t/b, zeroconcgrad t/b; need LZ >= 3. */
+  int pressure_t_in[2], pressure_b_in[2];    /* 1 = rho_in                 */
+  int pressure_t_out[2], pressure_b_out[2];  /* 1 = rho_out                */
+  int constcon_t_in, constcon_b_in;          /* solute C = rho_sigma_in    */
+  int zeroconcgrad_t, zeroconcgrad_b;        /* solute zero gradient       */
+  double rho_sigma_in;
 } lbx_params;
 
 /* Device storage of the populations.  DENSE keeps the reference's
@@ -197,6 +211,23 @@ lbx_status lbx_info(lbx_domain* d, long long* fluid_nodes, int* faces_fused,
 
 /* Number of this library's kernels launched on the domain so far. */
 long long lbx_launch_count(lbx_domain* d);
+
+/* Breakthrough record (two-substance runs): from the next step on, every
+ * step appends the mean solute concentration C over the fluid nodes of
+ * `plane` -- the plane k = plane in 3D, the row j = plane in 2D -- summed in
+ * FP64 on the device (NaN for a step with the solute inactive).  Holds up
+ * to `capacity` steps; restarting clears it.  No counterpart in the
+ * reference, whose concentration output is the per-frame dump of
+ * src/lbio.c:2507-2562. */
+lbx_status lbx_btc_start(lbx_domain* d, int plane, int capacity);
+
+/* Copy up to `max` recorded values (oldest first) into `out` and the number
+ * of steps recorded since lbx_btc_start into `*count` (which may exceed
+ * capacity; later steps are then not stored). Synchronizes the stream. */
+lbx_status lbx_btc_read(lbx_domain* d, double* out, int max, long long* count);
+
+/* Stop recording and release the record. */
+lbx_status lbx_btc_stop(lbx_domain* d);
 
 /* ---- batches of independent lattices ---------------------------------------
  * Many samples of uneven size (same dims, precision and collision model;

@@ -68,10 +68,10 @@ struct lbx_domain {
   long long N = 0;
   size_t real_size = 0;
   void* f = nullptr;          // [nsubs][Q][N] dense (the exchange format)
-  void* fc = nullptr;         // [nsubs][Q][F] compact layout
+  void* fc = nullptr;         // [nsubs][Q][P] compact layout
   int* fidx = nullptr;        // [N] dense -> compact (-1 solid)
   int* fnode = nullptr;       // [F] compact -> dense
-  int16_t* nbd = nullptr;     // [Q-1][F] neighbour deltas, if they fit in 16 bits
+  long long P = 0;            // compact plane stride: fluid rounded up to 32
   int layout = LBX_LAYOUT_DENSE;
   bool dense_stale = false;   // compact state newer than the dense array
   void* mv = nullptr;         // [nsubs][1+D][N]
@@ -86,6 +86,15 @@ struct lbx_domain {
   long long fluid = 0;
   bool faces_active = false;  // any 2D face boundary configured
   bool faces_fused = false;   // fused into the step kernels
+  bool faces3_active = false; // any 3D z-face boundary configured
+  std::vector<long long> plane_fluid;  // fluid nodes per plane (k in 3D, j in 2D)
+  // breakthrough record (lbx_btc_*)
+  double* btc_vals = nullptr;  // C of the plane's nodes this step
+  double* btc_rec = nullptr;   // [btc_cap] means
+  int* btc_slot = nullptr;     // steps recorded
+  int btc_cap = 0;
+  int btc_lo = 0, btc_hi = 0;  // node (dense) or slot (compact) range
+  int btc_plane = 0;
   int parity = 0;             // 0: natural order (next step odd); 1: swapped
   long long launches = 0;
   // graph replay of frame-free, time-invariant runs: one captured AA pair
@@ -142,6 +151,11 @@ void fill_args(const lbx_domain* d, int t, unsigned flags, StepArgs<T>& A)
   A.sink1 = (T)(1.0 - (T)p.sink * (T)p.tau[1]);
   A.write_mv = (flags & LBX_WRITE_MV) ? 1 : 0;
   A.solute_on = (t >= p.sigma_t_on && t <= p.sigma_t_off) ? 1 : 0;
+  if (d->btc_vals) {
+    A.btc = d->btc_vals;
+    A.btc_lo = d->btc_lo;
+    A.btc_hi = d->btc_hi;
+  }
   if (d->faces_fused) {
     for (int s = 0; s < p.nsubs; ++s) {
       // last active boundary on each face wins (see FaceKind)
@@ -175,17 +189,13 @@ void launch_aa(lbx_domain* d, const StepArgs<T>& A, bool odd)
     C.s = A;
     C.fidx = d->fidx;
     C.fnode = d->fnode;
-    C.nbd = d->nbd;
     C.F = (int)d->fluid;
+    C.P = (int)d->P;
     C.faces = d->faces_fused ? 1 : 0;
     const unsigned blocks = (unsigned)((d->fluid + 255) / 256);
     if (blocks == 0) return;
-    if (odd) {
-      if (d->nbd) aa_step_compact<T, Q, NS, MODEL, true, 1><<<blocks, 256, 0, d->stream>>>(C);
-      else aa_step_compact<T, Q, NS, MODEL, true, 0><<<blocks, 256, 0, d->stream>>>(C);
-    } else {
-      aa_step_compact<T, Q, NS, MODEL, false, 0><<<blocks, 256, 0, d->stream>>>(C);
-    }
+    if (odd) aa_step_compact<T, Q, NS, MODEL, true><<<blocks, 256, 0, d->stream>>>(C);
+    else aa_step_compact<T, Q, NS, MODEL, false><<<blocks, 256, 0, d->stream>>>(C);
     d->launches++;
     return;
   }
@@ -214,7 +224,7 @@ void launch_faces_exact(lbx_domain* d, int t, bool second)
   dim3 block(128), grid((p.LX + 127) / 128);
   for (int s = 0; s < p.nsubs; ++s) {
     const bool compact = d->layout == LBX_LAYOUT_COMPACT;
-    T* fs = compact ? (T*)d->fc + (long long)s * d->Q * d->fluid
+    T* fs = compact ? (T*)d->fc + (long long)s * d->Q * d->P
                     : (T*)d->f + (long long)s * d->Q * d->N;
     const int shifted = p.accurate && !(s == 1 && p.nsubs == 2);
     const T rhoA = (T)p.rho_A[s];
@@ -222,7 +232,7 @@ void launch_faces_exact(lbx_domain* d, int t, bool second)
       const T drho = (T)((double)rho - (double)rhoA);
       if (compact)
         face_row_compact<T><<<grid, block, 0, d->stream>>>(fs, d->fidx, p.LX, p.LY,
-                                                           (int)d->fluid, north, kind,
+                                                           (int)d->P, north, kind,
                                                            second ? 1 : 0, rho, rhoA,
                                                            drho, shifted);
       else
@@ -240,11 +250,83 @@ void launch_faces_exact(lbx_domain* d, int t, bool second)
   }
 }
 
+// The z-face operations of step t in their fixed order (t_in, t_out, b_in,
+// b_out per substance, then the solute's constcon t/b and zeroconcgrad t/b),
+// as (top, kind, substance, drho) tuples; `run` is called for each.
+template <typename T, typename F>
+void for_each_face3(const lbx_domain* d, int t, F&& run)
+{
+  const lbx_params& p = d->p;
+  for (int s = 0; s < p.nsubs; ++s) {
+    const bool shifted = p.accurate && !(s == 1 && p.nsubs == 2);
+    const double rA = shifted ? (double)(T)p.rho_A[s] : 0.0;
+    auto dr = [&](bool in) {
+      return (T)((double)face_rho<T>(d, s, t, in ? 1 : 0, in, d->n_table) - rA);
+    };
+    if (p.pressure_t_in[s]) run(1, FACE_PRESSURE, s, dr(true));
+    if (p.pressure_t_out[s]) run(1, FACE_PRESSURE, s, dr(false));
+    if (p.pressure_b_in[s]) run(0, FACE_PRESSURE, s, dr(true));
+    if (p.pressure_b_out[s]) run(0, FACE_PRESSURE, s, dr(false));
+    if (s == 1 && p.nsubs == 2) {
+      if (p.constcon_t_in) run(1, FACE_CONSTCON, s, T(0));
+      if (p.constcon_b_in) run(0, FACE_CONSTCON, s, T(0));
+      if (p.zeroconcgrad_t) run(1, FACE_ZEROGRAD, s, T(0));
+      if (p.zeroconcgrad_b) run(0, FACE_ZEROGRAD, s, T(0));
+    }
+  }
+}
+
+int count_faces3(const lbx_domain* d)
+{
+  int n = 0;
+  if (d->faces3_active)
+    for_each_face3<double>(d, 1, [&](int, int, int, double) { ++n; });
+  return n;
+}
+
+template <typename T>
+void launch_faces3(lbx_domain* d, int t, bool second)
+{
+  const lbx_params& p = d->p;
+  const bool compact = d->layout == LBX_LAYOUT_COMPACT;
+  const long long stride = compact ? d->P : d->N;
+  const T conc = (T)p.rho_sigma_in;
+  dim3 block(128), grid((p.LX + 127) / 128, p.LY);
+  for_each_face3<T>(d, t, [&](int top, int kind, int s, T drho) {
+    T* fs = (T*)(compact ? d->fc : d->f) + (long long)s * d->Q * stride;
+    if (compact)
+      face_plane<T, true><<<grid, block, 0, d->stream>>>(fs, nullptr, d->fidx, p.LX, p.LY, p.LZ,
+                                                          stride, top, kind, second ? 1 : 0,
+                                                          drho, conc);
+    else
+      face_plane<T, false><<<grid, block, 0, d->stream>>>(fs, d->solids, nullptr, p.LX, p.LY,
+                                                           p.LZ, stride, top, kind,
+                                                           second ? 1 : 0, drho, conc);
+    d->launches++;
+  });
+}
+
+// Kernels one step launches (faces, the step, the breakthrough reduction).
+long long launches_per_step(const lbx_domain* d, bool solute_on)
+{
+  long long n = 1 + count_faces3(d);
+  if (d->faces_active && !d->faces_fused) {
+    for (int s = 0; s < d->p.nsubs; ++s)
+      n += (d->p.pressure_n_in[s] != 0) + (d->p.pressure_n_out[s] != 0) +
+           (d->p.pressure_s_in[s] != 0) + (d->p.pressure_s_out[s] != 0);
+    if (d->p.nsubs == 2) n += (d->p.zeroconcgrad_n != 0) + (d->p.zeroconcgrad_s != 0);
+  }
+  (void)solute_on;
+  if (d->btc_vals) n += 1;
+  return n;
+}
+
 template <typename T>
 lbx_status step_t(lbx_domain* d, int t, unsigned flags)
 {
   const bool odd = (t % 2) != 0;
   if (d->faces_active && !d->faces_fused) launch_faces_exact<T>(d, t, !odd);
+  if (d->faces3_active) launch_faces3<T>(d, t, !odd);
   StepArgs<T> A = make_args<T>(d, t, flags);
   if (d->Q == 9) {
     if (d->p.nsubs == 1) launch_model<T, 9, 1>(d, A, odd);
@@ -252,6 +334,14 @@ lbx_status step_t(lbx_domain* d, int t, unsigned flags)
   } else {
     if (d->p.nsubs == 1) launch_model<T, 19, 1>(d, A, odd);
     else launch_model<T, 19, 2>(d, A, odd);
+  }
+  if (d->btc_vals) {
+    const bool compact = d->layout == LBX_LAYOUT_COMPACT;
+    btc_reduce<<<1, kBtcThreads, 0, d->stream>>>(
+        d->btc_vals, d->btc_hi - d->btc_lo, compact ? nullptr : d->solids + d->btc_lo,
+        (double)d->plane_fluid[d->btc_plane], A.solute_on, d->btc_rec, d->btc_slot,
+        d->btc_cap);
+    d->launches++;
   }
   CK(cudaGetLastError());
   return LBX_OK;
@@ -285,7 +375,16 @@ lbx_status check_params(const lbx_params* p)
              p->pressure_s_out[s];
   faces |= p->nsubs == 2 && (p->zeroconcgrad_n || p->zeroconcgrad_s);
   if (faces && p->dims != 2)
-    return fail(LBX_ERR_INVALID, "face boundaries exist for 2D runs only");
+    return fail(LBX_ERR_INVALID, "north/south face boundaries exist for 2D runs only");
+  bool faces3 = false;
+  for (int s = 0; s < p->nsubs; ++s)
+    faces3 |= p->pressure_t_in[s] || p->pressure_b_in[s] || p->pressure_t_out[s] ||
+              p->pressure_b_out[s];
+  faces3 |= p->nsubs == 2 && (p->constcon_t_in || p->constcon_b_in || p->zeroconcgrad_t ||
+                              p->zeroconcgrad_b);
+  if (faces3 && p->dims != 3)
+    return fail(LBX_ERR_INVALID, "top/bottom face boundaries exist for 3D runs only");
+  if (faces3 && p->LZ < 3) return fail(LBX_ERR_INVALID, "top/bottom faces need LZ >= 3");
   if (faces && p->LY < 3) return fail(LBX_ERR_INVALID, "face boundaries need LY >= 3");
   for (int s = 0; s < p->nsubs; ++s) {
     if (p->pressure_n_in[s] == 2 && (!p->pressure_n_table || p->pressure_n_len < 1))
@@ -324,9 +423,10 @@ void release(lbx_domain* d)
 {
   if (d->graph) cudaGraphExecDestroy(d->graph);
   d->graph = nullptr;
-  cudaFree(d->fc); cudaFree(d->fidx); cudaFree(d->fnode); cudaFree(d->nbd);
+  cudaFree(d->fc); cudaFree(d->fidx); cudaFree(d->fnode);
   cudaFree(d->f); cudaFree(d->mv); cudaFree(d->solids); cudaFree(d->cls);
   cudaFree(d->nbm); cudaFree(d->red);
+  cudaFree(d->btc_vals); cudaFree(d->btc_rec); cudaFree(d->btc_slot);
   if (d->own_stream) cudaStreamDestroy(d->own_stream);
 }
 
@@ -355,8 +455,9 @@ lbx_status do_step(lbx_domain* d, int t, unsigned flags)
 // The launch arguments of the step at time t, as bytes (for comparing steps:
 // two steps with equal bytes launch identical work).
 constexpr size_t kKey = 640;   // one step's key: StepArgs bytes + face densities
-static_assert(sizeof(StepArgs<double>) + 8 * sizeof(double) <= kKey &&
-              sizeof(StepArgs<float>) + 8 * sizeof(double) <= kKey, "step key size");
+constexpr int kKeyFaces = 16;  // 2D: 4 per substance; 3D: 4 per substance
+static_assert(sizeof(StepArgs<double>) + kKeyFaces * sizeof(double) <= kKey &&
+              sizeof(StepArgs<float>) + kKeyFaces * sizeof(double) <= kKey, "step key size");
 
 // The launch arguments of the step at time t, as bytes, followed by the
 // densities of every configured face (the stand-alone face kernels take
@@ -372,18 +473,24 @@ size_t step_key(const lbx_domain* d, int t, unsigned char* out)
     fill_args<float>(d, t, 0, *reinterpret_cast<StepArgs<float>*>(out));
     len = sizeof(StepArgs<float>);
   }
+  double rho[kKeyFaces] = {0};
+  const lbx_params& p = d->p;
   if (d->faces_active) {
-    const lbx_params& p = d->p;
-    double rho[8] = {0};
     for (int s = 0; s < p.nsubs; ++s) {
       if (p.pressure_n_in[s]) rho[4 * s + 0] = face_rho<double>(d, s, t, p.pressure_n_in[s], true, d->n_table);
       if (p.pressure_n_out[s]) rho[4 * s + 1] = face_rho<double>(d, s, t, 0, false, d->n_table);
       if (p.pressure_s_in[s]) rho[4 * s + 2] = face_rho<double>(d, s, t, p.pressure_s_in[s], true, d->s_table);
       if (p.pressure_s_out[s]) rho[4 * s + 3] = face_rho<double>(d, s, t, 0, false, d->s_table);
     }
-    std::memcpy(out + len, rho, sizeof rho);
   }
-  return len + 8 * sizeof(double);
+  if (d->faces3_active) {
+    for (int s = 0; s < p.nsubs; ++s) {
+      if (p.pressure_t_in[s] || p.pressure_b_in[s]) rho[8 + 4 * s + 0] = face_rho<double>(d, s, t, 1, true, d->n_table);
+      if (p.pressure_t_out[s] || p.pressure_b_out[s]) rho[8 + 4 * s + 1] = face_rho<double>(d, s, t, 0, false, d->n_table);
+    }
+  }
+  std::memcpy(out + len, rho, sizeof rho);
+  return len + sizeof rho;
 }
 
 // Replay `pairs` AA pairs starting at odd time t from one captured pair.
@@ -416,19 +523,11 @@ lbx_status replay_pairs(lbx_domain* d, int t, int pairs)
     std::memcpy(d->graph_key, key, klen);
     d->graph_key_len = klen;
   }
-  const long long per_pair = (d->faces_active && !d->faces_fused) ? 0 : 2;
+  // the graph holds every kernel of both steps (faces and records included)
+  const long long per_pair = 2 * launches_per_step(d, true);
   for (int r = 0; r < pairs; ++r) {
     CK(cudaGraphLaunch(d->graph, d->stream));
     d->launches += per_pair;
-  }
-  if (per_pair == 0) {
-    // stand-alone face kernels are inside the graph too: count them
-    long long n = 0;
-    for (int s = 0; s < d->p.nsubs; ++s)
-      n += (d->p.pressure_n_in[s] != 0) + (d->p.pressure_n_out[s] != 0) +
-           (d->p.pressure_s_in[s] != 0) + (d->p.pressure_s_out[s] != 0);
-    if (d->p.nsubs == 2) n += (d->p.zeroconcgrad_n != 0) + (d->p.zeroconcgrad_s != 0);
-    d->launches += (long long)pairs * 2 * (n + 1);
   }
   if (d->layout == LBX_LAYOUT_COMPACT) d->dense_stale = true;
   return LBX_OK;
@@ -442,11 +541,11 @@ lbx_status exchange(lbx_domain* d, bool to_compact)
   const long long total = d->fluid * planes;
   const unsigned blocks = (unsigned)((total + 255) / 256);
   if (d->real_size == 8) {
-    if (to_compact) gather_compact<double><<<blocks, 256, 0, d->stream>>>((double*)d->fc, (const double*)d->f, d->fnode, (int)d->fluid, d->N, planes);
-    else scatter_compact<double><<<blocks, 256, 0, d->stream>>>((double*)d->f, (const double*)d->fc, d->fnode, (int)d->fluid, d->N, planes);
+    if (to_compact) gather_compact<double><<<blocks, 256, 0, d->stream>>>((double*)d->fc, (const double*)d->f, d->fnode, (int)d->fluid, (int)d->P, d->N, planes);
+    else scatter_compact<double><<<blocks, 256, 0, d->stream>>>((double*)d->f, (const double*)d->fc, d->fnode, (int)d->fluid, (int)d->P, d->N, planes);
   } else {
-    if (to_compact) gather_compact<float><<<blocks, 256, 0, d->stream>>>((float*)d->fc, (const float*)d->f, d->fnode, (int)d->fluid, d->N, planes);
-    else scatter_compact<float><<<blocks, 256, 0, d->stream>>>((float*)d->f, (const float*)d->fc, d->fnode, (int)d->fluid, d->N, planes);
+    if (to_compact) gather_compact<float><<<blocks, 256, 0, d->stream>>>((float*)d->fc, (const float*)d->f, d->fnode, (int)d->fluid, (int)d->P, d->N, planes);
+    else scatter_compact<float><<<blocks, 256, 0, d->stream>>>((float*)d->f, (const float*)d->fc, d->fnode, (int)d->fluid, (int)d->P, d->N, planes);
   }
   d->launches++;
   CK(cudaGetLastError());
@@ -467,6 +566,7 @@ void lbx_params_default(lbx_params* p)
   p->sigma_t_on = 0; p->sigma_t_off = -1;
   p->rho_in = p->rho_out = 1.0; p->pfadd = 1.0; p->pfmul = 0.1;
   p->bc_ramp_start = p->bc_ramp_stop = -1;
+  p->rho_sigma_in = 1.0;
 }
 
 lbx_status lbx_create(const lbx_params* p, const uint8_t* solids, lbx_domain** out)
@@ -491,7 +591,18 @@ lbx_status lbx_create(const lbx_params* p, const uint8_t* solids, lbx_domain** o
                        p->pressure_s_out[s];
   d->faces_active |= p->nsubs == 2 && (p->zeroconcgrad_n || p->zeroconcgrad_s);
   d->faces_fused = d->faces_active && faces_fusable(*p, solids);
-  for (long long n = 0; n < d->N; ++n) d->fluid += solids[n] != 1;
+  for (int s = 0; s < p->nsubs; ++s)
+    d->faces3_active |= p->pressure_t_in[s] || p->pressure_b_in[s] || p->pressure_t_out[s] ||
+                        p->pressure_b_out[s];
+  d->faces3_active |= p->nsubs == 2 && (p->constcon_t_in || p->constcon_b_in ||
+                                        p->zeroconcgrad_t || p->zeroconcgrad_b);
+  {
+    const int planes = p->dims == 2 ? p->LY : p->LZ;
+    const long long per = d->N / planes;
+    d->plane_fluid.assign(planes, 0);
+    for (long long n = 0; n < d->N; ++n) d->plane_fluid[n / per] += solids[n] != 1;
+    for (int q = 0; q < planes; ++q) d->fluid += d->plane_fluid[q];
+  }
   d->layout = p->layout == LBX_LAYOUT_AUTO
                   ? ((d->N - d->fluid) * 20 >= d->N ? LBX_LAYOUT_COMPACT : LBX_LAYOUT_DENSE)
                   : p->layout;
@@ -520,29 +631,13 @@ lbx_status lbx_create(const lbx_params* p, const uint8_t* solids, lbx_domain** o
       if (solids[n] == 1) fidx[n] = -1;
       else { fidx[n] = m; fnode[m++] = (int)n; }
     }
-    CKD(cudaMalloc(&d->fc, std::max<size_t>(1, (size_t)p->nsubs * d->Q * d->fluid * d->real_size)));
+    d->P = (d->fluid + 31) / 32 * 32;
+    CKD(cudaMalloc(&d->fc, std::max<size_t>(1, (size_t)p->nsubs * d->Q * d->P * d->real_size)));
     CKD(cudaMalloc(&d->fidx, d->N * sizeof(int)));
     CKD(cudaMalloc(&d->fnode, fnode.size() * sizeof(int)));
     CKD(cudaMemcpy(d->fidx, fidx.data(), d->N * sizeof(int), cudaMemcpyHostToDevice));
     CKD(cudaMemcpy(d->fnode, fnode.data(), fnode.size() * sizeof(int), cudaMemcpyHostToDevice));
-    CKD(cudaMemsetAsync(d->fc, 0, (size_t)p->nsubs * d->Q * d->fluid * d->real_size, d->stream));
-    // neighbour-delta table for the odd step, kept only if every delta fits
-    if (d->fluid > 0) {
-      int* ovf = nullptr;
-      int hovf = 0;
-      CKD(cudaMalloc(&d->nbd, (size_t)(d->Q - 1) * d->fluid * sizeof(int16_t)));
-      CKD(cudaMalloc(&ovf, sizeof(int)));
-      CKD(cudaMemsetAsync(ovf, 0, sizeof(int), d->stream));
-      const unsigned nb = (unsigned)((d->fluid + 255) / 256);
-      if (d->Q == 9) build_nbd<9><<<nb, 256, 0, d->stream>>>(d->nbd, d->fidx, d->fnode, (int)d->fluid, p->LX, p->LY, p->LZ, ovf);
-      else build_nbd<19><<<nb, 256, 0, d->stream>>>(d->nbd, d->fidx, d->fnode, (int)d->fluid, p->LX, p->LY, p->LZ, ovf);
-      d->launches++;
-      CKD(cudaGetLastError());
-      CKD(cudaMemcpyAsync(&hovf, ovf, sizeof(int), cudaMemcpyDeviceToHost, d->stream));
-      CKD(cudaStreamSynchronize(d->stream));
-      cudaFree(ovf);
-      if (hovf) { cudaFree(d->nbd); d->nbd = nullptr; }
-    }
+    CKD(cudaMemsetAsync(d->fc, 0, std::max<size_t>(1, (size_t)p->nsubs * d->Q * d->P * d->real_size), d->stream));
   }
   CKD(cudaMemsetAsync(d->f, 0, fbytes, d->stream));
   CKD(cudaMemsetAsync(d->mv, 0, mvbytes, d->stream));
@@ -783,6 +878,66 @@ lbx_status lbx_info(lbx_domain* d, long long* fluid_nodes, int* faces_fused, int
 }
 
 long long lbx_launch_count(lbx_domain* d) { return d ? d->launches : -1; }
+
+lbx_status lbx_btc_stop(lbx_domain* d)
+{
+  if (!d) return fail(LBX_ERR_INVALID, "domain is NULL");
+  if (d->btc_vals) {
+    CK(cudaStreamSynchronize(d->stream));
+    if (d->graph) { cudaGraphExecDestroy(d->graph); d->graph = nullptr; }
+  }
+  cudaFree(d->btc_vals); cudaFree(d->btc_rec); cudaFree(d->btc_slot);
+  d->btc_vals = nullptr; d->btc_rec = nullptr; d->btc_slot = nullptr;
+  d->btc_cap = 0;
+  return LBX_OK;
+}
+
+lbx_status lbx_btc_start(lbx_domain* d, int plane, int capacity)
+{
+  if (!d) return fail(LBX_ERR_INVALID, "domain is NULL");
+  if (d->p.nsubs != 2) return fail(LBX_ERR_INVALID, "a breakthrough record needs the solute lattice");
+  const int planes = d->p.dims == 2 ? d->p.LY : d->p.LZ;
+  if (plane < 0 || plane >= planes) return fail(LBX_ERR_INVALID, "plane %d out of range", plane);
+  if (capacity < 1) return fail(LBX_ERR_INVALID, "capacity must be positive");
+  lbx_status st = lbx_btc_stop(d);
+  if (st) return st;
+  const long long per = d->N / planes;
+  long long lo, hi;
+  if (d->layout == LBX_LAYOUT_COMPACT) {
+    lo = 0;
+    for (int q = 0; q < plane; ++q) lo += d->plane_fluid[q];
+    hi = lo + d->plane_fluid[plane];
+  } else {
+    lo = per * plane;
+    hi = lo + per;
+  }
+  d->btc_lo = (int)lo; d->btc_hi = (int)hi;
+  d->btc_plane = plane;
+  d->btc_cap = capacity;
+  CK(cudaMalloc(&d->btc_vals, std::max<long long>(1, hi - lo) * sizeof(double)));
+  CK(cudaMalloc(&d->btc_rec, (size_t)capacity * sizeof(double)));
+  CK(cudaMalloc(&d->btc_slot, sizeof(int)));
+  CK(cudaMemsetAsync(d->btc_slot, 0, sizeof(int), d->stream));
+  // the step arguments changed: a captured pair no longer matches
+  if (d->graph) { CK(cudaStreamSynchronize(d->stream)); cudaGraphExecDestroy(d->graph); d->graph = nullptr; }
+  return LBX_OK;
+}
+
+lbx_status lbx_btc_read(lbx_domain* d, double* out, int max, long long* count)
+{
+  if (!d || (!out && max > 0)) return fail(LBX_ERR_INVALID, "NULL argument");
+  if (!d->btc_slot) return fail(LBX_ERR_STATE, "no breakthrough record started");
+  int slot = 0;
+  CK(cudaMemcpyAsync(&slot, d->btc_slot, sizeof(int), cudaMemcpyDeviceToHost, d->stream));
+  CK(cudaStreamSynchronize(d->stream));
+  const int n = std::min(std::min(slot, d->btc_cap), std::max(max, 0));
+  if (n > 0) {
+    CK(cudaMemcpyAsync(out, d->btc_rec, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, d->stream));
+    CK(cudaStreamSynchronize(d->stream));
+  }
+  if (count) *count = slot;
+  return LBX_OK;
+}
 
 const char* lbx_last_error(void) { return g_err.c_str(); }
 

@@ -111,14 +111,17 @@ __device__ __forceinline__ void batch_block(const BatchArgs<T>& A, int b)
          + (cz(a) < 0 ? zm : (cz(a) > 0 ? zp : 0));
   };
   const int* const fidx_n = A.fidx + S.dbase + n;
+  auto nb_pull = [&](int a) -> int { return fidx_n[off(a)]; };
+  auto nb_push = [&](int a) -> int { return ld_reload(fidx_n + off(a)); };
   T* const fs = A.f;
   T d[Q];
   T u[3] = {T(0), T(0), T(0)};
   if (ODD) {
 #pragma unroll
     for (int a = 0; a < Q; ++a) {
-      const int up = (a == 0) ? m : fidx_n[off(opp(a))];
-      d[a] = (up >= 0) ? fs[a * F + up] : fs[opp(a) * F + m];
+      const int up = (a == 0) ? m : nb_pull(opp(a));
+      const size_t src = (up >= 0) ? (size_t)a * F + (size_t)up : (size_t)opp(a) * F + m;
+      d[a] = fs[src];
     }
   } else {
 #pragma unroll
@@ -130,9 +133,9 @@ __device__ __forceinline__ void batch_block(const BatchArgs<T>& A, int b)
     if (D == 3) { zm = opaque(zm); zp = opaque(zp); }
 #pragma unroll
     for (int a = 0; a < Q; ++a) {
-      const int dn = (a == 0) ? m : ld_reload(fidx_n + off(a));
-      if (dn >= 0) fs[opp(a) * F + dn] = d[a];
-      else fs[a * F + m] = d[a];
+      const int dn = (a == 0) ? m : nb_push(a);
+      const size_t dst = (dn >= 0) ? (size_t)opp(a) * F + (size_t)dn : (size_t)a * F + m;
+      fs[dst] = d[a];
     }
   } else {
     const int m2 = opaque(m);
@@ -764,5 +767,6 @@ lbx_status lbx_batch_reduce(lbx_batch* b, int s, lbx_reductions* out)
 }
 
 long long lbx_batch_launch_count(lbx_batch* b) { return b ? b->launches : -1; }
+
 
 }  // extern "C"

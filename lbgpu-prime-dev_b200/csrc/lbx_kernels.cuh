@@ -79,6 +79,14 @@ __device__ __forceinline__ int opaque(int x)
   return v;
 }
 
+template <typename P>
+__device__ __forceinline__ P* opaque(P* x)
+{
+  P* v;
+  asm volatile("mov.b64 %0, %1;" : "=l"(v) : "l"(x));
+  return v;
+}
+
 // Node class byte, built once per domain from the solids mask.
 enum : uint8_t {
   CLS_SOLID = 1,      // byte == 1 in the reference's mask
@@ -93,7 +101,7 @@ enum Model { SHIFTED_INC = 0, PLAIN_COMP = 1, SHIFTED_COMP = 2 };
 // Face action per substance (2D): what the last active boundary on that
 // face does; boundaries on one face all rewrite the same three unknowns from
 // the same knowns, so the last one in the reference's order wins.
-enum FaceKind { FACE_NONE = 0, FACE_PRESSURE = 1, FACE_ZEROGRAD = 2 };
+enum FaceKind { FACE_NONE = 0, FACE_PRESSURE = 1, FACE_ZEROGRAD = 2, FACE_CONSTCON = 3 };
 
 template <typename T>
 struct SubsConst {
@@ -118,6 +126,8 @@ struct StepArgs {
   int face_n[2], face_s[2];   // FaceKind per substance (2D, fused path)
   T rho_n[2], rho_s[2];       // face densities this step
   T drho_n[2], drho_s[2];     // face density minus rho_A, formed in double
+  double* btc;                // breakthrough record: C of the nodes [btc_lo, btc_hi)
+  int btc_lo, btc_hi;         // node (dense) or slot (compact) range of the plane
 };
 
 // ---- per-node collision ---------------------------------------------------
@@ -125,8 +135,9 @@ struct StepArgs {
 // fluid velocity to the solute as the reference's per-thread scratch does.
 // sinks: the solute sink applies once on odd steps and twice on even steps
 // (src/k_stream_collide_stream.c:254-256; src/k_collide.c:96-97, :261-262).
+// Returns the node's density (the solute's C), the value stored as rho.
 template <typename T, int Q, int MODEL>
-__device__ __forceinline__ void collide(const StepArgs<T>& A, int s, bool solute,
+__device__ __forceinline__ T collide(const StepArgs<T>& A, int s, bool solute,
                                         int sinks, T (&d)[Q], T (&u)[3],
                                         long long n)
 {
@@ -184,6 +195,7 @@ __device__ __forceinline__ void collide(const StepArgs<T>& A, int s, bool solute
                   mul_(mul_(mul_(w, rq), poly), c.itau));
     }
   }
+  return rho;
 }
 
 // ---- fused 2D faces ---------------------------------------------------------
@@ -295,8 +307,9 @@ aa_step(StepArgs<T> A)
       // pull: d_a = f[a][n - c_a], or own f[opp a][n] behind a solid
 #pragma unroll
       for (int a = 0; a < Q; ++a) {
-        if ((nb >> opp(a)) & 1u) d[a] = fs[opp(a) * N + n];
-        else d[a] = fs[a * N + (n + off(opp(a)))];
+        const size_t src = ((nb >> opp(a)) & 1u) ? (size_t)opp(a) * N + n
+                                                 : (size_t)a * N + (size_t)(n + off(opp(a)));
+        d[a] = fs[src];
       }
     } else {
 #pragma unroll
@@ -310,7 +323,9 @@ aa_step(StepArgs<T> A)
       if (cl & CLS_SOUTH)
         face_south<T>(A.face_s[s], A.rho_s[s], A.sc[s].rhoA, A.drho_s[s], shifted, d9);
     }
-    collide<T, Q, MODEL>(A, s, solute, ODD ? 1 : 2, d, u, n);
+    const T rho = collide<T, Q, MODEL>(A, s, solute, ODD ? 1 : 2, d, u, n);
+    if (NS == 2 && solute && A.btc && n >= A.btc_lo && n < A.btc_hi)
+      A.btc[n - A.btc_lo] = (double)rho;
     if (ODD) {
       // push: f[opp a][n + c_a] = d_a, or own f[a][n] in front of a solid
       // (offsets laundered so the pull addresses are not kept live)
@@ -318,8 +333,9 @@ aa_step(StepArgs<T> A)
       if (D == 3) { zm = opaque(zm); zp = opaque(zp); }
 #pragma unroll
       for (int a = 0; a < Q; ++a) {
-        if ((nb >> a) & 1u) fs[a * N + n] = d[a];
-        else fs[opp(a) * N + (n + off(a))] = d[a];
+        const size_t dst = ((nb >> a) & 1u) ? (size_t)a * N + n
+                                            : (size_t)opp(a) * N + (size_t)(n + off(a));
+        fs[dst] = d[a];
       }
     } else {
       const int n2 = opaque(n);   // do not keep the load addresses live
@@ -340,59 +356,12 @@ struct CompactArgs {
   StepArgs<T> s;          // f = compact populations; N = dense node count
   const int* fidx;        // [N]
   const int* fnode;       // [F]
-  const int16_t* nbd;     // [Q-1][F] neighbour deltas (NB == 1), see build_nbd
-  int F;
+  int F;                  // fluid nodes
+  int P;                  // plane stride of fc: F rounded up to 32 (aligned warps)
   int faces;              // 2D: fused face boundaries configured
 };
 
-// Neighbour table of the compact layout: for fluid node m and direction
-// a >= 1, nbd[a-1][m] = idx(n + c_a) - m, or kNbdSolid if that node is
-// solid.  Built once per domain when every delta fits in 16 bits; the odd
-// step then streams 36 B of coalesced deltas per node instead of walking
-// fnode -> coordinates -> fidx (three dependent round trips).
-constexpr int16_t kNbdSolid = -32768;
-
-__device__ __forceinline__ int ld_reload16(const int16_t* p)
-{
-  short v;
-  asm volatile("ld.global.nc.s16 %0, [%1];" : "=h"(v) : "l"(p));
-  return (int)v;
-}
-
-template <int Q>
-__global__ void build_nbd(int16_t* nbd, const int* fidx, const int* fnode, int F,
-                          int LX, int LY, int LZ, int* overflow)
-{
-  constexpr int D = (Q == 9) ? 2 : 3;
-  const int m = blockIdx.x * blockDim.x + threadIdx.x;
-  if (m >= F) return;
-  const int plane = LX * LY;
-  const int n = fnode[m];
-  const int k = n / plane, r = n - k * plane, j = r / LX, i = r - j * LX;
-  const int xm = (i == 0) ? LX - 1 : -1, xp = (i == LX - 1) ? 1 - LX : 1;
-  const int ym = (j == 0) ? plane - LX : -LX, yp = (j == LY - 1) ? LX - plane : LX;
-  int zm = 0, zp = 0;
-  if (D == 3) {
-    const int tot = plane * LZ;
-    zm = (k == 0) ? tot - plane : -plane;
-    zp = (k == LZ - 1) ? plane - tot : plane;
-  }
-#pragma unroll
-  for (int a = 1; a < Q; ++a) {
-    const int o = (cx(a) < 0 ? xm : (cx(a) > 0 ? xp : 0)) + (cy(a) < 0 ? ym : (cy(a) > 0 ? yp : 0))
-                + (cz(a) < 0 ? zm : (cz(a) > 0 ? zp : 0));
-    const int q = fidx[n + o];
-    int16_t v = kNbdSolid;
-    if (q >= 0) {
-      const int dlt = q - m;
-      if (dlt < -32767 || dlt > 32767) atomicOr(overflow, 1);
-      else v = (int16_t)dlt;
-    }
-    nbd[(size_t)(a - 1) * F + m] = v;
-  }
-}
-
-template <typename T, int Q, int NS, int MODEL, bool ODD, int NB>
+template <typename T, int Q, int NS, int MODEL, bool ODD>
 __global__ void __launch_bounds__(256)
 aa_step_compact(CompactArgs<T> C)
 {
@@ -400,20 +369,20 @@ aa_step_compact(CompactArgs<T> C)
   const StepArgs<T>& A = C.s;
   const int m = blockIdx.x * blockDim.x + threadIdx.x;
   if (m >= C.F) return;
-  const size_t F = (size_t)C.F;
+  const size_t F = (size_t)C.P;   // plane stride
   const int LX = A.LX, LY = A.LY;
   const int plane = LX * LY;
   const bool faces = (Q == 9) && C.faces;
   int n = 0, j = 0;
-  // dense offsets to the neighbours along each axis (odd step, no table)
+  // dense offsets to the neighbours along each axis (odd step)
   int xm = 0, xp = 0, ym = 0, yp = 0, zm = 0, zp = 0;
-  if ((ODD && NB == 0) || A.write_mv || faces) {
+  if (ODD || A.write_mv || faces) {
     n = C.fnode[m];
     const int k = n / plane;
     const int r = n - k * plane;
     j = r / LX;
     const int i = r - j * LX;
-    if (ODD && NB == 0) {
+    if (ODD) {
       xm = (i == 0) ? LX - 1 : -1; xp = (i == LX - 1) ? 1 - LX : 1;
       ym = (j == 0) ? plane - LX : -LX; yp = (j == LY - 1) ? LX - plane : LX;
       if (D == 3) {
@@ -429,16 +398,10 @@ aa_step_compact(CompactArgs<T> C)
          + (cz(a) < 0 ? zm : (cz(a) > 0 ? zp : 0));
   };
   const int* const fidx_n = C.fidx + n;
-  const int16_t* const nbd_m = C.nbd + m;
-  // compact index of neighbour n + c_a (a >= 1), -1 if solid
-  auto nb_pull = [&](int a) -> int {
-    if (NB) { const int v = nbd_m[(size_t)(a - 1) * F]; return v == kNbdSolid ? -1 : m + v; }
-    return fidx_n[off(a)];
-  };
-  auto nb_push = [&](int a) -> int {
-    if (NB) { const int v = ld_reload16(nbd_m + (size_t)(a - 1) * F); return v == kNbdSolid ? -1 : m + v; }
-    return ld_reload(fidx_n + off(a));
-  };
+  // compact index of neighbour n + c_a (a >= 1), -1 if solid; the push
+  // re-reads it rather than keeping 18 indices live across the collision
+  auto nb_pull = [&](int a) -> int { return fidx_n[off(a)]; };
+  auto nb_push = [&](int a) -> int { return ld_reload(fidx_n + off(a)); };
   T u[3] = {T(0), T(0), T(0)};
 #pragma unroll
   for (int s = 0; s < NS; ++s) {
@@ -447,11 +410,13 @@ aa_step_compact(CompactArgs<T> C)
     T* const fs = A.f + (size_t)s * Q * F;
     T d[Q];
     if (ODD) {
-      // pull: d_a = f[a][idx(n - c_a)], or own f[opp a] behind a solid
+      // pull: d_a = f[a][idx(n - c_a)], or own f[opp a] behind a solid; the
+      // slot is chosen by integer select so every load issues unconditionally
 #pragma unroll
       for (int a = 0; a < Q; ++a) {
         const int up = (a == 0) ? m : nb_pull(opp(a));
-        d[a] = (up >= 0) ? fs[a * F + up] : fs[opp(a) * F + m];
+        const size_t src = (up >= 0) ? (size_t)a * F + (size_t)up : (size_t)opp(a) * F + m;
+        d[a] = fs[src];
       }
     } else {
 #pragma unroll
@@ -465,7 +430,9 @@ aa_step_compact(CompactArgs<T> C)
       if (j == 0)
         face_south<T>(A.face_s[s], A.rho_s[s], A.sc[s].rhoA, A.drho_s[s], shifted, d9);
     }
-    collide<T, Q, MODEL>(A, s, solute, ODD ? 1 : 2, d, u, n);
+    const T rho = collide<T, Q, MODEL>(A, s, solute, ODD ? 1 : 2, d, u, n);
+    if (NS == 2 && solute && A.btc && m >= A.btc_lo && m < A.btc_hi)
+      A.btc[m - A.btc_lo] = (double)rho;
     if (ODD) {
       // push: f[opp a][idx(n + c_a)] = d_a, or own f[a] in front of a solid;
       // the neighbour indices are re-read rather than kept in registers
@@ -474,8 +441,8 @@ aa_step_compact(CompactArgs<T> C)
 #pragma unroll
       for (int a = 0; a < Q; ++a) {
         const int dn = (a == 0) ? m : nb_push(a);
-        if (dn >= 0) fs[opp(a) * F + dn] = d[a];
-        else fs[a * F + m] = d[a];
+        const size_t dst = (dn >= 0) ? (size_t)opp(a) * F + (size_t)dn : (size_t)a * F + m;
+        fs[dst] = d[a];
       }
     } else {
       const int m2 = opaque(m);   // do not keep the load addresses live
@@ -487,23 +454,23 @@ aa_step_compact(CompactArgs<T> C)
 
 // Dense <-> compact exchange of all substances' populations.
 template <typename T>
-__global__ void gather_compact(T* fc, const T* fdense, const int* fnode, int F,
+__global__ void gather_compact(T* fc, const T* fdense, const int* fnode, int F, int P,
                                long long N, int planes)
 {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (long long)F * planes) return;
   const int pl = (int)(t / F), m = (int)(t - (long long)pl * F);
-  fc[t] = fdense[(long long)pl * N + fnode[m]];
+  fc[(long long)pl * P + m] = fdense[(long long)pl * N + fnode[m]];
 }
 
 template <typename T>
-__global__ void scatter_compact(T* fdense, const T* fc, const int* fnode, int F,
+__global__ void scatter_compact(T* fdense, const T* fc, const int* fnode, int F, int P,
                                 long long N, int planes)
 {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (long long)F * planes) return;
   const int pl = (int)(t / F), m = (int)(t - (long long)pl * F);
-  fdense[(long long)pl * N + fnode[m]] = fc[t];
+  fdense[(long long)pl * N + fnode[m]] = fc[(long long)pl * P + m];
 }
 
 // Stand-alone face kernel on the compact layout: the same deposits as
@@ -511,7 +478,7 @@ __global__ void scatter_compact(T* fdense, const T* fc, const int* fnode, int F,
 template <typename T>
 __global__ void face_row_compact(T* fs, const int* fidx, int LX, int LY, int F,
                                  int north, int kind, int second, T rho_bc, T rhoA,
-                                 T drho, int shifted)
+                                 T drho, int shifted)  // F: plane stride of fs
 {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= LX) return;
@@ -596,6 +563,165 @@ __global__ void face_row(T* fs, const uint8_t* solids, int LX, int LY,
       if (solids[up] == 1) fs[(long long)a * N + n] = d[a];
       else fs[(long long)a * N + up] = d[a];
     }
+  }
+}
+
+// ---- 3D z faces (stand-alone, before each step) ------------------------------
+// top = plane k = LZ-1 (unknowns: the five cz = -1 directions), bottom =
+// plane k = 0 (unknowns: cz = +1).  No reference device code exists for
+// these faces: the rules are the 2D kernels' carried to z.  Zou-He density
+// with zero tangential velocity (D3Q19 reconstruction as in the reference's
+// CPU top/bottom code, src/bcs.c:596-870):
+//   J = rho u_z from the density balance against drho (= rho_bc - rho_A in
+//   shifted form, rho_bc otherwise, formed in double by the host), then
+//   bottom: d_T = d_B + J/3, d_TE = d_BW + J/6 - Nx, d_TW = d_BE + J/6 + Nx,
+//           d_TN = d_BS + J/6 - Ny, d_TS = d_BN + J/6 + Ny;
+//   top:    d_B = d_T - J/3, d_BW = d_TE - J/6 + Nx, d_BE = d_TW - J/6 - Nx,
+//           d_BS = d_TN - J/6 + Ny, d_BN = d_TS - J/6 - Ny,
+// Nx, Ny half the in-plane x / y momentum.  Zero gradient: unknowns w_a X,
+// X = (sum of the populations opposite them) / (sum of their weights), the
+// rule of src/system_boundary_kernels.c:503-521.  Constant concentration:
+// unknowns w_a X with X = (conc - sum of the known populations) / (sum of
+// the unknowns' weights).  Operation order is fixed (FP64 is bit-compatible
+// with the CPU restatement).
+enum { D3T = 9, D3B, D3TE, D3BW, D3TW, D3BE, D3TN, D3BS, D3TS, D3BN };
+
+__device__ __forceinline__ int face3_unknown(bool top, int q)
+{
+  return top ? D3B + 2 * q : D3T + 2 * q;   // B,BW,BE,BS,BN / T,TE,TW,TN,TS
+}
+
+template <typename T>
+__device__ __forceinline__ void face3_apply(T (&d)[19], bool top, int kind, T drho, T conc)
+{
+  if (kind == FACE_PRESSURE) {
+    T S0 = d[DC];
+#pragma unroll
+    for (int a = 1; a < 9; ++a) S0 = add_(S0, d[a]);
+    const T Nx = mul_(T(0.5), sub_(add_(add_(d[DE], d[DNE]), d[DSE]), add_(add_(d[DW], d[DSW]), d[DNW])));
+    const T Ny = mul_(T(0.5), sub_(add_(add_(d[DN], d[DNE]), d[DNW]), add_(add_(d[DS], d[DSW]), d[DSE])));
+    if (top) {
+      const T Sp = add_(add_(add_(add_(d[D3T], d[D3TE]), d[D3TW]), d[D3TN]), d[D3TS]);
+      const T J = sub_(add_(S0, mul_(T(2), Sp)), drho);
+      const T J3 = J / T(3), J6 = J / T(6);
+      d[D3B] = sub_(d[D3T], J3);
+      d[D3BW] = add_(sub_(d[D3TE], J6), Nx);
+      d[D3BE] = sub_(sub_(d[D3TW], J6), Nx);
+      d[D3BS] = add_(sub_(d[D3TN], J6), Ny);
+      d[D3BN] = sub_(sub_(d[D3TS], J6), Ny);
+    } else {
+      const T Sm = add_(add_(add_(add_(d[D3B], d[D3BW]), d[D3BE]), d[D3BS]), d[D3BN]);
+      const T J = sub_(drho, add_(S0, mul_(T(2), Sm)));
+      const T J3 = J / T(3), J6 = J / T(6);
+      d[D3T] = add_(d[D3B], J3);
+      d[D3TE] = sub_(add_(d[D3BW], J6), Nx);
+      d[D3TW] = add_(add_(d[D3BE], J6), Nx);
+      d[D3TN] = sub_(add_(d[D3BS], J6), Ny);
+      d[D3TS] = add_(add_(d[D3BN], J6), Ny);
+    }
+  } else {
+    T wsum = wgt<T, 19>(face3_unknown(top, 0));
+#pragma unroll
+    for (int q = 1; q < 5; ++q) wsum = add_(wsum, wgt<T, 19>(face3_unknown(top, q)));
+    T X;
+    if (kind == FACE_ZEROGRAD) {
+      T num = d[opp(face3_unknown(top, 0))];
+#pragma unroll
+      for (int q = 1; q < 5; ++q) num = add_(num, d[opp(face3_unknown(top, q))]);
+      X = num / wsum;
+    } else {
+      T known = d[0];
+#pragma unroll
+      for (int a = 1; a < 19; ++a)
+        if (cz(a) != (top ? -1 : 1)) known = add_(known, d[a]);
+      X = sub_(conc, known) / wsum;
+    }
+#pragma unroll
+    for (int q = 0; q < 5; ++q) {
+      const int a = face3_unknown(top, q);
+      d[a] = mul_(wgt<T, 19>(a), X);
+    }
+  }
+}
+
+// One face operation on the plane, one thread per (i, j).  `_1` form
+// (second == 0, before an odd step): loads what the odd step will pull and
+// deposits the unknowns where it will pull them from (slot a of the
+// upstream node, or of the node itself behind a solid, as set_f1d_d does);
+// `_2` form (before an even step): the node's own swapped slots.  The dense
+// layout tests solids, the compact one maps nodes through fidx.
+template <typename T, bool COMPACT>
+__global__ void face_plane(T* fs, const uint8_t* solids, const int* fidx, int LX, int LY,
+                           int LZ, long long stride, int top, int kind, int second, T drho,
+                           T conc)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= LX) return;
+  const int j = blockIdx.y;
+  const int k = top ? LZ - 1 : 0;
+  const int plane = LX * LY;
+  const int n = i + LX * j + plane * k;
+  int self;
+  if (COMPACT) { self = fidx[n]; if (self < 0) return; }
+  else { if (solids[n] == 1) return; self = n; }
+  // slot of the upstream node n - c_a, -1 if it is solid
+  auto upstream = [&](int a) -> int {
+    int ii = i - cx(a), jj = j - cy(a), kk = k - cz(a);
+    ii = ii < 0 ? LX - 1 : (ii == LX ? 0 : ii);
+    jj = jj < 0 ? LY - 1 : (jj == LY ? 0 : jj);
+    kk = kk < 0 ? LZ - 1 : (kk == LZ ? 0 : kk);
+    const int q = ii + LX * jj + plane * kk;
+    if (COMPACT) return fidx[q];
+    return solids[q] == 1 ? -1 : q;
+  };
+  T d[19];
+#pragma unroll
+  for (int a = 0; a < 19; ++a) {
+    if (second) {
+      d[a] = fs[opp(a) * stride + self];
+    } else {
+      const int up = upstream(a);
+      d[a] = (up < 0) ? fs[opp(a) * stride + self] : fs[a * stride + up];
+    }
+  }
+  face3_apply<T>(d, top != 0, kind, drho, conc);
+#pragma unroll
+  for (int q = 0; q < 5; ++q) {
+    const int a = face3_unknown(top != 0, q);
+    if (second) {
+      fs[opp(a) * stride + self] = d[a];
+    } else {
+      const int up = upstream(a);
+      fs[a * stride + (up < 0 ? self : up)] = d[a];
+    }
+  }
+}
+
+// ---- breakthrough record ------------------------------------------------------
+// One block: the mean of the plane's recorded C values (skipping solid nodes
+// of a dense plane) into rec[*slot], then the slot advances.  The sum order
+// is fixed, so the record is reproducible run to run.
+constexpr int kBtcThreads = 1024;
+
+static __global__ void __launch_bounds__(kBtcThreads)
+btc_reduce(const double* vals, int count, const uint8_t* plane_solids, double fluid,
+           int on, double* rec, int* slot, int capacity)
+{
+  __shared__ double part[kBtcThreads];
+  double s = 0.0;
+  if (on)
+    for (int q = threadIdx.x; q < count; q += kBtcThreads)
+      if (!plane_solids || plane_solids[q] != 1) s += vals[q];
+  part[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = kBtcThreads / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) part[threadIdx.x] += part[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    const int k = *slot;
+    if (k < capacity) rec[k] = (on && fluid > 0.0) ? part[0] / fluid : __longlong_as_double(0x7ff8000000000000LL);
+    *slot = k + 1;
   }
 }
 

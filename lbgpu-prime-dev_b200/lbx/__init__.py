@@ -43,6 +43,11 @@ class _CParams(C.Structure):
         ("pressure_n_table", C.POINTER(C.c_double)), ("pressure_n_len", C.c_int),
         ("pressure_s_table", C.POINTER(C.c_double)), ("pressure_s_len", C.c_int),
         ("device", C.c_int), ("layout", C.c_int),
+        ("pressure_t_in", _I2), ("pressure_b_in", _I2),
+        ("pressure_t_out", _I2), ("pressure_b_out", _I2),
+        ("constcon_t_in", C.c_int), ("constcon_b_in", C.c_int),
+        ("zeroconcgrad_t", C.c_int), ("zeroconcgrad_b", C.c_int),
+        ("rho_sigma_in", C.c_double),
     ]
 
 
@@ -93,6 +98,10 @@ _SIGNATURES = {
     "lbx_batch_sync": (C.c_int, [C.c_void_p]),
     "lbx_batch_reduce": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(_CReductions)]),
     "lbx_batch_launch_count": (C.c_longlong, [C.c_void_p]),
+    "lbx_btc_start": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    "lbx_btc_read": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.c_int,
+                               C.POINTER(C.c_longlong)]),
+    "lbx_btc_stop": (C.c_int, [C.c_void_p]),
     "lbx_last_error": (C.c_char_p, []),
 }
 
@@ -161,6 +170,16 @@ class Params:
     pressure_s_table: Optional[np.ndarray] = None
     device: int = 0
     layout: int = LBX_LAYOUT_AUTO
+    # 3D z faces: top = plane k = LZ-1, bottom = plane k = 0
+    pressure_t_in: Sequence[int] = (0, 0)
+    pressure_b_in: Sequence[int] = (0, 0)
+    pressure_t_out: Sequence[int] = (0, 0)
+    pressure_b_out: Sequence[int] = (0, 0)
+    constcon_t_in: int = 0
+    constcon_b_in: int = 0
+    zeroconcgrad_t: int = 0
+    zeroconcgrad_b: int = 0
+    rho_sigma_in: float = 1.0
 
     @property
     def Q(self) -> int:
@@ -328,6 +347,23 @@ class Domain:
 
     def launch_count(self) -> int:
         return int(_lib.lbx_launch_count(self._h))
+
+    def btc_start(self, plane: int, capacity: int):
+        """Record the mean solute C over the fluid nodes of `plane` (k in
+        3D, j in 2D) after every following step."""
+        _check(_lib.lbx_btc_start(self._h, plane, capacity))
+
+    def btc_read(self) -> np.ndarray:
+        n = C.c_longlong()
+        _check(_lib.lbx_btc_read(self._h, None, 0, C.byref(n)))
+        out = np.empty(max(int(n.value), 0), dtype=np.float64)
+        got = C.c_longlong()
+        _check(_lib.lbx_btc_read(self._h, out.ctypes.data_as(C.POINTER(C.c_double)),
+                                 out.size, C.byref(got)))
+        return out[:min(out.size, int(got.value))]
+
+    def btc_stop(self):
+        _check(_lib.lbx_btc_stop(self._h))
 
 
 def exported_symbols() -> list:

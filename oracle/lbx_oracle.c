@@ -15,6 +15,9 @@
  *   - per-step order          src/lbgpu_prime.cu:369-915
  *   - equilibrium init        src/latman.c:1786-1840
  *   - weights                 src/latman.c:161-192
+ *   - 3D z faces: no reference device code; the 2D rules above carried to
+ *     the planes k = 0 / k = LZ-1, Zou-He reconstruction as in the
+ *     reference's CPU top/bottom code (src/bcs.c:596-870) -- parity unpinned
  * Semantics are those of a serial run: periodic wrap on every axis using the
  * true solid flag of the wrapped node; a node is solid iff its byte == 1
  * (src/lattice.c:2291, :2314).
@@ -446,6 +449,155 @@ static void apply_bcs(const ctx_t* c, real_t* f, const uint8_t* sol, int t,
   }
 }
 
+/* ---- 3D z faces (parity unpinned) ------------------------------------------
+ * top = plane k = LZ-1 (unknowns: the five cz = -1 directions), bottom =
+ * plane k = 0 (unknowns: cz = +1).  Load/store follow face_load/face_store
+ * above: `_1` pulls as the odd step and deposits upstream, `_2` works on the
+ * node's own swapped slots. */
+enum { DT = 9, DB, DTE, DBW, DTW, DBE, DTN, DBS, DTS, DBN };
+
+static void face3_load(const ctx_t* c, const real_t* fs, const uint8_t* sol,
+                       int second, int i, int j, int k, real_t* d)
+{
+  const orc_params* p = c->p;
+  const long NN = c->NN;
+  long n = node_of(p, i, j, k);
+  int a;
+  for (a = 0; a < 19; a++) {
+    if (second) {
+      d[a] = fs[(long)opp(a) * NN + n];
+    } else {
+      long up = wrap_nbr(p, i, j, k, -CX[a], -CY[a], -CZ[a]);
+      d[a] = is_solid(sol, up) ? fs[(long)opp(a) * NN + n]
+                               : fs[(long)a * NN + up];
+    }
+  }
+}
+
+static void face3_store(const ctx_t* c, real_t* fs, const uint8_t* sol,
+                        int second, int i, int j, int k, int a, real_t v)
+{
+  const orc_params* p = c->p;
+  const long NN = c->NN;
+  long n = node_of(p, i, j, k);
+  if (second) {
+    fs[(long)opp(a) * NN + n] = v;
+  } else {
+    long up = wrap_nbr(p, i, j, k, -CX[a], -CY[a], -CZ[a]);
+    if (is_solid(sol, up)) fs[(long)a * NN + n] = v;
+    else fs[(long)a * NN + up] = v;
+  }
+}
+
+/* Unknown directions of a face, and the known directions opposite them. */
+static const int UNK_TOP[5] = {DB, DBW, DBE, DBS, DBN};
+static const int UNK_BOT[5] = {DT, DTE, DTW, DTN, DTS};
+
+/* Zou-He density (Hecht & Harting's D3Q19 form, zero tangential velocity):
+ * J = rho u_z from the density balance, then
+ *   bottom: d_T = d_B + J/3, d_TE = d_BW + J/6 - Nx, d_TW = d_BE + J/6 + Nx,
+ *           d_TN = d_BS + J/6 - Ny, d_TS = d_BN + J/6 + Ny;
+ *   top:    d_B = d_T - J/3, d_BW = d_TE - J/6 + Nx, d_BE = d_TW - J/6 - Nx,
+ *           d_BS = d_TN - J/6 + Ny, d_BN = d_TS - J/6 - Ny;
+ * with Nx, Ny half the in-plane x / y momentum.  In shifted form the rho_A
+ * weights cancel from every difference, and the balance uses rho_bc - rho_A
+ * (`drho`, formed in double). */
+static void zou_he_3d(real_t* d, int top, real_t drho)
+{
+  real_t S0 = d[DC] + d[DE] + d[DW] + d[DN] + d[DS] + d[DNE] + d[DSW] + d[DNW] + d[DSE];
+  real_t Nx = 0.5 * ((d[DE] + d[DNE] + d[DSE]) - (d[DW] + d[DSW] + d[DNW]));
+  real_t Ny = 0.5 * ((d[DN] + d[DNE] + d[DNW]) - (d[DS] + d[DSW] + d[DSE]));
+  real_t J;
+  if (top) {
+    real_t Sp = d[DT] + d[DTE] + d[DTW] + d[DTN] + d[DTS];
+    J = (S0 + 2. * Sp) - drho;
+    d[DB] = d[DT] - J / 3.;
+    d[DBW] = d[DTE] - J / 6. + Nx;
+    d[DBE] = d[DTW] - J / 6. - Nx;
+    d[DBS] = d[DTN] - J / 6. + Ny;
+    d[DBN] = d[DTS] - J / 6. - Ny;
+  } else {
+    real_t Sm = d[DB] + d[DBW] + d[DBE] + d[DBS] + d[DBN];
+    J = drho - (S0 + 2. * Sm);
+    d[DT] = d[DB] + J / 3.;
+    d[DTE] = d[DBW] + J / 6. - Nx;
+    d[DTW] = d[DBE] + J / 6. + Nx;
+    d[DTN] = d[DBS] + J / 6. - Ny;
+    d[DTS] = d[DBN] + J / 6. + Ny;
+  }
+}
+
+enum { F3_PRESSURE = 1, F3_ZEROGRAD = 2, F3_CONSTCON = 3 };
+
+static void face3(const ctx_t* c, real_t* fs, const uint8_t* sol, int top,
+                  int kind, int second, real_t drho, real_t conc)
+{
+  const orc_params* p = c->p;
+  const int k = top ? p->LZ - 1 : 0;
+  const int* unk = top ? UNK_TOP : UNK_BOT;
+  int i, j, q;
+  for (j = 0; j < p->LY; j++)
+    for (i = 0; i < p->LX; i++) {
+      real_t d[19];
+      if (is_solid(sol, node_of(p, i, j, k))) continue;
+      face3_load(c, fs, sol, second, i, j, k, d);
+      if (kind == F3_PRESSURE) {
+        zou_he_3d(d, top, drho);
+      } else {
+        /* unknowns set to w_a X: zero gradient takes X from the outgoing
+         * populations opposite the unknowns (the 2D rule of
+         * src/system_boundary_kernels.c:503-521), constant concentration
+         * from C minus the known populations */
+        real_t wsum = c->w[unk[0]] + c->w[unk[1]] + c->w[unk[2]] + c->w[unk[3]] + c->w[unk[4]];
+        real_t X;
+        if (kind == F3_ZEROGRAD) {
+          X = (d[opp(unk[0])] + d[opp(unk[1])] + d[opp(unk[2])] + d[opp(unk[3])]
+               + d[opp(unk[4])]) / wsum;
+        } else {
+          real_t known = 0;
+          int a;
+          for (a = 0; a < 19; a++)
+            if (CZ[a] != (top ? -1 : 1)) known += d[a];
+          X = (conc - known) / wsum;
+        }
+        for (q = 0; q < 5; q++) d[unk[q]] = c->w[unk[q]] * X;
+      }
+      for (q = 0; q < 5; q++) face3_store(c, fs, sol, second, i, j, k, unk[q], d[unk[q]]);
+    }
+}
+
+/* Order: pressure t_in, t_out, b_in, b_out per substance (as n/s in 2D),
+ * then the solute's constant-concentration and zero-gradient faces. */
+static void apply_bcs3(const ctx_t* c, real_t* f, const uint8_t* sol, int t,
+                       int second)
+{
+  const orc_params* p = c->p;
+  int s;
+  for (s = 0; s < c->NS; s++) {
+    real_t* fs = f + (long)s * c->Q * c->NN;
+    const int shifted = p->accurate && !(s == 1 && p->nsubs == 2);
+    const double rA = shifted ? (double)c->rho_A[s] : 0.;
+    if (p->pressure_t_in[s])
+      face3(c, fs, sol, 1, F3_PRESSURE, second,
+            (real_t)((double)face_rho(c, s, t, 1, 1, 0, 0) - rA), 0);
+    if (p->pressure_t_out[s])
+      face3(c, fs, sol, 1, F3_PRESSURE, second,
+            (real_t)((double)face_rho(c, s, t, 0, 0, 0, 0) - rA), 0);
+    if (p->pressure_b_in[s])
+      face3(c, fs, sol, 0, F3_PRESSURE, second,
+            (real_t)((double)face_rho(c, s, t, 1, 1, 0, 0) - rA), 0);
+    if (p->pressure_b_out[s])
+      face3(c, fs, sol, 0, F3_PRESSURE, second,
+            (real_t)((double)face_rho(c, s, t, 0, 0, 0, 0) - rA), 0);
+    if (s == 1 && p->nsubs == 2) {
+      if (p->constcon_t_in) face3(c, fs, sol, 1, F3_CONSTCON, second, 0, (real_t)p->rho_sigma_in);
+      if (p->constcon_b_in) face3(c, fs, sol, 0, F3_CONSTCON, second, 0, (real_t)p->rho_sigma_in);
+      if (p->zeroconcgrad_t) face3(c, fs, sol, 1, F3_ZEROGRAD, second, 0, 0);
+      if (p->zeroconcgrad_b) face3(c, fs, sol, 0, F3_ZEROGRAD, second, 0, 0);
+    }
+  }
+}
+
 int SFX(orc_run)(const orc_params* p, REAL* f, const uint8_t* solids,
                  REAL* mv, int t0, int nsteps, int frame_rate, int nthreads)
 {
@@ -458,8 +610,52 @@ int SFX(orc_run)(const orc_params* p, REAL* f, const uint8_t* solids,
     int wmv = frame_rate > 0 && t % frame_rate == 0;
     int odd = (t % 2) == 1;
     if (p->dims == 2) apply_bcs(&c, f, solids, t, !odd);
+    else apply_bcs3(&c, f, solids, t, !odd);
     half_step(&c, f, solids, mv, t, wmv, odd, nthreads);
   }
+  return 0;
+}
+
+/* orc_run plus a breakthrough record: btc[i] = mean over the fluid nodes of
+ * the plane k = `plane` (3D) or row j = `plane` (2D) of the solute
+ * concentration C computed by the step at time t0+1+i (FP64 sum in node
+ * order); NaN for steps with the solute inactive. */
+int SFX(orc_run_btc)(const orc_params* p, REAL* f, const uint8_t* solids,
+                     REAL* mv, int t0, int nsteps, int frame_rate, int nthreads,
+                     int plane, double* btc)
+{
+  ctx_t c;
+  int t;
+  long per, base, q, cnt = 0;
+  REAL* scratch;
+  if (t0 % 2 != 0 || p->LX < 1 || p->LY < 1 || p->LZ < 1 || p->nsubs != 2) return -1;
+  if (p->dims == 2 && p->LZ != 1) return -1;
+  if (plane < 0 || plane >= (p->dims == 2 ? p->LY : p->LZ)) return -1;
+  make_ctx(&c, p);
+  per = p->dims == 2 ? (long)p->LX : (long)p->LX * p->LY;
+  base = per * plane;
+  for (q = 0; q < per; q++) cnt += !is_solid(solids, base + q);
+  scratch = (REAL*)malloc(sizeof(REAL) * (size_t)2 * (1 + c.D) * c.NN);
+  if (!scratch) return -2;
+  for (t = t0 + 1; t <= t0 + nsteps; t++) {
+    int wmv = frame_rate > 0 && t % frame_rate == 0;
+    int odd = (t % 2) == 1;
+    REAL* m = wmv ? mv : scratch;
+    const REAL* C;
+    double sum = 0;
+    if (p->dims == 2) apply_bcs(&c, f, solids, t, !odd);
+    else apply_bcs3(&c, f, solids, t, !odd);
+    half_step(&c, f, solids, m, t, 1, odd, nthreads);
+    if (!(t >= p->sigma_t_on && t <= p->sigma_t_off) || cnt == 0) {
+      btc[t - t0 - 1] = 0. / 0.;
+      continue;
+    }
+    C = m + (long)(1 + c.D) * c.NN;   /* subs 1, rho */
+    for (q = 0; q < per; q++)
+      if (!is_solid(solids, base + q)) sum += (double)C[base + q];
+    btc[t - t0 - 1] = sum / (double)cnt;
+  }
+  free(scratch);
   return 0;
 }
 

@@ -24,6 +24,14 @@ typedef struct {
   int bc_ramp_start, bc_ramp_stop;
   const double* pressure_n_table; int pressure_n_len;
   const double* pressure_s_table; int pressure_s_len;
+  /* 3D faces: top = plane k = LZ-1, bottom = plane k = 0.  The reference
+   * reads these flags (src/params.h:191-198, :282-307) but has no device
+   * code for them: the rules restated here are the 2D kernels carried to
+   * the z faces (parity unpinned). */
+  int pressure_t_in[2], pressure_b_in[2], pressure_t_out[2], pressure_b_out[2];
+  int constcon_t_in, constcon_b_in;   /* solute: C = rho_sigma_in on the face */
+  int zeroconcgrad_t, zeroconcgrad_b;
+  double rho_sigma_in;
 } orc_params;
 
 int orc_run_f64(const orc_params*, double* f, const uint8_t* solids,
@@ -32,6 +40,12 @@ int orc_run_f64(const orc_params*, double* f, const uint8_t* solids,
 int orc_run_f32(const orc_params*, float* f, const uint8_t* solids,
                 float* mv, int t0, int nsteps, int frame_rate,
                 int nthreads);
+int orc_run_btc_f64(const orc_params*, double* f, const uint8_t* solids,
+                    double* mv, int t0, int nsteps, int frame_rate,
+                    int nthreads, int plane, double* btc);
+int orc_run_btc_f32(const orc_params*, float* f, const uint8_t* solids,
+                    float* mv, int t0, int nsteps, int frame_rate,
+                    int nthreads, int plane, double* btc);
 int orc_init_feq_f64(const orc_params*, const double* rho, const double* ux,
                      const double* uy, const double* uz, double* f);
 int orc_init_feq_f32(const orc_params*, const float* rho, const float* ux,

@@ -53,6 +53,16 @@ class Params:
     bc_ramp_stop: int = -1
     pressure_n_table: Optional[np.ndarray] = None
     pressure_s_table: Optional[np.ndarray] = None
+    # 3D z faces (top = k = LZ-1, bottom = k = 0)
+    pressure_t_in: tuple = (0, 0)
+    pressure_b_in: tuple = (0, 0)
+    pressure_t_out: tuple = (0, 0)
+    pressure_b_out: tuple = (0, 0)
+    constcon_t_in: int = 0
+    constcon_b_in: int = 0
+    zeroconcgrad_t: int = 0
+    zeroconcgrad_b: int = 0
+    rho_sigma_in: float = 1.0
 
     @property
     def Q(self) -> int:
@@ -82,6 +92,11 @@ class _OrcParams(C.Structure):
         ("bc_ramp_start", C.c_int), ("bc_ramp_stop", C.c_int),
         ("pressure_n_table", C.POINTER(C.c_double)), ("pressure_n_len", C.c_int),
         ("pressure_s_table", C.POINTER(C.c_double)), ("pressure_s_len", C.c_int),
+        ("pressure_t_in", _I2), ("pressure_b_in", _I2),
+        ("pressure_t_out", _I2), ("pressure_b_out", _I2),
+        ("constcon_t_in", C.c_int), ("constcon_b_in", C.c_int),
+        ("zeroconcgrad_t", C.c_int), ("zeroconcgrad_b", C.c_int),
+        ("rho_sigma_in", C.c_double),
     ]
 
 
@@ -136,6 +151,11 @@ def _lib():
             fn.argtypes = [C.POINTER(_OrcParams), C.POINTER(ct), C.c_void_p,
                            C.POINTER(ct), C.c_int, C.c_int, C.c_int, C.c_int]
             fn.restype = C.c_int
+            fn = getattr(lib, "orc_run_btc_" + sfx)
+            fn.argtypes = [C.POINTER(_OrcParams), C.POINTER(ct), C.c_void_p,
+                           C.POINTER(ct), C.c_int, C.c_int, C.c_int, C.c_int,
+                           C.c_int, C.POINTER(C.c_double)]
+            fn.restype = C.c_int
             fn = getattr(lib, "orc_init_feq_" + sfx)
             fn.argtypes = [C.POINTER(_OrcParams)] + [C.POINTER(ct)] * 4 + [C.POINTER(ct)]
             fn.restype = C.c_int
@@ -172,6 +192,30 @@ def run_oracle(p: Params, f: np.ndarray, solids: np.ndarray, t0: int,
     if rc != 0:
         raise ValueError("orc_run rejected the parameters")
     return f, mv
+
+
+def run_oracle_btc(p: Params, f: np.ndarray, solids: np.ndarray, t0: int,
+                   nsteps: int, plane: int, frame_rate: int = 0,
+                   mv: Optional[np.ndarray] = None, threads: int = 0):
+    """run_oracle plus the breakthrough record of the plane k (3D) / row j
+    (2D) = `plane`: the mean solute C over its fluid nodes after every step
+    (NaN while the solute is inactive).  Returns (f, mv, btc)."""
+    dtype = f.dtype
+    assert f.flags.c_contiguous and f.size == p.nsubs * p.Q * p.NN
+    sol = np.ascontiguousarray(solids, dtype=np.uint8).reshape(-1)
+    if mv is None:
+        mv = np.zeros((p.nsubs, 1 + p.dims, p.NN), dtype=dtype)
+    btc = np.zeros(nsteps, dtype=np.float64)
+    st = _OrcParams()
+    _fill(st, p, [])
+    nt = threads or min(os.cpu_count() or 1, 64)
+    rc = getattr(_lib(), "orc_run_btc_" + _sfx(dtype))(
+        C.byref(st), f.ctypes.data_as(C.POINTER(_ct(dtype))),
+        sol.ctypes.data, mv.ctypes.data_as(C.POINTER(_ct(dtype))),
+        t0, nsteps, frame_rate, nt, plane, btc.ctypes.data_as(C.POINTER(C.c_double)))
+    if rc != 0:
+        raise ValueError("orc_run_btc rejected the parameters")
+    return f, mv, btc
 
 
 def init_feq(p: Params, rho: np.ndarray, ux: np.ndarray, uy: np.ndarray,
