@@ -89,6 +89,7 @@ struct lbx_domain {
   bool faces3_active = false; // any 3D z-face boundary configured
   std::vector<long long> plane_fluid;  // fluid nodes per plane (k in 3D, j in 2D)
   // breakthrough record (lbx_btc_*)
+  void* ubuf = nullptr;        // [3][P or N] flow velocity for the solute launch
   double* btc_vals = nullptr;  // C of the plane's nodes this step
   double* btc_rec = nullptr;   // [btc_cap] means
   int* btc_slot = nullptr;     // steps recorded
@@ -151,6 +152,8 @@ void fill_args(const lbx_domain* d, int t, unsigned flags, StepArgs<T>& A)
   A.sink1 = (T)(1.0 - (T)p.sink * (T)p.tau[1]);
   A.write_mv = (flags & LBX_WRITE_MV) ? 1 : 0;
   A.solute_on = (t >= p.sigma_t_on && t <= p.sigma_t_off) ? 1 : 0;
+  A.ubuf = (T*)d->ubuf;
+  A.ustride = d->layout == LBX_LAYOUT_COMPACT ? d->P : d->N;
   if (d->btc_vals) {
     A.btc = d->btc_vals;
     A.btc_lo = d->btc_lo;
@@ -181,8 +184,8 @@ StepArgs<T> make_args(const lbx_domain* d, int t, unsigned flags)
   return A;
 }
 
-template <typename T, int Q, int NS, int MODEL>
-void launch_aa(lbx_domain* d, const StepArgs<T>& A, bool odd)
+template <typename T, int Q, int NS, int MODEL, int PART>
+void launch_part(lbx_domain* d, const StepArgs<T>& A, bool odd)
 {
   if (d->layout == LBX_LAYOUT_COMPACT) {
     CompactArgs<T> C;
@@ -191,19 +194,40 @@ void launch_aa(lbx_domain* d, const StepArgs<T>& A, bool odd)
     C.fnode = d->fnode;
     C.F = (int)d->fluid;
     C.P = (int)d->P;
+    C.div_plane = make_fastdiv((unsigned)(A.LX * A.LY));
+    C.div_lx = make_fastdiv((unsigned)A.LX);
     C.faces = d->faces_fused ? 1 : 0;
     const unsigned blocks = (unsigned)((d->fluid + 255) / 256);
     if (blocks == 0) return;
-    if (odd) aa_step_compact<T, Q, NS, MODEL, true><<<blocks, 256, 0, d->stream>>>(C);
-    else aa_step_compact<T, Q, NS, MODEL, false><<<blocks, 256, 0, d->stream>>>(C);
+    const bool idx32 = (unsigned long long)Q * (unsigned long long)d->P < (1ull << 32);
+    if (idx32) {
+      if (odd) aa_step_compact<T, Q, NS, MODEL, true, PART, true><<<blocks, 256, 0, d->stream>>>(C);
+      else aa_step_compact<T, Q, NS, MODEL, false, PART, true><<<blocks, 256, 0, d->stream>>>(C);
+    } else {
+      if (odd) aa_step_compact<T, Q, NS, MODEL, true, PART, false><<<blocks, 256, 0, d->stream>>>(C);
+      else aa_step_compact<T, Q, NS, MODEL, false, PART, false><<<blocks, 256, 0, d->stream>>>(C);
+    }
     d->launches++;
     return;
   }
   dim3 block(128, 1, 1);
   dim3 grid((A.LX + 127) / 128, A.LY, A.LZ);
-  if (odd) aa_step<T, Q, NS, MODEL, true><<<grid, block, 0, d->stream>>>(A);
-  else aa_step<T, Q, NS, MODEL, false><<<grid, block, 0, d->stream>>>(A);
+  if (odd) aa_step<T, Q, NS, MODEL, true, PART><<<grid, block, 0, d->stream>>>(A);
+  else aa_step<T, Q, NS, MODEL, false, PART><<<grid, block, 0, d->stream>>>(A);
   d->launches++;
+}
+
+// One step: a single launch for the flow alone; flow then solute for two
+// substances (the solute launch only while the solute is active).
+template <typename T, int Q, int NS, int MODEL>
+void launch_aa(lbx_domain* d, const StepArgs<T>& A, bool odd)
+{
+  if constexpr (NS == 1) {
+    launch_part<T, Q, NS, MODEL, PART_ALL>(d, A, odd);
+  } else {
+    launch_part<T, Q, NS, MODEL, PART_FLOW>(d, A, odd);
+    if (A.solute_on) launch_part<T, Q, NS, MODEL, PART_SOLUTE>(d, A, odd);
+  }
 }
 
 template <typename T, int Q, int NS>
@@ -309,14 +333,13 @@ void launch_faces3(lbx_domain* d, int t, bool second)
 // Kernels one step launches (faces, the step, the breakthrough reduction).
 long long launches_per_step(const lbx_domain* d, bool solute_on)
 {
-  long long n = 1 + count_faces3(d);
+  long long n = 1 + (d->p.nsubs == 2 && solute_on ? 1 : 0) + count_faces3(d);
   if (d->faces_active && !d->faces_fused) {
     for (int s = 0; s < d->p.nsubs; ++s)
       n += (d->p.pressure_n_in[s] != 0) + (d->p.pressure_n_out[s] != 0) +
            (d->p.pressure_s_in[s] != 0) + (d->p.pressure_s_out[s] != 0);
     if (d->p.nsubs == 2) n += (d->p.zeroconcgrad_n != 0) + (d->p.zeroconcgrad_s != 0);
   }
-  (void)solute_on;
   if (d->btc_vals) n += 1;
   return n;
 }
@@ -427,6 +450,7 @@ void release(lbx_domain* d)
   cudaFree(d->f); cudaFree(d->mv); cudaFree(d->solids); cudaFree(d->cls);
   cudaFree(d->nbm); cudaFree(d->red);
   cudaFree(d->btc_vals); cudaFree(d->btc_rec); cudaFree(d->btc_slot);
+  cudaFree(d->ubuf);
   if (d->own_stream) cudaStreamDestroy(d->own_stream);
 }
 
@@ -524,7 +548,8 @@ lbx_status replay_pairs(lbx_domain* d, int t, int pairs)
     d->graph_key_len = klen;
   }
   // the graph holds every kernel of both steps (faces and records included)
-  const long long per_pair = 2 * launches_per_step(d, true);
+  auto on = [&](int tt) { return tt >= d->p.sigma_t_on && tt <= d->p.sigma_t_off; };
+  const long long per_pair = launches_per_step(d, on(t)) + launches_per_step(d, on(t + 1));
   for (int r = 0; r < pairs; ++r) {
     CK(cudaGraphLaunch(d->graph, d->stream));
     d->launches += per_pair;
@@ -638,6 +663,10 @@ lbx_status lbx_create(const lbx_params* p, const uint8_t* solids, lbx_domain** o
     CKD(cudaMemcpy(d->fidx, fidx.data(), d->N * sizeof(int), cudaMemcpyHostToDevice));
     CKD(cudaMemcpy(d->fnode, fnode.data(), fnode.size() * sizeof(int), cudaMemcpyHostToDevice));
     CKD(cudaMemsetAsync(d->fc, 0, std::max<size_t>(1, (size_t)p->nsubs * d->Q * d->P * d->real_size), d->stream));
+  }
+  if (p->nsubs == 2) {
+    const long long us = d->layout == LBX_LAYOUT_COMPACT ? d->P : d->N;
+    CKD(cudaMalloc(&d->ubuf, std::max<size_t>(1, (size_t)3 * us * d->real_size)));
   }
   CKD(cudaMemsetAsync(d->f, 0, fbytes, d->stream));
   CKD(cudaMemsetAsync(d->mv, 0, mvbytes, d->stream));

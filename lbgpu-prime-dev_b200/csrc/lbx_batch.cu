@@ -56,6 +56,7 @@ struct SampleDesc {
   long long mvbase;     // first macro-variable element: [1+D][N]
   int cbase;            // first compact index (a multiple of kAlign)
   int F;                // fluid nodes
+  FastDiv div_plane, div_lx;
   SubsConst<T> sc;
 };
 
@@ -94,9 +95,9 @@ __device__ __forceinline__ void batch_block(const BatchArgs<T>& A, int b)
   L.write_mv = A.write_mv;
   int xm = 0, xp = 0, ym = 0, yp = 0, zm = 0, zp = 0;
   if (ODD) {
-    const int k = n / plane;
+    const int k = fast_div(n, S.div_plane);
     const int r = n - k * plane;
-    const int j = r / LX;
+    const int j = fast_div(r, S.div_lx);
     const int i = r - j * LX;
     xm = (i == 0) ? LX - 1 : -1; xp = (i == LX - 1) ? 1 - LX : 1;
     ym = (j == 0) ? plane - LX : -LX; yp = (j == LY - 1) ? LX - plane : LX;
@@ -333,6 +334,8 @@ void fill_desc(lbx_batch* b, std::vector<unsigned char>& out)
     x.LX = p.LX; x.LY = p.LY; x.LZ = p.LZ; x.plane = p.LX * p.LY;
     x.N = b->N[s]; x.dbase = b->dbase[s]; x.mvbase = b->mvbase[s];
     x.cbase = b->cbase[s]; x.F = b->F[s];
+    x.div_plane = make_fastdiv((unsigned)(p.LX * p.LY));
+    x.div_lx = make_fastdiv((unsigned)p.LX);
     const T tau = (T)p.tau[0];
     const T itau = (T)(1. / tau);
     x.sc.itau = itau; x.sc.omc = (T)(1. - itau); x.sc.rhoA = (T)p.rho_A[0];

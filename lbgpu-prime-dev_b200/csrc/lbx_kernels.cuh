@@ -15,6 +15,7 @@
 #pragma once
 
 #include <cstdint>
+#include <type_traits>
 #include <cuda_runtime.h>
 
 namespace lbx {
@@ -87,6 +88,33 @@ __device__ __forceinline__ P* opaque(P* x)
   return v;
 }
 
+// Division of a node index by a lattice extent without a hardware divide:
+// q = umulhi(n, m) >> s with l = ceil(log2 d), m = ceil(2^(31+l) / d),
+// s = l - 1, exact for 0 <= n < 2^31 (Granlund & Montgomery, "Division by
+// invariant integers using multiplication", PLDI 1994, Theorem 4.2 with
+// N = 31).  d == 1 is the identity (s = -1).
+struct FastDiv {
+  unsigned m;
+  int s;
+};
+
+inline FastDiv make_fastdiv(unsigned d)
+{
+  FastDiv f{0u, -1};
+  if (d <= 1) return f;
+  int l = 0;
+  while ((1ull << l) < d) ++l;                       // ceil(log2 d)
+  const unsigned long long num = 1ull << (31 + l);
+  f.m = (unsigned)((num + d - 1) / d);
+  f.s = l - 1;
+  return f;
+}
+
+__device__ __forceinline__ int fast_div(int n, FastDiv f)
+{
+  return f.s < 0 ? n : (int)(__umulhi((unsigned)n, f.m) >> f.s);
+}
+
 // Node class byte, built once per domain from the solids mask.
 enum : uint8_t {
   CLS_SOLID = 1,      // byte == 1 in the reference's mask
@@ -128,7 +156,16 @@ struct StepArgs {
   T drho_n[2], drho_s[2];     // face density minus rho_A, formed in double
   double* btc;                // breakthrough record: C of the nodes [btc_lo, btc_hi)
   int btc_lo, btc_hi;         // node (dense) or slot (compact) range of the plane
+  T* ubuf;                    // [3][stride]: the flow's u, handed to the solute
+  long long ustride;          // N (dense) or P (compact)
 };
+
+// Which substances one launch of a step kernel advances.  Two-substance
+// steps run as two launches: the flow (PART_FLOW), which also stores its
+// post-force u, then the solute (PART_SOLUTE), which reads it.  One fused
+// body holding both substances needs about twice the registers of either
+// alone (halving occupancy); the split costs 24 B per FP32 node instead.
+enum StepPart { PART_ALL = 0, PART_FLOW = 1, PART_SOLUTE = 2 };
 
 // ---- per-node collision ---------------------------------------------------
 // d[] holds the node's incoming populations of substance s; u carries the
@@ -263,7 +300,7 @@ __device__ __forceinline__ void face_south(int kind, T rho_bc, T rhoA, T drho, b
 // EVEN: d_a = f[opp a][n], collide, f[a][n] = d_a.
 // Each node reads and writes one fixed slot set, disjoint from every other
 // node's, so the update is in place with no ordering between threads.
-template <typename T, int Q, int NS, int MODEL, bool ODD>
+template <typename T, int Q, int NS, int MODEL, bool ODD, int PART>
 __global__ void __launch_bounds__(128)
 aa_step(StepArgs<T> A)
 {
@@ -296,10 +333,24 @@ aa_step(StepArgs<T> A)
   };
 
   T u[3] = {T(0), T(0), T(0)};
+  constexpr int S_BEGIN = (PART == PART_SOLUTE) ? 1 : 0;
+  constexpr int S_END = (PART == PART_FLOW) ? 1 : NS;
+  if (PART == PART_SOLUTE) {
 #pragma unroll
-  for (int s = 0; s < NS; ++s) {
+    for (int c = 0; c < D; ++c) u[c] = A.ubuf[c * A.ustride + n];
+  }
+#pragma unroll
+  for (int s = S_BEGIN; s < S_END; ++s) {
     const bool solute = (NS == 2 && s == 1);
     if (solute && !A.solute_on) break;
+    if (s > 0) {
+      // recompute the solute's neighbour addresses rather than keeping the
+      // flow's live across the flow's collision and push, and start only
+      // after the flow's stores are issued
+      asm volatile("" ::: "memory");
+      xm = opaque(xm); xp = opaque(xp); ym = opaque(ym); yp = opaque(yp);
+      if (D == 3) { zm = opaque(zm); zp = opaque(zp); }
+    }
     T* const fs = A.f + (size_t)s * Q * (size_t)A.N;
     const size_t N = (size_t)A.N;
     T d[Q];
@@ -324,6 +375,10 @@ aa_step(StepArgs<T> A)
         face_south<T>(A.face_s[s], A.rho_s[s], A.sc[s].rhoA, A.drho_s[s], shifted, d9);
     }
     const T rho = collide<T, Q, MODEL>(A, s, solute, ODD ? 1 : 2, d, u, n);
+    if (PART == PART_FLOW && A.solute_on) {
+#pragma unroll
+      for (int c = 0; c < D; ++c) A.ubuf[c * A.ustride + n] = u[c];
+    }
     if (NS == 2 && solute && A.btc && n >= A.btc_lo && n < A.btc_hi)
       A.btc[n - A.btc_lo] = (double)rho;
     if (ODD) {
@@ -358,18 +413,32 @@ struct CompactArgs {
   const int* fnode;       // [F]
   int F;                  // fluid nodes
   int P;                  // plane stride of fc: F rounded up to 32 (aligned warps)
+  FastDiv div_plane, div_lx;   // n / (LX*LY), r / LX
   int faces;              // 2D: fused face boundaries configured
 };
 
-template <typename T, int Q, int NS, int MODEL, bool ODD>
-__global__ void __launch_bounds__(256)
+// Resident 256-thread blocks asked of the compiler: five (48 registers) for
+// the FP32 flow kernels, where that measured fastest; for the others the
+// cap closest above their natural register count (FP32 solute 85, FP64 flow
+// 85, FP64 solute 128), since a lower cap spills.
+template <typename T, int PART>
+constexpr int compact_min_blocks()
+{
+  return sizeof(T) == 4 ? (PART == PART_SOLUTE ? 3 : 5) : (PART == PART_SOLUTE ? 2 : 3);
+}
+
+// IDX32: population offsets within one substance's [Q][P] block fit in 32
+// bits (Q * P < 2^32), so slot selects and address arithmetic stay 32-bit.
+template <typename T, int Q, int NS, int MODEL, bool ODD, int PART, bool IDX32>
+__global__ void __launch_bounds__(256, (compact_min_blocks<T, PART>()))
 aa_step_compact(CompactArgs<T> C)
 {
+  using Idx = typename std::conditional<IDX32, unsigned, size_t>::type;
   constexpr int D = (Q == 9) ? 2 : 3;
   const StepArgs<T>& A = C.s;
   const int m = blockIdx.x * blockDim.x + threadIdx.x;
   if (m >= C.F) return;
-  const size_t F = (size_t)C.P;   // plane stride
+  const Idx F = (Idx)C.P;   // plane stride
   const int LX = A.LX, LY = A.LY;
   const int plane = LX * LY;
   const bool faces = (Q == 9) && C.faces;
@@ -378,9 +447,9 @@ aa_step_compact(CompactArgs<T> C)
   int xm = 0, xp = 0, ym = 0, yp = 0, zm = 0, zp = 0;
   if (ODD || A.write_mv || faces) {
     n = C.fnode[m];
-    const int k = n / plane;
+    const int k = fast_div(n, C.div_plane);
     const int r = n - k * plane;
-    j = r / LX;
+    j = fast_div(r, C.div_lx);
     const int i = r - j * LX;
     if (ODD) {
       xm = (i == 0) ? LX - 1 : -1; xp = (i == LX - 1) ? 1 - LX : 1;
@@ -403,10 +472,24 @@ aa_step_compact(CompactArgs<T> C)
   auto nb_pull = [&](int a) -> int { return fidx_n[off(a)]; };
   auto nb_push = [&](int a) -> int { return ld_reload(fidx_n + off(a)); };
   T u[3] = {T(0), T(0), T(0)};
+  constexpr int S_BEGIN = (PART == PART_SOLUTE) ? 1 : 0;
+  constexpr int S_END = (PART == PART_FLOW) ? 1 : NS;
+  if (PART == PART_SOLUTE) {
 #pragma unroll
-  for (int s = 0; s < NS; ++s) {
+    for (int c = 0; c < D; ++c) u[c] = A.ubuf[c * A.ustride + m];
+  }
+#pragma unroll
+  for (int s = S_BEGIN; s < S_END; ++s) {
     const bool solute = (NS == 2 && s == 1);
     if (solute && !A.solute_on) break;
+    if (s > 0) {
+      // the solute re-reads its neighbour indices (L1 hits) rather than
+      // keeping the flow's live across the flow's collision and push, and
+      // starts only after the flow's stores are issued
+      asm volatile("" ::: "memory");
+      xm = opaque(xm); xp = opaque(xp); ym = opaque(ym); yp = opaque(yp);
+      if (D == 3) { zm = opaque(zm); zp = opaque(zp); }
+    }
     T* const fs = A.f + (size_t)s * Q * F;
     T d[Q];
     if (ODD) {
@@ -415,7 +498,7 @@ aa_step_compact(CompactArgs<T> C)
 #pragma unroll
       for (int a = 0; a < Q; ++a) {
         const int up = (a == 0) ? m : nb_pull(opp(a));
-        const size_t src = (up >= 0) ? (size_t)a * F + (size_t)up : (size_t)opp(a) * F + m;
+        const Idx src = (up >= 0) ? (Idx)a * F + (Idx)up : (Idx)opp(a) * F + (Idx)m;
         d[a] = fs[src];
       }
     } else {
@@ -431,6 +514,10 @@ aa_step_compact(CompactArgs<T> C)
         face_south<T>(A.face_s[s], A.rho_s[s], A.sc[s].rhoA, A.drho_s[s], shifted, d9);
     }
     const T rho = collide<T, Q, MODEL>(A, s, solute, ODD ? 1 : 2, d, u, n);
+    if (PART == PART_FLOW && A.solute_on) {
+#pragma unroll
+      for (int c = 0; c < D; ++c) A.ubuf[c * A.ustride + m] = u[c];
+    }
     if (NS == 2 && solute && A.btc && m >= A.btc_lo && m < A.btc_hi)
       A.btc[m - A.btc_lo] = (double)rho;
     if (ODD) {
@@ -441,7 +528,7 @@ aa_step_compact(CompactArgs<T> C)
 #pragma unroll
       for (int a = 0; a < Q; ++a) {
         const int dn = (a == 0) ? m : nb_push(a);
-        const size_t dst = (dn >= 0) ? (size_t)opp(a) * F + (size_t)dn : (size_t)a * F + m;
+        const Idx dst = (dn >= 0) ? (Idx)opp(a) * F + (Idx)dn : (Idx)a * F + (Idx)m;
         fs[dst] = d[a];
       }
     } else {

@@ -2,6 +2,7 @@
 
     python -m lbx.configs cfg1 [--steps 2000]
     python -m lbx.configs cfg2 [--steps 10000]
+    python -m lbx.configs cfg3 [--steps 20000]
 
 cfg1: D2Q9 BGK 256x256, FP64, tau = 1.0, non-overlapping discs r = 8 to
       porosity 0.6 (the inlet/outlet rows kept fluid), Zou-He pressure
@@ -17,6 +18,16 @@ cfg2: D3Q19 BGK 256^3, tau = 0.8, overlapping spheres r = 6 to porosity 0.4,
       permeability k = nu <u_x> / gx of each with the relative error of the
       FP32 run against the FP64 run.
 
+cfg3: D3Q19 flow + D3Q19 solute, 192x192x384, FP32, tau = 0.9, tau_s = 0.7,
+      overlapping spheres r = 5 to porosity 0.35 with the two z face planes
+      kept fluid (reservoir layers), Zou-He density rho_in = 1.0005 on the
+      bottom plane (k = 0) and rho_out = 1.0 on the top plane, solute C = 1
+      held on the bottom plane, zero gradient on the top, C = 0 elsewhere at
+      t = 0.  Reports MLUPS, the outlet breakthrough curve (mean C over the
+      fluid nodes of the top plane, every step, FP64 sums), the solute mass
+      (FP64) every 1000 steps, the same run in FP64 for the precision
+      comparison, and the solute mass drift of a closed periodic box (no
+      faces, no sink) holding a blob of solute, where mass must be conserved.
 cfg4: 512 independent D3Q19 samples, FP32 shifted, cubic edges drawn from
       U{32..96}, tau ~ U[0.6, 1.2], porosity ~ U[0.3, 0.7], sphere radius
       ~ U{3..6} (seed base + i), gx = 1e-6, periodic.  One batch; reports the
@@ -127,6 +138,92 @@ def run_cfg2(steps: int = 10000, n: int = 256) -> list:
     return out
 
 
+def cfg3_params(precision: int = 4, shape=(192, 192, 384), faces: bool = True,
+                seed: int = 3003):
+    LX, LY, LZ = shape
+    mask = geometry.sphere_pack(LX, LY, LZ, radius=5, porosity=0.35, seed=seed)
+    if faces:
+        m3 = mask.reshape(LZ, LY, LX)
+        m3[0] = 0
+        m3[-1] = 0
+        kw = dict(pressure_b_in=(1, 0), pressure_t_out=(1, 0), rho_in=1.0005, rho_out=1.0,
+                  constcon_b_in=1, zeroconcgrad_t=1, rho_sigma_in=1.0)
+    else:
+        kw = {}
+    p = Params(dims=3, LX=LX, LY=LY, LZ=LZ, nsubs=2, precision=precision, tau=(0.9, 0.7),
+               sigma_t_on=0, sigma_t_off=1 << 30, **kw)
+    return p, mask
+
+
+def _cfg3_run(p, mask, steps: int, chunk: int, blob: bool = False):
+    import torch
+    LX, LY, LZ = p.LX, p.LY, p.LZ
+    with Domain(p, mask) as dom:
+        dom.init_equilibrium(0, 1.0, 0.0, 0.0, 0.0)
+        if blob:
+            k, j, i = np.meshgrid(np.arange(LZ), np.arange(LY), np.arange(LX), indexing="ij")
+            r2 = (i - LX / 2) ** 2 + (j - LY / 2) ** 2 + (k - LZ / 2) ** 2
+            c0 = np.where(r2 < (min(LX, LY, LZ) / 4) ** 2, 1.0, 0.0).reshape(-1)
+        else:
+            c0 = np.zeros(p.NN)
+        dom.init_equilibrium(1, c0, 0.0, 0.0, 0.0)
+        s = torch.cuda.Stream()
+        dom.set_stream(s.cuda_stream)
+        dom.step(1, write_mv=False)
+        dom.step(2, write_mv=True)
+        m0 = dom.reduce()["solute_mass"]
+        dom.btc_start(LZ - 1, steps)
+        masses = []
+        secs = 0.0
+        t = 2
+        while t < steps + 2:
+            n = min(chunk, steps + 2 - t)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(s)
+            dom.run(t, n, n)
+            e1.record(s)
+            s.synchronize()
+            secs += e0.elapsed_time(e1) / 1e3
+            t += n
+            masses.append((t, dom.reduce()["solute_mass"]))
+        btc = dom.btc_read()
+        r = dom.reduce()
+    return dict(seconds=secs, m0=m0, masses=masses, btc=btc, reduce=r)
+
+
+def run_cfg3(steps: int = 20000, shape=(192, 192, 384), chunk: int = 1000) -> list:
+    out = []
+    res = {}
+    for name, prec in (("fp32", 4), ("fp64", 8)):
+        p, mask = cfg3_params(prec, shape)
+        r = _cfg3_run(p, mask, steps, chunk)
+        res[name] = r
+        btc = r["btc"]
+        first = lambda x: int(np.argmax(btc > x)) + 3 if (btc > x).any() else None
+        out.append({"config": "cfg3", "run": name, "lattice": list(shape), "steps": steps,
+                    "mlups": p.NN * steps / r["seconds"] / 1e6, "seconds": r["seconds"],
+                    "fluid_nodes": int((mask != 1).sum()),
+                    "btc_every_1000": [float(btc[i]) for i in range(999, len(btc), 1000)],
+                    "btc_first_above_0.01": first(0.01), "btc_first_above_0.5": first(0.5),
+                    "solute_mass_every_chunk": [[t, m] for t, m in r["masses"]],
+                    "flow_mass": r["reduce"]["mass"]})
+    b32, b64 = res["fp32"]["btc"], res["fp64"]["btc"]
+    m32, m64 = res["fp32"]["masses"][-1][1], res["fp64"]["masses"][-1][1]
+    out.append({"config": "cfg3", "compare": "fp32_vs_fp64",
+                "btc_max_abs_diff": float(np.abs(b32 - b64).max()),
+                "btc_max": float(np.abs(b64).max()),
+                "solute_mass_rel_diff": abs(m32 - m64) / abs(m64)})
+    for name, prec in (("fp32", 4), ("fp64", 8)):
+        p, mask = cfg3_params(prec, shape, faces=False)
+        r = _cfg3_run(p, mask, steps, chunk * 5, blob=True)
+        out.append({"config": "cfg3", "run": "closed_box_" + name, "steps": steps,
+                    "solute_mass_start": r["m0"], "solute_mass_end": r["masses"][-1][1],
+                    "solute_mass_rel_drift": (r["masses"][-1][1] - r["m0"]) / r["m0"],
+                    "mlups": p.NN * steps / r["seconds"] / 1e6})
+    return out
+
+
 def cfg4_samples(nsamples: int = 512, seed: int = 4000):
     rng = np.random.default_rng(seed)
     params, masks = [], []
@@ -198,7 +295,7 @@ def run_cfg4(nsamples: int = 512, steps: int = 200, perm_steps: int = 0) -> list
 
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
-    ap.add_argument("config", choices=["cfg1", "cfg2", "cfg4"])
+    ap.add_argument("config", choices=["cfg1", "cfg2", "cfg3", "cfg4"])
     ap.add_argument("--steps", type=int, default=None)
     ap.add_argument("--edge", type=int, default=256)
     ap.add_argument("--samples", type=int, default=512)
@@ -206,6 +303,9 @@ def main(argv=None) -> int:
     a = ap.parse_args(argv)
     if a.config == "cfg1":
         print(json.dumps(run_cfg1(a.steps or 2000)))
+    elif a.config == "cfg3":
+        for line in run_cfg3(a.steps or 20000):
+            print(json.dumps(line))
     elif a.config == "cfg4":
         for line in run_cfg4(a.samples, a.steps or 200, a.perm_steps):
             print(json.dumps(line))
