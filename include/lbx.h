@@ -212,22 +212,64 @@ lbx_status lbx_info(lbx_domain* d, long long* fluid_nodes, int* faces_fused,
 /* Number of this library's kernels launched on the domain so far. */
 long long lbx_launch_count(lbx_domain* d);
 
-/* Breakthrough record (two-substance runs): from the next step on, every
- * step appends the mean solute concentration C over the fluid nodes of
- * `plane` -- the plane k = plane in 3D, the row j = plane in 2D -- summed in
- * FP64 on the device (NaN for a step with the solute inactive).  Holds up
- * to `capacity` steps; restarting clears it.  No counterpart in the
- * reference, whose concentration output is the per-frame dump of
- * src/lbio.c:2507-2562. */
+/* Plane record: from the next step on, every step appends the means over
+ * the fluid nodes of `plane` -- the plane k = plane in 3D, the row j = plane
+ * in 2D -- of the solute concentration C (NaN for a step with no active
+ * solute) and of the flow velocity u_x, summed in FP64 on the device.  The
+ * C channel is the breakthrough curve at that plane.  Holds up to
+ * `capacity` steps; restarting clears it.  No counterpart in the reference,
+ * whose observables are the per-frame dumps of src/lbio.c:2507-2562. */
 lbx_status lbx_btc_start(lbx_domain* d, int plane, int capacity);
 
-/* Copy up to `max` recorded values (oldest first) into `out` and the number
- * of steps recorded since lbx_btc_start into `*count` (which may exceed
- * capacity; later steps are then not stored). Synchronizes the stream. */
-lbx_status lbx_btc_read(lbx_domain* d, double* out, int max, long long* count);
+/* Copy up to `max` recorded steps (oldest first) into `c_out` (C means) and
+ * `ux_out` (u_x means), either may be NULL, and the number of steps recorded
+ * since lbx_btc_start into `*count` (which may exceed capacity; later steps
+ * are then not stored).  Synchronizes the stream. */
+lbx_status lbx_btc_read(lbx_domain* d, double* c_out, double* ux_out, int max,
+                        long long* count);
+
+/* Constant-concentration face with a per-node concentration: `conc` holds
+ * LX*LY values (i fastest) for the top (top != 0) or bottom face, used
+ * instead of rho_sigma_in; NULL returns to rho_sigma_in.  Copied. */
+lbx_status lbx_set_face_profile(lbx_domain* d, int top, const double* conc);
 
 /* Stop recording and release the record. */
 lbx_status lbx_btc_stop(lbx_domain* d);
+
+/* ---- Discrete adjoint (no counterpart in the reference) -----------------
+ * Objective over a plane (k in 3D, j in 2D), averaged over the steps
+ * t_first..t_last:
+ *   J = w_c  * mean_t (mean over the plane's fluid nodes of the solute C)
+ *     + w_ux * mean_t (mean over the plane's fluid nodes of the flow u_x),
+ * with C and u the values the steps compute (those lbx_btc_* records).
+ * lbx_adjoint_forward runs `nsteps` steps from the current natural-order
+ * state at even time t0 (as lbx_run does), storing the state every
+ * `checkpoint_every` steps on the device, and returns J.
+ * lbx_adjoint_backward then runs the reverse stream-collide sweep,
+ * recomputing each checkpoint interval, and returns dJ/d(gaccel[0..2]),
+ * dJ/dtau[0], dJ/dtau[1] and, when the arrays are given, dJ/d(profile) of
+ * the bottom / top constant-concentration faces (LX*LY values, i fastest;
+ * lbx_set_face_profile).  Adjoint populations are in the run's precision;
+ * gradient sums are FP64.  Covers the compact layout, the shifted
+ * incompressible model, flow + solute with the solute's z faces; other
+ * configurations are rejected with LBX_ERR_INVALID. */
+typedef struct lbx_objective {
+  int plane;
+  int t_first, t_last;
+  double w_c, w_ux;
+} lbx_objective;
+
+typedef struct lbx_gradient {
+  double J;
+  double d_gaccel[3];       /* flow body force */
+  double d_tau;             /* tau[0] */
+  double d_tau_s;           /* tau[1] */
+} lbx_gradient;
+
+lbx_status lbx_adjoint_forward(lbx_domain* d, int t0, int nsteps, int checkpoint_every,
+                               const lbx_objective* obj, double* J);
+lbx_status lbx_adjoint_backward(lbx_domain* d, lbx_gradient* out, double* d_profile_b,
+                                double* d_profile_t);
 
 /* ---- batches of independent lattices ---------------------------------------
  * Many samples of uneven size (same dims, precision and collision model;

@@ -8,6 +8,7 @@
 // No CPU compute path exists here: every step is a CUDA launch, and a
 // failed launch is an error returned to the caller.
 #include "lbx.h"
+#include "lbx_internal.h"
 #include "lbx_kernels.cuh"
 
 #include <cstdarg>
@@ -16,6 +17,7 @@
 #include <algorithm>
 #include <cstring>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 using namespace lbx;
@@ -62,48 +64,6 @@ namespace {
 
 }  // namespace
 
-struct lbx_domain {
-  lbx_params p;
-  int Q = 0, D = 0;
-  long long N = 0;
-  size_t real_size = 0;
-  void* f = nullptr;          // [nsubs][Q][N] dense (the exchange format)
-  void* fc = nullptr;         // [nsubs][Q][P] compact layout
-  int* fidx = nullptr;        // [N] dense -> compact (-1 solid)
-  int* fnode = nullptr;       // [F] compact -> dense
-  long long P = 0;            // compact plane stride: fluid rounded up to 32
-  int layout = LBX_LAYOUT_DENSE;
-  bool dense_stale = false;   // compact state newer than the dense array
-  void* mv = nullptr;         // [nsubs][1+D][N]
-  uint8_t* solids = nullptr;  // [N] as given (device rule: == 1)
-  uint8_t* cls = nullptr;     // [N]
-  uint32_t* nbm = nullptr;    // [N]
-  void* red = nullptr;        // reduction partials
-  int red_blocks = 0;
-  cudaStream_t stream = nullptr;      // stream all work is queued on
-  cudaStream_t own_stream = nullptr;  // the library's stream
-  std::vector<double> n_table, s_table;
-  long long fluid = 0;
-  bool faces_active = false;  // any 2D face boundary configured
-  bool faces_fused = false;   // fused into the step kernels
-  bool faces3_active = false; // any 3D z-face boundary configured
-  std::vector<long long> plane_fluid;  // fluid nodes per plane (k in 3D, j in 2D)
-  // breakthrough record (lbx_btc_*)
-  void* ubuf = nullptr;        // [3][P or N] flow velocity for the solute launch
-  double* btc_vals = nullptr;  // C of the plane's nodes this step
-  double* btc_rec = nullptr;   // [btc_cap] means
-  int* btc_slot = nullptr;     // steps recorded
-  int btc_cap = 0;
-  int btc_lo = 0, btc_hi = 0;  // node (dense) or slot (compact) range
-  int btc_plane = 0;
-  int parity = 0;             // 0: natural order (next step odd); 1: swapped
-  long long launches = 0;
-  // graph replay of frame-free, time-invariant runs: one captured AA pair
-  cudaGraphExec_t graph = nullptr;
-  cudaStream_t graph_stream = nullptr;   // stream the pair was captured on
-  unsigned char graph_key[2 * 640];      // keys of the odd and the even step
-  size_t graph_key_len = 0;
-};
 
 namespace {
 
@@ -153,6 +113,7 @@ void fill_args(const lbx_domain* d, int t, unsigned flags, StepArgs<T>& A)
   A.write_mv = (flags & LBX_WRITE_MV) ? 1 : 0;
   A.solute_on = (t >= p.sigma_t_on && t <= p.sigma_t_off) ? 1 : 0;
   A.ubuf = (T*)d->ubuf;
+  A.fout = (T*)d->fout;
   A.ustride = d->layout == LBX_LAYOUT_COMPACT ? d->P : d->N;
   if (d->btc_vals) {
     A.btc = d->btc_vals;
@@ -200,12 +161,18 @@ void launch_part(lbx_domain* d, const StepArgs<T>& A, bool odd)
     const unsigned blocks = (unsigned)((d->fluid + 255) / 256);
     if (blocks == 0) return;
     const bool idx32 = (unsigned long long)Q * (unsigned long long)d->P < (1ull << 32);
-    if (idx32) {
-      if (odd) aa_step_compact<T, Q, NS, MODEL, true, PART, true><<<blocks, 256, 0, d->stream>>>(C);
-      else aa_step_compact<T, Q, NS, MODEL, false, PART, true><<<blocks, 256, 0, d->stream>>>(C);
+    auto go = [&](auto odd_c, auto idx_c, auto oop_c) {
+      aa_step_compact<T, Q, NS, MODEL, decltype(odd_c)::value, PART, decltype(idx_c)::value,
+                      decltype(oop_c)::value><<<blocks, 256, 0, d->stream>>>(C);
+    };
+    using TT = std::true_type;
+    using FF = std::false_type;
+    if (A.fout) {
+      if (idx32) { if (odd) go(TT{}, TT{}, TT{}); else go(FF{}, TT{}, TT{}); }
+      else { if (odd) go(TT{}, FF{}, TT{}); else go(FF{}, FF{}, TT{}); }
     } else {
-      if (odd) aa_step_compact<T, Q, NS, MODEL, true, PART, false><<<blocks, 256, 0, d->stream>>>(C);
-      else aa_step_compact<T, Q, NS, MODEL, false, PART, false><<<blocks, 256, 0, d->stream>>>(C);
+      if (idx32) { if (odd) go(TT{}, TT{}, FF{}); else go(FF{}, TT{}, FF{}); }
+      else { if (odd) go(TT{}, FF{}, FF{}); else go(FF{}, FF{}, FF{}); }
     }
     d->launches++;
     return;
@@ -318,14 +285,15 @@ void launch_faces3(lbx_domain* d, int t, bool second)
   dim3 block(128), grid((p.LX + 127) / 128, p.LY);
   for_each_face3<T>(d, t, [&](int top, int kind, int s, T drho) {
     T* fs = (T*)(compact ? d->fc : d->f) + (long long)s * d->Q * stride;
+    const T* prof = kind == FACE_CONSTCON ? (const T*)(top ? d->prof_t : d->prof_b) : nullptr;
     if (compact)
       face_plane<T, true><<<grid, block, 0, d->stream>>>(fs, nullptr, d->fidx, p.LX, p.LY, p.LZ,
                                                           stride, top, kind, second ? 1 : 0,
-                                                          drho, conc);
+                                                          drho, conc, prof);
     else
       face_plane<T, false><<<grid, block, 0, d->stream>>>(fs, d->solids, nullptr, p.LX, p.LY,
                                                            p.LZ, stride, top, kind,
-                                                           second ? 1 : 0, drho, conc);
+                                                           second ? 1 : 0, drho, conc, prof);
     d->launches++;
   });
 }
@@ -362,8 +330,8 @@ lbx_status step_t(lbx_domain* d, int t, unsigned flags)
     const bool compact = d->layout == LBX_LAYOUT_COMPACT;
     btc_reduce<<<1, kBtcThreads, 0, d->stream>>>(
         d->btc_vals, d->btc_hi - d->btc_lo, compact ? nullptr : d->solids + d->btc_lo,
-        (double)d->plane_fluid[d->btc_plane], A.solute_on, d->btc_rec, d->btc_slot,
-        d->btc_cap);
+        (double)d->plane_fluid[d->btc_plane], d->p.nsubs == 2 && A.solute_on, d->btc_rec,
+        d->btc_slot, d->btc_cap);
     d->launches++;
   }
   CK(cudaGetLastError());
@@ -450,7 +418,8 @@ void release(lbx_domain* d)
   cudaFree(d->f); cudaFree(d->mv); cudaFree(d->solids); cudaFree(d->cls);
   cudaFree(d->nbm); cudaFree(d->red);
   cudaFree(d->btc_vals); cudaFree(d->btc_rec); cudaFree(d->btc_slot);
-  cudaFree(d->ubuf);
+  cudaFree(d->ubuf); cudaFree(d->prof_t); cudaFree(d->prof_b);
+  lbx_internal_adjoint_free(d);
   if (d->own_stream) cudaStreamDestroy(d->own_stream);
 }
 
@@ -475,6 +444,24 @@ lbx_status do_step(lbx_domain* d, int t, unsigned flags)
   }
   return st;
 }
+
+}  // namespace
+
+// The step at time t on the compact state `src` (its face operations in
+// place), writing the result to `dst`; no plane record.  Used to recompute
+// stored forward states for the adjoint.
+lbx_status lbx_internal_step_into(lbx_domain* d, int t, void* src, void* dst)
+{
+  if (d->layout != LBX_LAYOUT_COMPACT) return fail(LBX_ERR_INVALID, "compact layout required");
+  void* fc = d->fc;
+  double* bv = d->btc_vals;
+  d->fc = src; d->fout = dst; d->btc_vals = nullptr;
+  lbx_status st = d->real_size == 8 ? step_t<double>(d, t, 0) : step_t<float>(d, t, 0);
+  d->fc = fc; d->fout = nullptr; d->btc_vals = bv;
+  return st;
+}
+
+namespace {
 
 // The launch arguments of the step at time t, as bytes (for comparing steps:
 // two steps with equal bytes launch identical work).
@@ -924,7 +911,6 @@ lbx_status lbx_btc_stop(lbx_domain* d)
 lbx_status lbx_btc_start(lbx_domain* d, int plane, int capacity)
 {
   if (!d) return fail(LBX_ERR_INVALID, "domain is NULL");
-  if (d->p.nsubs != 2) return fail(LBX_ERR_INVALID, "a breakthrough record needs the solute lattice");
   const int planes = d->p.dims == 2 ? d->p.LY : d->p.LZ;
   if (plane < 0 || plane >= planes) return fail(LBX_ERR_INVALID, "plane %d out of range", plane);
   if (capacity < 1) return fail(LBX_ERR_INVALID, "capacity must be positive");
@@ -943,8 +929,8 @@ lbx_status lbx_btc_start(lbx_domain* d, int plane, int capacity)
   d->btc_lo = (int)lo; d->btc_hi = (int)hi;
   d->btc_plane = plane;
   d->btc_cap = capacity;
-  CK(cudaMalloc(&d->btc_vals, std::max<long long>(1, hi - lo) * sizeof(double)));
-  CK(cudaMalloc(&d->btc_rec, (size_t)capacity * sizeof(double)));
+  CK(cudaMalloc(&d->btc_vals, 2 * std::max<long long>(1, hi - lo) * sizeof(double)));
+  CK(cudaMalloc(&d->btc_rec, (size_t)capacity * 2 * sizeof(double)));
   CK(cudaMalloc(&d->btc_slot, sizeof(int)));
   CK(cudaMemsetAsync(d->btc_slot, 0, sizeof(int), d->stream));
   // the step arguments changed: a captured pair no longer matches
@@ -952,19 +938,44 @@ lbx_status lbx_btc_start(lbx_domain* d, int plane, int capacity)
   return LBX_OK;
 }
 
-lbx_status lbx_btc_read(lbx_domain* d, double* out, int max, long long* count)
+lbx_status lbx_btc_read(lbx_domain* d, double* c_out, double* ux_out, int max,
+                        long long* count)
 {
-  if (!d || (!out && max > 0)) return fail(LBX_ERR_INVALID, "NULL argument");
-  if (!d->btc_slot) return fail(LBX_ERR_STATE, "no breakthrough record started");
+  if (!d || (!c_out && !ux_out && max > 0)) return fail(LBX_ERR_INVALID, "NULL argument");
+  if (!d->btc_slot) return fail(LBX_ERR_STATE, "no plane record started");
   int slot = 0;
   CK(cudaMemcpyAsync(&slot, d->btc_slot, sizeof(int), cudaMemcpyDeviceToHost, d->stream));
   CK(cudaStreamSynchronize(d->stream));
   const int n = std::min(std::min(slot, d->btc_cap), std::max(max, 0));
   if (n > 0) {
-    CK(cudaMemcpyAsync(out, d->btc_rec, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, d->stream));
+    std::vector<double> rec((size_t)2 * n);
+    CK(cudaMemcpyAsync(rec.data(), d->btc_rec, rec.size() * sizeof(double),
+                       cudaMemcpyDeviceToHost, d->stream));
     CK(cudaStreamSynchronize(d->stream));
+    for (int q = 0; q < n; ++q) {
+      if (c_out) c_out[q] = rec[2 * q];
+      if (ux_out) ux_out[q] = rec[2 * q + 1];
+    }
   }
   if (count) *count = slot;
+  return LBX_OK;
+}
+
+lbx_status lbx_set_face_profile(lbx_domain* d, int top, const double* conc)
+{
+  if (!d) return fail(LBX_ERR_INVALID, "domain is NULL");
+  void*& dst = top ? d->prof_t : d->prof_b;
+  CK(cudaStreamSynchronize(d->stream));
+  if (d->graph) { cudaGraphExecDestroy(d->graph); d->graph = nullptr; }
+  if (!conc) { cudaFree(dst); dst = nullptr; return LBX_OK; }
+  const size_t n = (size_t)d->p.LX * d->p.LY;
+  if (!dst) CK(cudaMalloc(&dst, n * d->real_size));
+  if (d->real_size == 8) {
+    CK(cudaMemcpy(dst, conc, n * sizeof(double), cudaMemcpyHostToDevice));
+  } else {
+    std::vector<float> h(conc, conc + n);
+    CK(cudaMemcpy(dst, h.data(), n * sizeof(float), cudaMemcpyHostToDevice));
+  }
   return LBX_OK;
 }
 

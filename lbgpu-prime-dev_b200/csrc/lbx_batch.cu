@@ -18,6 +18,7 @@
 // lbx_batch_autotune times each mode and block size on a few steps and
 // keeps the fastest.
 #include "lbx.h"
+#include "lbx_internal.h"
 #include "lbx_kernels.cuh"
 
 #include <cooperative_groups.h>
@@ -32,7 +33,6 @@
 namespace cg = cooperative_groups;
 using namespace lbx;
 
-lbx_status lbx_internal_fail(lbx_status code, const char* msg);
 
 namespace {
 

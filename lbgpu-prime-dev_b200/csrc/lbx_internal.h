@@ -1,0 +1,62 @@
+// lbx_internal.h -- the domain handle's layout, shared by the library's
+// translation units (not part of the ABI).
+#pragma once
+
+#include "lbx.h"
+
+#include <cuda_runtime.h>
+
+#include <vector>
+
+struct lbx_domain {
+  lbx_params p;
+  int Q = 0, D = 0;
+  long long N = 0;
+  size_t real_size = 0;
+  void* f = nullptr;          // [nsubs][Q][N] dense (the exchange format)
+  void* fc = nullptr;         // [nsubs][Q][P] compact layout
+  int* fidx = nullptr;        // [N] dense -> compact (-1 solid)
+  int* fnode = nullptr;       // [F] compact -> dense
+  long long P = 0;            // compact plane stride: fluid rounded up to 32
+  int layout = LBX_LAYOUT_DENSE;
+  bool dense_stale = false;   // compact state newer than the dense array
+  void* mv = nullptr;         // [nsubs][1+D][N]
+  uint8_t* solids = nullptr;  // [N] as given (device rule: == 1)
+  uint8_t* cls = nullptr;     // [N]
+  uint32_t* nbm = nullptr;    // [N]
+  void* red = nullptr;        // reduction partials
+  int red_blocks = 0;
+  cudaStream_t stream = nullptr;      // stream all work is queued on
+  cudaStream_t own_stream = nullptr;  // the library's stream
+  std::vector<double> n_table, s_table;
+  long long fluid = 0;
+  bool faces_active = false;  // any 2D face boundary configured
+  bool faces_fused = false;   // fused into the step kernels
+  bool faces3_active = false; // any 3D z-face boundary configured
+  std::vector<long long> plane_fluid;  // fluid nodes per plane (k in 3D, j in 2D)
+  void* ubuf = nullptr;        // [3][P or N] flow velocity for the solute launch
+  void* prof_t = nullptr;      // [LX*LY] constant-concentration profiles (real)
+  void* prof_b = nullptr;
+  // plane record (lbx_btc_*)
+  double* btc_vals = nullptr;  // [2][plane nodes]: C and u_x this step
+  double* btc_rec = nullptr;   // [btc_cap][2] means
+  int* btc_slot = nullptr;     // steps recorded
+  int btc_cap = 0;
+  int btc_lo = 0, btc_hi = 0;  // node (dense) or slot (compact) range
+  int btc_plane = 0;
+  void* fout = nullptr;        // set only while recomputing states (OOP step)
+  void* adj = nullptr;         // adjoint checkpoints and objective (lbx_adjoint.cu)
+  int parity = 0;             // 0: natural order (next step odd); 1: swapped
+  long long launches = 0;
+  // graph replay of frame-free, time-invariant runs: one captured AA pair
+  cudaGraphExec_t graph = nullptr;
+  cudaStream_t graph_stream = nullptr;   // stream the pair was captured on
+  unsigned char graph_key[2 * 640];      // keys of the odd and the even step
+  size_t graph_key_len = 0;
+};
+
+// Hidden helpers of the library's translation units (not exported).
+#define LBX_HIDDEN __attribute__((visibility("hidden")))
+LBX_HIDDEN lbx_status lbx_internal_fail(lbx_status code, const char* msg);
+LBX_HIDDEN lbx_status lbx_internal_step_into(lbx_domain* d, int t, void* src, void* dst);
+LBX_HIDDEN void lbx_internal_adjoint_free(lbx_domain* d);

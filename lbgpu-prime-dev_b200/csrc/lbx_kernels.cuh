@@ -154,10 +154,11 @@ struct StepArgs {
   int face_n[2], face_s[2];   // FaceKind per substance (2D, fused path)
   T rho_n[2], rho_s[2];       // face densities this step
   T drho_n[2], drho_s[2];     // face density minus rho_A, formed in double
-  double* btc;                // breakthrough record: C of the nodes [btc_lo, btc_hi)
+  double* btc;                // plane record: [0][.] C, [1][.] u_x of the nodes [btc_lo, btc_hi)
   int btc_lo, btc_hi;         // node (dense) or slot (compact) range of the plane
   T* ubuf;                    // [3][stride]: the flow's u, handed to the solute
   long long ustride;          // N (dense) or P (compact)
+  T* fout;                    // compact, OOP kernels: where the step's result goes
 };
 
 // Which substances one launch of a step kernel advances.  Two-substance
@@ -379,8 +380,10 @@ aa_step(StepArgs<T> A)
 #pragma unroll
       for (int c = 0; c < D; ++c) A.ubuf[c * A.ustride + n] = u[c];
     }
-    if (NS == 2 && solute && A.btc && n >= A.btc_lo && n < A.btc_hi)
-      A.btc[n - A.btc_lo] = (double)rho;
+    if (A.btc && n >= A.btc_lo && n < A.btc_hi) {
+      if (NS == 2 && solute) A.btc[n - A.btc_lo] = (double)rho;
+      else if (!solute) A.btc[(A.btc_hi - A.btc_lo) + (n - A.btc_lo)] = (double)u[0];
+    }
     if (ODD) {
       // push: f[opp a][n + c_a] = d_a, or own f[a][n] in front of a solid
       // (offsets laundered so the pull addresses are not kept live)
@@ -429,7 +432,9 @@ constexpr int compact_min_blocks()
 
 // IDX32: population offsets within one substance's [Q][P] block fit in 32
 // bits (Q * P < 2^32), so slot selects and address arithmetic stay 32-bit.
-template <typename T, int Q, int NS, int MODEL, bool ODD, int PART, bool IDX32>
+// OOP: write the step's result to C.s.fout instead of in place (used to
+// recompute stored forward states for the adjoint).
+template <typename T, int Q, int NS, int MODEL, bool ODD, int PART, bool IDX32, bool OOP>
 __global__ void __launch_bounds__(256, (compact_min_blocks<T, PART>()))
 aa_step_compact(CompactArgs<T> C)
 {
@@ -491,6 +496,7 @@ aa_step_compact(CompactArgs<T> C)
       if (D == 3) { zm = opaque(zm); zp = opaque(zp); }
     }
     T* const fs = A.f + (size_t)s * Q * F;
+    T* const fo = (OOP ? A.fout : A.f) + (size_t)s * Q * F;
     T d[Q];
     if (ODD) {
       // pull: d_a = f[a][idx(n - c_a)], or own f[opp a] behind a solid; the
@@ -518,8 +524,10 @@ aa_step_compact(CompactArgs<T> C)
 #pragma unroll
       for (int c = 0; c < D; ++c) A.ubuf[c * A.ustride + m] = u[c];
     }
-    if (NS == 2 && solute && A.btc && m >= A.btc_lo && m < A.btc_hi)
-      A.btc[m - A.btc_lo] = (double)rho;
+    if (A.btc && m >= A.btc_lo && m < A.btc_hi) {
+      if (NS == 2 && solute) A.btc[m - A.btc_lo] = (double)rho;
+      else if (!solute) A.btc[(A.btc_hi - A.btc_lo) + (m - A.btc_lo)] = (double)u[0];
+    }
     if (ODD) {
       // push: f[opp a][idx(n + c_a)] = d_a, or own f[a] in front of a solid;
       // the neighbour indices are re-read rather than kept in registers
@@ -529,12 +537,12 @@ aa_step_compact(CompactArgs<T> C)
       for (int a = 0; a < Q; ++a) {
         const int dn = (a == 0) ? m : nb_push(a);
         const Idx dst = (dn >= 0) ? (Idx)opp(a) * F + (Idx)dn : (Idx)a * F + (Idx)m;
-        fs[dst] = d[a];
+        fo[dst] = d[a];
       }
     } else {
       const int m2 = opaque(m);   // do not keep the load addresses live
 #pragma unroll
-      for (int a = 0; a < Q; ++a) fs[a * F + m2] = d[a];
+      for (int a = 0; a < Q; ++a) fo[a * F + m2] = d[a];
     }
   }
 }
@@ -731,7 +739,8 @@ __device__ __forceinline__ void face3_apply(T (&d)[19], bool top, int kind, T dr
   }
 }
 
-// One face operation on the plane, one thread per (i, j).  `_1` form
+// One face operation on the plane, one thread per (i, j); a constant-
+// concentration face takes its C from `profile[i + LX*j]` when given.  `_1` form
 // (second == 0, before an odd step): loads what the odd step will pull and
 // deposits the unknowns where it will pull them from (slot a of the
 // upstream node, or of the node itself behind a solid, as set_f1d_d does);
@@ -740,7 +749,7 @@ __device__ __forceinline__ void face3_apply(T (&d)[19], bool top, int kind, T dr
 template <typename T, bool COMPACT>
 __global__ void face_plane(T* fs, const uint8_t* solids, const int* fidx, int LX, int LY,
                            int LZ, long long stride, int top, int kind, int second, T drho,
-                           T conc)
+                           T conc, const T* profile)
 {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= LX) return;
@@ -771,7 +780,7 @@ __global__ void face_plane(T* fs, const uint8_t* solids, const int* fidx, int LX
       d[a] = (up < 0) ? fs[opp(a) * stride + self] : fs[a * stride + up];
     }
   }
-  face3_apply<T>(d, top != 0, kind, drho, conc);
+  face3_apply<T>(d, top != 0, kind, drho, profile ? profile[i + LX * j] : conc);
 #pragma unroll
   for (int q = 0; q < 5; ++q) {
     const int a = face3_unknown(top != 0, q);
@@ -784,30 +793,41 @@ __global__ void face_plane(T* fs, const uint8_t* solids, const int* fidx, int LX
   }
 }
 
-// ---- breakthrough record ------------------------------------------------------
-// One block: the mean of the plane's recorded C values (skipping solid nodes
-// of a dense plane) into rec[*slot], then the slot advances.  The sum order
-// is fixed, so the record is reproducible run to run.
+// ---- plane record ---------------------------------------------------------------
+// One block: the means over the plane's fluid nodes of the recorded C
+// (channel 0, when the solute was active) and u_x (channel 1) into
+// rec[2 * slot + channel] (skipping solid nodes of a dense plane), then the
+// slot advances.  The sum order is fixed, so the record is reproducible.
 constexpr int kBtcThreads = 1024;
 
 static __global__ void __launch_bounds__(kBtcThreads)
 btc_reduce(const double* vals, int count, const uint8_t* plane_solids, double fluid,
-           int on, double* rec, int* slot, int capacity)
+           int on_c, double* rec, int* slot, int capacity)
 {
-  __shared__ double part[kBtcThreads];
-  double s = 0.0;
-  if (on)
-    for (int q = threadIdx.x; q < count; q += kBtcThreads)
-      if (!plane_solids || plane_solids[q] != 1) s += vals[q];
-  part[threadIdx.x] = s;
+  __shared__ double part[2][kBtcThreads];
+  double sc = 0.0, su = 0.0;
+  for (int q = threadIdx.x; q < count; q += kBtcThreads)
+    if (!plane_solids || plane_solids[q] != 1) {
+      if (on_c) sc += vals[q];
+      su += vals[count + q];
+    }
+  part[0][threadIdx.x] = sc;
+  part[1][threadIdx.x] = su;
   __syncthreads();
   for (int w = kBtcThreads / 2; w > 0; w >>= 1) {
-    if (threadIdx.x < w) part[threadIdx.x] += part[threadIdx.x + w];
+    if (threadIdx.x < w) {
+      part[0][threadIdx.x] += part[0][threadIdx.x + w];
+      part[1][threadIdx.x] += part[1][threadIdx.x + w];
+    }
     __syncthreads();
   }
   if (threadIdx.x == 0) {
     const int k = *slot;
-    if (k < capacity) rec[k] = (on && fluid > 0.0) ? part[0] / fluid : __longlong_as_double(0x7ff8000000000000LL);
+    const double nan = __longlong_as_double(0x7ff8000000000000LL);
+    if (k < capacity) {
+      rec[2 * k] = (on_c && fluid > 0.0) ? part[0][0] / fluid : nan;
+      rec[2 * k + 1] = fluid > 0.0 ? part[1][0] / fluid : nan;
+    }
     *slot = k + 1;
   }
 }

@@ -51,6 +51,16 @@ class _CParams(C.Structure):
     ]
 
 
+class _CObjective(C.Structure):
+    _fields_ = [("plane", C.c_int), ("t_first", C.c_int), ("t_last", C.c_int),
+                ("w_c", C.c_double), ("w_ux", C.c_double)]
+
+
+class _CGradient(C.Structure):
+    _fields_ = [("J", C.c_double), ("d_gaccel", C.c_double * 3), ("d_tau", C.c_double),
+                ("d_tau_s", C.c_double)]
+
+
 class _CReductions(C.Structure):
     _fields_ = [
         ("mass", C.c_double), ("solute_mass", C.c_double),
@@ -99,8 +109,13 @@ _SIGNATURES = {
     "lbx_batch_reduce": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(_CReductions)]),
     "lbx_batch_launch_count": (C.c_longlong, [C.c_void_p]),
     "lbx_btc_start": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
-    "lbx_btc_read": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.c_int,
-                               C.POINTER(C.c_longlong)]),
+    "lbx_btc_read": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                               C.c_int, C.POINTER(C.c_longlong)]),
+    "lbx_set_face_profile": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_double)]),
+    "lbx_adjoint_forward": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int,
+                                      C.POINTER(_CObjective), C.POINTER(C.c_double)]),
+    "lbx_adjoint_backward": (C.c_int, [C.c_void_p, C.POINTER(_CGradient),
+                                       C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "lbx_btc_stop": (C.c_int, [C.c_void_p]),
     "lbx_last_error": (C.c_char_p, []),
 }
@@ -349,18 +364,62 @@ class Domain:
         return int(_lib.lbx_launch_count(self._h))
 
     def btc_start(self, plane: int, capacity: int):
-        """Record the mean solute C over the fluid nodes of `plane` (k in
-        3D, j in 2D) after every following step."""
+        """Record the means of the solute C and the flow u_x over the fluid
+        nodes of `plane` (k in 3D, j in 2D) after every following step."""
         _check(_lib.lbx_btc_start(self._h, plane, capacity))
 
-    def btc_read(self) -> np.ndarray:
+    def btc_read(self, ux: bool = False):
+        """The recorded C means (the breakthrough curve); with ux=True the
+        pair (C means, u_x means)."""
         n = C.c_longlong()
-        _check(_lib.lbx_btc_read(self._h, None, 0, C.byref(n)))
-        out = np.empty(max(int(n.value), 0), dtype=np.float64)
+        _check(_lib.lbx_btc_read(self._h, None, None, 0, C.byref(n)))
+        c = np.empty(max(int(n.value), 0), dtype=np.float64)
+        u = np.empty_like(c)
+        P = C.POINTER(C.c_double)
         got = C.c_longlong()
-        _check(_lib.lbx_btc_read(self._h, out.ctypes.data_as(C.POINTER(C.c_double)),
-                                 out.size, C.byref(got)))
-        return out[:min(out.size, int(got.value))]
+        _check(_lib.lbx_btc_read(self._h, c.ctypes.data_as(P), u.ctypes.data_as(P),
+                                 c.size, C.byref(got)))
+        k = min(c.size, int(got.value))
+        return (c[:k], u[:k]) if ux else c[:k]
+
+    def adjoint_forward(self, t0: int, nsteps: int, checkpoint_every: int, plane: int,
+                        t_first: int, t_last: int, w_c: float = 1.0, w_ux: float = 0.0) -> float:
+        """Run `nsteps` steps storing checkpoints; return the plane
+        objective J (see lbx_adjoint_forward)."""
+        ob = _CObjective(plane, t_first, t_last, w_c, w_ux)
+        J = C.c_double()
+        _check(_lib.lbx_adjoint_forward(self._h, t0, nsteps, checkpoint_every, C.byref(ob),
+                                        C.byref(J)))
+        return J.value
+
+    def adjoint_backward(self, profile_b: bool = False, profile_t: bool = False) -> dict:
+        """Gradients of the last adjoint_forward's J."""
+        g = _CGradient()
+        n = self.p.LX * self.p.LY
+        pb = np.zeros(n) if profile_b else None
+        pt = np.zeros(n) if profile_t else None
+        P = C.POINTER(C.c_double)
+        _check(_lib.lbx_adjoint_backward(self._h, C.byref(g),
+                                         pb.ctypes.data_as(P) if pb is not None else None,
+                                         pt.ctypes.data_as(P) if pt is not None else None))
+        out = dict(J=g.J, d_gaccel=tuple(g.d_gaccel), d_tau=g.d_tau, d_tau_s=g.d_tau_s)
+        if pb is not None:
+            out["d_profile_b"] = pb
+        if pt is not None:
+            out["d_profile_t"] = pt
+        return out
+
+    def set_face_profile(self, top: bool, conc):
+        """Per-node concentration (LX*LY, i fastest) of a constant-
+        concentration face; None returns to rho_sigma_in."""
+        if conc is None:
+            _check(_lib.lbx_set_face_profile(self._h, 1 if top else 0, None))
+            return
+        a = np.ascontiguousarray(conc, dtype=np.float64).reshape(-1)
+        if a.size != self.p.LX * self.p.LY:
+            raise ValueError("profile must hold LX*LY values")
+        _check(_lib.lbx_set_face_profile(self._h, 1 if top else 0,
+                                         a.ctypes.data_as(C.POINTER(C.c_double))))
 
     def btc_stop(self):
         _check(_lib.lbx_btc_stop(self._h))

@@ -3,6 +3,7 @@
     python -m lbx.configs cfg1 [--steps 2000]
     python -m lbx.configs cfg2 [--steps 10000]
     python -m lbx.configs cfg3 [--steps 20000]
+    python -m lbx.configs cfg5 [--steps 4000]
 
 cfg1: D2Q9 BGK 256x256, FP64, tau = 1.0, non-overlapping discs r = 8 to
       porosity 0.6 (the inlet/outlet rows kept fluid), Zou-He pressure
@@ -28,6 +29,16 @@ cfg3: D3Q19 flow + D3Q19 solute, 192x192x384, FP32, tau = 0.9, tau_s = 0.7,
       (FP64) every 1000 steps, the same run in FP64 for the precision
       comparison, and the solute mass drift of a closed periodic box (no
       faces, no sink) holding a blob of solute, where mass must be conserved.
+cfg5: discrete adjoint, D3Q19 flow + solute, 128^3, FP32 (FP64 gradient
+      sums), spheres r = 4 to porosity 0.45 (face planes kept fluid),
+      tau = 0.8, tau_s = 0.75, body force gx = 1e-5 (periodic flow along x),
+      solute held at the bottom plane by a 128x128 profile ~ U[0, 1] (seeded),
+      zero gradient at the top, 4000 steps, checkpoints every 100.
+      Objectives over the last 500 steps on the top plane: mean C, and mean
+      u_x (the outlet x-flux).  Gradients w.r.t. gx, tau, tau_s and the
+      profile, checked against FP64 central differences (h = 1e-6, relative
+      for the scalars, along random unit directions for the profile);
+      reports the adjoint's cost relative to one forward solve.
 cfg4: 512 independent D3Q19 samples, FP32 shifted, cubic edges drawn from
       U{32..96}, tau ~ U[0.6, 1.2], porosity ~ U[0.3, 0.7], sphere radius
       ~ U{3..6} (seed base + i), gx = 1e-6, periodic.  One batch; reports the
@@ -224,6 +235,100 @@ def run_cfg3(steps: int = 20000, shape=(192, 192, 384), chunk: int = 1000) -> li
     return out
 
 
+def cfg5_params(precision: int = 4, n: int = 128, gx: float = 1e-5, tau: float = 0.8,
+                tau_s: float = 0.75, seed: int = 5005):
+    mask = geometry.sphere_pack(n, n, n, radius=4, porosity=0.45, seed=seed)
+    m3 = mask.reshape(n, n, n)
+    m3[0] = 0
+    m3[-1] = 0
+    p = Params(dims=3, LX=n, LY=n, LZ=n, nsubs=2, precision=precision, tau=(tau, tau_s),
+               gaccel=(gx, 0, 0, 0, 0, 0), sigma_t_on=0, sigma_t_off=1 << 30,
+               constcon_b_in=1, zeroconcgrad_t=1, rho_sigma_in=1.0)
+    profile = np.random.default_rng(seed + 1).uniform(0.0, 1.0, n * n)
+    return p, mask, profile
+
+
+def _cfg5_objective(p, mask, profile, steps, K, obj, grads, stream=None):
+    import torch
+    with Domain(p, mask) as dom:
+        if stream is not None:
+            dom.set_stream(stream.cuda_stream)
+        dom.set_face_profile(False, profile)
+        dom.init_equilibrium(0, 1.0, 0.0, 0.0, 0.0)
+        dom.init_equilibrium(1, 0.0, 0.0, 0.0, 0.0)
+        torch.cuda.synchronize()
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        s = stream or torch.cuda.current_stream()
+        e0.record(s)
+        J = dom.adjoint_forward(0, steps, K, *obj)
+        e1.record(s)
+        g = dom.adjoint_backward(profile_b=True) if grads else None
+        e2.record(s)
+        s.synchronize()
+        return J, g, e0.elapsed_time(e1) / 1e3, (e1.elapsed_time(e2) / 1e3 if grads else 0.0)
+
+
+def run_cfg5(steps: int = 4000, n: int = 128, K: int = 100, window: int = 500,
+             fd_dirs: int = 2) -> list:
+    import torch
+    s = torch.cuda.Stream()
+    out = []
+    plane = n - 1
+    objs = {"outlet_C": (plane, steps - window + 1, steps, 1.0, 0.0),
+            "outlet_ux": (plane, steps - window + 1, steps, 0.0, 1.0)}
+    p32, mask, prof = cfg5_params(4, n)
+    # plain forward solve (the cost unit): lbx_run, no checkpoints
+    with Domain(p32, mask) as dom:
+        dom.set_stream(s.cuda_stream)
+        dom.set_face_profile(False, prof)
+        dom.init_equilibrium(0, 1.0, 0.0, 0.0, 0.0)
+        dom.init_equilibrium(1, 0.0, 0.0, 0.0, 0.0)
+        dom.run(0, 20, 0)
+        dom.init_equilibrium(0, 1.0, 0.0, 0.0, 0.0)
+        dom.init_equilibrium(1, 0.0, 0.0, 0.0, 0.0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        dom.run(0, steps, 0)
+        e1.record(s)
+        s.synchronize()
+        t_plain = e0.elapsed_time(e1) / 1e3
+    rng = np.random.default_rng(77)
+    dirs = [v / np.linalg.norm(v) for v in rng.standard_normal((fd_dirs, n * n))]
+    base = dict(gx=1e-5, tau=0.8, tau_s=0.75)
+    for name, obj in objs.items():
+        J32, g, t_fwd, t_bwd = _cfg5_objective(p32, mask, prof, steps, K, obj, True, s)
+        p64, _, _ = cfg5_params(8, n)
+        J64 = _cfg5_objective(p64, mask, prof, steps, steps, obj, False, s)[0]
+
+        def J_at(**kw):
+            q = dict(base, **{k: v for k, v in kw.items() if k != "dprof"})
+            pp, _, _ = cfg5_params(8, n, **q)
+            return _cfg5_objective(pp, mask, prof + kw.get("dprof", 0.0), steps, steps, obj,
+                                   False, s)[0]
+
+        checks = {}
+        for key, adj in (("gx", g["d_gaccel"][0]), ("tau", g["d_tau"]), ("tau_s", g["d_tau_s"])):
+            h = 1e-6 * base[key]
+            fd = (J_at(**{key: base[key] + h}) - J_at(**{key: base[key] - h})) / (2 * h)
+            checks[key] = {"adjoint_fp32": adj, "fd_fp64": fd,
+                           "rel_err": abs(adj - fd) / max(abs(fd), 1e-300) if fd != 0 else abs(adj)}
+        for q, v in enumerate(dirs):
+            h = 1e-6
+            fd = (J_at(dprof=h * v) - J_at(dprof=-h * v)) / (2 * h)
+            adj = float(g["d_profile_b"] @ v)
+            checks["profile_dir%d" % q] = {"adjoint_fp32": adj, "fd_fp64": fd,
+                                           "rel_err": abs(adj - fd) / max(abs(fd), 1e-300) if fd != 0 else abs(adj)}
+        out.append({"config": "cfg5", "objective": name, "lattice": [n] * 3, "steps": steps,
+                    "checkpoint_every": K, "J_fp32": J32, "J_fp64": J64,
+                    "J_rel_err": abs(J32 - J64) / abs(J64) if J64 else None,
+                    "gradients": checks,
+                    "profile_grad_norm": float(np.linalg.norm(g["d_profile_b"])),
+                    "seconds_plain_forward": t_plain, "seconds_adjoint_forward": t_fwd,
+                    "seconds_adjoint_backward": t_bwd,
+                    "cost_vs_forward": (t_fwd + t_bwd) / t_plain})
+    return out
+
+
 def cfg4_samples(nsamples: int = 512, seed: int = 4000):
     rng = np.random.default_rng(seed)
     params, masks = [], []
@@ -295,7 +400,7 @@ def run_cfg4(nsamples: int = 512, steps: int = 200, perm_steps: int = 0) -> list
 
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
-    ap.add_argument("config", choices=["cfg1", "cfg2", "cfg3", "cfg4"])
+    ap.add_argument("config", choices=["cfg1", "cfg2", "cfg3", "cfg4", "cfg5"])
     ap.add_argument("--steps", type=int, default=None)
     ap.add_argument("--edge", type=int, default=256)
     ap.add_argument("--samples", type=int, default=512)
@@ -303,6 +408,9 @@ def main(argv=None) -> int:
     a = ap.parse_args(argv)
     if a.config == "cfg1":
         print(json.dumps(run_cfg1(a.steps or 2000)))
+    elif a.config == "cfg5":
+        for line in run_cfg5(a.steps or 4000):
+            print(json.dumps(line))
     elif a.config == "cfg3":
         for line in run_cfg3(a.steps or 20000):
             print(json.dumps(line))

@@ -530,7 +530,8 @@ static void zou_he_3d(real_t* d, int top, real_t drho)
 enum { F3_PRESSURE = 1, F3_ZEROGRAD = 2, F3_CONSTCON = 3 };
 
 static void face3(const ctx_t* c, real_t* fs, const uint8_t* sol, int top,
-                  int kind, int second, real_t drho, real_t conc)
+                  int kind, int second, real_t drho, real_t conc,
+                  const double* profile)
 {
   const orc_params* p = c->p;
   const int k = top ? p->LZ - 1 : 0;
@@ -558,7 +559,7 @@ static void face3(const ctx_t* c, real_t* fs, const uint8_t* sol, int top,
           int a;
           for (a = 0; a < 19; a++)
             if (CZ[a] != (top ? -1 : 1)) known += d[a];
-          X = (conc - known) / wsum;
+          X = ((profile ? (real_t)profile[i + (long)p->LX * j] : conc) - known) / wsum;
         }
         for (q = 0; q < 5; q++) d[unk[q]] = c->w[unk[q]] * X;
       }
@@ -579,21 +580,25 @@ static void apply_bcs3(const ctx_t* c, real_t* f, const uint8_t* sol, int t,
     const double rA = shifted ? (double)c->rho_A[s] : 0.;
     if (p->pressure_t_in[s])
       face3(c, fs, sol, 1, F3_PRESSURE, second,
-            (real_t)((double)face_rho(c, s, t, 1, 1, 0, 0) - rA), 0);
+            (real_t)((double)face_rho(c, s, t, 1, 1, 0, 0) - rA), 0, 0);
     if (p->pressure_t_out[s])
       face3(c, fs, sol, 1, F3_PRESSURE, second,
-            (real_t)((double)face_rho(c, s, t, 0, 0, 0, 0) - rA), 0);
+            (real_t)((double)face_rho(c, s, t, 0, 0, 0, 0) - rA), 0, 0);
     if (p->pressure_b_in[s])
       face3(c, fs, sol, 0, F3_PRESSURE, second,
-            (real_t)((double)face_rho(c, s, t, 1, 1, 0, 0) - rA), 0);
+            (real_t)((double)face_rho(c, s, t, 1, 1, 0, 0) - rA), 0, 0);
     if (p->pressure_b_out[s])
       face3(c, fs, sol, 0, F3_PRESSURE, second,
-            (real_t)((double)face_rho(c, s, t, 0, 0, 0, 0) - rA), 0);
+            (real_t)((double)face_rho(c, s, t, 0, 0, 0, 0) - rA), 0, 0);
     if (s == 1 && p->nsubs == 2) {
-      if (p->constcon_t_in) face3(c, fs, sol, 1, F3_CONSTCON, second, 0, (real_t)p->rho_sigma_in);
-      if (p->constcon_b_in) face3(c, fs, sol, 0, F3_CONSTCON, second, 0, (real_t)p->rho_sigma_in);
-      if (p->zeroconcgrad_t) face3(c, fs, sol, 1, F3_ZEROGRAD, second, 0, 0);
-      if (p->zeroconcgrad_b) face3(c, fs, sol, 0, F3_ZEROGRAD, second, 0, 0);
+      if (p->constcon_t_in)
+        face3(c, fs, sol, 1, F3_CONSTCON, second, 0, (real_t)p->rho_sigma_in,
+              p->constcon_profile_t);
+      if (p->constcon_b_in)
+        face3(c, fs, sol, 0, F3_CONSTCON, second, 0, (real_t)p->rho_sigma_in,
+              p->constcon_profile_b);
+      if (p->zeroconcgrad_t) face3(c, fs, sol, 1, F3_ZEROGRAD, second, 0, 0, 0);
+      if (p->zeroconcgrad_b) face3(c, fs, sol, 0, F3_ZEROGRAD, second, 0, 0, 0);
     }
   }
 }
@@ -616,44 +621,43 @@ int SFX(orc_run)(const orc_params* p, REAL* f, const uint8_t* solids,
   return 0;
 }
 
-/* orc_run plus a breakthrough record: btc[i] = mean over the fluid nodes of
- * the plane k = `plane` (3D) or row j = `plane` (2D) of the solute
- * concentration C computed by the step at time t0+1+i (FP64 sum in node
- * order); NaN for steps with the solute inactive. */
+/* orc_run plus a plane record: btc[i] = mean over the fluid nodes of the
+ * plane k = `plane` (3D) or row j = `plane` (2D) of the solute concentration
+ * C computed by the step at time t0+1+i (FP64 sum in node order; NaN for
+ * steps with no active solute), btc_ux[i] the same mean of the flow u_x. */
 int SFX(orc_run_btc)(const orc_params* p, REAL* f, const uint8_t* solids,
                      REAL* mv, int t0, int nsteps, int frame_rate, int nthreads,
-                     int plane, double* btc)
+                     int plane, double* btc, double* btc_ux)
 {
   ctx_t c;
   int t;
   long per, base, q, cnt = 0;
   REAL* scratch;
-  if (t0 % 2 != 0 || p->LX < 1 || p->LY < 1 || p->LZ < 1 || p->nsubs != 2) return -1;
+  if (t0 % 2 != 0 || p->LX < 1 || p->LY < 1 || p->LZ < 1) return -1;
   if (p->dims == 2 && p->LZ != 1) return -1;
   if (plane < 0 || plane >= (p->dims == 2 ? p->LY : p->LZ)) return -1;
   make_ctx(&c, p);
   per = p->dims == 2 ? (long)p->LX : (long)p->LX * p->LY;
   base = per * plane;
   for (q = 0; q < per; q++) cnt += !is_solid(solids, base + q);
-  scratch = (REAL*)malloc(sizeof(REAL) * (size_t)2 * (1 + c.D) * c.NN);
+  scratch = (REAL*)malloc(sizeof(REAL) * (size_t)p->nsubs * (1 + c.D) * c.NN);
   if (!scratch) return -2;
   for (t = t0 + 1; t <= t0 + nsteps; t++) {
     int wmv = frame_rate > 0 && t % frame_rate == 0;
     int odd = (t % 2) == 1;
     REAL* m = wmv ? mv : scratch;
-    const REAL* C;
-    double sum = 0;
+    double sc = 0, su = 0;
     if (p->dims == 2) apply_bcs(&c, f, solids, t, !odd);
     else apply_bcs3(&c, f, solids, t, !odd);
     half_step(&c, f, solids, m, t, 1, odd, nthreads);
-    if (!(t >= p->sigma_t_on && t <= p->sigma_t_off) || cnt == 0) {
-      btc[t - t0 - 1] = 0. / 0.;
-      continue;
-    }
-    C = m + (long)(1 + c.D) * c.NN;   /* subs 1, rho */
     for (q = 0; q < per; q++)
-      if (!is_solid(solids, base + q)) sum += (double)C[base + q];
-    btc[t - t0 - 1] = sum / (double)cnt;
+      if (!is_solid(solids, base + q)) {
+        su += (double)m[c.NN + base + q];                      /* subs 0, u_x */
+        if (p->nsubs == 2) sc += (double)m[(long)(1 + c.D) * c.NN + base + q];
+      }
+    btc_ux[t - t0 - 1] = cnt ? su / (double)cnt : 0. / 0.;
+    btc[t - t0 - 1] = (p->nsubs == 2 && t >= p->sigma_t_on && t <= p->sigma_t_off && cnt)
+                          ? sc / (double)cnt : 0. / 0.;
   }
   free(scratch);
   return 0;

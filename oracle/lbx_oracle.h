@@ -32,6 +32,10 @@ typedef struct {
   int constcon_t_in, constcon_b_in;   /* solute: C = rho_sigma_in on the face */
   int zeroconcgrad_t, zeroconcgrad_b;
   double rho_sigma_in;
+  /* per-node concentration of a constant-concentration face (LX*LY, i
+   * fastest), used instead of rho_sigma_in when not NULL */
+  const double* constcon_profile_t;
+  const double* constcon_profile_b;
 } orc_params;
 
 int orc_run_f64(const orc_params*, double* f, const uint8_t* solids,
@@ -42,10 +46,10 @@ int orc_run_f32(const orc_params*, float* f, const uint8_t* solids,
                 int nthreads);
 int orc_run_btc_f64(const orc_params*, double* f, const uint8_t* solids,
                     double* mv, int t0, int nsteps, int frame_rate,
-                    int nthreads, int plane, double* btc);
+                    int nthreads, int plane, double* btc, double* btc_ux);
 int orc_run_btc_f32(const orc_params*, float* f, const uint8_t* solids,
                     float* mv, int t0, int nsteps, int frame_rate,
-                    int nthreads, int plane, double* btc);
+                    int nthreads, int plane, double* btc, double* btc_ux);
 int orc_init_feq_f64(const orc_params*, const double* rho, const double* ux,
                      const double* uy, const double* uz, double* f);
 int orc_init_feq_f32(const orc_params*, const float* rho, const float* ux,

@@ -63,6 +63,8 @@ class Params:
     zeroconcgrad_t: int = 0
     zeroconcgrad_b: int = 0
     rho_sigma_in: float = 1.0
+    constcon_profile_t: Optional[np.ndarray] = None
+    constcon_profile_b: Optional[np.ndarray] = None
 
     @property
     def Q(self) -> int:
@@ -97,6 +99,8 @@ class _OrcParams(C.Structure):
         ("constcon_t_in", C.c_int), ("constcon_b_in", C.c_int),
         ("zeroconcgrad_t", C.c_int), ("zeroconcgrad_b", C.c_int),
         ("rho_sigma_in", C.c_double),
+        ("constcon_profile_t", C.POINTER(C.c_double)),
+        ("constcon_profile_b", C.POINTER(C.c_double)),
     ]
 
 
@@ -118,6 +122,13 @@ class _RefParams(C.Structure):
 
 def _fill(st, p: Params, keep):
     for name, _ in st._fields_:
+        if name.startswith("constcon_profile"):
+            v = getattr(p, name)
+            if v is not None:
+                arr = np.ascontiguousarray(v, dtype=np.float64).reshape(-1)
+                keep.append(arr)
+                setattr(st, name, arr.ctypes.data_as(C.POINTER(C.c_double)))
+            continue
         if name.endswith("_table"):
             tab = getattr(p, name)
             if tab is not None:
@@ -154,7 +165,7 @@ def _lib():
             fn = getattr(lib, "orc_run_btc_" + sfx)
             fn.argtypes = [C.POINTER(_OrcParams), C.POINTER(ct), C.c_void_p,
                            C.POINTER(ct), C.c_int, C.c_int, C.c_int, C.c_int,
-                           C.c_int, C.POINTER(C.c_double)]
+                           C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]
             fn.restype = C.c_int
             fn = getattr(lib, "orc_init_feq_" + sfx)
             fn.argtypes = [C.POINTER(_OrcParams)] + [C.POINTER(ct)] * 4 + [C.POINTER(ct)]
@@ -197,25 +208,29 @@ def run_oracle(p: Params, f: np.ndarray, solids: np.ndarray, t0: int,
 def run_oracle_btc(p: Params, f: np.ndarray, solids: np.ndarray, t0: int,
                    nsteps: int, plane: int, frame_rate: int = 0,
                    mv: Optional[np.ndarray] = None, threads: int = 0):
-    """run_oracle plus the breakthrough record of the plane k (3D) / row j
-    (2D) = `plane`: the mean solute C over its fluid nodes after every step
-    (NaN while the solute is inactive).  Returns (f, mv, btc)."""
+    """run_oracle plus the plane record of the plane k (3D) / row j (2D) =
+    `plane`: the mean solute C over its fluid nodes after every step (NaN
+    while the solute is inactive) and the mean flow u_x.  Returns
+    (f, mv, btc, btc_ux)."""
     dtype = f.dtype
     assert f.flags.c_contiguous and f.size == p.nsubs * p.Q * p.NN
     sol = np.ascontiguousarray(solids, dtype=np.uint8).reshape(-1)
     if mv is None:
         mv = np.zeros((p.nsubs, 1 + p.dims, p.NN), dtype=dtype)
     btc = np.zeros(nsteps, dtype=np.float64)
+    btc_ux = np.zeros(nsteps, dtype=np.float64)
     st = _OrcParams()
-    _fill(st, p, [])
+    keep = []
+    _fill(st, p, keep)
     nt = threads or min(os.cpu_count() or 1, 64)
+    P = C.POINTER(C.c_double)
     rc = getattr(_lib(), "orc_run_btc_" + _sfx(dtype))(
         C.byref(st), f.ctypes.data_as(C.POINTER(_ct(dtype))),
         sol.ctypes.data, mv.ctypes.data_as(C.POINTER(_ct(dtype))),
-        t0, nsteps, frame_rate, nt, plane, btc.ctypes.data_as(C.POINTER(C.c_double)))
+        t0, nsteps, frame_rate, nt, plane, btc.ctypes.data_as(P), btc_ux.ctypes.data_as(P))
     if rc != 0:
         raise ValueError("orc_run_btc rejected the parameters")
-    return f, mv, btc
+    return f, mv, btc, btc_ux
 
 
 def init_feq(p: Params, rho: np.ndarray, ux: np.ndarray, uy: np.ndarray,
@@ -225,7 +240,8 @@ def init_feq(p: Params, rho: np.ndarray, ux: np.ndarray, uy: np.ndarray,
     arrs = [np.ascontiguousarray(x, dtype=dtype).reshape(p.nsubs, p.NN)
             for x in (rho, ux, uy, uz if uz is not None else np.zeros_like(rho))]
     st = _OrcParams()
-    _fill(st, p, [])
+    keep = []
+    _fill(st, p, keep)
     ct = C.POINTER(_ct(dtype))
     getattr(_lib(), "orc_init_feq_" + _sfx(dtype))(
         C.byref(st), *[a.ctypes.data_as(ct) for a in arrs], f.ctypes.data_as(ct))

@@ -77,8 +77,8 @@ def test_gpu_breakthrough_record_matches_oracle(dtype, layout):
         d.upload_f(f0)
         d.btc_start(p.LZ - 1, 100)
         d.run(0, steps, 0)
-        btc = d.btc_read()
-    _, _, btc_o = po.run_oracle_btc(p, f0.copy(), sol, 0, steps, p.LZ - 1)
+        btc, ux = d.btc_read(ux=True)
+    _, _, btc_o, ux_o = po.run_oracle_btc(p, f0.copy(), sol, 0, steps, p.LZ - 1)
     assert btc.shape == (steps,)
     assert np.isnan(btc[:2]).all() and np.isnan(btc_o[:2]).all()   # solute off at t=1,2
     live = ~np.isnan(btc_o)
@@ -86,6 +86,8 @@ def test_gpu_breakthrough_record_matches_oracle(dtype, layout):
     scale = np.abs(btc_o[live]).max()
     assert scale > 0
     assert np.abs(btc[live] - btc_o[live]).max() <= tol * scale
+    uscale = np.abs(ux_o).max()
+    assert uscale > 0 and np.abs(ux - ux_o).max() <= tol * uscale
 
 
 def test_gpu_breakthrough_record_through_graph_replay():
@@ -114,3 +116,41 @@ def test_z_faces_rejected_in_2d_and_thin_lattices():
     for lp in bad:
         with pytest.raises(lbx.LbxError):
             lbx.Domain(lp, np.zeros(lp.NN, np.uint8))
+
+
+@pytest.mark.parametrize("layout", ["dense", "compact"])
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_gpu_constcon_profile_matches_oracle(dtype, layout):
+    """A per-node inlet concentration on the bottom face."""
+    p, sol, f0 = _flow_solute(18, 16, 14, 0.6, 11, **CASES["inlet_bottom"])
+    prof = np.random.default_rng(5).uniform(0.0, 1.0, p.LX * p.LY)
+    p.constcon_profile_b = prof
+    f0 = f0.astype(dtype)
+    with lbx.Domain(to_lbx(p, dtype, layout), sol) as d:
+        d.set_face_profile(False, prof)
+        d.upload_f(f0)
+        d.run(0, 30, 30)
+        d.sync()
+        f, mv = d.download_f(), d.download_mv()
+    fo, mvo = po.run_oracle(p, f0.copy(), sol, 0, 30, 30)
+    assert_close(f, mv, fo, mvo, sol, dtype,
+                 fp64_truth(p, f0, sol, 30, 30) if dtype == np.float32 else None)
+    # the inlet plane holds the profile after an even step
+    C = mvo[1, 0].reshape(p.LZ, p.LY, p.LX)[0].reshape(-1)
+    fl = (sol.reshape(p.LZ, -1)[0] != 1)
+    assert np.abs(C[fl] - prof[fl]).max() < (1e-12 if dtype == np.float64 else 1e-6)
+
+
+def test_gpu_flow_only_record_has_ux():
+    """A flow-only lattice records u_x means (C channel NaN)."""
+    p = po.Params(dims=3, LX=16, LY=12, LZ=10, tau=(0.8, 1.0), gaccel=(1e-5, 0, 0, 0, 0, 0))
+    sol = geometry.sphere_pack(16, 12, 10, radius=2, porosity=0.6, seed=2)
+    f0 = np.zeros((1, 19, p.NN))
+    with lbx.Domain(to_lbx(p, np.float64, "compact"), sol) as d:
+        d.upload_f(f0)
+        d.btc_start(4, 20)
+        d.run(0, 20, 0)
+        c, ux = d.btc_read(ux=True)
+    _, _, _, ux_o = po.run_oracle_btc(p, f0.copy(), sol, 0, 20, 4)
+    assert np.isnan(c).all()
+    assert np.abs(ux - ux_o).max() <= 1e-12 * np.abs(ux_o).max()
