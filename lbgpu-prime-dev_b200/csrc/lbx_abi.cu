@@ -267,12 +267,27 @@ void for_each_face3(const lbx_domain* d, int t, F&& run)
   }
 }
 
+// The face operations of step t that have an effect (the last configured
+// one on each face and substance), in one table.
+template <typename T>
+FaceOps<T> face3_table(const lbx_domain* d, int t)
+{
+  FaceOps<T> ops;
+  std::memset(&ops, 0, sizeof ops);
+  ops.conc = (T)d->p.rho_sigma_in;
+  for_each_face3<T>(d, t, [&](int top, int kind, int s, T drho) {
+    int q = 0;
+    while (q < ops.n && !(ops.top[q] == top && ops.subs[q] == s)) ++q;
+    if (q == ops.n) ++ops.n;
+    ops.top[q] = top; ops.kind[q] = kind; ops.subs[q] = s; ops.drho[q] = drho;
+    ops.profile[q] = kind == FACE_CONSTCON ? (const T*)(top ? d->prof_t : d->prof_b) : nullptr;
+  });
+  return ops;
+}
+
 int count_faces3(const lbx_domain* d)
 {
-  int n = 0;
-  if (d->faces3_active)
-    for_each_face3<double>(d, 1, [&](int, int, int, double) { ++n; });
-  return n;
+  return (d->faces3_active && face3_table<double>(d, 1).n > 0) ? 1 : 0;
 }
 
 template <typename T>
@@ -281,21 +296,17 @@ void launch_faces3(lbx_domain* d, int t, bool second)
   const lbx_params& p = d->p;
   const bool compact = d->layout == LBX_LAYOUT_COMPACT;
   const long long stride = compact ? d->P : d->N;
-  const T conc = (T)p.rho_sigma_in;
-  dim3 block(128), grid((p.LX + 127) / 128, p.LY);
-  for_each_face3<T>(d, t, [&](int top, int kind, int s, T drho) {
-    T* fs = (T*)(compact ? d->fc : d->f) + (long long)s * d->Q * stride;
-    const T* prof = kind == FACE_CONSTCON ? (const T*)(top ? d->prof_t : d->prof_b) : nullptr;
-    if (compact)
-      face_plane<T, true><<<grid, block, 0, d->stream>>>(fs, nullptr, d->fidx, p.LX, p.LY, p.LZ,
-                                                          stride, top, kind, second ? 1 : 0,
-                                                          drho, conc, prof);
-    else
-      face_plane<T, false><<<grid, block, 0, d->stream>>>(fs, d->solids, nullptr, p.LX, p.LY,
-                                                           p.LZ, stride, top, kind,
-                                                           second ? 1 : 0, drho, conc, prof);
-    d->launches++;
-  });
+  const FaceOps<T> ops = face3_table<T>(d, t);
+  if (ops.n == 0) return;
+  dim3 block(128), grid((p.LX + 127) / 128, p.LY, ops.n);
+  T* f = (T*)(compact ? d->fc : d->f);
+  if (compact)
+    face_plane<T, true><<<grid, block, 0, d->stream>>>(f, nullptr, d->fidx, p.LX, p.LY, p.LZ,
+                                                        stride, second ? 1 : 0, ops);
+  else
+    face_plane<T, false><<<grid, block, 0, d->stream>>>(f, d->solids, nullptr, p.LX, p.LY, p.LZ,
+                                                         stride, second ? 1 : 0, ops);
+  d->launches++;
 }
 
 // Kernels one step launches (faces, the step, the breakthrough reduction).

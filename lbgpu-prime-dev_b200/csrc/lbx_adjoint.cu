@@ -39,6 +39,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 
 using namespace lbx;
@@ -68,6 +69,7 @@ struct AdjArgs {
   const T* S;              // forward state before the step's AA kernel [nsubs][Q][P]
   T* L;                    // adjoint state [nsubs][Q][P], updated in place
   T* mu;                   // [3][P]: dJ/du from the solute, for the flow
+  const T* uhist;          // [3][P]: the flow's u of this step (solute kernel)
   const int* fidx;
   const int* fnode;
   int F, P, LX, LY, LZ;
@@ -78,10 +80,14 @@ struct AdjArgs {
   int obj_lo, obj_hi;      // compact range of the objective plane's nodes
   T wc, wu;                // this step's seeds: dJ/dC_eff, dJ/du_x per plane node
   int mu_in;               // flow: add the solute's mu
-  double* acc;             // [5]: dJ/dg_x, dJ/dg_y, dJ/dg_z, dJ/dtau, dJ/dtau_s
+  double* acc;             // [blocks][5]: per-block sums of dJ/dg_x, dJ/dg_y,
+                           // dJ/dg_z, dJ/dtau, dJ/dtau_s over all steps
 };
 
-// Sum of v over the block, added to *out by one thread.
+// Sum of v over the block, added by one thread to this block's own row of
+// partial sums (out[q], q < NV).  A block index covers the same nodes in
+// every step, so rows need no atomics, and the final sum over rows (on the
+// host, in block order) is reproducible.
 template <int NV>
 __device__ __forceinline__ void block_add(double (&v)[NV], double* out)
 {
@@ -100,149 +106,164 @@ __device__ __forceinline__ void block_add(double (&v)[NV], double* out)
     for (int q = 0; q < NV; ++q) {
       double x = 0.0;
       for (int w = 0; w < (int)(blockDim.x >> 5); ++w) x += part[q][w];
-      if (x != 0.0) atomicAdd(out + q, x);
+      out[q] += x;
     }
   }
 }
 
 // Adjoint of one AA kernel launch for one substance (SOLUTE) on the compact
 // layout.  256 threads per block, every thread reaches the block reduction.
-template <typename T, int Q, bool ODD, bool SOLUTE>
-__global__ void __launch_bounds__(256)
+// Neighbour indices are re-read where used (L1 hits) rather than held, as
+// in the forward kernel; lam' is loaded first and the forward populations
+// stream through running sums, so one 19-value array is live at a time.
+// The solute reads the flow's u of the step from the recompute pass.
+// Four resident 256-thread blocks (64 registers) in FP32; FP64 keeps its
+// natural register count (a 64-register cap spills).
+template <typename T>
+constexpr int adj_min_blocks() { return sizeof(T) == 4 ? 4 : 2; }
+
+template <typename T, int Q, bool ODD, bool SOLUTE, bool IDX32>
+__global__ void __launch_bounds__(256, (adj_min_blocks<T>()))
 adj_step(AdjArgs<T> A)
 {
   constexpr int D = (Q == 9) ? 2 : 3;
+  using Idx = typename std::conditional<IDX32, unsigned, size_t>::type;
   const int m = blockIdx.x * blockDim.x + threadIdx.x;
   const bool live = m < A.F;
   double acc[4] = {0.0, 0.0, 0.0, 0.0};
   if (live) {
-    const size_t F = (size_t)A.P;
-    // neighbour slots exactly as the forward step forms them
-    int nb[Q];
-    nb[0] = m;
+    const Idx F = (Idx)A.P;
+    int n = 0, xm = 0, xp = 0, ym = 0, yp = 0, zm = 0, zp = 0;
     if (ODD) {
       const int plane = A.LX * A.LY;
-      const int n = A.fnode[m];
+      n = A.fnode[m];
       const int k = fast_div(n, A.div_plane);
       const int r = n - k * plane;
       const int j = fast_div(r, A.div_lx);
       const int i = r - j * A.LX;
-      const int xm = (i == 0) ? A.LX - 1 : -1, xp = (i == A.LX - 1) ? 1 - A.LX : 1;
-      const int ym = (j == 0) ? plane - A.LX : -A.LX, yp = (j == A.LY - 1) ? A.LX - plane : A.LX;
-      int zm = 0, zp = 0;
+      xm = (i == 0) ? A.LX - 1 : -1; xp = (i == A.LX - 1) ? 1 - A.LX : 1;
+      ym = (j == 0) ? plane - A.LX : -A.LX; yp = (j == A.LY - 1) ? A.LX - plane : A.LX;
       if (D == 3) {
         const int tot = plane * A.LZ;
         zm = (k == 0) ? tot - plane : -plane;
         zp = (k == A.LZ - 1) ? plane - tot : plane;
       }
-#pragma unroll
-      for (int a = 1; a < Q; ++a) {
-        const int o = (cx(a) < 0 ? xm : (cx(a) > 0 ? xp : 0)) +
-                      (cy(a) < 0 ? ym : (cy(a) > 0 ? yp : 0)) +
-                      (cz(a) < 0 ? zm : (cz(a) > 0 ? zp : 0));
-        nb[a] = A.fidx[n + o];     // compact index of n + c_a, -1 if solid
-      }
     }
+    auto off = [&](int a) -> int {
+      return (cx(a) < 0 ? xm : (cx(a) > 0 ? xp : 0)) + (cy(a) < 0 ? ym : (cy(a) > 0 ? yp : 0)) +
+             (cz(a) < 0 ? zm : (cz(a) > 0 ? zp : 0));
+    };
+    const int* const fidx_n = A.fidx + n;
+    int mm = m;   // laundered between phases so slot addresses are not kept live
     // slot the forward read d_a from / wrote d'_a to
-    auto src = [&](int a) -> size_t {
-      if (!ODD) return (size_t)opp(a) * F + m;
-      const int up = nb[opp(a)];
-      return up >= 0 ? (size_t)a * F + (size_t)up : (size_t)opp(a) * F + m;
+    auto src = [&](int a) -> Idx {
+      if (!ODD || a == 0) return (Idx)opp(a) * F + (Idx)mm;
+      const int up = ld_reload(fidx_n + off(opp(a)));
+      return up >= 0 ? (Idx)a * F + (Idx)up : (Idx)opp(a) * F + (Idx)mm;
     };
-    auto dst = [&](int a) -> size_t {
-      if (!ODD) return (size_t)a * F + m;
-      const int dn = nb[a];
-      return dn >= 0 ? (size_t)opp(a) * F + (size_t)dn : (size_t)a * F + m;
+    auto dst = [&](int a) -> Idx {
+      if (!ODD || a == 0) return (Idx)a * F + (Idx)mm;
+      const int dn = ld_reload(fidx_n + off(a));
+      return dn >= 0 ? (Idx)opp(a) * F + (Idx)dn : (Idx)a * F + (Idx)mm;
     };
-    // the flow's velocity at this node (the forward collide's u)
-    const T* Sf = A.S;
-    const SubsConst<T>& cf = A.sc[0];
-    T u[3] = {T(0), T(0), T(0)};
-    {
-      T d[Q];
+    auto launder = [&]() {
+      xm = opaque(xm); xp = opaque(xp); ym = opaque(ym); yp = opaque(yp);
+      if (D == 3) { zm = opaque(zm); zp = opaque(zp); }
+      mm = opaque(mm);
+    };
+    if (!SOLUTE) {
+      // sum lam'(d - deq) = sum lam' d - rho S0 - rho_A sum lam' W P(u)
+      const T* Sf = A.S;
+      T* Lf = A.L;
+      const SubsConst<T>& cf = A.sc[0];
+      T lam[Q];
 #pragma unroll
-      for (int a = 0; a < Q; ++a) d[a] = Sf[src(a)];
-      T m0 = T(0), m1 = T(0), m2 = T(0);
+      for (int a = 0; a < Q; ++a) lam[a] = Lf[dst(a)];
+      launder();
+      T rho = T(0), m0 = T(0), m1 = T(0), m2 = T(0);
+      double sLD = 0.0;
 #pragma unroll
       for (int a = 0; a < Q; ++a) {
-        if (cx(a) > 0) m0 += d[a]; else if (cx(a) < 0) m0 -= d[a];
-        if (cy(a) > 0) m1 += d[a]; else if (cy(a) < 0) m1 -= d[a];
-        if (D == 3) { if (cz(a) > 0) m2 += d[a]; else if (cz(a) < 0) m2 -= d[a]; }
+        const T da = Sf[src(a)];
+        rho = (a == 0) ? da : rho + da;
+        if (cx(a) > 0) m0 += da; else if (cx(a) < 0) m0 -= da;
+        if (cy(a) > 0) m1 += da; else if (cy(a) < 0) m1 -= da;
+        if (D == 3) { if (cz(a) > 0) m2 += da; else if (cz(a) < 0) m2 -= da; }
+        sLD += (double)lam[a] * (double)da;
       }
+      T u[3];
       u[0] = add_(m0 / cf.rhoA, cf.tg[0]);
       u[1] = add_(m1 / cf.rhoA, cf.tg[1]);
       u[2] = (D == 3) ? add_(m2 / cf.rhoA, cf.tg[2]) : T(0);
-      if (!SOLUTE) {
-        // flow adjoint
-        T rho = d[0];
-#pragma unroll
-        for (int a = 1; a < Q; ++a) rho += d[a];
-        const T w = cf.itau;
-        const T rA = cf.rhoA;
-        T lam[Q];
-#pragma unroll
-        for (int a = 0; a < Q; ++a) lam[a] = A.L[dst(a)];
-        T mux = T(0), muy = T(0), muz = T(0);
-        if (A.mu_in) {
-          mux = A.mu[m];
-          muy = A.mu[F + m];
-          if (D == 3) muz = A.mu[2 * F + m];
-        }
-        if (m >= A.obj_lo && m < A.obj_hi) mux += A.wu;
-        const T usq = u[0] * u[0] + u[1] * u[1] + (D == 3 ? u[2] * u[2] : T(0));
-        T S0 = T(0), V0 = T(0), V1 = T(0), V2 = T(0);
-        double dt = 0.0;
-#pragma unroll
-        for (int a = 0; a < Q; ++a) {
-          const T W = wgt<T, Q>(a);
-          const T cu = T(cx(a)) * u[0] + T(cy(a)) * u[1] + (D == 3 ? T(cz(a)) * u[2] : T(0));
-          const T wl = W * lam[a];
-          S0 += wl;
-          const T k3 = T(3) + T(9) * cu;
-          V0 += wl * (k3 * T(cx(a)) - T(3) * u[0]);
-          V1 += wl * (k3 * T(cy(a)) - T(3) * u[1]);
-          if (D == 3) V2 += wl * (k3 * T(cz(a)) - T(3) * u[2]);
-          const T deq = W * rho + W * rA * (T(3) * cu + T(4.5) * cu * cu - T(1.5) * usq);
-          dt += (double)lam[a] * ((double)d[a] - (double)deq);
-        }
-        mux += w * rA * V0;
-        muy += w * rA * V1;
-        if (D == 3) muz += w * rA * V2;
-        const T omw = cf.omc;
-        const T iA = T(1) / rA;
-#pragma unroll
-        for (int b = 0; b < Q; ++b) {
-          const T cm = T(cx(b)) * mux + T(cy(b)) * muy + (D == 3 ? T(cz(b)) * muz : T(0));
-          A.L[src(b)] = omw * lam[b] + w * S0 + cm * iA;
-        }
-        const double tau = A.tau[0];
-        acc[0] = tau * (double)mux;
-        acc[1] = tau * (double)muy;
-        acc[2] = tau * (double)muz;
-        acc[3] = dt / (tau * tau) + (double)mux * A.g[0] + (double)muy * A.g[1] +
-                 (double)muz * A.g[2];
+      const T w = cf.itau;
+      const T rA = cf.rhoA;
+      T mux = T(0), muy = T(0), muz = T(0);
+      if (A.mu_in) {
+        mux = A.mu[m];
+        muy = A.mu[(Idx)A.P + m];
+        if (D == 3) muz = A.mu[2 * (Idx)A.P + m];
       }
-    }
-    if (SOLUTE) {
-      const T* Ss = A.S + (size_t)Q * F;
-      T* Ls = A.L + (size_t)Q * F;
+      if (m >= A.obj_lo && m < A.obj_hi) mux += A.wu;
+      const T usq = u[0] * u[0] + u[1] * u[1] + (D == 3 ? u[2] * u[2] : T(0));
+      T S0 = T(0), V0 = T(0), V1 = T(0), V2 = T(0), SP = T(0);
+#pragma unroll
+      for (int a = 0; a < Q; ++a) {
+        const T W = wgt<T, Q>(a);
+        const T cu = T(cx(a)) * u[0] + T(cy(a)) * u[1] + (D == 3 ? T(cz(a)) * u[2] : T(0));
+        const T wl = W * lam[a];
+        S0 += wl;
+        const T k3 = T(3) + T(9) * cu;
+        V0 += wl * (k3 * T(cx(a)) - T(3) * u[0]);
+        V1 += wl * (k3 * T(cy(a)) - T(3) * u[1]);
+        if (D == 3) V2 += wl * (k3 * T(cz(a)) - T(3) * u[2]);
+        SP += wl * (T(3) * cu + T(4.5) * cu * cu - T(1.5) * usq);
+      }
+      const double dt = sLD - (double)rho * (double)S0 - (double)rA * (double)SP;
+      mux += w * rA * V0;
+      muy += w * rA * V1;
+      if (D == 3) muz += w * rA * V2;
+      const T omw = cf.omc;
+      const T iA = T(1) / rA;
+      const T wS0 = w * S0;
+      launder();
+#pragma unroll
+      for (int b = 0; b < Q; ++b) {
+        const T cm = T(cx(b)) * mux + T(cy(b)) * muy + (D == 3 ? T(cz(b)) * muz : T(0));
+        Lf[src(b)] = omw * lam[b] + wS0 + cm * iA;
+      }
+      const double tau = A.tau[0];
+      acc[0] = tau * (double)mux;
+      acc[1] = tau * (double)muy;
+      acc[2] = tau * (double)muz;
+      acc[3] = dt / (tau * tau) + (double)mux * A.g[0] + (double)muy * A.g[1] +
+               (double)muz * A.g[2];
+    } else {
+      // sum lam'(g - W C_eff q) = sum lam' g - C_eff sum lam' W q
+      const T* Ss = A.S + (size_t)Q * A.P;
+      T* Ls = A.L + (size_t)Q * A.P;
       const SubsConst<T>& cs = A.sc[1];
-      T g[Q];
+      T u[3];
+      u[0] = A.uhist[m];
+      u[1] = A.uhist[(Idx)A.P + m];
+      u[2] = (D == 3) ? A.uhist[2 * (Idx)A.P + m] : T(0);
+      T lam[Q];
 #pragma unroll
-      for (int a = 0; a < Q; ++a) g[a] = Ss[src(a)];
-      T C = g[0];
+      for (int a = 0; a < Q; ++a) lam[a] = Ls[dst(a)];
+      launder();
+      T C = T(0);
+      double sLG = 0.0;
 #pragma unroll
-      for (int a = 1; a < Q; ++a) C += g[a];
+      for (int a = 0; a < Q; ++a) {
+        const T ga = Ss[src(a)];
+        C = (a == 0) ? ga : C + ga;
+        sLG += (double)lam[a] * (double)ga;
+      }
       T Ce = C;
       if (!ODD) Ce *= A.sink1;
       Ce *= A.sink1;
       const T s1k = ODD ? A.sink1 : A.sink1 * A.sink1;
       const T w = cs.itau;
-      T lam[Q];
-#pragma unroll
-      for (int a = 0; a < Q; ++a) lam[a] = Ls[dst(a)];
       T Bs = T(0), M0 = T(0), M1 = T(0), M2 = T(0);
-      double dt = 0.0;
 #pragma unroll
       for (int a = 0; a < Q; ++a) {
         const T W = wgt<T, Q>(a);
@@ -252,44 +273,56 @@ adj_step(AdjArgs<T> A)
         M0 += wl * T(cx(a));
         M1 += wl * T(cy(a));
         if (D == 3) M2 += wl * T(cz(a));
-        dt += (double)lam[a] * ((double)g[a] - (double)(W * Ce * (T(1) + T(3) * cu)));
       }
+      const double dt = sLG - (double)Ce * (double)Bs;
       T B = w * Bs;
       if (m >= A.obj_lo && m < A.obj_hi) B += A.wc;
       const T omw = cs.omc;
+      const T sB = s1k * B;
+      launder();
 #pragma unroll
-      for (int b = 0; b < Q; ++b) Ls[src(b)] = omw * lam[b] + s1k * B;
+      for (int b = 0; b < Q; ++b) Ls[src(b)] = omw * lam[b] + sB;
       const T k3 = T(3) * w * Ce;
       A.mu[m] = k3 * M0;
-      A.mu[F + m] = k3 * M1;
-      if (D == 3) A.mu[2 * F + m] = k3 * M2;
+      A.mu[(Idx)A.P + m] = k3 * M1;
+      if (D == 3) A.mu[2 * (Idx)A.P + m] = k3 * M2;
       const double taus = A.tau[1];
       // dC_eff/dtau_s through s1 = 1 - sink tau_s
       const double dce = -A.sink * (double)C * (ODD ? 1.0 : 2.0 * (double)A.sink1);
       acc[3] = dt / (taus * taus) + (double)B * dce;
     }
   }
+  double* row = A.acc + (size_t)blockIdx.x * 5;
   if (SOLUTE) {
     double v[1] = {acc[3]};
-    block_add<1>(v, A.acc + 4);
+    block_add<1>(v, row + 4);
   } else {
-    block_add<4>(acc, A.acc);
+    block_add<4>(acc, row);
   }
 }
 
-// Adjoint of one solute face operation (zero gradient or constant
-// concentration) on the compact layout, one thread per (i, j).  The forward
-// overwrote the five unknown slots with W_u X: their adjoints feed X and are
-// cleared first, then X's adjoint goes to the slots X was computed from (and,
-// for a constant concentration, to the face's concentration profile).
+// Adjoint of the solute's face operations of one step (the effective one
+// on each face, one per blockIdx.z), compact layout, one thread per (i, j).
+// The forward overwrote the five unknown slots with W_u X: their adjoints
+// feed X and are cleared first, then X's adjoint goes to the slots X was
+// computed from (and, for a constant concentration, to the face's
+// concentration profile).
+struct AdjFaceOps {
+  int n;
+  int top[2], kind[2];
+  double* dprof[2];
+};
+
 template <typename T>
 __global__ void adj_face_plane(T* Ls, const int* fidx, int LX, int LY, int LZ,
-                               long long stride, int top, int kind, int second,
-                               double* dprof)
+                               long long stride, int second, AdjFaceOps ops)
 {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= LX) return;
   const int j = blockIdx.y;
+  const int top = ops.top[blockIdx.z];
+  const int kind = ops.kind[blockIdx.z];
+  double* const dprof = ops.dprof[blockIdx.z];
   const int k = top ? LZ - 1 : 0;
   const int plane = LX * LY;
   const int n = i + LX * j + plane * k;
@@ -342,7 +375,70 @@ struct AdjState {
   std::vector<void*> ckpt;
   double J = 0.0;
   size_t state_bytes = 0;
+  // backward workspace, allocated with the checkpoints and kept for later
+  // runs of the same shape
+  std::vector<void*> snap;     // K+1 recomputed states
+  void* L = nullptr;           // adjoint state
+  void* mu = nullptr;          // [3][P]
+  void* uh = nullptr;          // [K+1][3][P] the flow's u per recomputed step
+  double* acc = nullptr;       // [blocks][5] gradient rows
+  double* dpb = nullptr;       // [LX*LY] profile gradients
+  double* dpt = nullptr;
+  size_t nblk = 0;
 };
+
+void free_state(AdjState* st)
+{
+  for (void* c : st->ckpt) cudaFree(c);
+  for (void* c : st->snap) cudaFree(c);
+  cudaFree(st->L); cudaFree(st->mu); cudaFree(st->uh);
+  cudaFree(st->acc); cudaFree(st->dpb); cudaFree(st->dpt);
+  st->ckpt.clear(); st->snap.clear();
+  st->L = st->mu = st->uh = nullptr;
+  st->acc = st->dpb = st->dpt = nullptr;
+}
+
+// Checkpoints for nseg segments of K steps.
+lbx_status alloc_checkpoints(AdjState* st, int nseg)
+{
+  st->ckpt.assign(nseg, nullptr);
+  cudaError_t e = cudaSuccess;
+  for (int q = 0; q < nseg && e == cudaSuccess; ++q) e = cudaMalloc(&st->ckpt[q], st->state_bytes);
+  if (e != cudaSuccess) {
+    free_state(st);
+    return afail(LBX_ERR_NOMEM, "adjoint checkpoints: %s", cudaGetErrorString(e));
+  }
+  return LBX_OK;
+}
+
+// The backward sweep's workspace, allocated by its first call and kept.
+lbx_status alloc_workspace(const lbx_domain* d, AdjState* st)
+{
+  if (st->L) return LBX_OK;
+  const lbx_params& p = d->p;
+  const size_t plane2 = (size_t)p.LX * p.LY;
+  const size_t ustep = (size_t)3 * d->P * d->real_size;
+  st->nblk = std::max<size_t>(1, (size_t)((d->fluid + 255) / 256));
+  st->snap.assign(st->K + 1, nullptr);
+  cudaError_t e = cudaSuccess;
+  for (int q = 0; q <= st->K && e == cudaSuccess; ++q) e = cudaMalloc(&st->snap[q], st->state_bytes);
+  if (e == cudaSuccess) e = cudaMalloc(&st->L, st->state_bytes);
+  if (e == cudaSuccess) e = cudaMalloc(&st->mu, std::max<size_t>(1, ustep));
+  if (e == cudaSuccess && p.nsubs == 2) e = cudaMalloc(&st->uh, (size_t)(st->K + 1) * ustep);
+  if (e == cudaSuccess) e = cudaMalloc(&st->acc, st->nblk * 5 * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc(&st->dpb, plane2 * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc(&st->dpt, plane2 * sizeof(double));
+  if (e != cudaSuccess) {
+    for (void* c : st->snap) cudaFree(c);
+    cudaFree(st->L); cudaFree(st->mu); cudaFree(st->uh);
+    cudaFree(st->acc); cudaFree(st->dpb); cudaFree(st->dpt);
+    st->snap.clear();
+    st->L = st->mu = st->uh = nullptr;
+    st->acc = st->dpb = st->dpt = nullptr;
+    return afail(LBX_ERR_NOMEM, "adjoint workspace: %s", cudaGetErrorString(e));
+  }
+  return LBX_OK;
+}
 
 bool solute_on(const lbx_params& p, int t) { return t >= p.sigma_t_on && t <= p.sigma_t_off; }
 
@@ -393,34 +489,49 @@ void launch_adj(lbx_domain* d, bool odd, bool solute, const AdjArgs<T>& A)
 {
   const unsigned blocks = (unsigned)((d->fluid + 255) / 256);
   if (blocks == 0) return;
-  if (solute) {
-    if (odd) adj_step<T, Q, true, true><<<blocks, 256, 0, d->stream>>>(A);
-    else adj_step<T, Q, false, true><<<blocks, 256, 0, d->stream>>>(A);
+  const bool idx32 = (unsigned long long)Q * (unsigned long long)d->P < (1ull << 32);
+  auto go = [&](auto o, auto s, auto i) {
+    adj_step<T, Q, decltype(o)::value, decltype(s)::value, decltype(i)::value>
+        <<<blocks, 256, 0, d->stream>>>(A);
+  };
+  using TT = std::true_type;
+  using FF = std::false_type;
+  if (idx32) {
+    if (solute) { if (odd) go(TT{}, TT{}, TT{}); else go(FF{}, TT{}, TT{}); }
+    else { if (odd) go(TT{}, FF{}, TT{}); else go(FF{}, FF{}, TT{}); }
   } else {
-    if (odd) adj_step<T, Q, true, false><<<blocks, 256, 0, d->stream>>>(A);
-    else adj_step<T, Q, false, false><<<blocks, 256, 0, d->stream>>>(A);
+    if (solute) { if (odd) go(TT{}, TT{}, FF{}); else go(FF{}, TT{}, FF{}); }
+    else { if (odd) go(TT{}, FF{}, FF{}); else go(FF{}, FF{}, FF{}); }
   }
   d->launches++;
 }
 
-// Adjoint of the solute face operations of step t, in reverse order.
+// Adjoint of the solute face operations of a step: per face the last
+// configured one (zero gradient over constant concentration), as the
+// forward's face launch applies them.
 template <typename T>
 void launch_adj_faces(lbx_domain* d, int t, T* L, double* dprof_t, double* dprof_b)
 {
   const lbx_params& p = d->p;
   if (p.nsubs != 2 || d->p.dims != 3) return;
+  AdjFaceOps ops;
+  std::memset(&ops, 0, sizeof ops);
+  auto add = [&](int top, bool cc, bool zg) {
+    if (!cc && !zg) return;
+    ops.top[ops.n] = top;
+    ops.kind[ops.n] = zg ? FACE_ZEROGRAD : FACE_CONSTCON;
+    ops.dprof[ops.n] = zg ? nullptr : (top ? dprof_t : dprof_b);
+    ++ops.n;
+  };
+  add(1, p.constcon_t_in != 0, p.zeroconcgrad_t != 0);
+  add(0, p.constcon_b_in != 0, p.zeroconcgrad_b != 0);
+  if (ops.n == 0) return;
   const bool second = (t % 2) == 0;
   T* Ls = L + (size_t)d->Q * d->P;
-  dim3 block(128), grid((p.LX + 127) / 128, p.LY);
-  auto run = [&](int top, int kind, double* dp) {
-    adj_face_plane<T><<<grid, block, 0, d->stream>>>(Ls, d->fidx, p.LX, p.LY, p.LZ, d->P, top,
-                                                     kind, second ? 1 : 0, dp);
-    d->launches++;
-  };
-  if (p.zeroconcgrad_b) run(0, FACE_ZEROGRAD, nullptr);
-  if (p.zeroconcgrad_t) run(1, FACE_ZEROGRAD, nullptr);
-  if (p.constcon_b_in) run(0, FACE_CONSTCON, dprof_b);
-  if (p.constcon_t_in) run(1, FACE_CONSTCON, dprof_t);
+  dim3 block(128), grid((p.LX + 127) / 128, p.LY, ops.n);
+  adj_face_plane<T><<<grid, block, 0, d->stream>>>(Ls, d->fidx, p.LX, p.LY, p.LZ, d->P,
+                                                   second ? 1 : 0, ops);
+  d->launches++;
 }
 
 template <typename T>
@@ -428,38 +539,22 @@ lbx_status backward_t(lbx_domain* d, lbx_gradient* out, double* dprof_b, double*
 {
   AdjState* st = (AdjState*)d->adj;
   const lbx_params& p = d->p;
+  if (lbx_status rc0 = alloc_workspace(d, st)) return rc0;
   const size_t sb = st->state_bytes;
   const int K = st->K;
-  std::vector<void*> snap(K + 1, nullptr);
-  void *L = nullptr, *mu = nullptr;
-  double *acc = nullptr, *dpb = nullptr, *dpt = nullptr;
   const size_t plane2 = (size_t)p.LX * p.LY;
+  const size_t ustep = (size_t)3 * d->P;
+  const size_t nblk = st->nblk;
+  std::vector<void*>& snap = st->snap;
+  void* L = st->L;
+  T* uh = (T*)st->uh;
+  double* acc = st->acc;
   lbx_status rc = LBX_OK;
-  auto cleanup = [&]() {
-    for (void* s : snap) cudaFree(s);
-    cudaFree(L); cudaFree(mu); cudaFree(acc); cudaFree(dpb); cudaFree(dpt);
-  };
-#define BCK(call)                                                                 \
-  do {                                                                            \
-    cudaError_t e_ = (call);                                                      \
-    if (e_ != cudaSuccess) {                                                      \
-      rc = afail(e_ == cudaErrorMemoryAllocation ? LBX_ERR_NOMEM : LBX_ERR_CUDA,  \
-                 "%s: %s", #call, cudaGetErrorString(e_));                        \
-      cleanup();                                                                  \
-      return rc;                                                                  \
-    }                                                                             \
-  } while (0)
-  for (int q = 0; q <= K; ++q) BCK(cudaMalloc(&snap[q], sb));
-  BCK(cudaMalloc(&L, sb));
-  BCK(cudaMalloc(&mu, std::max<size_t>(1, (size_t)3 * d->P * sizeof(T))));
-  BCK(cudaMalloc(&acc, 5 * sizeof(double)));
-  BCK(cudaMalloc(&dpb, plane2 * sizeof(double)));
-  BCK(cudaMalloc(&dpt, plane2 * sizeof(double)));
-  BCK(cudaMemsetAsync(L, 0, sb, d->stream));
-  BCK(cudaMemsetAsync(mu, 0, (size_t)3 * d->P * sizeof(T), d->stream));
-  BCK(cudaMemsetAsync(acc, 0, 5 * sizeof(double), d->stream));
-  BCK(cudaMemsetAsync(dpb, 0, plane2 * sizeof(double), d->stream));
-  BCK(cudaMemsetAsync(dpt, 0, plane2 * sizeof(double), d->stream));
+  ACK(cudaMemsetAsync(L, 0, sb, d->stream));
+  ACK(cudaMemsetAsync(st->mu, 0, ustep * sizeof(T), d->stream));
+  ACK(cudaMemsetAsync(acc, 0, nblk * 5 * sizeof(double), d->stream));
+  ACK(cudaMemsetAsync(st->dpb, 0, plane2 * sizeof(double), d->stream));
+  ACK(cudaMemsetAsync(st->dpt, 0, plane2 * sizeof(double), d->stream));
 
   // objective plane and seeds
   const lbx_objective& ob = st->obj;
@@ -471,24 +566,32 @@ lbx_status backward_t(lbx_domain* d, lbx_gradient* out, double* dprof_b, double*
   const double nwin = (double)std::max(0, t_last - t_first + 1);
   const double nout = (double)std::max<long long>(1, hi - lo);
 
+  // the solute's adjoint stays exactly zero until the first C seed (going
+  // back in time); until then its kernels are skipped
+  bool solute_live = false;
   const int nseg = (int)st->ckpt.size();
   for (int seg = nseg - 1; seg >= 0; --seg) {
     const int tc = st->t0 + seg * K;
     const int len = std::min(K, st->t0 + st->nsteps - tc);
-    BCK(cudaMemcpyAsync(snap[0], st->ckpt[seg], sb, cudaMemcpyDeviceToDevice, d->stream));
+    ACK(cudaMemcpyAsync(snap[0], st->ckpt[seg], sb, cudaMemcpyDeviceToDevice, d->stream));
+    void* ubuf = d->ubuf;
     for (int q = 1; q <= len; ++q) {
+      if (uh) d->ubuf = uh + (size_t)q * ustep;
       rc = lbx_internal_step_into(d, tc + q, snap[q - 1], snap[q]);
-      if (rc) { cleanup(); return rc; }
+      if (rc) { d->ubuf = ubuf; return rc; }
     }
+    d->ubuf = ubuf;
     for (int q = len; q >= 1; --q) {
       const int t = tc + q;
       const bool odd = (t % 2) != 0;
-      AdjArgs<T> A = make_adj<T>(d, snap[q - 1], L, mu, acc);
+      AdjArgs<T> A = make_adj<T>(d, snap[q - 1], L, st->mu, acc);
+      A.uhist = uh ? uh + (size_t)q * ustep : nullptr;
       A.obj_lo = (int)lo; A.obj_hi = (int)hi;
       const bool in_win = nwin > 0 && t >= t_first && t <= t_last;
       A.wc = in_win ? (T)(ob.w_c / (nwin * nout)) : T(0);
       A.wu = in_win ? (T)(ob.w_ux / (nwin * nout)) : T(0);
-      const bool sol = p.nsubs == 2 && solute_on(p, t);
+      solute_live = solute_live || (p.nsubs == 2 && A.wc != T(0));
+      const bool sol = p.nsubs == 2 && solute_on(p, t) && solute_live;
       if (sol) {
         if (d->Q == 19) launch_adj<T, 19>(d, odd, true, A);
         else launch_adj<T, 9>(d, odd, true, A);
@@ -496,21 +599,23 @@ lbx_status backward_t(lbx_domain* d, lbx_gradient* out, double* dprof_b, double*
       A.mu_in = sol ? 1 : 0;
       if (d->Q == 19) launch_adj<T, 19>(d, odd, false, A);
       else launch_adj<T, 9>(d, odd, false, A);
-      launch_adj_faces<T>(d, t, (T*)L, dpt, dpb);
-      BCK(cudaGetLastError());
+      if (solute_live) launch_adj_faces<T>(d, t, (T*)L, st->dpt, st->dpb);
+      ACK(cudaGetLastError());
     }
   }
-  double h[5];
-  BCK(cudaMemcpyAsync(h, acc, sizeof h, cudaMemcpyDeviceToHost, d->stream));
-  if (dprof_b) BCK(cudaMemcpyAsync(dprof_b, dpb, plane2 * sizeof(double), cudaMemcpyDeviceToHost, d->stream));
-  if (dprof_t) BCK(cudaMemcpyAsync(dprof_t, dpt, plane2 * sizeof(double), cudaMemcpyDeviceToHost, d->stream));
-  BCK(cudaStreamSynchronize(d->stream));
-#undef BCK
+  std::vector<double> rows(nblk * 5);
+  ACK(cudaMemcpyAsync(rows.data(), acc, rows.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                      d->stream));
+  if (dprof_b) ACK(cudaMemcpyAsync(dprof_b, st->dpb, plane2 * sizeof(double), cudaMemcpyDeviceToHost, d->stream));
+  if (dprof_t) ACK(cudaMemcpyAsync(dprof_t, st->dpt, plane2 * sizeof(double), cudaMemcpyDeviceToHost, d->stream));
+  ACK(cudaStreamSynchronize(d->stream));
+  double h[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  for (size_t b = 0; b < nblk; ++b)
+    for (int q = 0; q < 5; ++q) h[q] += rows[b * 5 + q];
   out->J = st->J;
   for (int c = 0; c < 3; ++c) out->d_gaccel[c] = h[c];
   out->d_tau = h[3];
   out->d_tau_s = h[4];
-  cleanup();
   return LBX_OK;
 }
 
@@ -520,7 +625,8 @@ void lbx_internal_adjoint_free(lbx_domain* d)
 {
   AdjState* st = (AdjState*)d->adj;
   if (!st) return;
-  for (void* c : st->ckpt) cudaFree(c);
+  cudaStreamSynchronize(d->stream);
+  free_state(st);
   delete st;
   d->adj = nullptr;
 }
@@ -539,43 +645,61 @@ lbx_status lbx_adjoint_forward(lbx_domain* d, int t0, int nsteps, int checkpoint
     return afail(LBX_ERR_STATE, "the adjoint run starts from the natural-order state at an even time");
   const int planes = d->p.dims == 2 ? d->p.LY : d->p.LZ;
   if (obj->plane < 0 || obj->plane >= planes) return afail(LBX_ERR_INVALID, "objective plane out of range");
-  lbx_internal_adjoint_free(d);
-  AdjState* st = new AdjState();
-  d->adj = st;
-  st->t0 = t0; st->nsteps = nsteps; st->K = checkpoint_every; st->obj = *obj;
-  st->state_bytes = (size_t)d->p.nsubs * d->Q * d->P * d->real_size;
+  const size_t sbytes = (size_t)d->p.nsubs * d->Q * d->P * d->real_size;
   const int nseg = (nsteps + checkpoint_every - 1) / checkpoint_every;
-  st->ckpt.assign(nseg, nullptr);
-  for (int q = 0; q < nseg; ++q) {
-    cudaError_t e = cudaMalloc(&st->ckpt[q], st->state_bytes);
-    if (e != cudaSuccess) {
-      lbx_internal_adjoint_free(d);
-      return afail(LBX_ERR_NOMEM, "adjoint checkpoints: %s", cudaGetErrorString(e));
-    }
+  AdjState* st = (AdjState*)d->adj;
+  if (st && (st->K != checkpoint_every || (int)st->ckpt.size() != nseg ||
+             st->state_bytes != sbytes)) {
+    lbx_internal_adjoint_free(d);
+    st = nullptr;
   }
-  rc = lbx_btc_start(d, obj->plane, nsteps);
-  if (rc) { lbx_internal_adjoint_free(d); return rc; }
-  for (int q = 0; q < nseg; ++q) {
-    const int tc = t0 + q * checkpoint_every;
-    const int len = std::min(checkpoint_every, t0 + nsteps - tc);
-    ACK(cudaMemcpyAsync(st->ckpt[q], d->fc, st->state_bytes, cudaMemcpyDeviceToDevice, d->stream));
-    rc = lbx_run(d, tc, len, 0);
-    if (rc) { lbx_internal_adjoint_free(d); return rc; }
+  if (!st) {
+    st = new AdjState();
+    st->K = checkpoint_every;
+    st->state_bytes = sbytes;
+    rc = alloc_checkpoints(st, nseg);
+    if (rc) { delete st; return rc; }
+    d->adj = st;
   }
-  std::vector<double> c(nsteps), ux(nsteps);
-  long long cnt = 0;
-  rc = lbx_btc_read(d, c.data(), ux.data(), nsteps, &cnt);
-  lbx_btc_stop(d);
-  if (rc) { lbx_internal_adjoint_free(d); return rc; }
+  st->t0 = t0; st->nsteps = nsteps; st->obj = *obj;
+  // plane means are recorded over the objective's steps only
   const int t_first = std::max(obj->t_first, t0 + 1);
   const int t_last = std::min(obj->t_last, t0 + nsteps);
-  double sc = 0.0, su = 0.0;
-  int nw = 0;
-  for (int t = t_first; t <= t_last; ++t, ++nw) {
-    if (obj->w_c != 0.0) sc += c[t - t0 - 1];
-    su += ux[t - t0 - 1];
+  const int nwin = std::max(0, t_last - t_first + 1);
+  bool recording = false;
+  for (int q = 0; q < nseg; ++q) {
+    const int tc = t0 + q * checkpoint_every;
+    const int te = std::min(tc + checkpoint_every, t0 + nsteps);
+    ACK(cudaMemcpyAsync(st->ckpt[q], d->fc, st->state_bytes, cudaMemcpyDeviceToDevice, d->stream));
+    int t = tc;
+    while (t < te) {
+      if (!recording && nwin > 0 && t == t_first - 1) {
+        rc = lbx_btc_start(d, obj->plane, nwin);
+        if (rc) { lbx_internal_adjoint_free(d); return rc; }
+        recording = true;
+        continue;
+      }
+      int stop = te;
+      if (!recording && nwin > 0 && t < t_first - 1 && t_first - 1 < te) stop = t_first - 1;
+      rc = lbx_run(d, t, stop - t, 0);
+      if (rc) { lbx_internal_adjoint_free(d); return rc; }
+      t = stop;
+    }
   }
-  st->J = nw ? (obj->w_c * (sc / nw) + obj->w_ux * (su / nw)) : 0.0;
+  st->J = 0.0;
+  if (recording) {
+    std::vector<double> c(nwin), ux(nwin);
+    long long cnt = 0;
+    rc = lbx_btc_read(d, c.data(), ux.data(), nwin, &cnt);
+    lbx_btc_stop(d);
+    if (rc) { lbx_internal_adjoint_free(d); return rc; }
+    double sc = 0.0, su = 0.0;
+    for (int q = 0; q < nwin; ++q) {
+      if (obj->w_c != 0.0) sc += c[q];
+      su += ux[q];
+    }
+    st->J = obj->w_c * (sc / nwin) + obj->w_ux * (su / nwin);
+  }
   if (J) *J = st->J;
   return LBX_OK;
 }

@@ -739,21 +739,37 @@ __device__ __forceinline__ void face3_apply(T (&d)[19], bool top, int kind, T dr
   }
 }
 
-// One face operation on the plane, one thread per (i, j); a constant-
-// concentration face takes its C from `profile[i + LX*j]` when given.  `_1` form
-// (second == 0, before an odd step): loads what the odd step will pull and
-// deposits the unknowns where it will pull them from (slot a of the
-// upstream node, or of the node itself behind a solid, as set_f1d_d does);
-// `_2` form (before an even step): the node's own swapped slots.  The dense
-// layout tests solids, the compact one maps nodes through fidx.
+// The face operations of one step that have an effect: on each (face,
+// substance) pair every operation reads only the known slots and rewrites
+// all five unknowns, so the last configured one decides the result, and for
+// LZ >= 3 the pairs touch disjoint slots.  They run as one launch
+// (blockIdx.z = operation) with the result of running them in order.
+template <typename T>
+struct FaceOps {
+  int n;
+  int top[4], kind[4], subs[4];
+  T drho[4];
+  const T* profile[4];   // constant concentration per node, or NULL
+  T conc;                // constant concentration otherwise
+};
+
+// One thread per (i, j) of one operation.  `_1` form (second == 0, before
+// an odd step): loads what the odd step will pull and deposits the unknowns
+// where it will pull them from (slot a of the upstream node, or of the node
+// itself behind a solid, as set_f1d_d does); `_2` form (before an even
+// step): the node's own swapped slots.  The dense layout tests solids, the
+// compact one maps nodes through fidx.  f is [nsubs][Q][stride].
 template <typename T, bool COMPACT>
-__global__ void face_plane(T* fs, const uint8_t* solids, const int* fidx, int LX, int LY,
-                           int LZ, long long stride, int top, int kind, int second, T drho,
-                           T conc, const T* profile)
+__global__ void face_plane(T* f, const uint8_t* solids, const int* fidx, int LX, int LY,
+                           int LZ, long long stride, int second, FaceOps<T> ops)
 {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= LX) return;
   const int j = blockIdx.y;
+  const int op = blockIdx.z;
+  const int top = ops.top[op];
+  const int kind = ops.kind[op];
+  T* const fs = f + (long long)ops.subs[op] * 19 * stride;
   const int k = top ? LZ - 1 : 0;
   const int plane = LX * LY;
   const int n = i + LX * j + plane * k;
@@ -780,7 +796,8 @@ __global__ void face_plane(T* fs, const uint8_t* solids, const int* fidx, int LX
       d[a] = (up < 0) ? fs[opp(a) * stride + self] : fs[a * stride + up];
     }
   }
-  face3_apply<T>(d, top != 0, kind, drho, profile ? profile[i + LX * j] : conc);
+  const T* prof = ops.profile[op];
+  face3_apply<T>(d, top != 0, kind, ops.drho[op], prof ? prof[i + LX * j] : ops.conc);
 #pragma unroll
   for (int q = 0; q < 5; ++q) {
     const int a = face3_unknown(top != 0, q);
