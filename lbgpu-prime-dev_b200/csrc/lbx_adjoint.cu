@@ -68,7 +68,6 @@ template <typename T>
 struct AdjArgs {
   const T* S;              // forward state before the step's AA kernel [nsubs][Q][P]
   T* L;                    // adjoint state [nsubs][Q][P], updated in place
-  T* mu;                   // [3][P]: dJ/du from the solute, for the flow
   const T* uhist;          // [3][P]: the flow's u of this step (solute kernel)
   const int* fidx;
   const int* fnode;
@@ -79,7 +78,6 @@ struct AdjArgs {
   double tau[2], g[3], sink;
   int obj_lo, obj_hi;      // compact range of the objective plane's nodes
   T wc, wu;                // this step's seeds: dJ/dC_eff, dJ/du_x per plane node
-  int mu_in;               // flow: add the solute's mu
   double* acc;             // [blocks][5]: per-block sums of dJ/dg_x, dJ/dg_y,
                            // dJ/dg_z, dJ/dtau, dJ/dtau_s over all steps
 };
@@ -111,26 +109,28 @@ __device__ __forceinline__ void block_add(double (&v)[NV], double* out)
   }
 }
 
-// Adjoint of one AA kernel launch for one substance (SOLUTE) on the compact
-// layout.  256 threads per block, every thread reaches the block reduction.
+// Adjoint of one AA kernel launch on the compact layout: the solute's
+// (WITH_SOLUTE, first, as the forward's solute depends on the flow's u) and
+// then the flow's, handing dJ/du between them in registers.  256 threads per block, every thread reaches the block reduction.
 // Neighbour indices are re-read where used (L1 hits) rather than held, as
 // in the forward kernel; lam' is loaded first and the forward populations
 // stream through running sums, so one 19-value array is live at a time.
 // The solute reads the flow's u of the step from the recompute pass.
-// Four resident 256-thread blocks (64 registers) in FP32; FP64 keeps its
-// natural register count (a 64-register cap spills).
-template <typename T>
-constexpr int adj_min_blocks() { return sizeof(T) == 4 ? 4 : 2; }
+// Resident 256-thread blocks: in FP32 four (64 registers) for the flow
+// alone and three (85) with the solute phase; FP64 keeps about its natural
+// register count (lower caps spill).
+template <typename T, bool WITH_SOLUTE>
+constexpr int adj_min_blocks() { return sizeof(T) == 4 ? (WITH_SOLUTE ? 3 : 4) : 2; }
 
-template <typename T, int Q, bool ODD, bool SOLUTE, bool IDX32>
-__global__ void __launch_bounds__(256, (adj_min_blocks<T>()))
+template <typename T, int Q, bool ODD, bool WITH_SOLUTE, bool IDX32>
+__global__ void __launch_bounds__(256, (adj_min_blocks<T, WITH_SOLUTE>()))
 adj_step(AdjArgs<T> A)
 {
   constexpr int D = (Q == 9) ? 2 : 3;
   using Idx = typename std::conditional<IDX32, unsigned, size_t>::type;
   const int m = blockIdx.x * blockDim.x + threadIdx.x;
   const bool live = m < A.F;
-  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
   if (live) {
     const Idx F = (Idx)A.P;
     int n = 0, xm = 0, xp = 0, ym = 0, yp = 0, zm = 0, zp = 0;
@@ -171,73 +171,9 @@ adj_step(AdjArgs<T> A)
       if (D == 3) { zm = opaque(zm); zp = opaque(zp); }
       mm = opaque(mm);
     };
-    if (!SOLUTE) {
-      // sum lam'(d - deq) = sum lam' d - rho S0 - rho_A sum lam' W P(u)
-      const T* Sf = A.S;
-      T* Lf = A.L;
-      const SubsConst<T>& cf = A.sc[0];
-      T lam[Q];
-#pragma unroll
-      for (int a = 0; a < Q; ++a) lam[a] = Lf[dst(a)];
-      launder();
-      T rho = T(0), m0 = T(0), m1 = T(0), m2 = T(0);
-      double sLD = 0.0;
-#pragma unroll
-      for (int a = 0; a < Q; ++a) {
-        const T da = Sf[src(a)];
-        rho = (a == 0) ? da : rho + da;
-        if (cx(a) > 0) m0 += da; else if (cx(a) < 0) m0 -= da;
-        if (cy(a) > 0) m1 += da; else if (cy(a) < 0) m1 -= da;
-        if (D == 3) { if (cz(a) > 0) m2 += da; else if (cz(a) < 0) m2 -= da; }
-        sLD += (double)lam[a] * (double)da;
-      }
-      T u[3];
-      u[0] = add_(m0 / cf.rhoA, cf.tg[0]);
-      u[1] = add_(m1 / cf.rhoA, cf.tg[1]);
-      u[2] = (D == 3) ? add_(m2 / cf.rhoA, cf.tg[2]) : T(0);
-      const T w = cf.itau;
-      const T rA = cf.rhoA;
-      T mux = T(0), muy = T(0), muz = T(0);
-      if (A.mu_in) {
-        mux = A.mu[m];
-        muy = A.mu[(Idx)A.P + m];
-        if (D == 3) muz = A.mu[2 * (Idx)A.P + m];
-      }
-      if (m >= A.obj_lo && m < A.obj_hi) mux += A.wu;
-      const T usq = u[0] * u[0] + u[1] * u[1] + (D == 3 ? u[2] * u[2] : T(0));
-      T S0 = T(0), V0 = T(0), V1 = T(0), V2 = T(0), SP = T(0);
-#pragma unroll
-      for (int a = 0; a < Q; ++a) {
-        const T W = wgt<T, Q>(a);
-        const T cu = T(cx(a)) * u[0] + T(cy(a)) * u[1] + (D == 3 ? T(cz(a)) * u[2] : T(0));
-        const T wl = W * lam[a];
-        S0 += wl;
-        const T k3 = T(3) + T(9) * cu;
-        V0 += wl * (k3 * T(cx(a)) - T(3) * u[0]);
-        V1 += wl * (k3 * T(cy(a)) - T(3) * u[1]);
-        if (D == 3) V2 += wl * (k3 * T(cz(a)) - T(3) * u[2]);
-        SP += wl * (T(3) * cu + T(4.5) * cu * cu - T(1.5) * usq);
-      }
-      const double dt = sLD - (double)rho * (double)S0 - (double)rA * (double)SP;
-      mux += w * rA * V0;
-      muy += w * rA * V1;
-      if (D == 3) muz += w * rA * V2;
-      const T omw = cf.omc;
-      const T iA = T(1) / rA;
-      const T wS0 = w * S0;
-      launder();
-#pragma unroll
-      for (int b = 0; b < Q; ++b) {
-        const T cm = T(cx(b)) * mux + T(cy(b)) * muy + (D == 3 ? T(cz(b)) * muz : T(0));
-        Lf[src(b)] = omw * lam[b] + wS0 + cm * iA;
-      }
-      const double tau = A.tau[0];
-      acc[0] = tau * (double)mux;
-      acc[1] = tau * (double)muy;
-      acc[2] = tau * (double)muz;
-      acc[3] = dt / (tau * tau) + (double)mux * A.g[0] + (double)muy * A.g[1] +
-               (double)muz * A.g[2];
-    } else {
+    // dJ/du at this node from the solute phase (and the objective)
+    T mux = T(0), muy = T(0), muz = T(0);
+    if (WITH_SOLUTE) {
       // sum lam'(g - W C_eff q) = sum lam' g - C_eff sum lam' W q
       const T* Ss = A.S + (size_t)Q * A.P;
       T* Ls = A.L + (size_t)Q * A.P;
@@ -283,22 +219,79 @@ adj_step(AdjArgs<T> A)
 #pragma unroll
       for (int b = 0; b < Q; ++b) Ls[src(b)] = omw * lam[b] + sB;
       const T k3 = T(3) * w * Ce;
-      A.mu[m] = k3 * M0;
-      A.mu[(Idx)A.P + m] = k3 * M1;
-      if (D == 3) A.mu[2 * (Idx)A.P + m] = k3 * M2;
+      mux = k3 * M0;
+      muy = k3 * M1;
+      muz = (D == 3) ? k3 * M2 : T(0);
       const double taus = A.tau[1];
       // dC_eff/dtau_s through s1 = 1 - sink tau_s
       const double dce = -A.sink * (double)C * (ODD ? 1.0 : 2.0 * (double)A.sink1);
-      acc[3] = dt / (taus * taus) + (double)B * dce;
+      acc[4] = dt / (taus * taus) + (double)B * dce;
+      launder();
+      asm volatile("" ::: "memory");
+    }
+    {
+      // sum lam'(d - deq) = sum lam' d - rho S0 - rho_A sum lam' W P(u)
+      const T* Sf = A.S;
+      T* Lf = A.L;
+      const SubsConst<T>& cf = A.sc[0];
+      T lam[Q];
+#pragma unroll
+      for (int a = 0; a < Q; ++a) lam[a] = Lf[dst(a)];
+      launder();
+      T rho = T(0), m0 = T(0), m1 = T(0), m2 = T(0);
+      double sLD = 0.0;
+#pragma unroll
+      for (int a = 0; a < Q; ++a) {
+        const T da = Sf[src(a)];
+        rho = (a == 0) ? da : rho + da;
+        if (cx(a) > 0) m0 += da; else if (cx(a) < 0) m0 -= da;
+        if (cy(a) > 0) m1 += da; else if (cy(a) < 0) m1 -= da;
+        if (D == 3) { if (cz(a) > 0) m2 += da; else if (cz(a) < 0) m2 -= da; }
+        sLD += (double)lam[a] * (double)da;
+      }
+      T u[3];
+      u[0] = add_(m0 / cf.rhoA, cf.tg[0]);
+      u[1] = add_(m1 / cf.rhoA, cf.tg[1]);
+      u[2] = (D == 3) ? add_(m2 / cf.rhoA, cf.tg[2]) : T(0);
+      const T w = cf.itau;
+      const T rA = cf.rhoA;
+      if (m >= A.obj_lo && m < A.obj_hi) mux += A.wu;
+      const T usq = u[0] * u[0] + u[1] * u[1] + (D == 3 ? u[2] * u[2] : T(0));
+      T S0 = T(0), V0 = T(0), V1 = T(0), V2 = T(0), SP = T(0);
+#pragma unroll
+      for (int a = 0; a < Q; ++a) {
+        const T W = wgt<T, Q>(a);
+        const T cu = T(cx(a)) * u[0] + T(cy(a)) * u[1] + (D == 3 ? T(cz(a)) * u[2] : T(0));
+        const T wl = W * lam[a];
+        S0 += wl;
+        const T k3 = T(3) + T(9) * cu;
+        V0 += wl * (k3 * T(cx(a)) - T(3) * u[0]);
+        V1 += wl * (k3 * T(cy(a)) - T(3) * u[1]);
+        if (D == 3) V2 += wl * (k3 * T(cz(a)) - T(3) * u[2]);
+        SP += wl * (T(3) * cu + T(4.5) * cu * cu - T(1.5) * usq);
+      }
+      const double dt = sLD - (double)rho * (double)S0 - (double)rA * (double)SP;
+      mux += w * rA * V0;
+      muy += w * rA * V1;
+      if (D == 3) muz += w * rA * V2;
+      const T omw = cf.omc;
+      const T iA = T(1) / rA;
+      const T wS0 = w * S0;
+      launder();
+#pragma unroll
+      for (int b = 0; b < Q; ++b) {
+        const T cm = T(cx(b)) * mux + T(cy(b)) * muy + (D == 3 ? T(cz(b)) * muz : T(0));
+        Lf[src(b)] = omw * lam[b] + wS0 + cm * iA;
+      }
+      const double tau = A.tau[0];
+      acc[0] = tau * (double)mux;
+      acc[1] = tau * (double)muy;
+      acc[2] = tau * (double)muz;
+      acc[3] = dt / (tau * tau) + (double)mux * A.g[0] + (double)muy * A.g[1] +
+               (double)muz * A.g[2];
     }
   }
-  double* row = A.acc + (size_t)blockIdx.x * 5;
-  if (SOLUTE) {
-    double v[1] = {acc[3]};
-    block_add<1>(v, row + 4);
-  } else {
-    block_add<4>(acc, row);
-  }
+  block_add<5>(acc, A.acc + (size_t)blockIdx.x * 5);
 }
 
 // Adjoint of the solute's face operations of one step (the effective one
@@ -379,7 +372,6 @@ struct AdjState {
   // runs of the same shape
   std::vector<void*> snap;     // K+1 recomputed states
   void* L = nullptr;           // adjoint state
-  void* mu = nullptr;          // [3][P]
   void* uh = nullptr;          // [K+1][3][P] the flow's u per recomputed step
   double* acc = nullptr;       // [blocks][5] gradient rows
   double* dpb = nullptr;       // [LX*LY] profile gradients
@@ -391,10 +383,10 @@ void free_state(AdjState* st)
 {
   for (void* c : st->ckpt) cudaFree(c);
   for (void* c : st->snap) cudaFree(c);
-  cudaFree(st->L); cudaFree(st->mu); cudaFree(st->uh);
+  cudaFree(st->L); cudaFree(st->uh);
   cudaFree(st->acc); cudaFree(st->dpb); cudaFree(st->dpt);
   st->ckpt.clear(); st->snap.clear();
-  st->L = st->mu = st->uh = nullptr;
+  st->L = st->uh = nullptr;
   st->acc = st->dpb = st->dpt = nullptr;
 }
 
@@ -423,17 +415,16 @@ lbx_status alloc_workspace(const lbx_domain* d, AdjState* st)
   cudaError_t e = cudaSuccess;
   for (int q = 0; q <= st->K && e == cudaSuccess; ++q) e = cudaMalloc(&st->snap[q], st->state_bytes);
   if (e == cudaSuccess) e = cudaMalloc(&st->L, st->state_bytes);
-  if (e == cudaSuccess) e = cudaMalloc(&st->mu, std::max<size_t>(1, ustep));
   if (e == cudaSuccess && p.nsubs == 2) e = cudaMalloc(&st->uh, (size_t)(st->K + 1) * ustep);
   if (e == cudaSuccess) e = cudaMalloc(&st->acc, st->nblk * 5 * sizeof(double));
   if (e == cudaSuccess) e = cudaMalloc(&st->dpb, plane2 * sizeof(double));
   if (e == cudaSuccess) e = cudaMalloc(&st->dpt, plane2 * sizeof(double));
   if (e != cudaSuccess) {
     for (void* c : st->snap) cudaFree(c);
-    cudaFree(st->L); cudaFree(st->mu); cudaFree(st->uh);
+    cudaFree(st->L); cudaFree(st->uh);
     cudaFree(st->acc); cudaFree(st->dpb); cudaFree(st->dpt);
     st->snap.clear();
-    st->L = st->mu = st->uh = nullptr;
+    st->L = st->uh = nullptr;
     st->acc = st->dpb = st->dpt = nullptr;
     return afail(LBX_ERR_NOMEM, "adjoint workspace: %s", cudaGetErrorString(e));
   }
@@ -457,12 +448,12 @@ lbx_status check_adjoint(const lbx_domain* d)
 }
 
 template <typename T>
-AdjArgs<T> make_adj(const lbx_domain* d, const void* S, void* L, void* mu, double* acc)
+AdjArgs<T> make_adj(const lbx_domain* d, const void* S, void* L, double* acc)
 {
   const lbx_params& p = d->p;
   AdjArgs<T> A;
   std::memset(&A, 0, sizeof A);
-  A.S = (const T*)S; A.L = (T*)L; A.mu = (T*)mu;
+  A.S = (const T*)S; A.L = (T*)L;
   A.fidx = d->fidx; A.fnode = d->fnode;
   A.F = (int)d->fluid; A.P = (int)d->P;
   A.LX = p.LX; A.LY = p.LY; A.LZ = p.LZ;
@@ -551,7 +542,6 @@ lbx_status backward_t(lbx_domain* d, lbx_gradient* out, double* dprof_b, double*
   double* acc = st->acc;
   lbx_status rc = LBX_OK;
   ACK(cudaMemsetAsync(L, 0, sb, d->stream));
-  ACK(cudaMemsetAsync(st->mu, 0, ustep * sizeof(T), d->stream));
   ACK(cudaMemsetAsync(acc, 0, nblk * 5 * sizeof(double), d->stream));
   ACK(cudaMemsetAsync(st->dpb, 0, plane2 * sizeof(double), d->stream));
   ACK(cudaMemsetAsync(st->dpt, 0, plane2 * sizeof(double), d->stream));
@@ -584,7 +574,7 @@ lbx_status backward_t(lbx_domain* d, lbx_gradient* out, double* dprof_b, double*
     for (int q = len; q >= 1; --q) {
       const int t = tc + q;
       const bool odd = (t % 2) != 0;
-      AdjArgs<T> A = make_adj<T>(d, snap[q - 1], L, st->mu, acc);
+      AdjArgs<T> A = make_adj<T>(d, snap[q - 1], L, acc);
       A.uhist = uh ? uh + (size_t)q * ustep : nullptr;
       A.obj_lo = (int)lo; A.obj_hi = (int)hi;
       const bool in_win = nwin > 0 && t >= t_first && t <= t_last;
@@ -592,13 +582,8 @@ lbx_status backward_t(lbx_domain* d, lbx_gradient* out, double* dprof_b, double*
       A.wu = in_win ? (T)(ob.w_ux / (nwin * nout)) : T(0);
       solute_live = solute_live || (p.nsubs == 2 && A.wc != T(0));
       const bool sol = p.nsubs == 2 && solute_on(p, t) && solute_live;
-      if (sol) {
-        if (d->Q == 19) launch_adj<T, 19>(d, odd, true, A);
-        else launch_adj<T, 9>(d, odd, true, A);
-      }
-      A.mu_in = sol ? 1 : 0;
-      if (d->Q == 19) launch_adj<T, 19>(d, odd, false, A);
-      else launch_adj<T, 9>(d, odd, false, A);
+      if (d->Q == 19) launch_adj<T, 19>(d, odd, sol, A);
+      else launch_adj<T, 9>(d, odd, sol, A);
       if (solute_live) launch_adj_faces<T>(d, t, (T*)L, st->dpt, st->dpb);
       ACK(cudaGetLastError());
     }

@@ -786,9 +786,14 @@ __global__ void face_plane(T* f, const uint8_t* solids, const int* fidx, int LX,
     if (COMPACT) return fidx[q];
     return solids[q] == 1 ? -1 : q;
   };
+  // only the populations the rule reads: the knowns (cz != the unknowns'),
+  // or for the zero gradient the five opposite the unknowns
+  const int cz_unknown = top ? -1 : 1;
   T d[19];
 #pragma unroll
   for (int a = 0; a < 19; ++a) {
+    const bool need = kind == FACE_ZEROGRAD ? cz(a) == -cz_unknown : cz(a) != cz_unknown;
+    if (!need) { d[a] = T(0); continue; }
     if (second) {
       d[a] = fs[opp(a) * stride + self];
     } else {
