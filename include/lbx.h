@@ -302,7 +302,7 @@ lbx_status lbx_batch_init_equilibrium(lbx_batch* b, int sample, const void* rho,
 /* Steps t0+1 .. t0+nsteps of every sample, macro variables at multiples of
  * frame_rate, in `mode` (LBX_BATCH_*). */
 lbx_status lbx_batch_run(lbx_batch* b, int t0, int nsteps, int frame_rate, int mode);
-/* Times FUSED at block sizes 128/256/512 and PERSISTENT on `steps` trial
+/* Times FUSED at block sizes 128/256 and PERSISTENT on `steps` trial
  * steps, restores the populations, and keeps the fastest for AUTO. */
 lbx_status lbx_batch_autotune(lbx_batch* b, int steps, int* mode, int* block);
 lbx_status lbx_batch_set_stream(lbx_batch* b, void* stream);

@@ -28,6 +28,7 @@
 #include <cstdio>
 #include <cstring>
 #include <numeric>
+#include <type_traits>
 #include <vector>
 
 namespace cg = cooperative_groups;
@@ -76,15 +77,16 @@ struct BatchArgs {
 
 // One block of the batch: the compact AA step of aa_step_compact, with the
 // sample's extents and constants.
-template <typename T, int Q, int MODEL, bool ODD>
+template <typename T, int Q, int MODEL, bool ODD, bool IDX32>
 __device__ __forceinline__ void batch_block(const BatchArgs<T>& A, int b)
 {
+  using Idx = typename std::conditional<IDX32, unsigned, size_t>::type;
   constexpr int D = (Q == 9) ? 2 : 3;
   const int s = A.blk_sample[b];
   const SampleDesc<T>& S = A.samples[s];
   const int m = b * blockDim.x + threadIdx.x;            // global compact index
   if (m - S.cbase >= S.F) return;                        // padding after the sample
-  const size_t F = (size_t)A.Ftot;
+  const Idx F = (Idx)A.Ftot;
   const int n = A.fnode[m];
   if (n < 0) return;
   const int LX = S.LX, LY = S.LY, plane = S.plane;
@@ -121,7 +123,7 @@ __device__ __forceinline__ void batch_block(const BatchArgs<T>& A, int b)
 #pragma unroll
     for (int a = 0; a < Q; ++a) {
       const int up = (a == 0) ? m : nb_pull(opp(a));
-      const size_t src = (up >= 0) ? (size_t)a * F + (size_t)up : (size_t)opp(a) * F + m;
+      const Idx src = (up >= 0) ? (Idx)a * F + (Idx)up : (Idx)opp(a) * F + (Idx)m;
       d[a] = fs[src];
     }
   } else {
@@ -135,7 +137,7 @@ __device__ __forceinline__ void batch_block(const BatchArgs<T>& A, int b)
 #pragma unroll
     for (int a = 0; a < Q; ++a) {
       const int dn = (a == 0) ? m : nb_push(a);
-      const size_t dst = (dn >= 0) ? (size_t)opp(a) * F + (size_t)dn : (size_t)a * F + m;
+      const Idx dst = (dn >= 0) ? (Idx)opp(a) * F + (Idx)dn : (Idx)a * F + (Idx)m;
       fs[dst] = d[a];
     }
   } else {
@@ -145,16 +147,18 @@ __device__ __forceinline__ void batch_block(const BatchArgs<T>& A, int b)
   }
 }
 
-template <typename T, int Q, int MODEL, bool ODD>
-__global__ void __launch_bounds__(512)
+// Up to 256 threads per block; five resident blocks of 256 (48 registers)
+// in FP32, three in FP64.
+template <typename T, int Q, int MODEL, bool ODD, bool IDX32>
+__global__ void __launch_bounds__(256, (sizeof(T) == 4 ? 5 : 3))
 aa_step_batch(BatchArgs<T> A)
 {
-  batch_block<T, Q, MODEL, ODD>(A, A.block0 + blockIdx.x);
+  batch_block<T, Q, MODEL, ODD, IDX32>(A, A.block0 + blockIdx.x);
 }
 
 // Persistent: a resident grid walks all blocks of the batch for `steps`
 // lattice steps starting at parity `odd0`, with a grid barrier between steps.
-template <typename T, int Q, int MODEL>
+template <typename T, int Q, int MODEL, bool IDX32>
 __global__ void __launch_bounds__(256)
 aa_run_batch_persistent(BatchArgs<T> A, int steps, int odd0)
 {
@@ -162,8 +166,8 @@ aa_run_batch_persistent(BatchArgs<T> A, int steps, int odd0)
   for (int st = 0; st < steps; ++st) {
     const bool odd = ((odd0 + st) & 1) != 0;
     for (int b = blockIdx.x; b < A.nblocks; b += gridDim.x) {
-      if (odd) batch_block<T, Q, MODEL, true>(A, b);
-      else batch_block<T, Q, MODEL, false>(A, b);
+      if (odd) batch_block<T, Q, MODEL, true, IDX32>(A, b);
+      else batch_block<T, Q, MODEL, false, IDX32>(A, b);
     }
     g.sync();
   }
@@ -204,8 +208,8 @@ struct lbx_batch {
   int* fnode = nullptr;
   uint8_t* solids = nullptr;
   void* samples = nullptr;    // SampleDesc<T>[nsamples]
-  int* blk_sample[3] = {nullptr, nullptr, nullptr};   // block sizes 128, 256, 512
-  int nblocks[3] = {0, 0, 0};
+  int* blk_sample[2] = {nullptr, nullptr};   // block sizes 128, 256
+  int nblocks[2] = {0, 0};
   void* red = nullptr;
   cudaStream_t stream = nullptr, own_stream = nullptr;
   int parity = 0;
@@ -221,7 +225,8 @@ struct lbx_batch {
 
 namespace {
 
-const int kBlockSizes[3] = {128, 256, 512};
+const int kBlockSizes[2] = {128, 256};
+constexpr int kNumBlockSizes = 2;
 
 template <typename T, int Q, int MODEL>
 BatchArgs<T> batch_args(lbx_batch* b, int write_mv)
@@ -241,20 +246,26 @@ lbx_status launch_step(lbx_batch* b, bool odd, int write_mv, int mode)
 {
   BatchArgs<T> A = batch_args<T, Q, MODEL>(b, write_mv);
   const int bs = kBlockSizes[b->bs_index];
+  const bool idx32 = (unsigned long long)Q * (unsigned long long)b->Ftot < (1ull << 32);
+  auto go = [&](unsigned nb) {
+    if (idx32) {
+      if (odd) aa_step_batch<T, Q, MODEL, true, true><<<nb, bs, 0, b->stream>>>(A);
+      else aa_step_batch<T, Q, MODEL, false, true><<<nb, bs, 0, b->stream>>>(A);
+    } else {
+      if (odd) aa_step_batch<T, Q, MODEL, true, false><<<nb, bs, 0, b->stream>>>(A);
+      else aa_step_batch<T, Q, MODEL, false, false><<<nb, bs, 0, b->stream>>>(A);
+    }
+    b->launches++;
+  };
   if (mode == LBX_BATCH_SEQUENTIAL) {
     for (int s : b->order) {
       if (b->F[s] == 0) continue;
       A.block0 = b->cbase[s] / bs;
-      const unsigned nb = (unsigned)((b->F[s] + bs - 1) / bs);
-      if (odd) aa_step_batch<T, Q, MODEL, true><<<nb, bs, 0, b->stream>>>(A);
-      else aa_step_batch<T, Q, MODEL, false><<<nb, bs, 0, b->stream>>>(A);
-      b->launches++;
+      go((unsigned)((b->F[s] + bs - 1) / bs));
     }
   } else {
     if (A.nblocks == 0) return LBX_OK;
-    if (odd) aa_step_batch<T, Q, MODEL, true><<<A.nblocks, bs, 0, b->stream>>>(A);
-    else aa_step_batch<T, Q, MODEL, false><<<A.nblocks, bs, 0, b->stream>>>(A);
-    b->launches++;
+    go((unsigned)A.nblocks);
   }
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return bfail(LBX_ERR_CUDA, "batch step: %s", cudaGetErrorString(e));
@@ -268,13 +279,15 @@ lbx_status launch_persistent(lbx_batch* b, int steps, bool odd_first)
   // the persistent kernel is compiled for 256-thread blocks
   A.blk_sample = b->blk_sample[1];
   A.nblocks = b->nblocks[1];
+  const bool idx32 = (unsigned long long)Q * (unsigned long long)b->Ftot < (1ull << 32);
   if (b->coop_grid == 0) {
     int dev = 0, sms = 0, per_sm = 0, coop = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-        &per_sm, aa_run_batch_persistent<T, Q, MODEL>, 256, 0);
+        &per_sm, idx32 ? (const void*)aa_run_batch_persistent<T, Q, MODEL, true>
+                       : (const void*)aa_run_batch_persistent<T, Q, MODEL, false>, 256, 0);
     if (e != cudaSuccess || !coop || per_sm < 1)
       return bfail(LBX_ERR_CUDA, "persistent mode unavailable (%s)", cudaGetErrorString(e));
     b->coop_grid = sms * per_sm;
@@ -282,8 +295,10 @@ lbx_status launch_persistent(lbx_batch* b, int steps, bool odd_first)
   const int grid = std::min(b->coop_grid, std::max(1, A.nblocks));
   int odd0 = odd_first ? 1 : 0;
   void* args[] = {&A, &steps, &odd0};
-  cudaError_t e = cudaLaunchCooperativeKernel((const void*)aa_run_batch_persistent<T, Q, MODEL>,
-                                              grid, 256, args, 0, b->stream);
+  cudaError_t e = cudaLaunchCooperativeKernel(
+      idx32 ? (const void*)aa_run_batch_persistent<T, Q, MODEL, true>
+            : (const void*)aa_run_batch_persistent<T, Q, MODEL, false>,
+      grid, 256, args, 0, b->stream);
   if (e != cudaSuccess) return bfail(LBX_ERR_CUDA, "persistent launch: %s", cudaGetErrorString(e));
   b->launches++;
   return LBX_OK;
@@ -350,7 +365,7 @@ void release(lbx_batch* b)
   if (b->graph) cudaGraphExecDestroy(b->graph);
   cudaFree(b->fc); cudaFree(b->fdense); cudaFree(b->mv); cudaFree(b->fidx);
   cudaFree(b->fnode); cudaFree(b->solids); cudaFree(b->samples); cudaFree(b->red);
-  for (int i = 0; i < 3; ++i) cudaFree(b->blk_sample[i]);
+  for (int i = 0; i < kNumBlockSizes; ++i) cudaFree(b->blk_sample[i]);
   if (b->own_stream) cudaStreamDestroy(b->own_stream);
 }
 
@@ -556,7 +571,7 @@ lbx_status lbx_batch_create(int nsamples, const lbx_params* params, const uint8_
     BCKD(cudaMalloc(&b->samples, desc.size()));
     BCKD(cudaMemcpy(b->samples, desc.data(), desc.size(), cudaMemcpyHostToDevice));
   }
-  for (int i = 0; i < 3; ++i) {
+  for (int i = 0; i < kNumBlockSizes; ++i) {
     // every block of a sample's padded range belongs to that sample, so a
     // padding thread finds m - cbase >= F and exits
     const int bs = kBlockSizes[i];
@@ -691,7 +706,7 @@ lbx_status lbx_batch_autotune(lbx_batch* b, int steps, int* mode_out, int* block
   const int modes[2] = {LBX_BATCH_FUSED, LBX_BATCH_PERSISTENT};
   lbx_status st = LBX_OK;
   for (int mi = 0; mi < 2 && st == LBX_OK; ++mi) {
-    for (int bi = 0; bi < 3 && st == LBX_OK; ++bi) {
+    for (int bi = 0; bi < kNumBlockSizes && st == LBX_OK; ++bi) {
       if (modes[mi] == LBX_BATCH_PERSISTENT && bi != 1) continue;
       b->bs_index = bi;
       st = run_steps(b, 0, 2, 0, modes[mi]);            // warm-up (and graph capture)
