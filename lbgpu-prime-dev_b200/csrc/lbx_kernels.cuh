@@ -420,14 +420,14 @@ struct CompactArgs {
   int faces;              // 2D: fused face boundaries configured
 };
 
-// Resident 256-thread blocks asked of the compiler: five (48 registers) for
+// Resident 256-thread blocks asked of the compiler: six (40 registers) for
 // the FP32 flow kernels, where that measured fastest; for the others the
 // cap closest above their natural register count (FP32 solute 85, FP64 flow
 // 85, FP64 solute 128), since a lower cap spills.
 template <typename T, int PART>
 constexpr int compact_min_blocks()
 {
-  return sizeof(T) == 4 ? (PART == PART_SOLUTE ? 3 : 5) : (PART == PART_SOLUTE ? 2 : 3);
+  return sizeof(T) == 4 ? (PART == PART_SOLUTE ? 3 : 6) : (PART == PART_SOLUTE ? 2 : 3);
 }
 
 // IDX32: population offsets within one substance's [Q][P] block fit in 32
@@ -497,6 +497,11 @@ aa_step_compact(CompactArgs<T> C)
     }
     T* const fs = A.f + (size_t)s * Q * F;
     T* const fo = (OOP ? A.fout : A.f) + (size_t)s * Q * F;
+    // the odd step's pull slots: the push writes d_a back to the slot it
+    // pulled d_opp(a) from (the AA pattern's in-place pairing), so the
+    // push reads them here instead of repeating the 18 index lookups;
+    // one column per thread, no barrier needed
+    __shared__ unsigned sslot[ODD ? Q : 1][256];
     T d[Q];
     if (ODD) {
       // pull: d_a = f[a][idx(n - c_a)], or own f[opp a] behind a solid; the
@@ -505,6 +510,7 @@ aa_step_compact(CompactArgs<T> C)
       for (int a = 0; a < Q; ++a) {
         const int up = (a == 0) ? m : nb_pull(opp(a));
         const Idx src = (up >= 0) ? (Idx)a * F + (Idx)up : (Idx)opp(a) * F + (Idx)m;
+        sslot[a][threadIdx.x] = (unsigned)src;
         d[a] = fs[src];
       }
     } else {
@@ -534,11 +540,7 @@ aa_step_compact(CompactArgs<T> C)
       xm = opaque(xm); xp = opaque(xp); ym = opaque(ym); yp = opaque(yp);
       if (D == 3) { zm = opaque(zm); zp = opaque(zp); }
 #pragma unroll
-      for (int a = 0; a < Q; ++a) {
-        const int dn = (a == 0) ? m : nb_push(a);
-        const Idx dst = (dn >= 0) ? (Idx)opp(a) * F + (Idx)dn : (Idx)a * F + (Idx)m;
-        fo[dst] = d[a];
-      }
+      for (int a = 0; a < Q; ++a) fo[(Idx)sslot[opp(a)][threadIdx.x]] = d[a];
     } else {
       const int m2 = opaque(m);   // do not keep the load addresses live
 #pragma unroll
