@@ -5,6 +5,7 @@
  *
  *   lbgpu_b200 [name] [--dims 2|3] [--subs 1|2] [--precision 4|8]
  *              [--model shifted|plain|shifted-compressible] [--device N]
+ *              [--solid-rule device|nonzero]
  *
  * Reads ./in/params.in (./in_<name>/params.in with a name, src/latman.c:
  * 108-116), the mask ./in/<LX>x<LY>.bmp (2D) or ./in/<LX>x<LY>x<LZ>.raw (3D)
@@ -104,6 +105,7 @@ int main(int argc, char** argv)
   char dir[512], path[1024], err[512];
   const char* name = NULL;
   const char* model = "shifted";
+  const char* solid_rule = "device";
   int device = 0, i, s, time, frame;
   double* ntab = NULL, *stab = NULL;
   int nlen = 0, slen = 0;
@@ -115,6 +117,7 @@ int main(int argc, char** argv)
     else if (!strcmp(argv[i], "--precision") && i + 1 < argc) r.prec = atoi(argv[++i]);
     else if (!strcmp(argv[i], "--model") && i + 1 < argc) model = argv[++i];
     else if (!strcmp(argv[i], "--device") && i + 1 < argc) device = atoi(argv[++i]);
+    else if (!strcmp(argv[i], "--solid-rule") && i + 1 < argc) solid_rule = argv[++i];
     else if (argv[i][0] != '-') name = argv[i];
     else DIE("unknown option %s", argv[i]);
   }
@@ -130,6 +133,16 @@ int main(int argc, char** argv)
   } else {
     snprintf(path, sizeof path, "./in/%dx%dx%d.raw", r.hp.LX, r.hp.LY, r.hp.LZ);
     if (lbh_read_raw_mask(path, r.hp.NumNodes, r.mask, err, sizeof err)) DIE("%s", err);
+  }
+  {
+    const int rule = !strcmp(solid_rule, "nonzero") ? LBH_SOLID_NONZERO
+                   : !strcmp(solid_rule, "device") ? LBH_SOLID_DEVICE : -1;
+    long long odd;
+    if (rule < 0) DIE("--solid-rule must be device or nonzero");
+    odd = lbh_apply_solid_rule(r.mask, r.hp.NumNodes, rule);
+    if (odd && rule == LBH_SOLID_DEVICE)
+      fprintf(stderr, "warning: %lld mask bytes are neither 0 nor 1; the device rule "
+              "runs them as fluid (--solid-rule nonzero makes them solid)\n", odd);
   }
 
   lbx_params_default(&p);

@@ -317,3 +317,15 @@ void lbh_frame_filename(char* buf, int buflen, const char* outdir, const char* p
   if (nsubs == 1) sb[0] = '\0'; else snprintf(sb, sizeof sb, "_subs%02d", subs);
   snprintf(buf, (size_t)buflen, "%s/cuda_%s%s%s%s%s", outdir, prefix, size, fr, sb, suffix);
 }
+
+long long lbh_apply_solid_rule(uint8_t* mask, long long N, int rule)
+{
+  long long n, odd = 0;
+  for (n = 0; n < N; n++) {
+    if (mask[n] > 1) {
+      ++odd;
+      if (rule == LBH_SOLID_NONZERO) mask[n] = 1;
+    }
+  }
+  return odd;
+}

@@ -81,6 +81,17 @@ int lbh_read_bmp_mask(const char* path, int LX, int LY, uint8_t* out,
 int lbh_read_raw_mask(const char* path, long long N, uint8_t* out,
                       char* err, int errlen);
 
+/* Solid-flag rule.  The reference's device treats a mask byte as solid iff
+ * it equals 1 (src/lattice.c:2291, :2314) while its frame writer blanks every
+ * non-zero byte (src/lbio.c:2530-2540): a RAW mask that marks solids with
+ * 255 runs them as fluid yet zeroes them in the output frames.
+ * LBH_SOLID_DEVICE leaves the bytes as they are (parity with the reference);
+ * LBH_SOLID_NONZERO maps every non-zero byte to 1, so the device and the
+ * writer agree.  Returns the number of bytes whose meaning differs between
+ * the two rules (non-zero bytes other than 1), counted before any change. */
+enum { LBH_SOLID_DEVICE = 0, LBH_SOLID_NONZERO = 1 };
+long long lbh_apply_solid_rule(uint8_t* mask, long long N, int rule);
+
 /* Write a 24-bit BMP / raw mask in the same conventions (for generators). */
 int lbh_write_bmp_mask(const char* path, int LX, int LY, const uint8_t* mask);
 int lbh_write_raw_mask(const char* path, long long N, const uint8_t* mask);

@@ -88,6 +88,8 @@ def load():
         lib.lbh_write_raw_mask.argtypes = [C.c_char_p, C.c_longlong, C.c_void_p]
         lib.lbh_initial_rho.argtypes = [C.POINTER(HostParams), C.c_int, C.c_int, C.c_int,
                                         C.c_void_p]
+        lib.lbh_apply_solid_rule.argtypes = [C.c_void_p, C.c_longlong, C.c_int]
+        lib.lbh_apply_solid_rule.restype = C.c_longlong
         _lib = lib
     return _lib
 
@@ -118,6 +120,16 @@ def read_raw_mask(path: str, N: int) -> np.ndarray:
     if load().lbh_read_raw_mask(path.encode(), N, out.ctypes.data, err, 512):
         raise HostError(err.value.decode())
     return out
+
+
+SOLID_DEVICE, SOLID_NONZERO = 0, 1
+
+
+def apply_solid_rule(mask: np.ndarray, rule: int) -> int:
+    """lbh_apply_solid_rule in place on a uint8 mask; returns how many bytes
+    are neither 0 nor 1."""
+    assert mask.dtype == np.uint8 and mask.flags.c_contiguous
+    return int(load().lbh_apply_solid_rule(mask.ctypes.data, mask.size, rule))
 
 
 def write_bmp_mask(path: str, LX: int, LY: int, mask: np.ndarray):

@@ -176,3 +176,15 @@ def test_initial_density_cube_and_uniform(tmp_path):
     p.initial_condition = 7
     with pytest.raises(host.HostError):
         host.initial_rho(p, 2, 1, 0)
+
+
+def test_solid_rule_device_keeps_bytes_nonzero_maps_to_one():
+    from lbx import host
+    m = np.array([0, 1, 255, 2, 0, 1], np.uint8)
+    d = m.copy()
+    assert host.apply_solid_rule(d, host.SOLID_DEVICE) == 2
+    assert np.array_equal(d, m)
+    z = m.copy()
+    assert host.apply_solid_rule(z, host.SOLID_NONZERO) == 2
+    assert np.array_equal(z, [0, 1, 1, 1, 0, 1])
+    assert host.apply_solid_rule(z, host.SOLID_DEVICE) == 0
