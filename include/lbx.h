@@ -90,6 +90,9 @@ typedef struct lbx_params {
   int constcon_t_in, constcon_b_in;          /* solute C = rho_sigma_in    */
   int zeroconcgrad_t, zeroconcgrad_b;        /* solute zero gradient       */
   double rho_sigma_in;
+  int kahan;                /* KAHAN_SUMMATION (src/flags.h:46-49): the flow's
+                               density sums are compensated (fk_add,
+                               src/lattice.c:3099-3114)                    */
 } lbx_params;
 
 /* Device storage of the populations.  DENSE keeps the reference's

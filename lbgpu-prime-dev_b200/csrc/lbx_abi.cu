@@ -112,6 +112,7 @@ void fill_args(const lbx_domain* d, int t, unsigned flags, StepArgs<T>& A)
   A.sink1 = (T)(1.0 - (T)p.sink * (T)p.tau[1]);
   A.write_mv = (flags & LBX_WRITE_MV) ? 1 : 0;
   A.solute_on = (t >= p.sigma_t_on && t <= p.sigma_t_off) ? 1 : 0;
+  A.kahan = p.kahan ? 1 : 0;
   A.ubuf = (T*)d->ubuf;
   A.fout = (T*)d->fout;
   A.ustride = d->layout == LBX_LAYOUT_COMPACT ? d->P : d->N;

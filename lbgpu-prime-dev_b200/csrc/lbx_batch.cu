@@ -73,6 +73,7 @@ struct BatchArgs {
   int nblocks;                  // blocks of the current block size
   int block0;                   // first block (SEQUENTIAL mode)
   int write_mv;
+  int kahan;                    // compensated density sums
 };
 
 // One block of the batch: the compact AA step of aa_step_compact, with the
@@ -95,6 +96,7 @@ __device__ __forceinline__ void batch_block(const BatchArgs<T>& A, int b)
   L.N = S.N;
   L.sc[0] = S.sc;
   L.write_mv = A.write_mv;
+  L.kahan = A.kahan;
   int xm = 0, xp = 0, ym = 0, yp = 0, zm = 0, zp = 0;
   if (ODD) {
     const int k = fast_div(n, S.div_plane);
@@ -196,7 +198,7 @@ __global__ void batch_scatter(T* fdense, const T* fc, const int* fnode, long lon
 }  // namespace
 
 struct lbx_batch {
-  int nsamples = 0, dims = 0, Q = 0, precision = 0, model = 0;
+  int nsamples = 0, dims = 0, Q = 0, precision = 0, model = 0, kahan = 0;
   std::vector<lbx_params> params;         // per sample (as given)
   std::vector<long long> N, dbase, fbase_dense, mvbase;
   std::vector<int> cbase, F, order;
@@ -238,6 +240,7 @@ BatchArgs<T> batch_args(lbx_batch* b, int write_mv)
   A.blk_sample = b->blk_sample[b->bs_index];
   A.Ftot = b->Ftot; A.nblocks = b->nblocks[b->bs_index];
   A.write_mv = write_mv;
+  A.kahan = b->kahan;
   return A;
 }
 
@@ -487,8 +490,9 @@ lbx_status lbx_batch_create(int nsamples, const lbx_params* params, const uint8_
   for (int s = 0; s < nsamples; ++s) {
     const lbx_params& p = params[s];
     if (p.dims != p0.dims || p.precision != p0.precision || p.accurate != p0.accurate ||
-        p.compressible != p0.compressible)
-      return bfail(LBX_ERR_INVALID, "sample %d: dims, precision and model must match sample 0", s);
+        p.compressible != p0.compressible || (p.kahan != 0) != (p0.kahan != 0))
+      return bfail(LBX_ERR_INVALID,
+                   "sample %d: dims, precision, model and kahan must match sample 0", s);
     if ((p.dims != 2 && p.dims != 3) || p.LX < 1 || p.LY < 1 || p.LZ < 1 ||
         (p.dims == 2 && p.LZ != 1))
       return bfail(LBX_ERR_INVALID, "sample %d: bad extents", s);
@@ -508,6 +512,7 @@ lbx_status lbx_batch_create(int nsamples, const lbx_params* params, const uint8_
   b->Q = p0.dims == 2 ? 9 : 19;
   b->precision = p0.precision;
   b->model = p0.accurate ? (p0.compressible ? SHIFTED_COMP : SHIFTED_INC) : PLAIN_COMP;
+  b->kahan = p0.kahan ? 1 : 0;
   b->params.assign(params, params + nsamples);
   b->N.resize(nsamples); b->dbase.resize(nsamples); b->fbase_dense.resize(nsamples);
   b->mvbase.resize(nsamples); b->cbase.resize(nsamples); b->F.resize(nsamples);

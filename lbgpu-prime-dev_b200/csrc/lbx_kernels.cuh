@@ -151,6 +151,7 @@ struct StepArgs {
   T sink1;               // (1 - sink * tau[1]) for the solute
   int write_mv;
   int solute_on;
+  int kahan;                  // compensated density sums (flow lattice)
   int face_n[2], face_s[2];   // FaceKind per substance (2D, fused path)
   T rho_n[2], rho_s[2];       // face densities this step
   T drho_n[2], drho_s[2];     // face density minus rho_A, formed in double
@@ -182,8 +183,20 @@ __device__ __forceinline__ T collide(const StepArgs<T>& A, int s, bool solute,
   constexpr int D = (Q == 9) ? 2 : 3;
   const SubsConst<T>& c = A.sc[s];
   T rho = d[0];
+  if (A.kahan && !solute) {
+    // compensated sum (KAHAN_SUMMATION: fk_add, src/lattice.c:3099-3114)
+    T corr = T(0);
 #pragma unroll
-  for (int a = 1; a < Q; ++a) rho += d[a];
+    for (int a = 1; a < Q; ++a) {
+      const T next = sub_(d[a], corr);
+      const T sum = add_(rho, next);
+      corr = sub_(sub_(sum, rho), next);
+      rho = sum;
+    }
+  } else {
+#pragma unroll
+    for (int a = 1; a < Q; ++a) rho += d[a];
+  }
   if (solute) {
     if (sinks == 2) rho *= A.sink1;
     rho *= A.sink1;

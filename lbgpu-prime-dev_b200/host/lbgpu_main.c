@@ -5,7 +5,7 @@
  *
  *   lbgpu_b200 [name] [--dims 2|3] [--subs 1|2] [--precision 4|8]
  *              [--model shifted|plain|shifted-compressible] [--device N]
- *              [--solid-rule device|nonzero]
+ *              [--solid-rule device|nonzero] [--kahan]
  *
  * Reads ./in/params.in (./in_<name>/params.in with a name, src/latman.c:
  * 108-116), the mask ./in/<LX>x<LY>.bmp (2D) or ./in/<LX>x<LY>x<LZ>.raw (3D)
@@ -106,6 +106,7 @@ int main(int argc, char** argv)
   const char* name = NULL;
   const char* model = "shifted";
   const char* solid_rule = "device";
+  int kahan = 0;
   int device = 0, i, s, time, frame;
   double* ntab = NULL, *stab = NULL;
   int nlen = 0, slen = 0;
@@ -118,6 +119,7 @@ int main(int argc, char** argv)
     else if (!strcmp(argv[i], "--model") && i + 1 < argc) model = argv[++i];
     else if (!strcmp(argv[i], "--device") && i + 1 < argc) device = atoi(argv[++i]);
     else if (!strcmp(argv[i], "--solid-rule") && i + 1 < argc) solid_rule = argv[++i];
+    else if (!strcmp(argv[i], "--kahan")) kahan = 1;
     else if (argv[i][0] != '-') name = argv[i];
     else DIE("unknown option %s", argv[i]);
   }
@@ -148,6 +150,7 @@ int main(int argc, char** argv)
   lbx_params_default(&p);
   p.dims = r.dims; p.LX = r.hp.LX; p.LY = r.hp.LY; p.LZ = r.hp.LZ;
   p.nsubs = r.nsubs; p.precision = r.prec; p.device = device;
+  p.kahan = kahan;
   if (!strcmp(model, "shifted")) { p.accurate = 1; p.compressible = 0; }
   else if (!strcmp(model, "plain")) { p.accurate = 0; p.compressible = 1; }
   else if (!strcmp(model, "shifted-compressible")) { p.accurate = 1; p.compressible = 1; }

@@ -48,6 +48,7 @@ class _CParams(C.Structure):
         ("constcon_t_in", C.c_int), ("constcon_b_in", C.c_int),
         ("zeroconcgrad_t", C.c_int), ("zeroconcgrad_b", C.c_int),
         ("rho_sigma_in", C.c_double),
+        ("kahan", C.c_int),
     ]
 
 
@@ -195,6 +196,7 @@ class Params:
     zeroconcgrad_t: int = 0
     zeroconcgrad_b: int = 0
     rho_sigma_in: float = 1.0
+    kahan: int = 0
 
     @property
     def Q(self) -> int:

@@ -15,6 +15,7 @@
  *   - per-step order          src/lbgpu_prime.cu:369-915
  *   - equilibrium init        src/latman.c:1786-1840
  *   - weights                 src/latman.c:161-192
+ *   - Kahan density sums      src/lattice.c:3099-3114 (KAHAN_SUMMATION)
  *   - 3D z faces: no reference device code; the 2D rules above carried to
  *     the planes k = 0 / k = LZ-1, Zou-He reconstruction as in the
  *     reference's CPU top/bottom code (src/bcs.c:596-870) -- parity unpinned
@@ -125,7 +126,18 @@ static void collide_node(const ctx_t* c, int s, real_t* d, real_t* uvec,
   const int Q = c->Q, D = c->D;
   int a;
   real_t rho = d[0];
-  for (a = 1; a < Q; a++) rho += d[a];
+  if (p->kahan && !(s == 1 && p->nsubs == 2)) {
+    /* compensated sum of fk_add (src/lattice.c:3099-3114) */
+    real_t correction = 0.0, next, sum;
+    for (a = 1; a < Q; a++) {
+      next = d[a] - correction;
+      sum = rho + next;
+      correction = (sum - rho) - next;
+      rho = sum;
+    }
+  } else {
+    for (a = 1; a < Q; a++) rho += d[a];
+  }
   if (s == 1 && p->nsubs == 2) {
     /* solute: C = sum g; velocity is the fluid's */
     if (sinks == 2) rho *= (1.0 - c->sink * c->tau[1]);

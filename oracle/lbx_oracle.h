@@ -36,6 +36,9 @@ typedef struct {
    * fastest), used instead of rho_sigma_in when not NULL */
   const double* constcon_profile_t;
   const double* constcon_profile_b;
+  /* KAHAN_SUMMATION (src/flags.h:46-49): the flow's density sum is
+   * compensated (fk_add, src/lattice.c:3099-3114) */
+  int kahan;
 } orc_params;
 
 int orc_run_f64(const orc_params*, double* f, const uint8_t* solids,

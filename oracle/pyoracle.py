@@ -65,6 +65,7 @@ class Params:
     rho_sigma_in: float = 1.0
     constcon_profile_t: Optional[np.ndarray] = None
     constcon_profile_b: Optional[np.ndarray] = None
+    kahan: int = 0
 
     @property
     def Q(self) -> int:
@@ -101,6 +102,7 @@ class _OrcParams(C.Structure):
         ("rho_sigma_in", C.c_double),
         ("constcon_profile_t", C.POINTER(C.c_double)),
         ("constcon_profile_b", C.POINTER(C.c_double)),
+        ("kahan", C.c_int),
     ]
 
 
@@ -124,7 +126,7 @@ def _fill(st, p: Params, keep):
     for name, _ in st._fields_:
         if name.startswith("constcon_profile"):
             v = getattr(p, name)
-            if v is not None:
+            if v is not None and np.size(v) > 0:
                 arr = np.ascontiguousarray(v, dtype=np.float64).reshape(-1)
                 keep.append(arr)
                 setattr(st, name, arr.ctypes.data_as(C.POINTER(C.c_double)))
@@ -292,6 +294,8 @@ def variant_name(p: Params, dtype) -> str:
         base += "p"
     elif p.compressible:
         base += "c"
+    if getattr(p, "kahan", 0):
+        base += "k"
     return base + "_" + _sfx(dtype)
 
 

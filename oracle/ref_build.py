@@ -57,6 +57,11 @@ VARIANTS = {
     "d2q9p_f32": dict(NUM_DIMENSIONS=2, NUM_FLUID_COMPONENTS=1, DP_ON=0,
                       ACCURATE=0, COMPRESSIBLE=1),
     "d2q9s_f32": dict(NUM_DIMENSIONS=2, NUM_FLUID_COMPONENTS=2, DP_ON=0),
+    # compensated (Kahan) density sums
+    "d3q19k_f32": dict(NUM_DIMENSIONS=3, NUM_FLUID_COMPONENTS=1, DP_ON=0, KAHAN_SUMMATION=1),
+    "d3q19k_f64": dict(NUM_DIMENSIONS=3, NUM_FLUID_COMPONENTS=1, DP_ON=1, KAHAN_SUMMATION=1),
+    "d2q9k_f32": dict(NUM_DIMENSIONS=2, NUM_FLUID_COMPONENTS=1, DP_ON=0, KAHAN_SUMMATION=1),
+    "d3q19sk_f32": dict(NUM_DIMENSIONS=3, NUM_FLUID_COMPONENTS=2, DP_ON=0, KAHAN_SUMMATION=1),
 }
 
 def variant_flags(src: str, overrides: dict) -> str:

@@ -21,7 +21,7 @@ def load(name):
             continue
         k = key[2:]
         v = z[key]
-        if k.endswith("_table"):
+        if k.endswith("_table") or k.startswith("constcon_profile"):
             setattr(p, k, None if v.size == 0 else v.astype(np.float64))
         elif v.ndim == 0:
             setattr(p, k, v.item())

@@ -6,7 +6,7 @@ stores inputs and outputs as .npz.  Needs oracle/_ref (built where the
 reference tree is available); the fixtures are committed so the tests need
 neither the reference nor the harness.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [name ...]
 """
 import os
 import sys
@@ -54,6 +54,18 @@ def cases():
     ]:
         p = po.Params(dims=2, LX=12, LY=10, LZ=1, tau=(0.9, 0.75), gaccel=g2, **kw)
         out.append((name, p, dt, 18, 6))
+    # compensated density sums (KAHAN_SUMMATION); last, so that the inputs of
+    # the fixtures above keep their seeded draws
+    for name, kw, dt in [
+        ("d3q19k_f32", dict(kahan=1), np.float32),
+        ("d3q19k_f64", dict(kahan=1), np.float64),
+        ("d3q19sk_f32", dict(nsubs=2, kahan=1, sink=2e-3, sigma_t_on=3, sigma_t_off=40),
+         np.float32),
+    ]:
+        p = po.Params(dims=3, LX=10, LY=9, LZ=8, tau=(0.8, 0.7), gaccel=g3, **kw)
+        out.append((name, p, dt, 16, 4))
+    p = po.Params(dims=2, LX=12, LY=10, LZ=1, tau=(0.9, 0.75), gaccel=g2, kahan=1)
+    out.append(("d2q9k_f32", p, np.float32, 18, 6))
     return out
 
 
@@ -72,13 +84,17 @@ def make_inputs(name, p, dtype, rng, fluid_faces):
     return sol, f.astype(dtype)
 
 
-def main():
+def main(only=None):
+    """Writes every fixture, or only those named in `only` (the inputs of the
+    others are still drawn, so each fixture's seeded inputs never change)."""
     rng = np.random.default_rng(20261203)
     for name, p, dtype, steps, fr in cases():
         variant = po.variant_name(p, dtype)
         for tag, fluid_faces in (("", True),) if "bc" not in name and "table" not in name \
                 else (("", True), ("_wrapsolid", False)):
             sol, f0 = make_inputs(name, p, dtype, rng, fluid_faces)
+            if only and name + tag not in only:
+                continue
             f = f0.copy()
             f, mv = po.run_reference(variant, p, f, sol, 0, steps, frame_rate=fr)
             pd = {k: (np.asarray(v) if v is not None else np.array([]))
@@ -91,4 +107,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:] or None)
