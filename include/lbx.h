@@ -93,6 +93,12 @@ typedef struct lbx_params {
   int kahan;                /* KAHAN_SUMMATION (src/flags.h:46-49): the flow's
                                density sums are compensated (fk_add,
                                src/lattice.c:3099-3114)                    */
+  int walsh;                /* WALSH_NS_ON with COMPUTE_ON_SOLIDS
+                               (src/flags.h:56-63): partial bounce-back by a
+                               per-node fraction ns (lbx_set_ns, default 0);
+                               every node is updated and streaming ignores
+                               the solids.  Dense layout; no face
+                               boundaries, batches or adjoint runs.        */
 } lbx_params;
 
 /* Device storage of the populations.  DENSE keeps the reference's
@@ -235,6 +241,14 @@ lbx_status lbx_btc_read(lbx_domain* d, double* c_out, double* ux_out, int max,
  * LX*LY values (i fastest) for the top (top != 0) or bottom face, used
  * instead of rho_sigma_in; NULL returns to rho_sigma_in.  Copied. */
 lbx_status lbx_set_face_profile(lbx_domain* d, int top, const double* conc);
+
+/* Walsh runs (params.walsh = 1): the per-node solid fraction ns, N values in
+ * dense node order, each in [0, 1], stored in the run's precision (the
+ * reference's ns_mem_d, src/lbgpu_prime.cu:259-264, filled from ns_memblock:
+ * src/latman.c:48-80 sets ns where the mask is solid and 0 elsewhere,
+ * src/lbio.c:694-743 reads byte/255 from a .raw file).  LBX_ERR_STATE for a
+ * domain created without walsh, LBX_ERR_INVALID for a value outside [0, 1]. */
+lbx_status lbx_set_ns(lbx_domain* d, const double* ns);
 
 /* Stop recording and release the record. */
 lbx_status lbx_btc_stop(lbx_domain* d);

@@ -116,6 +116,13 @@ void fill_args(const lbx_domain* d, int t, unsigned flags, StepArgs<T>& A)
   A.ubuf = (T*)d->ubuf;
   A.fout = (T*)d->fout;
   A.ustride = d->layout == LBX_LAYOUT_COMPACT ? d->P : d->N;
+  if (d->ns) {
+    A.ns = (const T*)d->ns;
+    for (int s = 0; s < 2; ++s) {
+      A.wtau[s] = (double)(T)p.tau[s];
+      for (int c = 0; c < 3; ++c) A.wg[s * 3 + c] = (double)(T)p.gaccel[s * 3 + c];
+    }
+  }
   if (d->btc_vals) {
     A.btc = d->btc_vals;
     A.btc_lo = d->btc_lo;
@@ -180,8 +187,13 @@ void launch_part(lbx_domain* d, const StepArgs<T>& A, bool odd)
   }
   dim3 block(128, 1, 1);
   dim3 grid((A.LX + 127) / 128, A.LY, A.LZ);
-  if (odd) aa_step<T, Q, NS, MODEL, true, PART><<<grid, block, 0, d->stream>>>(A);
-  else aa_step<T, Q, NS, MODEL, false, PART><<<grid, block, 0, d->stream>>>(A);
+  if (A.ns) {
+    if (odd) aa_step<T, Q, NS, MODEL, true, PART, true><<<grid, block, 0, d->stream>>>(A);
+    else aa_step<T, Q, NS, MODEL, false, PART, true><<<grid, block, 0, d->stream>>>(A);
+  } else {
+    if (odd) aa_step<T, Q, NS, MODEL, true, PART><<<grid, block, 0, d->stream>>>(A);
+    else aa_step<T, Q, NS, MODEL, false, PART><<<grid, block, 0, d->stream>>>(A);
+  }
   d->launches++;
 }
 
@@ -388,6 +400,10 @@ lbx_status check_params(const lbx_params* p)
   if (faces3 && p->dims != 3)
     return fail(LBX_ERR_INVALID, "top/bottom face boundaries exist for 3D runs only");
   if (faces3 && p->LZ < 3) return fail(LBX_ERR_INVALID, "top/bottom faces need LZ >= 3");
+  if (p->walsh && (faces || faces3))
+    return fail(LBX_ERR_INVALID, "Walsh runs take no face boundaries");
+  if (p->walsh && p->layout == LBX_LAYOUT_COMPACT)
+    return fail(LBX_ERR_INVALID, "Walsh runs update every node: dense layout only");
   if (faces && p->LY < 3) return fail(LBX_ERR_INVALID, "face boundaries need LY >= 3");
   for (int s = 0; s < p->nsubs; ++s) {
     if (p->pressure_n_in[s] == 2 && (!p->pressure_n_table || p->pressure_n_len < 1))
@@ -430,7 +446,7 @@ void release(lbx_domain* d)
   cudaFree(d->f); cudaFree(d->mv); cudaFree(d->solids); cudaFree(d->cls);
   cudaFree(d->nbm); cudaFree(d->red);
   cudaFree(d->btc_vals); cudaFree(d->btc_rec); cudaFree(d->btc_slot);
-  cudaFree(d->ubuf); cudaFree(d->prof_t); cudaFree(d->prof_b);
+  cudaFree(d->ubuf); cudaFree(d->prof_t); cudaFree(d->prof_b); cudaFree(d->ns);
   lbx_internal_adjoint_free(d);
   if (d->own_stream) cudaStreamDestroy(d->own_stream);
 }
@@ -628,7 +644,8 @@ lbx_status lbx_create(const lbx_params* p, const uint8_t* solids, lbx_domain** o
     for (int q = 0; q < planes; ++q) d->fluid += d->plane_fluid[q];
   }
   d->layout = p->layout == LBX_LAYOUT_AUTO
-                  ? ((d->N - d->fluid) * 20 >= d->N ? LBX_LAYOUT_COMPACT : LBX_LAYOUT_DENSE)
+                  ? ((d->N - d->fluid) * 20 >= d->N && !p->walsh ? LBX_LAYOUT_COMPACT
+                                                                 : LBX_LAYOUT_DENSE)
                   : p->layout;
 
   auto bail = [&](lbx_status s) { release(d); delete d; return s; };
@@ -666,6 +683,10 @@ lbx_status lbx_create(const lbx_params* p, const uint8_t* solids, lbx_domain** o
   if (p->nsubs == 2) {
     const long long us = d->layout == LBX_LAYOUT_COMPACT ? d->P : d->N;
     CKD(cudaMalloc(&d->ubuf, std::max<size_t>(1, (size_t)3 * us * d->real_size)));
+  }
+  if (p->walsh) {
+    CKD(cudaMalloc(&d->ns, d->N * d->real_size));
+    CKD(cudaMemsetAsync(d->ns, 0, d->N * d->real_size, d->stream));
   }
   CKD(cudaMemsetAsync(d->f, 0, fbytes, d->stream));
   CKD(cudaMemsetAsync(d->mv, 0, mvbytes, d->stream));
@@ -987,6 +1008,24 @@ lbx_status lbx_set_face_profile(lbx_domain* d, int top, const double* conc)
   } else {
     std::vector<float> h(conc, conc + n);
     CK(cudaMemcpy(dst, h.data(), n * sizeof(float), cudaMemcpyHostToDevice));
+  }
+  return LBX_OK;
+}
+
+lbx_status lbx_set_ns(lbx_domain* d, const double* ns)
+{
+  if (!d) return fail(LBX_ERR_INVALID, "domain is NULL");
+  if (!d->ns) return fail(LBX_ERR_STATE, "domain was created without walsh");
+  if (!ns) return fail(LBX_ERR_INVALID, "ns is NULL");
+  for (long long n = 0; n < d->N; ++n)
+    if (!(ns[n] >= 0. && ns[n] <= 1.))
+      return fail(LBX_ERR_INVALID, "ns[%lld] = %g is outside [0, 1]", n, ns[n]);
+  CK(cudaStreamSynchronize(d->stream));
+  if (d->real_size == 8) {
+    CK(cudaMemcpy(d->ns, ns, d->N * sizeof(double), cudaMemcpyHostToDevice));
+  } else {
+    std::vector<float> h(ns, ns + d->N);
+    CK(cudaMemcpy(d->ns, h.data(), d->N * sizeof(float), cudaMemcpyHostToDevice));
   }
   return LBX_OK;
 }

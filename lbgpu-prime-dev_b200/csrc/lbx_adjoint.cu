@@ -436,6 +436,7 @@ bool solute_on(const lbx_params& p, int t) { return t >= p.sigma_t_on && t <= p.
 lbx_status check_adjoint(const lbx_domain* d)
 {
   const lbx_params& p = d->p;
+  if (p.walsh) return afail(LBX_ERR_INVALID, "the adjoint has no Walsh partial bounce-back");
   if (d->layout != LBX_LAYOUT_COMPACT)
     return afail(LBX_ERR_INVALID, "the adjoint runs on the compact layout");
   if (!p.accurate || p.compressible)

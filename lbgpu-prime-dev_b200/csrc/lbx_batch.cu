@@ -497,6 +497,7 @@ lbx_status lbx_batch_create(int nsamples, const lbx_params* params, const uint8_
         (p.dims == 2 && p.LZ != 1))
       return bfail(LBX_ERR_INVALID, "sample %d: bad extents", s);
     if (p.nsubs != 1) return bfail(LBX_ERR_INVALID, "sample %d: batches hold one substance", s);
+    if (p.walsh) return bfail(LBX_ERR_INVALID, "sample %d: batches take no Walsh runs", s);
     if (p.precision != 4 && p.precision != 8) return bfail(LBX_ERR_INVALID, "bad precision");
     if (!p.accurate && !p.compressible) return bfail(LBX_ERR_INVALID, "accurate=0 needs compressible=1");
     if (!(p.tau[0] > 0.5)) return bfail(LBX_ERR_INVALID, "sample %d: tau must exceed 0.5", s);

@@ -37,6 +37,7 @@ struct lbx_domain {
   void* ubuf = nullptr;        // [3][P or N] flow velocity for the solute launch
   void* prof_t = nullptr;      // [LX*LY] constant-concentration profiles (real)
   void* prof_b = nullptr;
+  void* ns = nullptr;        // Walsh fraction per node, [N] in the run's precision
   // plane record (lbx_btc_*)
   double* btc_vals = nullptr;  // [2][plane nodes]: C and u_x this step
   double* btc_rec = nullptr;   // [btc_cap][2] means

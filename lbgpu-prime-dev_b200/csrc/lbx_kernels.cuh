@@ -160,6 +160,11 @@ struct StepArgs {
   T* ubuf;                    // [3][stride]: the flow's u, handed to the solute
   long long ustride;          // N (dense) or P (compact)
   T* fout;                    // compact, OOP kernels: where the step's result goes
+  // Walsh partial bounce-back (dense layout only): per-node fraction ns[N],
+  // and tau and g as the reference's double-precision force term uses them
+  const T* ns;
+  double wtau[2];
+  double wg[6];
 };
 
 // Which substances one launch of a step kernel advances.  Two-substance
@@ -175,13 +180,28 @@ enum StepPart { PART_ALL = 0, PART_FLOW = 1, PART_SOLUTE = 2 };
 // sinks: the solute sink applies once on odd steps and twice on even steps
 // (src/k_stream_collide_stream.c:254-256; src/k_collide.c:96-97, :261-262).
 // Returns the node's density (the solute's C), the value stored as rho.
-template <typename T, int Q, int MODEL>
+// WALSH: partial bounce-back with the node's fraction ns (WALSH_NS_ON,
+// src/k_stream_collide_stream.c:129-215, :363-386; src/lattice.c:2936-2939):
+// the momentum is scaled by (1 - ns) before the division, the force term by
+// (1 - ns), and each collided population is blended with the opposite
+// incoming one, f_a <- f_a (1 - ns) + ns f_opp(a).  The factor 1 - ns is a
+// double (the reference writes `1.`), so those products round once from
+// double in FP32 as well.
+template <typename T, int Q, int MODEL, bool WALSH = false>
 __device__ __forceinline__ T collide(const StepArgs<T>& A, int s, bool solute,
                                         int sinks, T (&d)[Q], T (&u)[3],
                                         long long n)
 {
   constexpr int D = (Q == 9) ? 2 : 3;
   const SubsConst<T>& c = A.sc[s];
+  T nsv = T(0), pre[WALSH ? Q : 1];
+  double om = 1.;
+  if (WALSH) {
+    nsv = A.ns[n];
+    om = __dsub_rn(1., (double)nsv);
+#pragma unroll
+    for (int a = 0; a < Q; ++a) pre[WALSH ? a : 0] = d[a];
+  }
   T rho = d[0];
   if (A.kahan && !solute) {
     // compensated sum (KAHAN_SUMMATION: fk_add, src/lattice.c:3099-3114)
@@ -210,9 +230,21 @@ __device__ __forceinline__ T collide(const StepArgs<T>& A, int s, bool solute,
     }
     T den = (MODEL == SHIFTED_INC) ? c.rhoA
           : (MODEL == PLAIN_COMP) ? rho : (c.rhoA + rho);
-    u[0] = add_(m0 / den, c.tg[0]);
-    u[1] = add_(m1 / den, c.tg[1]);
-    u[2] = (D == 3) ? add_(m2 / den, c.tg[2]) : T(0);
+    if (WALSH) {
+      m0 = (T)__dmul_rn((double)m0, om);
+      m1 = (T)__dmul_rn((double)m1, om);
+      if (D == 3) m2 = (T)__dmul_rn((double)m2, om);
+      // u += ((1 - ns) tau) g, formed in double
+      const double ot = __dmul_rn(om, A.wtau[s]);
+      u[0] = (T)__dadd_rn((double)(m0 / den), __dmul_rn(ot, A.wg[s * 3 + 0]));
+      u[1] = (T)__dadd_rn((double)(m1 / den), __dmul_rn(ot, A.wg[s * 3 + 1]));
+      u[2] = (D == 3) ? (T)__dadd_rn((double)(m2 / den), __dmul_rn(ot, A.wg[s * 3 + 2]))
+                      : T(0);
+    } else {
+      u[0] = add_(m0 / den, c.tg[0]);
+      u[1] = add_(m1 / den, c.tg[1]);
+      u[2] = (D == 3) ? add_(m2 / den, c.tg[2]) : T(0);
+    }
   }
   if (A.write_mv) {
     T* m = A.mv + (long long)s * (1 + D) * A.N;
@@ -245,6 +277,11 @@ __device__ __forceinline__ T collide(const StepArgs<T>& A, int s, bool solute,
       d[a] = add_(add_(mul_(d[a], c.omc), mul_(mul_(w, rho), c.itau)),
                   mul_(mul_(mul_(w, rq), poly), c.itau));
     }
+  }
+  if (WALSH) {
+#pragma unroll
+    for (int a = 0; a < Q; ++a)
+      d[a] = add_((T)__dmul_rn((double)d[a], om), mul_(nsv, pre[WALSH ? opp(a) : 0]));
   }
   return rho;
 }
@@ -314,7 +351,10 @@ __device__ __forceinline__ void face_south(int kind, T rho_bc, T rhoA, T drho, b
 // EVEN: d_a = f[opp a][n], collide, f[a][n] = d_a.
 // Each node reads and writes one fixed slot set, disjoint from every other
 // node's, so the update is in place with no ordering between threads.
-template <typename T, int Q, int NS, int MODEL, bool ODD, int PART>
+// WALSH (partial bounce-back, COMPUTE_ON_SOLIDS): every node is updated and
+// streams periodically with no solid checks (src/lattice.c:2704-2707,
+// :2812-2815); the collision blends by ns (see collide).
+template <typename T, int Q, int NS, int MODEL, bool ODD, int PART, bool WALSH = false>
 __global__ void __launch_bounds__(128)
 aa_step(StepArgs<T> A)
 {
@@ -327,7 +367,7 @@ aa_step(StepArgs<T> A)
   // are reached through 64-bit base pointers, which are uniform per warp.
   const int plane = LX * LY;
   const int n = i + LX * j + plane * k;
-  const uint8_t cl = A.cls[n];
+  const uint8_t cl = WALSH ? uint8_t(0) : A.cls[n];
   if (cl & CLS_SOLID) return;
   const uint32_t nb = (cl & CLS_NEAR) ? A.nbm[n] : 0u;
 
@@ -388,7 +428,7 @@ aa_step(StepArgs<T> A)
       if (cl & CLS_SOUTH)
         face_south<T>(A.face_s[s], A.rho_s[s], A.sc[s].rhoA, A.drho_s[s], shifted, d9);
     }
-    const T rho = collide<T, Q, MODEL>(A, s, solute, ODD ? 1 : 2, d, u, n);
+    const T rho = collide<T, Q, MODEL, WALSH>(A, s, solute, ODD ? 1 : 2, d, u, n);
     if (PART == PART_FLOW && A.solute_on) {
 #pragma unroll
       for (int c = 0; c < D; ++c) A.ubuf[c * A.ustride + n] = u[c];

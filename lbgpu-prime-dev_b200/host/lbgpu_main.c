@@ -5,7 +5,7 @@
  *
  *   lbgpu_b200 [name] [--dims 2|3] [--subs 1|2] [--precision 4|8]
  *              [--model shifted|plain|shifted-compressible] [--device N]
- *              [--solid-rule device|nonzero] [--kahan]
+ *              [--solid-rule device|nonzero] [--kahan] [--walsh]
  *
  * Reads ./in/params.in (./in_<name>/params.in with a name, src/latman.c:
  * 108-116), the mask ./in/<LX>x<LY>.bmp (2D) or ./in/<LX>x<LY>x<LZ>.raw (3D)
@@ -15,8 +15,13 @@
  * a line to ./out/cuda_frames<size>[_subsNN].dat.
  *
  * The build-time flags of the reference (NUM_DIMENSIONS, NUM_FLUID_COMPONENTS,
- * DP_ON, ACCURATE/COMPRESSIBLE) are the options above; the defaults are the
- * reference's shipped flags.h (2D, one substance, double, shifted).
+ * DP_ON, ACCURATE/COMPRESSIBLE, KAHAN_SUMMATION, WALSH_NS_ON with
+ * COMPUTE_ON_SOLIDS) are the options above; the defaults are the reference's
+ * shipped flags.h (2D, one substance, double, shifted).  --walsh takes its
+ * fraction field from the mask and the params.in value `ns` (the field the
+ * reference's 2D runs upload); a 3D run with ns_flag 1 reads
+ * ./in/ns<LX>x<LY>x<LZ>.raw (byte / 255) instead, as read_ns does (the
+ * reference's own 3D runs leave the uploaded field unset).
  */
 #include <stdio.h>
 #include <stdlib.h>
@@ -106,7 +111,7 @@ int main(int argc, char** argv)
   const char* name = NULL;
   const char* model = "shifted";
   const char* solid_rule = "device";
-  int kahan = 0;
+  int kahan = 0, walsh = 0;
   int device = 0, i, s, time, frame;
   double* ntab = NULL, *stab = NULL;
   int nlen = 0, slen = 0;
@@ -120,6 +125,7 @@ int main(int argc, char** argv)
     else if (!strcmp(argv[i], "--device") && i + 1 < argc) device = atoi(argv[++i]);
     else if (!strcmp(argv[i], "--solid-rule") && i + 1 < argc) solid_rule = argv[++i];
     else if (!strcmp(argv[i], "--kahan")) kahan = 1;
+    else if (!strcmp(argv[i], "--walsh")) walsh = 1;
     else if (argv[i][0] != '-') name = argv[i];
     else DIE("unknown option %s", argv[i]);
   }
@@ -151,6 +157,7 @@ int main(int argc, char** argv)
   p.dims = r.dims; p.LX = r.hp.LX; p.LY = r.hp.LY; p.LZ = r.hp.LZ;
   p.nsubs = r.nsubs; p.precision = r.prec; p.device = device;
   p.kahan = kahan;
+  p.walsh = walsh;
   if (!strcmp(model, "shifted")) { p.accurate = 1; p.compressible = 0; }
   else if (!strcmp(model, "plain")) { p.accurate = 0; p.compressible = 1; }
   else if (!strcmp(model, "shifted-compressible")) { p.accurate = 1; p.compressible = 1; }
@@ -188,6 +195,16 @@ int main(int argc, char** argv)
     p.pressure_s_table = stab; p.pressure_s_len = slen;
   }
   LBX(lbx_create(&p, r.mask, &r.dom));
+  if (walsh) {
+    double* ns = (double*)malloc((size_t)r.hp.NumNodes * sizeof(double));
+    const int src = r.dims == 3 && r.hp.ns_flag == 1 ? LBH_NS_FILE : LBH_NS_MASK;
+    snprintf(path, sizeof path, "./in/ns%dx%dx%d.raw", r.hp.LX, r.hp.LY, r.hp.LZ);
+    if (lbh_walsh_ns(rv(&r.hp.ns, r.prec), src, r.mask, r.hp.NumNodes, path, ns, err,
+                     sizeof err))
+      DIE("%s", err);
+    LBX(lbx_set_ns(r.dom, ns));
+    free(ns);
+  }
 
   /* initial state (init_problem, src/latman.c:1270-1959): rho per
    * initial_condition, u = 0, f = feq; the same [rho, u] planes are the

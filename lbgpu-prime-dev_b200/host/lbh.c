@@ -318,6 +318,30 @@ void lbh_frame_filename(char* buf, int buflen, const char* outdir, const char* p
   snprintf(buf, (size_t)buflen, "%s/cuda_%s%s%s%s%s", outdir, prefix, size, fr, sb, suffix);
 }
 
+int lbh_walsh_ns(double ns_value, int source, const uint8_t* mask, long long N,
+                 const char* path, double* ns, char* err, int errlen)
+{
+  long long n;
+  if (source == LBH_NS_MASK) {
+    if (!(ns_value >= 0. && ns_value <= 1.)) {
+      snprintf(err, (size_t)errlen, "ns = %g: should have 0 <= ns <= 1", ns_value);
+      return -1;
+    }
+    for (n = 0; n < N; n++) ns[n] = mask[n] == 1 ? ns_value : 0.;
+    return 0;
+  }
+  if (source == LBH_NS_FILE) {
+    uint8_t* raw = (uint8_t*)malloc((size_t)(N > 0 ? N : 1));
+    if (!raw) { snprintf(err, (size_t)errlen, "out of host memory"); return -1; }
+    if (lbh_read_raw_mask(path, N, raw, err, errlen)) { free(raw); return -1; }
+    for (n = 0; n < N; n++) ns[n] = raw[n] / 255.0;
+    free(raw);
+    return 0;
+  }
+  snprintf(err, (size_t)errlen, "unknown ns source %d", source);
+  return -1;
+}
+
 long long lbh_apply_solid_rule(uint8_t* mask, long long N, int rule)
 {
   long long n, odd = 0;

@@ -92,6 +92,18 @@ int lbh_read_raw_mask(const char* path, long long N, uint8_t* out,
 enum { LBH_SOLID_DEVICE = 0, LBH_SOLID_NONZERO = 1 };
 long long lbh_apply_solid_rule(uint8_t* mask, long long N, int rule);
 
+/* Walsh fraction field ns (N doubles) for a WALSH_NS_ON run.
+ * LBH_NS_MASK: ns = the params.in value `ns` where the mask byte is 1, else
+ *   0 (process_ns, src/latman.c:48-80: the field the reference's 2D runs
+ *   upload, src/lbgpu_prime.cu:259-264).
+ * LBH_NS_FILE: ns = byte / 255 of the N-byte file `path` (read_ns,
+ *   src/lbio.c:694-743, ./in/ns<LX>x<LY>x<LZ>.raw).
+ * The value `ns` must lie in [0, 1] (src/latman.c:677-689).  Returns 0, or
+ * -1 with a message in err. */
+enum { LBH_NS_MASK = 0, LBH_NS_FILE = 1 };
+int lbh_walsh_ns(double ns_value, int source, const uint8_t* mask, long long N,
+                 const char* path, double* ns, char* err, int errlen);
+
 /* Write a 24-bit BMP / raw mask in the same conventions (for generators). */
 int lbh_write_bmp_mask(const char* path, int LX, int LY, const uint8_t* mask);
 int lbh_write_raw_mask(const char* path, long long N, const uint8_t* mask);

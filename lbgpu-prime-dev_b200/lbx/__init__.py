@@ -49,6 +49,7 @@ class _CParams(C.Structure):
         ("zeroconcgrad_t", C.c_int), ("zeroconcgrad_b", C.c_int),
         ("rho_sigma_in", C.c_double),
         ("kahan", C.c_int),
+        ("walsh", C.c_int),
     ]
 
 
@@ -113,6 +114,7 @@ _SIGNATURES = {
     "lbx_btc_read": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double),
                                C.c_int, C.POINTER(C.c_longlong)]),
     "lbx_set_face_profile": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_double)]),
+    "lbx_set_ns": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
     "lbx_adjoint_forward": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int,
                                       C.POINTER(_CObjective), C.POINTER(C.c_double)]),
     "lbx_adjoint_backward": (C.c_int, [C.c_void_p, C.POINTER(_CGradient),
@@ -197,6 +199,7 @@ class Params:
     zeroconcgrad_b: int = 0
     rho_sigma_in: float = 1.0
     kahan: int = 0
+    walsh: int = 0          # partial bounce-back by a per-node fraction (set_ns)
 
     @property
     def Q(self) -> int:
@@ -422,6 +425,14 @@ class Domain:
             raise ValueError("profile must hold LX*LY values")
         _check(_lib.lbx_set_face_profile(self._h, 1 if top else 0,
                                          a.ctypes.data_as(C.POINTER(C.c_double))))
+
+    def set_ns(self, ns):
+        """Walsh runs: the per-node fraction ns (N values, dense node order,
+        each in [0, 1])."""
+        a = np.ascontiguousarray(ns, dtype=np.float64).reshape(-1)
+        if a.size != self.p.NN:
+            raise ValueError("ns must hold LX*LY*LZ values")
+        _check(_lib.lbx_set_ns(self._h, a.ctypes.data_as(C.POINTER(C.c_double))))
 
     def btc_stop(self):
         _check(_lib.lbx_btc_stop(self._h))

@@ -90,6 +90,8 @@ def load():
                                         C.c_void_p]
         lib.lbh_apply_solid_rule.argtypes = [C.c_void_p, C.c_longlong, C.c_int]
         lib.lbh_apply_solid_rule.restype = C.c_longlong
+        lib.lbh_walsh_ns.argtypes = [C.c_double, C.c_int, C.c_void_p, C.c_longlong,
+                                     C.c_char_p, C.c_void_p, C.c_char_p, C.c_int]
         _lib = lib
     return _lib
 
@@ -130,6 +132,24 @@ def apply_solid_rule(mask: np.ndarray, rule: int) -> int:
     are neither 0 nor 1."""
     assert mask.dtype == np.uint8 and mask.flags.c_contiguous
     return int(load().lbh_apply_solid_rule(mask.ctypes.data, mask.size, rule))
+
+
+NS_MASK, NS_FILE = 0, 1
+
+
+def walsh_ns(ns_value: float, source: int, mask: np.ndarray = None, N: int = None,
+             path: str = "") -> np.ndarray:
+    """lbh_walsh_ns: the Walsh fraction field from the mask (ns_value where
+    the byte is 1, else 0) or from an N-byte file (byte / 255)."""
+    if mask is not None:
+        mask = np.ascontiguousarray(mask, dtype=np.uint8).reshape(-1)
+        N = mask.size
+    out = np.zeros(N, np.float64)
+    err = C.create_string_buffer(512)
+    if load().lbh_walsh_ns(ns_value, source, mask.ctypes.data if mask is not None else None,
+                           N, path.encode(), out.ctypes.data, err, 512):
+        raise HostError(err.value.decode())
+    return out
 
 
 def write_bmp_mask(path: str, LX: int, LY: int, mask: np.ndarray):

@@ -16,6 +16,8 @@
  *   - equilibrium init        src/latman.c:1786-1840
  *   - weights                 src/latman.c:161-192
  *   - Kahan density sums      src/lattice.c:3099-3114 (KAHAN_SUMMATION)
+ *   - Walsh partial bounce-back src/k_stream_collide_stream.c:129-215,
+ *     :363-386, src/lattice.c:2704, :2812, :2936 (WALSH_NS_ON)
  *   - 3D z faces: no reference device code; the 2D rules above carried to
  *     the planes k = 0 / k = LZ-1, Zou-He reconstruction as in the
  *     reference's CPU top/bottom code (src/bcs.c:596-870) -- parity unpinned
@@ -125,7 +127,11 @@ static void collide_node(const ctx_t* c, int s, real_t* d, real_t* uvec,
   const orc_params* p = c->p;
   const int Q = c->Q, D = c->D;
   int a;
+  const real_t ns = p->walsh ? (real_t)p->ns[n] : (real_t)0;
+  real_t pre[19];
   real_t rho = d[0];
+  if (p->walsh)
+    for (a = 0; a < Q; a++) pre[a] = d[a];
   if (p->kahan && !(s == 1 && p->nsubs == 2)) {
     /* compensated sum of fk_add (src/lattice.c:3099-3114) */
     real_t correction = 0.0, next, sum;
@@ -149,6 +155,7 @@ static void collide_node(const ctx_t* c, int s, real_t* d, real_t* uvec,
       if (D == 3) u[2] += ((real_t)CZ[a]) * d[a];
     }
     for (a = 0; a < D; a++) {
+      if (p->walsh) u[a] *= (1. - ns);
       if (p->compressible) {
         if (p->accurate) u[a] /= (c->rho_A[s] + rho);
         else u[a] /= rho;
@@ -161,6 +168,8 @@ static void collide_node(const ctx_t* c, int s, real_t* d, real_t* uvec,
   /* body force (src/lattice.c:2928-2944) or solute sink */
   if (s == 1 && p->nsubs == 2) {
     rho *= (1.0 - c->sink * c->tau[1]);
+  } else if (p->walsh) {
+    for (a = 0; a < D; a++) uvec[a] += (1. - ns) * c->tau[s] * c->g[s * 3 + a];
   } else {
     for (a = 0; a < D; a++) uvec[a] += c->tau[s] * c->g[s * 3 + a];
   }
@@ -198,6 +207,12 @@ static void collide_node(const ctx_t* c, int s, real_t* d, real_t* uvec,
               * (3. * cu + 4.5 * cu * cu - 1.5 * usq) * c->inv_tau[s];
       }
     }
+    /* Walsh: blend with the opposite pre-collision population */
+    if (p->walsh)
+      for (a = 0; a < Q; a++) {
+        d[a] *= 1. - ns;
+        d[a] += ns * pre[opp(a)];
+      }
   }
 }
 
@@ -220,20 +235,21 @@ static void odd_range(const ctx_t* c, real_t* f, const uint8_t* sol,
     real_t d[19], uvec[3] = {0, 0, 0};
     long nb[19];
     int a, s;
-    if (is_solid(sol, n)) continue;
+    const int wl = p->walsh;
+    if (!wl && is_solid(sol, n)) continue;
     for (a = 0; a < Q; a++) nb[a] = wrap_nbr(p, i, j, k, CX[a], CY[a], CZ[a]);
     for (s = 0; s < c->NS; s++) {
       real_t* fs = f + (long)s * Q * NN;
       if (s == 1 && !solute_on(p, t)) continue;
       for (a = 0; a < Q; a++) {
         long up = nb[opp(a)];                /* n - c_a */
-        d[a] = is_solid(sol, up) ? fs[(long)opp(a) * NN + n]
-                                 : fs[(long)a * NN + up];
+        d[a] = (!wl && is_solid(sol, up)) ? fs[(long)opp(a) * NN + n]
+                                          : fs[(long)a * NN + up];
       }
       collide_node(c, s, d, uvec, 1, write_mv, mv, n);
       for (a = 0; a < Q; a++) {
         long dn = nb[a];                     /* n + c_a */
-        if (is_solid(sol, dn)) fs[(long)a * NN + n] = d[a];
+        if (!wl && is_solid(sol, dn)) fs[(long)a * NN + n] = d[a];
         else fs[(long)opp(a) * NN + dn] = d[a];
       }
     }
@@ -251,7 +267,7 @@ static void even_range(const ctx_t* c, real_t* f, const uint8_t* sol,
   for (n = n0; n < n1; n++) {
     real_t d[19], uvec[3] = {0, 0, 0};
     int a, s;
-    if (is_solid(sol, n)) continue;
+    if (!c->p->walsh && is_solid(sol, n)) continue;
     for (s = 0; s < c->NS; s++) {
       real_t* fs = f + (long)s * Q * NN;
       if (s == 1 && !solute_on(c->p, t)) continue;

@@ -39,6 +39,13 @@ typedef struct {
   /* KAHAN_SUMMATION (src/flags.h:46-49): the flow's density sum is
    * compensated (fk_add, src/lattice.c:3099-3114) */
   int kahan;
+  /* WALSH_NS_ON with COMPUTE_ON_SOLIDS (src/flags.h:56-63): every node is
+   * updated, streaming ignores the solid flags, and the collision blends
+   * with the opposite populations by the node's fraction ns[n] (N values)
+   * (src/k_stream_collide_stream.c:129-215, :363-386; src/lattice.c:2704,
+   * :2812, :2936) */
+  int walsh;
+  const double* ns;
 } orc_params;
 
 int orc_run_f64(const orc_params*, double* f, const uint8_t* solids,

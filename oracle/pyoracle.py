@@ -66,6 +66,8 @@ class Params:
     constcon_profile_t: Optional[np.ndarray] = None
     constcon_profile_b: Optional[np.ndarray] = None
     kahan: int = 0
+    walsh: int = 0
+    ns: Optional[np.ndarray] = None     # per-node Walsh fraction (walsh == 1)
 
     @property
     def Q(self) -> int:
@@ -103,6 +105,8 @@ class _OrcParams(C.Structure):
         ("constcon_profile_t", C.POINTER(C.c_double)),
         ("constcon_profile_b", C.POINTER(C.c_double)),
         ("kahan", C.c_int),
+        ("walsh", C.c_int),
+        ("ns", C.POINTER(C.c_double)),
     ]
 
 
@@ -124,7 +128,7 @@ class _RefParams(C.Structure):
 
 def _fill(st, p: Params, keep):
     for name, _ in st._fields_:
-        if name.startswith("constcon_profile"):
+        if name.startswith("constcon_profile") or name == "ns":
             v = getattr(p, name)
             if v is not None and np.size(v) > 0:
                 arr = np.ascontiguousarray(v, dtype=np.float64).reshape(-1)
@@ -278,6 +282,14 @@ def run_reference(variant: str, p: Params, f: np.ndarray, solids: np.ndarray,
     keep = []
     st = _RefParams()
     _fill(st, p, keep)
+    lib.refk_walsh.restype = C.c_int
+    assert lib.refk_walsh() == (1 if getattr(p, "walsh", 0) else 0)
+    ns = None
+    if getattr(p, "walsh", 0):
+        ns = np.ascontiguousarray(np.zeros(p.NN) if p.ns is None else p.ns, dtype=f.dtype)
+        lib.refk_set_ns(ns.ctypes.data_as(C.c_void_p))
+    else:
+        lib.refk_set_ns(None)
     rc = lib.refk_run(C.byref(st), f.ctypes.data_as(C.c_void_p),
                       sol.ctypes.data_as(C.c_void_p),
                       mv.ctypes.data_as(C.c_void_p), t0, nsteps, frame_rate)
@@ -296,6 +308,8 @@ def variant_name(p: Params, dtype) -> str:
         base += "c"
     if getattr(p, "kahan", 0):
         base += "k"
+    if getattr(p, "walsh", 0):
+        base += "w"
     return base + "_" + _sfx(dtype)
 
 

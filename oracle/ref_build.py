@@ -62,6 +62,15 @@ VARIANTS = {
     "d3q19k_f64": dict(NUM_DIMENSIONS=3, NUM_FLUID_COMPONENTS=1, DP_ON=1, KAHAN_SUMMATION=1),
     "d2q9k_f32": dict(NUM_DIMENSIONS=2, NUM_FLUID_COMPONENTS=1, DP_ON=0, KAHAN_SUMMATION=1),
     "d3q19sk_f32": dict(NUM_DIMENSIONS=3, NUM_FLUID_COMPONENTS=2, DP_ON=0, KAHAN_SUMMATION=1),
+    # Walsh partial bounce-back (needs computing on solid nodes)
+    "d3q19w_f64": dict(NUM_DIMENSIONS=3, NUM_FLUID_COMPONENTS=1, DP_ON=1,
+                       COMPUTE_ON_SOLIDS=1, WALSH_NS_ON=1),
+    "d3q19w_f32": dict(NUM_DIMENSIONS=3, NUM_FLUID_COMPONENTS=1, DP_ON=0,
+                       COMPUTE_ON_SOLIDS=1, WALSH_NS_ON=1),
+    "d2q9w_f64": dict(NUM_DIMENSIONS=2, NUM_FLUID_COMPONENTS=1, DP_ON=1,
+                      COMPUTE_ON_SOLIDS=1, WALSH_NS_ON=1),
+    "d3q19sw_f64": dict(NUM_DIMENSIONS=3, NUM_FLUID_COMPONENTS=2, DP_ON=1,
+                        COMPUTE_ON_SOLIDS=1, WALSH_NS_ON=1),
 }
 
 def variant_flags(src: str, overrides: dict) -> str:

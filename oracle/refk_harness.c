@@ -178,6 +178,10 @@ typedef struct {
   refk_kernel k; int gx, gy, z0, z1; real* f; real* mv; unsigned char* sol;
 } grid_job;
 
+/* The per-node Walsh fraction n_s handed to the kernels as ns_mem_d
+ * (WALSH_NS_ON builds; NULL otherwise, as the other builds never read it). */
+static real* g_ns = NULL;
+
 static void* grid_worker(void* arg)
 {
   grid_job* g = (grid_job*)arg;
@@ -188,7 +192,7 @@ static void* grid_worker(void* arg)
     for (y = 0; y < (unsigned)g->gy; y++)
       for (x = 0; x < (unsigned)g->gx; x++) {
         blockIdx.x = x; blockIdx.y = y; blockIdx.z = z;
-        g->k(g->f, g->mv, g->sol, NULL);
+        g->k(g->f, g->mv, g->sol, g_ns);
       }
   return NULL;
 }
@@ -203,7 +207,7 @@ static void* grid_worker_rows(void* arg)
   for (y = 0; y < (unsigned)g->gy; y++)
     for (x = 0; x < (unsigned)g->gx; x++) {
       blockIdx.x = x; blockIdx.y = (unsigned)g->z0 + y;
-      g->k(g->f, g->mv, g->sol, NULL);
+      g->k(g->f, g->mv, g->sol, g_ns);
     }
   return NULL;
 }
@@ -318,6 +322,11 @@ static void bcs(const refk_params* p, int time, int second,
  * Per step, src/lbgpu_prime.cu:369-915: set time_c; 2D only: bcs_1 (odd) or
  * bcs_2 (even); then k_stream_collide_stream (odd) or k_collide (even).
  */
+/* Walsh builds: the per-node n_s (N reals, kept by the caller). */
+EXPORT void refk_set_ns(real* ns) { g_ns = ns; }
+
+EXPORT int refk_walsh(void) { return WALSH_NS_ON ? 1 : 0; }
+
 EXPORT int refk_run(const refk_params* p, real* f, const unsigned char* solids,
                     real* mv, int t0, int nsteps, int frame_rate)
 {

@@ -9,8 +9,15 @@ import pyoracle as po
 GOLDEN_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
 
-def golden_names():
-    return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN_DIR, "*.npz")))
+def _is_walsh(name):
+    # variant letters follow the lattice name: d3q19sw_f64 = solute + Walsh
+    return "w" in name.split("_")[0].replace("d3q19", "").replace("d2q9", "")
+
+
+def golden_names(walsh=None):
+    """All fixtures, or only the Walsh (walsh=True) or non-Walsh ones."""
+    names = sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN_DIR, "*.npz")))
+    return [n for n in names if walsh is None or _is_walsh(n) == walsh]
 
 
 def load(name):
@@ -21,7 +28,7 @@ def load(name):
             continue
         k = key[2:]
         v = z[key]
-        if k.endswith("_table") or k.startswith("constcon_profile"):
+        if k.endswith("_table") or k.startswith("constcon_profile") or k == "ns":
             setattr(p, k, None if v.size == 0 else v.astype(np.float64))
         elif v.ndim == 0:
             setattr(p, k, v.item())

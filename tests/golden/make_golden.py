@@ -66,6 +66,18 @@ def cases():
         out.append((name, p, dt, 16, 4))
     p = po.Params(dims=2, LX=12, LY=10, LZ=1, tau=(0.9, 0.75), gaccel=g2, kahan=1)
     out.append(("d2q9k_f32", p, np.float32, 18, 6))
+    # Walsh partial bounce-back (WALSH_NS_ON with COMPUTE_ON_SOLIDS); the
+    # per-node fraction ns is drawn with the inputs
+    for name, kw, dt in [
+        ("d3q19w_f64", dict(walsh=1), np.float64),
+        ("d3q19w_f32", dict(walsh=1), np.float32),
+        ("d3q19sw_f64", dict(nsubs=2, walsh=1, sink=2e-3, sigma_t_on=3, sigma_t_off=40),
+         np.float64),
+    ]:
+        p = po.Params(dims=3, LX=10, LY=9, LZ=8, tau=(0.8, 0.7), gaccel=g3, **kw)
+        out.append((name, p, dt, 16, 4))
+    p = po.Params(dims=2, LX=12, LY=10, LZ=1, tau=(0.9, 0.75), gaccel=g2, walsh=1)
+    out.append(("d2q9w_f64", p, np.float64, 18, 6))
     return out
 
 
@@ -81,6 +93,12 @@ def make_inputs(name, p, dtype, rng, fluid_faces):
         f[0] += W[:, None]
     if p.nsubs == 2:
         f[1] = np.abs(f[1]) + 0.5 * W[:, None]
+    if p.walsh:
+        # fractions in [0, 1] with exact 0 (open) and 1 (full bounce-back)
+        ns = rng.uniform(0.0, 1.0, size=p.NN)
+        pick = rng.choice([0, 1, 2], size=p.NN, p=[0.5, 0.3, 0.2])
+        ns = np.where(pick == 1, 0.0, np.where(pick == 2, 1.0, ns))
+        p.ns = ns.astype(dtype).astype(np.float64)
     return sol, f.astype(dtype)
 
 

@@ -50,6 +50,9 @@ def test_params_default_matches_reference_defaults():
     dict(dims=3, pressure_s_in=(1, 0)),
     dict(dims=2, LZ=1, LY=2, pressure_s_in=(1, 0)),
     dict(dims=2, LZ=1, pressure_n_in=(2, 0)),
+    dict(walsh=1, pressure_t_in=(1, 0)),
+    dict(dims=2, LZ=1, walsh=1, pressure_s_in=(1, 0)),
+    dict(walsh=1, layout=lbx.LBX_LAYOUT_COMPACT),
 ])
 def test_create_validates_before_touching_the_device(bad):
     kw = dict(dims=3, LX=4, LY=4, LZ=4)

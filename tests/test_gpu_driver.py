@@ -1,0 +1,127 @@
+"""The C host driver (bin/lbgpu_b200, the reference's main) end to end.
+
+Each case writes the reference's input files (in/params.in, the solid mask,
+the Walsh fraction file), runs the driver in a scratch directory and
+compares its last frame of .dat files -- binary reals, zero where the mask
+byte is non-zero -- with the CPU oracle run from the same initial state
+(equilibrium at the initial density, u = 0).  Tolerances (norm-wise
+relative): FP64 1e-12, FP32 1e-5.
+"""
+import glob
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import pyoracle as po
+from lbx import geometry, host
+from _golden import rel_err
+from _host_files import write_params
+
+pytestmark = pytest.mark.gpu
+
+DRIVER = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
+                      "lbgpu-prime-dev_b200", "bin", "lbgpu_b200")
+TOL = {8: 1e-12, 4: 1e-5}
+
+
+def run_driver(tmp, args):
+    r = subprocess.run([DRIVER] + args, cwd=tmp, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    return r
+
+
+def oracle_last_frame(hp, dims, prec, mask, steps, fr, **kw):
+    """The oracle's macro variables at the last frame, with the driver's
+    parameters and initial state."""
+    rv = (lambda x: x.f) if prec == 4 else (lambda x: x.d)
+    p = po.Params(dims=dims, LX=hp.LX, LY=hp.LY, LZ=hp.LZ,
+                  tau=(rv(hp.tau[0]), rv(hp.tau[1])), rho_A=(rv(hp.rho_A[0]), rv(hp.rho_A[1])),
+                  gaccel=tuple(rv(hp.gforce[s][c]) for s in range(2) for c in range(3)),
+                  rho_in=rv(hp.rho_in), rho_out=rv(hp.rho_out),
+                  bc_ramp_start=hp.bc_ramp_start, bc_ramp_stop=hp.bc_ramp_stop, **kw)
+    dtype = np.float32 if prec == 4 else np.float64
+    rho = host.initial_rho(hp, dims, 1, 0).astype(dtype).astype(np.float64)
+    z = np.zeros(p.NN)
+    f = po.init_feq(p, rho[None], z[None], z[None], z[None], dtype=dtype)
+    f, mv = po.run_oracle(p, f, mask, 0, steps, fr)
+    return mv
+
+
+def read_frame(tmp, name, frame, prec):
+    path, = glob.glob(os.path.join(tmp, "out", "cuda_%s*_frame%04d.dat" % (name, frame)))
+    return np.fromfile(path, dtype=np.float32 if prec == 4 else np.float64)
+
+
+def check_frame(tmp, mv, mask, dims, frame, prec):
+    solid = mask != 0
+    for c, name in enumerate(["rho", "u_x", "u_y", "u_z"][:dims + 1]):
+        a = read_frame(tmp, name, frame, prec)
+        assert np.all(a[solid] == 0)
+        e = rel_err(a[~solid], mv[0, c][~solid])
+        assert e <= TOL[prec], "%s: %g" % (name, e)
+
+
+BASE = {"NumFrames": 3, "FrameRate": 10, "tau[0]": 0.9, "tau[1]": 1.0, "rho_A[0]": 1.0,
+        "rho_A[1]": 1.0, "bc_ramp_start": -1, "bc_ramp_stop": -1, "sigma_t_on": -1,
+        "sigma_t_off": -1, "initial_condition": 0, "x0": -1, "r0": -1}
+
+
+def test_gpu_driver_2d_pressure_faces(tmp_path):
+    """The reference's default build (2D, FP64, shifted) between Zou-He
+    pressure faces, with a disc-pack .bmp mask."""
+    tmp = str(tmp_path)
+    os.makedirs(os.path.join(tmp, "in"))
+    LX, LY = 40, 32
+    write_params(os.path.join(tmp, "in", "params.in"),
+                 dict(BASE, LX=LX, LY=LY, LZ=1, rho_in=1.002, rho_out=1.0,
+                      **{"pressure_s_in[0]": 1, "pressure_n_out[0]": 1}))
+    mask = geometry.transpose_2d(geometry.disc_pack(LY, LX, radius=3, porosity=0.6, seed=4),
+                                 LY, LX)
+    host.write_bmp_mask(os.path.join(tmp, "in", "%dx%d.bmp" % (LX, LY)), LX, LY, mask)
+    run_driver(tmp, [])
+    hp = host.read_params(os.path.join(tmp, "in", "params.in"), 2, 1)
+    mv = oracle_last_frame(hp, 2, 8, mask, 30, 10, pressure_s_in=(1, 0),
+                           pressure_n_out=(1, 0))
+    check_frame(tmp, mv, mask, 2, 3, 8)
+    frames, = glob.glob(os.path.join(tmp, "out", "cuda_frames*.dat"))
+    lines = [ln for ln in open(frames) if not ln.startswith("#")]
+    assert [int(ln.split()[0]) for ln in lines] == [0, 10, 20, 30]
+
+
+@pytest.mark.parametrize("prec", [8, 4])
+def test_gpu_driver_3d_walsh_from_file(tmp_path, prec):
+    """--walsh in 3D with ns_flag 1: the fraction field is byte / 255 of
+    in/ns<LX>x<LY>x<LZ>.raw; every node is updated."""
+    tmp = str(tmp_path)
+    os.makedirs(os.path.join(tmp, "in"))
+    LX, LY, LZ = 20, 18, 16
+    write_params(os.path.join(tmp, "in", "params.in"),
+                 dict(BASE, LX=LX, LY=LY, LZ=LZ, ns_flag=1, **{"gforce[0][0]": 2e-5}))
+    mask = np.zeros(LX * LY * LZ, np.uint8)
+    host.write_raw_mask(os.path.join(tmp, "in", "%dx%dx%d.raw" % (LX, LY, LZ)), mask)
+    rng = np.random.default_rng(41)
+    raw = rng.integers(0, 256, LX * LY * LZ).astype(np.uint8)
+    raw.tofile(os.path.join(tmp, "in", "ns%dx%dx%d.raw" % (LX, LY, LZ)))
+    run_driver(tmp, ["--dims", "3", "--precision", str(prec), "--walsh"])
+    hp = host.read_params(os.path.join(tmp, "in", "params.in"), 3, 1)
+    mv = oracle_last_frame(hp, 3, prec, mask, 30, 10, walsh=1, ns=raw / 255.0)
+    check_frame(tmp, mv, mask, 3, 3, prec)
+
+
+def test_gpu_driver_2d_walsh_mask_rule(tmp_path):
+    """--walsh in 2D: ns = the params.in value where the mask is solid, 0
+    elsewhere (the field the reference's 2D runs upload)."""
+    tmp = str(tmp_path)
+    os.makedirs(os.path.join(tmp, "in"))
+    LX, LY = 36, 30
+    write_params(os.path.join(tmp, "in", "params.in"),
+                 dict(BASE, LX=LX, LY=LY, LZ=1, ns=0.6, **{"gforce[0][0]": 1e-5}))
+    mask = geometry.transpose_2d(geometry.disc_pack(LY, LX, radius=3, porosity=0.7, seed=5),
+                                 LY, LX)
+    host.write_bmp_mask(os.path.join(tmp, "in", "%dx%d.bmp" % (LX, LY)), LX, LY, mask)
+    run_driver(tmp, ["--walsh"])
+    hp = host.read_params(os.path.join(tmp, "in", "params.in"), 2, 1)
+    mv = oracle_last_frame(hp, 2, 8, mask, 30, 10, walsh=1, ns=np.where(mask == 1, 0.6, 0.0))
+    check_frame(tmp, mv, mask, 2, 3, 8)

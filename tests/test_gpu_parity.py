@@ -100,7 +100,7 @@ def fp64_truth(p, f0, sol, steps, fr):
 
 
 @pytest.mark.parametrize("layout", ["dense", "compact"])
-@pytest.mark.parametrize("name", golden_names())
+@pytest.mark.parametrize("name", golden_names(walsh=False))
 def test_gpu_matches_reference_golden(name, layout):
     p, z = load(name)
     dtype = z["f0"].dtype

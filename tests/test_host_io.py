@@ -12,17 +12,9 @@ import pytest
 
 import pyoracle as po
 from lbx import host
+from _host_files import write_params
 
 REF_IN = "/root/reference/in"
-
-
-def write_params(path, values):
-    """A params.in in the positional layout: 'label value' per line."""
-    with open(path, "w") as fh:
-        for (name, is_real) in host.params_layout():
-            v = values.get(name, 0.0 if is_real else 0)
-            label = name.replace("[", "_").replace("]", "")
-            fh.write("%-24s %s\n" % (label, repr(float(v)) if is_real else str(int(v))))
 
 
 VALUES = {
@@ -188,3 +180,19 @@ def test_solid_rule_device_keeps_bytes_nonzero_maps_to_one():
     assert host.apply_solid_rule(z, host.SOLID_NONZERO) == 2
     assert np.array_equal(z, [0, 1, 1, 1, 0, 1])
     assert host.apply_solid_rule(z, host.SOLID_DEVICE) == 0
+
+
+def test_walsh_ns_from_mask_and_file(tmp_path):
+    """The mask rule of process_ns (ns where the byte is 1, 0 elsewhere, so
+    255 bytes stay 0 as the device rule reads them) and the byte / 255 rule
+    of read_ns; ns outside [0, 1] and a short file are errors."""
+    m = np.array([0, 1, 255, 1, 0, 2], np.uint8)
+    assert np.array_equal(host.walsh_ns(0.3, host.NS_MASK, mask=m), [0, 0.3, 0, 0.3, 0, 0])
+    with pytest.raises(host.HostError):
+        host.walsh_ns(1.5, host.NS_MASK, mask=m)
+    raw = np.array([0, 255, 51, 128, 7], np.uint8)
+    path = str(tmp_path / "ns5x1x1.raw")
+    raw.tofile(path)
+    assert np.array_equal(host.walsh_ns(0.0, host.NS_FILE, N=5, path=path), raw / 255.0)
+    with pytest.raises(host.HostError):
+        host.walsh_ns(0.0, host.NS_FILE, N=6, path=path)
