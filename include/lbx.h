@@ -183,9 +183,11 @@ lbx_status lbx_set_stream(lbx_domain* d, void* stream);
 /* Wait for all queued work of the domain; reports asynchronous errors. */
 lbx_status lbx_sync(lbx_domain* d);
 
-/* FP64 on-device reductions over the macro variables last written (a step
- * with LBX_WRITE_MV).  Replaces the host-side compute_{max,min,ave}_rho /
- * _u of src/compute.c:1159-1416 used by the frame summary.  Synchronous. */
+/* FP64 on-device conservation diagnostics over the macro variables last
+ * written (a step with LBX_WRITE_MV): mass, momentum, solute mass, density
+ * range and a non-finite count over device-rule fluid nodes (mask byte not
+ * 1).  LBX_ERR_NUMERIC (with `out` filled) when a value is non-finite.
+ * Synchronous. */
 lbx_status lbx_reduce(lbx_domain* d, lbx_reductions* out);
 
 /* The reductions of lbx_reduce for callers that cannot allocate device
@@ -204,6 +206,47 @@ lbx_status lbx_reduce(lbx_domain* d, lbx_reductions* out);
 lbx_status lbx_reduce_mv_static(const void* mv, const uint8_t* solids,
                                 long long N, int dims, int nsubs, int precision,
                                 void* stream, lbx_reductions* out);
+
+/* ---- frame output ---------------------------------------------------------
+ * The statistics the reference's output_frame reports per substance
+ * (compute_{max,min,ave}_{u,rho}, src/compute.c:1159-1416, written by
+ * dump_frame_summary, src/lbio.c:140-290): over the nodes whose mask byte
+ * is 0 (the host rule, is_not_solid, src/lattice.c:163-194), the max and
+ * min of |rho| and |u_c| and the means of rho and u_c; u_z is 0 in 2D.  A
+ * NaN never replaces a running max or min (as in the reference); sums are
+ * FP64 on the device, in a fixed order (reproducible). */
+typedef struct lbx_frame_stats {
+  long long nodes;
+  double max_rho, min_rho, ave_rho;
+  double max_u[3], min_u[3], ave_u[3];
+} lbx_frame_stats;
+
+/* Statistics of substance `subs` from the macro variables last written.
+ * Synchronous. */
+lbx_status lbx_frame_stats_compute(lbx_domain* d, int subs, lbx_frame_stats* out);
+
+/* Asynchronous frame output.  lbx_frame_enqueue, called after a step with
+ * LBX_WRITE_MV, queues on the domain's stream the statistics of every
+ * substance and a device-side snapshot of the macro variables, then copies
+ * both to page-locked host memory on a second stream, and returns at once:
+ * the copies overlap the steps queued after it, and no later step waits
+ * for them (replaces the synchronous per-frame cudaMemcpy and
+ * cudaThreadSynchronize of src/lbgpu_prime.cu:544-583, :765-804).
+ * lbx_frame_wait blocks until the oldest queued frame has landed and
+ * returns it; its mv pointers ([1+D][N] reals per substance, page-locked)
+ * stay valid until the second lbx_frame_enqueue after the wait.  At most
+ * two frames are outstanding (LBX_ERR_STATE beyond); lbx_frame_wait with
+ * none outstanding is LBX_ERR_STATE.  The first enqueue allocates two
+ * device and two host buffers of the macro variables' size. */
+typedef struct lbx_frame {
+  int time;
+  int nsubs;
+  const void* mv[2];
+  lbx_frame_stats stats[2];
+} lbx_frame;
+
+lbx_status lbx_frame_enqueue(lbx_domain* d, int time);
+lbx_status lbx_frame_wait(lbx_domain* d, lbx_frame* out);
 
 /* Device pointers to the populations ([nsubs][Q][N], the dense exchange
  * format; with the compact layout this first writes the current state into

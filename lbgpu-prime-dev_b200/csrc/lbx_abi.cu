@@ -448,6 +448,7 @@ void release(lbx_domain* d)
   cudaFree(d->btc_vals); cudaFree(d->btc_rec); cudaFree(d->btc_slot);
   cudaFree(d->ubuf); cudaFree(d->prof_t); cudaFree(d->prof_b); cudaFree(d->ns);
   lbx_internal_adjoint_free(d);
+  lbx_internal_frames_free(d);
   if (d->own_stream) cudaStreamDestroy(d->own_stream);
 }
 

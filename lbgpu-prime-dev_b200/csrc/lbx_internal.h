@@ -47,6 +47,7 @@ struct lbx_domain {
   int btc_plane = 0;
   void* fout = nullptr;        // set only while recomputing states (OOP step)
   void* adj = nullptr;         // adjoint checkpoints and objective (lbx_adjoint.cu)
+  void* frames = nullptr;      // frame statistics and snapshots (lbx_frames.cu)
   int parity = 0;             // 0: natural order (next step odd); 1: swapped
   long long launches = 0;
   // graph replay of frame-free, time-invariant runs: one captured AA pair
@@ -61,3 +62,4 @@ struct lbx_domain {
 LBX_HIDDEN lbx_status lbx_internal_fail(lbx_status code, const char* msg);
 LBX_HIDDEN lbx_status lbx_internal_step_into(lbx_domain* d, int t, void* src, void* dst);
 LBX_HIDDEN void lbx_internal_adjoint_free(lbx_domain* d);
+LBX_HIDDEN void lbx_internal_frames_free(lbx_domain* d);

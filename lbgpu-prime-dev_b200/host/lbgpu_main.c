@@ -6,13 +6,17 @@
  *   lbgpu_b200 [name] [--dims 2|3] [--subs 1|2] [--precision 4|8]
  *              [--model shifted|plain|shifted-compressible] [--device N]
  *              [--solid-rule device|nonzero] [--kahan] [--walsh]
+ *              [--frames summary,raw,dat,txt|all|none]
  *
  * Reads ./in/params.in (./in_<name>/params.in with a name, src/latman.c:
  * 108-116), the mask ./in/<LX>x<LY>.bmp (2D) or ./in/<LX>x<LY>x<LZ>.raw (3D)
  * and, for pressure_{n,s}_in[0] == 2, ./in/pressure_{n,s}_in0.in; then runs
- * NumFrames*FrameRate steps in AA pairs and at every frame writes
- * ./out/cuda_{rho,u_x,u_y[,u_z]}<size>_frame<NNNN>[_subsNN].dat and appends
- * a line to ./out/cuda_frames<size>[_subsNN].dat.
+ * NumFrames*FrameRate steps and at every frame writes the files of the
+ * reference's output_frame into ./out: a line of cuda_frames<size>[_subsNN].dat
+ * (summary), in 3D the byte images cuda_{rho,u,u_x,u_y,u_z}<size>_frameNNNN.raw
+ * (raw), cuda_{rho,u_x,u_y[,u_z]}<size>_frameNNNN.dat (dat) and the text dumps
+ * cuda_{rho,ux,uy,uz}<size>_frameNNNN.txt (txt); --frames selects the kinds
+ * (default all, as the reference's build writes).
  *
  * The build-time flags of the reference (NUM_DIMENSIONS, NUM_FLUID_COMPONENTS,
  * DP_ON, ACCURATE/COMPRESSIBLE, KAHAN_SUMMATION, WALSH_NS_ON with
@@ -58,49 +62,54 @@ typedef struct {
   int dims, nsubs, prec;
   uint8_t* mask;
   lbx_domain* dom;
-  void* mv;       /* host copy of one substance's macro variables */
-  char size[64];
+  unsigned frame_files;   /* LBH_FRAME_* kinds written per frame */
 } run_t;
 
-static void output_frame(run_t* r, int time, int frame)
+/* The files of output_frame (src/lbio.c:37-131) for one frame that
+ * lbx_frame_wait returned: the summary line, the 3D byte images, the .dat
+ * files and the text dumps, with the statistics computed on the device. */
+static void write_frame(run_t* r, const lbx_frame* fr, int frame)
 {
-  const long long N = r->hp.NumNodes;
-  const size_t plane = (size_t)N * (size_t)r->prec;
-  char fn[1024];
+  lbh_frame_stats st[2];
+  const void* mv[2] = {fr->mv[0], fr->mv[1]};
   int s, c;
-  lbx_reductions red;
-  const char* names[4] = {"rho", "u_x", "u_y", "u_z"};
-  lbx_status st = lbx_reduce(r->dom, &red);
-  if (st != LBX_OK && st != LBX_ERR_NUMERIC) DIE("lbx_reduce: %s", lbx_last_error());
-  for (s = 0; s < r->nsubs; s++) {
-    char* base = (char*)r->mv;
-    FILE* o;
-    LBX(lbx_download_mv(r->dom, s, base, base + plane, base + 2 * plane,
-                        r->dims == 3 ? base + 3 * plane : NULL));
-    for (c = 0; c <= r->dims; c++) {
-      lbh_frame_filename(fn, sizeof fn, "./out", names[c], r->dims, r->hp.LX, r->hp.LY,
-                         r->hp.LZ, frame, r->nsubs, s, ".dat");
-      if (lbh_write_dat(fn, base + c * plane, r->prec, N, r->mask)) DIE("cannot write %s", fn);
+  for (s = 0; s < fr->nsubs; s++) {
+    st[s].nodes = fr->stats[s].nodes;
+    st[s].max_rho = fr->stats[s].max_rho;
+    st[s].min_rho = fr->stats[s].min_rho;
+    st[s].ave_rho = fr->stats[s].ave_rho;
+    for (c = 0; c < 3; c++) {
+      st[s].max_u[c] = fr->stats[s].max_u[c];
+      st[s].min_u[c] = fr->stats[s].min_u[c];
+      st[s].ave_u[c] = fr->stats[s].ave_u[c];
     }
-    lbh_frame_filename(fn, sizeof fn, "./out", "frames", r->dims, r->hp.LX, r->hp.LY,
-                       r->hp.LZ, -1, r->nsubs, s, ".dat");
-    o = fopen(fn, time == 0 ? "w" : "a");
-    if (!o) DIE("cannot write %s", fn);
-    if (time == 0)
-      fprintf(o, "# time frame fluid_nodes mass ave_u_x ave_u_y ave_u_z min_rho max_rho"
-                 " solute_mass nonfinite\n");
-    if (s == 0) {
-      const double nf = red.fluid_nodes > 0 ? (double)red.fluid_nodes : 1.0;
-      fprintf(o, "%d %d %lld %.17g %.10e %.10e %.10e %.17g %.17g %.17g %d\n", time, frame,
-              red.fluid_nodes, red.mass, red.u_sum[0] / nf, red.u_sum[1] / nf,
-              red.u_sum[2] / nf, red.rho_min, red.rho_max, red.solute_mass, red.nonfinite);
-    } else {
-      fprintf(o, "%d %d solute_mass %.17g\n", time, frame, red.solute_mass);
-    }
-    fclose(o);
+    if (st[s].ave_rho != st[s].ave_rho)
+      fprintf(stderr, "warning: subs %d holds non-finite densities at time %d\n", s, fr->time);
   }
-  printf("frame %d at time %d: mass %.12g, <ux> %.6e\n", frame, time, red.mass,
-         red.fluid_nodes ? red.u_sum[0] / (double)red.fluid_nodes : 0.0);
+  if (lbh_write_frame("./out", r->dims, r->nsubs, r->hp.LX, r->hp.LY, r->hp.LZ, fr->time, frame,
+                      r->prec, mv, st, r->mask, r->frame_files))
+    DIE("cannot write the files of frame %d in ./out", frame);
+  printf("frame %d (time %d): ave_rho = %.17g, ave_u = [ %g %g %g]\n", frame, fr->time,
+         st[0].ave_rho, st[0].ave_u[0], st[0].ave_u[1], st[0].ave_u[2]);
+}
+
+static unsigned parse_frame_files(const char* list)
+{
+  unsigned f = 0;
+  const char* p = list;
+  while (*p) {
+    size_t n = strcspn(p, ",");
+    if (n == 7 && !strncmp(p, "summary", 7)) f |= LBH_FRAME_SUMMARY;
+    else if (n == 3 && !strncmp(p, "raw", 3)) f |= LBH_FRAME_RAW;
+    else if (n == 3 && !strncmp(p, "dat", 3)) f |= LBH_FRAME_DAT;
+    else if (n == 3 && !strncmp(p, "txt", 3)) f |= LBH_FRAME_TXT;
+    else if (n == 3 && !strncmp(p, "all", 3)) f |= LBH_FRAME_ALL;
+    else if (n == 4 && !strncmp(p, "none", 4)) f |= 0;
+    else DIE("--frames takes a comma list of summary, raw, dat, txt, all, none");
+    p += n;
+    if (*p == ',') p++;
+  }
+  return f;
 }
 
 int main(int argc, char** argv)
@@ -112,6 +121,7 @@ int main(int argc, char** argv)
   const char* model = "shifted";
   const char* solid_rule = "device";
   int kahan = 0, walsh = 0;
+  const char* frames = "all";
   int device = 0, i, s, time, frame;
   double* ntab = NULL, *stab = NULL;
   int nlen = 0, slen = 0;
@@ -126,9 +136,11 @@ int main(int argc, char** argv)
     else if (!strcmp(argv[i], "--solid-rule") && i + 1 < argc) solid_rule = argv[++i];
     else if (!strcmp(argv[i], "--kahan")) kahan = 1;
     else if (!strcmp(argv[i], "--walsh")) walsh = 1;
+    else if (!strcmp(argv[i], "--frames") && i + 1 < argc) frames = argv[++i];
     else if (argv[i][0] != '-') name = argv[i];
     else DIE("unknown option %s", argv[i]);
   }
+  r.frame_files = parse_frame_files(frames);
   snprintf(dir, sizeof dir, name ? "./in_%s" : "./in", name);
   snprintf(path, sizeof path, "%s/params.in", dir);
   if (lbh_read_params(path, r.dims, r.nsubs, &r.hp, err, sizeof err)) DIE("%s", err);
@@ -230,35 +242,39 @@ int main(int argc, char** argv)
     free(b);
   }
   mkdir("./out", 0755);
-  r.mv = malloc((size_t)r.hp.NumNodes * (size_t)r.prec * (size_t)(1 + r.dims));
-  output_frame(&r, 0, 0);
-
-  /* the time loop of src/lbgpu_prime.cu:369-915: pairs of steps, frames at
-   * multiples of FrameRate, stop after the final frame */
   {
-    clock_t t0 = clock();
-    for (frame = 0, time = 1; time <= r.hp.NumTimeSteps; time++) {
-      int eof = (time % r.hp.FrameRate) == 0;
-      LBX(lbx_step(r.dom, time, eof ? LBX_WRITE_MV : 0));
-      if (eof) {
-        LBX(lbx_sync(r.dom));
-        output_frame(&r, time, ++frame);
-        if (frame == r.hp.NumFrames) break;
+    lbx_frame fr;
+    struct timespec t0, t1;
+    double secs;
+    LBX(lbx_frame_enqueue(r.dom, 0));
+    LBX(lbx_frame_wait(r.dom, &fr));
+    write_frame(&r, &fr, 0);
+    /* the time loop of src/lbgpu_prime.cu:369-915: NumFrames stretches of
+     * FrameRate steps, the last of each writing the macro variables.  Each
+     * frame is snapshotted on the device and copied to the host in the
+     * background; its files are written while the next stretch runs. */
+    clock_gettime(CLOCK_MONOTONIC, &t0);
+    for (frame = 1; frame <= r.hp.NumFrames; frame++) {
+      time = (frame - 1) * r.hp.FrameRate;
+      LBX(lbx_run(r.dom, time, r.hp.FrameRate, r.hp.FrameRate));
+      LBX(lbx_frame_enqueue(r.dom, time + r.hp.FrameRate));
+      if (frame > 1) {
+        LBX(lbx_frame_wait(r.dom, &fr));
+        write_frame(&r, &fr, frame - 1);
       }
-      time++;
-      eof = (time % r.hp.FrameRate) == 0;
-      LBX(lbx_step(r.dom, time, eof ? LBX_WRITE_MV : 0));
-      if (eof) {
-        LBX(lbx_sync(r.dom));
-        output_frame(&r, time, ++frame);
-      }
-      if (frame >= r.hp.NumFrames) break;
+    }
+    if (r.hp.NumFrames >= 1) {
+      LBX(lbx_frame_wait(r.dom, &fr));
+      write_frame(&r, &fr, r.hp.NumFrames);
     }
     LBX(lbx_sync(r.dom));
-    printf("ran %d steps of %lld nodes in %.3f s\n", time, r.hp.NumNodes,
-           (double)(clock() - t0) / CLOCKS_PER_SEC);
+    clock_gettime(CLOCK_MONOTONIC, &t1);
+    secs = (double)(t1.tv_sec - t0.tv_sec) + 1e-9 * (double)(t1.tv_nsec - t0.tv_nsec);
+    printf("ran %d steps of %lld nodes in %.3f s (%.1f MLUPS with frame output)\n",
+           r.hp.NumFrames * r.hp.FrameRate, r.hp.NumNodes, secs,
+           secs > 0 ? (double)r.hp.NumNodes * r.hp.NumFrames * r.hp.FrameRate / secs * 1e-6 : 0.);
   }
   LBX(lbx_destroy(r.dom));
-  free(r.mv); free(r.mask); free(ntab); free(stab);
+  free(r.mask); free(ntab); free(stab);
   return 0;
 }

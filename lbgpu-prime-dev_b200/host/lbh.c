@@ -6,6 +6,8 @@
 
 #include <ctype.h>
 #include <math.h>
+#include <pthread.h>
+#include <unistd.h>
 #include <stddef.h>
 #include <stdlib.h>
 #include <string.h>
@@ -289,20 +291,24 @@ int lbh_initial_rho(const lbh_params* p, int dims, int nsubs, int subs, double* 
 int lbh_write_dat(const char* path, const void* a, int real_size, long long N,
                   const uint8_t* mask)
 {
-  FILE* o = fopen(path, "wb");
+  const size_t bytes = (size_t)(N > 0 ? N : 1) * (size_t)real_size;
+  char* buf = (char*)malloc(bytes);
+  FILE* o;
   long long n;
-  if (!o) return -1;
-  for (n = 0; n < N; n++) {
-    if (real_size == 8) {
-      double v = mask[n] ? 0. : ((const double*)a)[n];
-      fwrite(&v, 8, 1, o);
-    } else {
-      float v = mask[n] ? 0.f : ((const float*)a)[n];
-      fwrite(&v, 4, 1, o);
-    }
+  int rc = 0;
+  if (!buf) return -1;
+  if (real_size == 8) {
+    double* v = (double*)buf;
+    for (n = 0; n < N; n++) v[n] = mask[n] ? 0. : ((const double*)a)[n];
+  } else {
+    float* v = (float*)buf;
+    for (n = 0; n < N; n++) v[n] = mask[n] ? 0.f : ((const float*)a)[n];
   }
-  fclose(o);
-  return 0;
+  if (!(o = fopen(path, "wb"))) { free(buf); return -1; }
+  if (N > 0 && fwrite(buf, (size_t)real_size, (size_t)N, o) != (size_t)N) rc = -1;
+  if (fclose(o)) rc = -1;
+  free(buf);
+  return rc;
 }
 
 void lbh_frame_filename(char* buf, int buflen, const char* outdir, const char* prefix,
@@ -316,6 +322,331 @@ void lbh_frame_filename(char* buf, int buflen, const char* outdir, const char* p
   if (frame >= 0) snprintf(fr, sizeof fr, "_frame%04d", frame); else fr[0] = '\0';
   if (nsubs == 1) sb[0] = '\0'; else snprintf(sb, sizeof sb, "_subs%02d", subs);
   snprintf(buf, (size_t)buflen, "%s/cuda_%s%s%s%s%s", outdir, prefix, size, fr, sb, suffix);
+}
+
+/* ---- per-frame files ---------------------------------------------------- */
+int lbh_write_frame_summary(const char* path, int time, int real_size,
+                            const lbh_frame_stats* st)
+{
+  FILE* o;
+  double r[4];
+  int c;
+  if (time == 0) {
+    static const char* cols[21] = {
+      "time", "|j|", "j_x", "j_y", "j_z", "min_u[x]", "min_u[y]", "min_u[z]",
+      "max_u[x]", "max_u[y]", "max_u[z]", "ave_u[x]", "ave_u[y]", "ave_u[z]",
+      "max/ave[x]", "max/ave[y]", "max/ave[z]", "min_rho", "max_rho", "ave_rho", "max/ave"};
+    if (!(o = fopen(path, "w+"))) return -1;
+    fprintf(o, "\n");
+    for (c = 0; c < 21; c++) fprintf(o, "%12s ", cols[c]);
+    fprintf(o, "\n");
+    for (c = 0; c < 21; c++) fprintf(o, "------------ ");
+    fprintf(o, "\n");
+    fclose(o);
+  }
+  if (!(o = fopen(path, "a+"))) return -1;
+  /* max / ave in the run's precision, +inf beyond 9999 */
+  for (c = 0; c < 4; c++) {
+    const double mx = c < 3 ? st->max_u[c] : st->max_rho;
+    const double av = c < 3 ? st->ave_u[c] : st->ave_rho;
+    double q;
+    if (real_size == 4) q = (float)av != 0.f ? (double)((float)mx / (float)av) : 1.;
+    else q = av != 0. ? mx / av : 1.;
+    r[c] = fabs(q) <= 9999. ? q : HUGE_VAL;
+  }
+#define LBH_R(x) (real_size == 4 ? (double)(float)(x) : (x))
+  fprintf(o,
+          "%12d "
+          "%12.7f %12.7f %12.7f %12.7f"
+          "%12.7f %12.7f %12.7f "
+          "%12.7f %12.7f %12.7f "
+          "%12.7f %12.7f %12.7f "
+          "%12.7f %12.7f %12.7f "
+          "%12.7f %12.7f %12.7f "
+          "%12.7f\n",
+          time, 0., 0., 0., 0.,
+          LBH_R(st->min_u[0]), LBH_R(st->min_u[1]), LBH_R(st->min_u[2]),
+          LBH_R(st->max_u[0]), LBH_R(st->max_u[1]), LBH_R(st->max_u[2]),
+          LBH_R(st->ave_u[0]), LBH_R(st->ave_u[1]), LBH_R(st->ave_u[2]),
+          r[0], r[1], r[2],
+          LBH_R(st->min_rho), LBH_R(st->max_rho), LBH_R(st->ave_rho), r[3]);
+#undef LBH_R
+  fclose(o);
+  return 0;
+}
+
+typedef struct {
+  const void* a;
+  int real_size, LX, LY;
+  long long r0, r1;      /* rows [r0, r1), row r = j + LY k */
+  char* buf;
+  size_t len, cap;
+  int fail;
+} txt_job;
+
+static void txt_put(txt_job* t, const char* s, size_t n)
+{
+  if (t->fail) return;
+  if (t->len + n > t->cap) {
+    size_t cap = t->cap ? t->cap : 4096;
+    char* b;
+    while (cap < t->len + n) cap *= 2;
+    if (!(b = (char*)realloc(t->buf, cap))) { t->fail = 1; return; }
+    t->buf = b; t->cap = cap;
+  }
+  memcpy(t->buf + t->len, s, n);
+  t->len += n;
+}
+
+static void* txt_rows(void* arg)
+{
+  txt_job* t = (txt_job*)arg;
+  char tmp[512];
+  long long r;
+  int i;
+  for (r = t->r0; r < t->r1; r++) {
+    const long long base = r * t->LX;
+    for (i = 0; i < t->LX; i++) {
+      double v = 0.;
+      int n;
+      if (t->a) v = t->real_size == 4 ? (double)((const float*)t->a)[base + i]
+                                      : ((const double*)t->a)[base + i];
+      n = snprintf(tmp, sizeof tmp, " %18.16f", v);
+      if (n < 0) { t->fail = 1; return NULL; }
+      if ((size_t)n < sizeof tmp) txt_put(t, tmp, (size_t)n);
+      else {   /* magnitudes beyond 1e490 do not occur in a lattice; format in full */
+        char* big = (char*)malloc((size_t)n + 1);
+        if (!big) { t->fail = 1; return NULL; }
+        snprintf(big, (size_t)n + 1, " %18.16f", v);
+        txt_put(t, big, (size_t)n);
+        free(big);
+      }
+    }
+    txt_put(t, "\n", 1);
+    if ((r + 1) % t->LY == 0) txt_put(t, "\n", 1);
+  }
+  return NULL;
+}
+
+int lbh_write_txt(const char* path, const void* a, int real_size, int LX, int LY, int LZ)
+{
+  const long long rows = (long long)LY * LZ;
+  long ncpu = sysconf(_SC_NPROCESSORS_ONLN);
+  int nt = (int)(ncpu > 0 ? (ncpu < 64 ? ncpu : 64) : 1), k, rc = 0;
+  txt_job* jobs;
+  pthread_t* th;
+  FILE* o;
+  if (rows < 1 || LX < 1) return -1;
+  if (nt > rows) nt = (int)rows;
+  jobs = (txt_job*)calloc((size_t)nt, sizeof *jobs);
+  th = (pthread_t*)calloc((size_t)nt, sizeof *th);
+  if (!jobs || !th) { free(jobs); free(th); return -1; }
+  for (k = 0; k < nt; k++) {
+    jobs[k].a = a; jobs[k].real_size = real_size; jobs[k].LX = LX; jobs[k].LY = LY;
+    jobs[k].r0 = rows * k / nt; jobs[k].r1 = rows * (k + 1) / nt;
+  }
+  for (k = 1; k < nt; k++)
+    if (pthread_create(&th[k], NULL, txt_rows, &jobs[k])) { jobs[k].fail = 2; txt_rows(&jobs[k]); }
+  txt_rows(&jobs[0]);
+  for (k = 1; k < nt; k++)
+    if (jobs[k].fail != 2) pthread_join(th[k], NULL);
+  o = fopen(path, "w+");
+  if (!o) rc = -1;
+  for (k = 0; k < nt; k++) {
+    if (jobs[k].fail == 1) rc = -1;
+    if (o && rc == 0 && jobs[k].len && fwrite(jobs[k].buf, 1, jobs[k].len, o) != jobs[k].len) rc = -1;
+    free(jobs[k].buf);
+  }
+  if (o && fclose(o)) rc = -1;
+  free(jobs); free(th);
+  return rc;
+}
+
+/* The reference stores (unsigned char)ROUND(x) with ROUND = floor; its
+ * build converts through a 32-bit integer and keeps the low byte, and a
+ * value outside the int range (or NaN) becomes INT_MIN, low byte 0. */
+static unsigned char raw_byte(double x)
+{
+  const double f = floor(x);
+  if (!(f >= -2147483648.0 && f <= 2147483647.0)) return 0;
+  return (unsigned char)((unsigned int)(int)f & 0xffu);
+}
+
+int lbh_write_raw_image(const char* path, const void* a, int real_size, long long N,
+                        const uint8_t* mask, double a_max, double a_min)
+{
+  unsigned char* px = (unsigned char*)malloc((size_t)(N > 0 ? N : 1));
+  long long n;
+  FILE* o;
+  int rc = 0;
+  if (!px) return -1;
+  for (n = 0; n < N; n++) {
+    if (mask[n]) { px[n] = 0; continue; }
+    if (real_size == 4) {
+      const float v = ((const float*)a)[n], lo = (float)a_min, hi = (float)a_max;
+      px[n] = raw_byte(1. + 254. * (v - lo) / (hi - lo));
+    } else {
+      const double v = ((const double*)a)[n];
+      px[n] = raw_byte(1. + 254. * (v - a_min) / (a_max - a_min));
+    }
+  }
+  if (!(o = fopen(path, "w"))) { free(px); return -1; }
+  if (N > 0 && fwrite(px, 1, (size_t)N, o) != (size_t)N) rc = -1;
+  if (fclose(o)) rc = -1;
+  free(px);
+  return rc;
+}
+
+int lbh_write_raw_u(const char* path, const void* ux, const void* uy, const void* uz,
+                    int real_size, int dims, long long N, const uint8_t* mask,
+                    const double max_u[3], const double min_u[3])
+{
+  unsigned char* px = (unsigned char*)malloc((size_t)(N > 0 ? N : 1));
+  long long n;
+  FILE* o;
+  int rc = 0;
+  if (!px) return -1;
+  if (real_size == 4) {
+    const float* x = (const float*)ux, *y = (const float*)uy, *z = (const float*)uz;
+    const float mx0 = (float)max_u[0], mx1 = (float)max_u[1], mx2 = (float)max_u[2];
+    const float mn0 = (float)min_u[0], mn1 = (float)min_u[1], mn2 = (float)min_u[2];
+    const float hi = (float)sqrt(mx0 * mx0 + mx1 * mx1 + mx2 * mx2);
+    const float lo = (float)sqrt(mn0 * mn0 + mn1 * mn1 + mn2 * mn2);
+    for (n = 0; n < N; n++) {
+      float m;
+      if (mask[n]) { px[n] = 0; continue; }
+      m = (float)sqrt(x[n] * x[n] + y[n] * y[n] + (dims == 2 ? 0.f : z[n] * z[n]));
+      px[n] = raw_byte(1. + 254. * (m - lo) / (hi - lo));
+    }
+  } else {
+    const double* x = (const double*)ux, *y = (const double*)uy, *z = (const double*)uz;
+    const double hi = sqrt(max_u[0] * max_u[0] + max_u[1] * max_u[1] + max_u[2] * max_u[2]);
+    const double lo = sqrt(min_u[0] * min_u[0] + min_u[1] * min_u[1] + min_u[2] * min_u[2]);
+    for (n = 0; n < N; n++) {
+      double m;
+      if (mask[n]) { px[n] = 0; continue; }
+      m = sqrt(x[n] * x[n] + y[n] * y[n] + (dims == 2 ? 0. : z[n] * z[n]));
+      px[n] = raw_byte(1. + 254. * (m - lo) / (hi - lo));
+    }
+  }
+  if (!(o = fopen(path, "w"))) { free(px); return -1; }
+  if (N > 0 && fwrite(px, 1, (size_t)N, o) != (size_t)N) rc = -1;
+  if (fclose(o)) rc = -1;
+  free(px);
+  return rc;
+}
+
+/* One file of a frame, for the worker pool of lbh_write_frame. */
+typedef struct {
+  int kind;                 /* 0 .dat, 1 byte image, 2 |u| byte image */
+  char path[1024];
+  const void* a[3];
+  double hi, lo;
+  const double* max_u;
+  const double* min_u;
+} frame_job;
+
+typedef struct {
+  frame_job* jobs;
+  int njobs, next, fail;
+  int real_size, dims;
+  long long N;
+  const uint8_t* mask;
+  pthread_mutex_t lock;
+} frame_pool;
+
+static void* frame_worker(void* arg)
+{
+  frame_pool* P = (frame_pool*)arg;
+  for (;;) {
+    int i, rc = 0;
+    frame_job* j;
+    pthread_mutex_lock(&P->lock);
+    i = P->next++;
+    pthread_mutex_unlock(&P->lock);
+    if (i >= P->njobs) return NULL;
+    j = &P->jobs[i];
+    if (j->kind == 0) rc = lbh_write_dat(j->path, j->a[0], P->real_size, P->N, P->mask);
+    else if (j->kind == 1)
+      rc = lbh_write_raw_image(j->path, j->a[0], P->real_size, P->N, P->mask, j->hi, j->lo);
+    else
+      rc = lbh_write_raw_u(j->path, j->a[0], j->a[1], j->a[2], P->real_size, P->dims, P->N,
+                           P->mask, j->max_u, j->min_u);
+    if (rc) {
+      pthread_mutex_lock(&P->lock);
+      P->fail = 1;
+      pthread_mutex_unlock(&P->lock);
+    }
+  }
+}
+
+int lbh_write_frame(const char* outdir, int dims, int nsubs, int LX, int LY, int LZ,
+                    int time, int frame, int real_size, const void* const* mv,
+                    const lbh_frame_stats* st, const uint8_t* mask, unsigned flags)
+{
+  const long long N = (long long)LX * LY * LZ;
+  const size_t plane = (size_t)N * (size_t)real_size;
+  char fn[1024];
+  int s, c, k, nt;
+  static const char* dat[4] = {"rho", "u_x", "u_y", "u_z"};
+  static const char* txt[4] = {"rho", "ux", "uy", "uz"};
+  frame_job jobs[2 * 9];
+  frame_pool P;
+  pthread_t th[18];
+  long ncpu = sysconf(_SC_NPROCESSORS_ONLN);
+  memset(&P, 0, sizeof P);
+  P.jobs = jobs; P.real_size = real_size; P.dims = dims; P.N = N; P.mask = mask;
+  for (s = 0; s < nsubs && s < 2; s++) {
+    const char* base = (const char*)mv[s];
+    if (flags & LBH_FRAME_SUMMARY) {
+      lbh_frame_filename(fn, sizeof fn, outdir, "frames", dims, LX, LY, LZ, -1, nsubs, s, ".dat");
+      if (lbh_write_frame_summary(fn, time, real_size, &st[s])) return -1;
+    }
+    if ((flags & LBH_FRAME_RAW) && dims == 3) {
+      frame_job* j = &jobs[P.njobs++];
+      memset(j, 0, sizeof *j);
+      j->kind = 1; j->a[0] = base; j->hi = st[s].max_rho; j->lo = st[s].min_rho;
+      lbh_frame_filename(j->path, sizeof j->path, outdir, "rho", dims, LX, LY, LZ, frame, nsubs, s, ".raw");
+      j = &jobs[P.njobs++];
+      memset(j, 0, sizeof *j);
+      j->kind = 2; j->a[0] = base + plane; j->a[1] = base + 2 * plane; j->a[2] = base + 3 * plane;
+      j->max_u = st[s].max_u; j->min_u = st[s].min_u;
+      lbh_frame_filename(j->path, sizeof j->path, outdir, "u", dims, LX, LY, LZ, frame, nsubs, s, ".raw");
+      for (c = 1; c <= 3; c++) {
+        j = &jobs[P.njobs++];
+        memset(j, 0, sizeof *j);
+        j->kind = 1; j->a[0] = base + c * plane; j->hi = st[s].max_u[c - 1]; j->lo = st[s].min_u[c - 1];
+        lbh_frame_filename(j->path, sizeof j->path, outdir, dat[c], dims, LX, LY, LZ, frame, nsubs, s, ".raw");
+      }
+    }
+    if (flags & LBH_FRAME_DAT)
+      for (c = 0; c <= dims; c++) {
+        frame_job* j = &jobs[P.njobs++];
+        memset(j, 0, sizeof *j);
+        j->kind = 0; j->a[0] = base + c * plane;
+        lbh_frame_filename(j->path, sizeof j->path, outdir, dat[c], dims, LX, LY, LZ, frame, nsubs, s, ".dat");
+      }
+  }
+  /* the binary files, one per worker at a time */
+  nt = (int)(ncpu > 1 ? ncpu : 1);
+  if (nt > P.njobs) nt = P.njobs;
+  pthread_mutex_init(&P.lock, NULL);
+  for (k = 1; k < nt; k++)
+    if (pthread_create(&th[k], NULL, frame_worker, &P)) { nt = k; break; }
+  if (P.njobs > 0) frame_worker(&P);
+  for (k = 1; k < nt; k++) pthread_join(th[k], NULL);
+  pthread_mutex_destroy(&P.lock);
+  if (P.fail) return -1;
+  /* the text dumps, each formatted on all cores */
+  if (flags & LBH_FRAME_TXT)
+    for (s = 0; s < nsubs; s++)
+      for (c = 0; c < 4; c++) {
+        lbh_frame_filename(fn, sizeof fn, outdir, txt[c], dims, LX, LY, LZ, frame, nsubs, s, ".txt");
+        if (lbh_write_txt(fn, c <= dims ? (const char*)mv[s] + c * plane : NULL, real_size, LX,
+                          LY, LZ))
+          return -1;
+      }
+  return 0;
 }
 
 int lbh_walsh_ns(double ns_value, int source, const uint8_t* mask, long long N,

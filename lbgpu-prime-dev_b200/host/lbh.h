@@ -92,6 +92,54 @@ int lbh_read_raw_mask(const char* path, long long N, uint8_t* out,
 enum { LBH_SOLID_DEVICE = 0, LBH_SOLID_NONZERO = 1 };
 long long lbh_apply_solid_rule(uint8_t* mask, long long N, int rule);
 
+/* ---- the reference's per-frame files (output_frame, src/lbio.c:37-131) ----
+ * Frame statistics of one substance as compute_{max,min,ave}_{u,rho}
+ * (src/compute.c:1159-1416) define them, over the nodes whose mask byte is
+ * 0 (is_not_solid, src/lattice.c:163-194).  The library's device reduction
+ * (lbx_frame_stats) fills the same fields. */
+typedef struct lbh_frame_stats {
+  long long nodes;
+  double max_rho, min_rho, ave_rho;
+  double max_u[3], min_u[3], ave_u[3];
+} lbh_frame_stats;
+
+/* Append one line to <outdir>/cuda_frames<size>[_subsNN].dat in the layout
+ * of dump_frame_summary (src/lbio.c:140-290): a new file with its header at
+ * time 0.  The flux columns are 0 (compute_flux has no body in the
+ * reference's build, src/compute.c:1418-1467); the max/ave ratios are
+ * formed in the run's precision (real_size 4 or 8).  Returns 0 or -1. */
+int lbh_write_frame_summary(const char* path, int time, int real_size,
+                            const lbh_frame_stats* st);
+
+/* rho / ux / uy / uz text dump (write_rho_txt, write_u_txt, src/lbio.c:
+ * 2864-2973): " %18.16f" per node, a newline per row, a blank line per
+ * plane, every node (no mask).  a = NULL writes zeros (u_z of a 2D run).
+ * Rows are formatted on all host cores.  Returns 0 or -1. */
+int lbh_write_txt(const char* path, const void* a, int real_size, int LX, int LY, int LZ);
+
+/* 3D byte images (write_raw and write_raw_u, src/lbio.c:934-1061): byte =
+ * floor(1 + 254 (a - a_min) / (a_max - a_min)) converted as the reference's
+ * build converts it, 0 where the mask byte is non-zero.  a_max / a_min are
+ * the frame statistics (max and min of |a|).  write_raw_u images |u| with
+ * the limits |(max_u)| and |(min_u)|.  Returns 0 or -1. */
+int lbh_write_raw_image(const char* path, const void* a, int real_size, long long N,
+                        const uint8_t* mask, double a_max, double a_min);
+int lbh_write_raw_u(const char* path, const void* ux, const void* uy, const void* uz,
+                    int real_size, int dims, long long N, const uint8_t* mask,
+                    const double max_u[3], const double min_u[3]);
+
+/* Every file output_frame writes for one frame into outdir: the summary
+ * line per substance, in 3D the byte images rho, u, u_x, u_y, u_z, the .dat
+ * files rho, u_x, u_y (u_z in 3D) and the text dumps rho, ux, uy, uz, under
+ * the reference's names (lbh_frame_filename).  mv[s] holds substance s's
+ * [1+D][N] reals, st[s] its statistics.  flags select the kinds (all four
+ * are the reference's default build).  Returns 0 or -1. */
+enum { LBH_FRAME_SUMMARY = 1, LBH_FRAME_RAW = 2, LBH_FRAME_DAT = 4, LBH_FRAME_TXT = 8,
+       LBH_FRAME_ALL = 15 };
+int lbh_write_frame(const char* outdir, int dims, int nsubs, int LX, int LY, int LZ,
+                    int time, int frame, int real_size, const void* const* mv,
+                    const lbh_frame_stats* st, const uint8_t* mask, unsigned flags);
+
 /* Walsh fraction field ns (N doubles) for a WALSH_NS_ON run.
  * LBH_NS_MASK: ns = the params.in value `ns` where the mask byte is 1, else
  *   0 (process_ns, src/latman.c:48-80: the field the reference's 2D runs

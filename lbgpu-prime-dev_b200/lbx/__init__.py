@@ -63,6 +63,22 @@ class _CGradient(C.Structure):
                 ("d_tau_s", C.c_double)]
 
 
+class _CFrameStats(C.Structure):
+    _fields_ = [("nodes", C.c_longlong), ("max_rho", C.c_double), ("min_rho", C.c_double),
+                ("ave_rho", C.c_double), ("max_u", C.c_double * 3), ("min_u", C.c_double * 3),
+                ("ave_u", C.c_double * 3)]
+
+    def as_dict(self) -> dict:
+        return dict(nodes=self.nodes, max_rho=self.max_rho, min_rho=self.min_rho,
+                    ave_rho=self.ave_rho, max_u=list(self.max_u), min_u=list(self.min_u),
+                    ave_u=list(self.ave_u))
+
+
+class _CFrame(C.Structure):
+    _fields_ = [("time", C.c_int), ("nsubs", C.c_int), ("mv", C.c_void_p * 2),
+                ("stats", _CFrameStats * 2)]
+
+
 class _CReductions(C.Structure):
     _fields_ = [
         ("mass", C.c_double), ("solute_mass", C.c_double),
@@ -88,6 +104,9 @@ _SIGNATURES = {
     "lbx_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
     "lbx_sync": (C.c_int, [C.c_void_p]),
     "lbx_reduce": (C.c_int, [C.c_void_p, C.POINTER(_CReductions)]),
+    "lbx_frame_stats_compute": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(_CFrameStats)]),
+    "lbx_frame_enqueue": (C.c_int, [C.c_void_p, C.c_int]),
+    "lbx_frame_wait": (C.c_int, [C.c_void_p, C.POINTER(_CFrame)]),
     "lbx_reduce_mv_static": (C.c_int, [C.c_void_p, C.c_void_p, C.c_longlong, C.c_int,
                                        C.c_int, C.c_int, C.c_void_p,
                                        C.POINTER(_CReductions)]),
@@ -303,6 +322,30 @@ class Domain:
                 ptrs.append(None)
             _check(_lib.lbx_download_mv(self._h, s, *ptrs))
         return out
+
+    def frame_stats(self, subs: int) -> dict:
+        """lbx_frame_stats_compute: the reference's frame statistics of one
+        substance (host mask rule, FP64)."""
+        st = _CFrameStats()
+        _check(_lib.lbx_frame_stats_compute(self._h, subs, C.byref(st)))
+        return st.as_dict()
+
+    def frame_enqueue(self, time: int):
+        _check(_lib.lbx_frame_enqueue(self._h, time))
+
+    def frame_wait(self, copy: bool = True) -> dict:
+        """lbx_frame_wait: the oldest queued frame.  Its macro variables are
+        copied out of the library's page-locked buffers, or with copy=False
+        returned as views of them, valid until the second frame_enqueue after
+        this call (the substances' blocks are adjacent in one buffer)."""
+        fr = _CFrame()
+        _check(_lib.lbx_frame_wait(self._h, C.byref(fr)))
+        p = self.p
+        n = fr.nsubs * (1 + p.dims) * p.NN
+        buf = (C.c_char * (n * np.dtype(p.dtype).itemsize)).from_address(fr.mv[0])
+        mv = np.frombuffer(buf, dtype=p.dtype, count=n).reshape(fr.nsubs, 1 + p.dims, p.NN)
+        return dict(time=fr.time, mv=mv.copy() if copy else mv,
+                    stats=[fr.stats[s].as_dict() for s in range(fr.nsubs)])
 
     def init_equilibrium(self, subs: int, rho, ux, uy, uz=None):
         p = self.p

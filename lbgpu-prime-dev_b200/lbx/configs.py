@@ -45,6 +45,15 @@ cfg4: 512 independent D3Q19 samples, FP32 shifted, cubic edges drawn from
       aggregate MLUPS of FUSED, PERSISTENT and SEQUENTIAL runs, the mode the
       autotuner picks, and the per-sample permeabilities.
 
+frames: the cfg2 lattice (FP32) with the reference's per-frame output every
+      --frame-rate steps (summary line, 3D byte images and .dat files; the
+      text dumps with --frame-files all) written to a scratch directory.
+      Reports the MLUPS without frames, with the reference's pattern (wait
+      for the frame step, copy the macro variables to pageable host memory,
+      statistics, files; the GPU idles meanwhile) and with the asynchronous
+      pipeline (lbx_frame_enqueue / lbx_frame_wait: the files of frame k are
+      written while the steps after it run).
+
 Each run prints one JSON line.  Times come from CUDA events on the stream
 the kernels run on.
 """
@@ -433,15 +442,87 @@ def run_cfg4(nsamples: int = 512, steps: int = 200, perm_steps: int = 0) -> list
     return out
 
 
+def run_frames(steps: int = 2000, frame_rate: int = 200, n: int = 256,
+               files: str = "summary,raw,dat") -> list:
+    import os
+    import shutil
+    import tempfile
+    import time
+
+    from . import host
+
+    kinds = {"summary": host.FRAME_SUMMARY, "raw": host.FRAME_RAW, "dat": host.FRAME_DAT,
+             "txt": host.FRAME_TXT, "all": host.FRAME_ALL}
+    flags = 0
+    for k in files.split(","):
+        flags |= kinds[k]
+    p, mask = cfg2_params(4, n=n)
+    out = []
+    nframes = steps // frame_rate
+    work = tempfile.mkdtemp(prefix="lbx_frames_")
+    try:
+        for mode in ("none", "sync", "async"):
+            with Domain(p, mask) as dom:
+                dom.init_equilibrium(0, np.ones(p.NN), np.zeros(p.NN), np.zeros(p.NN),
+                                     np.zeros(p.NN))
+                dom.run(0, 2 * frame_rate, frame_rate)      # warm-up (graphs, allocations)
+                dom.frame_enqueue(0)
+                dom.frame_wait()
+                dom.sync()
+                t0 = 2 * frame_rate
+                outdir = os.path.join(work, mode)
+                os.makedirs(outdir)
+                w0 = time.perf_counter()
+                if mode == "none":
+                    dom.run(t0, nframes * frame_rate, 0)
+                    dom.sync()
+                elif mode == "sync":
+                    for k in range(1, nframes + 1):
+                        dom.run(t0 + (k - 1) * frame_rate, frame_rate, frame_rate)
+                        dom.sync()
+                        mv = dom.download_mv()
+                        st = [dom.frame_stats(s) for s in range(p.nsubs)]
+                        host.write_frame(outdir, 3, p.LX, p.LY, p.LZ, t0 + k * frame_rate, k,
+                                         mv, st, mask, flags)
+                else:
+                    for k in range(1, nframes + 1):
+                        dom.run(t0 + (k - 1) * frame_rate, frame_rate, frame_rate)
+                        dom.frame_enqueue(t0 + k * frame_rate)
+                        if k > 1:
+                            fr = dom.frame_wait(copy=False)
+                            host.write_frame(outdir, 3, p.LX, p.LY, p.LZ, fr["time"], k - 1,
+                                             fr["mv"], fr["stats"], mask, flags)
+                    fr = dom.frame_wait(copy=False)
+                    host.write_frame(outdir, 3, p.LX, p.LY, p.LZ, fr["time"], nframes,
+                                     fr["mv"], fr["stats"], mask, flags)
+                    dom.sync()
+                wall = time.perf_counter() - w0
+                nbytes = sum(os.path.getsize(os.path.join(outdir, f)) for f in os.listdir(outdir))
+                shutil.rmtree(outdir)
+            out.append(dict(run="frames", mode=mode, edge=n, steps=nframes * frame_rate,
+                            frame_rate=frame_rate, frames=0 if mode == "none" else nframes,
+                            files=files, wall_s=round(wall, 4),
+                            mlups=round(p.NN * nframes * frame_rate / wall / 1e6, 1),
+                            bytes_per_frame=0 if mode == "none" else nbytes // nframes))
+    finally:
+        shutil.rmtree(work, ignore_errors=True)
+    base = out[0]["wall_s"]
+    for o in out[1:]:
+        o["overhead_ms_per_frame"] = round((o["wall_s"] - base) / o["frames"] * 1e3, 2)
+    return out
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
-    ap.add_argument("config", choices=["cfg1", "cfg2", "cfg3", "cfg4", "cfg5"])
+    ap.add_argument("config", choices=["cfg1", "cfg2", "cfg3", "cfg4", "cfg5", "frames"])
     ap.add_argument("--steps", type=int, default=None)
     ap.add_argument("--edge", type=int, default=256)
     ap.add_argument("--samples", type=int, default=512)
     ap.add_argument("--perm-steps", type=int, default=0)
     ap.add_argument("--checkpoint-every", type=int, default=100)
     ap.add_argument("--fd-dirs", type=int, default=2)
+    ap.add_argument("--frame-rate", type=int, default=200)
+    ap.add_argument("--frame-files", default="summary,raw,dat")
     a = ap.parse_args(argv)
     if a.config == "cfg1":
         print(json.dumps(run_cfg1(a.steps or 2000)))
@@ -451,6 +532,9 @@ def main(argv=None) -> int:
             print(json.dumps(line))
     elif a.config == "cfg3":
         for line in run_cfg3(a.steps or 20000):
+            print(json.dumps(line))
+    elif a.config == "frames":
+        for line in run_frames(a.steps or 2000, a.frame_rate, a.edge, a.frame_files):
             print(json.dumps(line))
     elif a.config == "cfg4":
         for line in run_cfg4(a.samples, a.steps or 200, a.perm_steps):

@@ -90,10 +90,33 @@ def load():
                                         C.c_void_p]
         lib.lbh_apply_solid_rule.argtypes = [C.c_void_p, C.c_longlong, C.c_int]
         lib.lbh_apply_solid_rule.restype = C.c_longlong
+        lib.lbh_write_frame.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_int,
+                                        C.c_int, C.c_int, C.c_int, C.c_int,
+                                        C.POINTER(C.c_void_p), C.POINTER(FrameStats),
+                                        C.c_void_p, C.c_uint]
         lib.lbh_walsh_ns.argtypes = [C.c_double, C.c_int, C.c_void_p, C.c_longlong,
                                      C.c_char_p, C.c_void_p, C.c_char_p, C.c_int]
         _lib = lib
     return _lib
+
+
+class FrameStats(C.Structure):
+    """Mirror of lbh_frame_stats (and of the ABI's lbx_frame_stats)."""
+    _fields_ = [("nodes", C.c_longlong), ("max_rho", C.c_double), ("min_rho", C.c_double),
+                ("ave_rho", C.c_double), ("max_u", C.c_double * 3), ("min_u", C.c_double * 3),
+                ("ave_u", C.c_double * 3)]
+
+    @classmethod
+    def from_dict(cls, d):
+        st = cls()
+        st.nodes = d["nodes"]
+        st.max_rho, st.min_rho, st.ave_rho = d["max_rho"], d["min_rho"], d["ave_rho"]
+        for c in range(3):
+            st.max_u[c], st.min_u[c], st.ave_u[c] = d["max_u"][c], d["min_u"][c], d["ave_u"][c]
+        return st
+
+
+FRAME_SUMMARY, FRAME_RAW, FRAME_DAT, FRAME_TXT, FRAME_ALL = 1, 2, 4, 8, 15
 
 
 class HostError(RuntimeError):
@@ -150,6 +173,22 @@ def walsh_ns(ns_value: float, source: int, mask: np.ndarray = None, N: int = Non
                            N, path.encode(), out.ctypes.data, err, 512):
         raise HostError(err.value.decode())
     return out
+
+
+def write_frame(outdir: str, dims: int, LX: int, LY: int, LZ: int, time: int, frame: int,
+                mv: np.ndarray, stats, mask: np.ndarray, flags: int = FRAME_ALL):
+    """lbh_write_frame: every per-frame file of the reference for the macro
+    variables mv ([nsubs][1+D][N], float32 or float64) with their statistics
+    (FrameStats or dicts, one per substance)."""
+    mv = np.ascontiguousarray(mv)
+    nsubs = mv.shape[0]
+    m = np.ascontiguousarray(mask, dtype=np.uint8).reshape(-1)
+    ptrs = (C.c_void_p * nsubs)(*[mv[s].ctypes.data for s in range(nsubs)])
+    st = (FrameStats * nsubs)(*[x if isinstance(x, FrameStats) else FrameStats.from_dict(x)
+                                for x in stats])
+    if load().lbh_write_frame(outdir.encode(), dims, nsubs, LX, LY, LZ, time, frame,
+                              mv.dtype.itemsize, ptrs, st, m.ctypes.data, flags):
+        raise HostError("cannot write the frame files in " + outdir)
 
 
 def write_bmp_mask(path: str, LX: int, LY: int, mask: np.ndarray):

@@ -362,3 +362,52 @@ def reference_read_raw(path: str, LX: int, LY: int, LZ: int):
     out = np.zeros(LX * LY * LZ, np.uint8)
     lib.refk_read_raw(path.encode(), LX, LY, LZ, out.ctypes.data_as(C.c_void_p))
     return out
+
+
+def frame_stats(mv_s: np.ndarray, mask: np.ndarray, dims: int) -> dict:
+    """The frame statistics of compute_{max,min,ave}_{u,rho}
+    (src/compute.c:1159-1416) for one substance's macro variables mv_s
+    ([1+D][N]) over the nodes whose mask byte is 0 (is_not_solid,
+    src/lattice.c:163-194): max and min of |rho| and |u_c| (a NaN never
+    replaces a running max or min), and the means of rho and u_c; u_z = 0 in
+    2D.  The sums are FP64."""
+    keep = np.asarray(mask).reshape(-1) == 0
+    nn = int(np.count_nonzero(keep))
+
+    def one(v):
+        v = np.asarray(v, dtype=np.float64)[keep]
+        a = np.abs(v)
+        ok = a[~np.isnan(a)]
+        mx = max(0.0, float(ok.max())) if ok.size else 0.0
+        mn = min(mx, float(ok.min())) if ok.size else mx
+        return mx, mn, (float(np.sum(v)) / nn if nn else 0.0)
+
+    r = one(mv_s[0])
+    us = [one(mv_s[1 + c]) if c < dims else (0.0, 0.0, 0.0) for c in range(3)]
+    return dict(nodes=nn, max_rho=r[0], min_rho=r[1], ave_rho=r[2],
+                max_u=[u[0] for u in us], min_u=[u[1] for u in us],
+                ave_u=[u[2] for u in us])
+
+
+def reference_output_frame(variant: str, LX: int, LY: int, LZ: int, mv: np.ndarray,
+                           sol: np.ndarray, time: int, frame: int, frame_rate: int,
+                           workdir: str) -> bool:
+    """The reference's output_frame (src/lbio.c:37-131) on macro variables
+    mv ([nsubs][1+D][N] in the variant's precision) and mask bytes sol,
+    writing into workdir/out.  False without the harness."""
+    if not reference_available(variant):
+        return False
+    if variant not in _refs:
+        _refs[variant] = C.CDLL(os.path.join(REF_DIR, "librefk_%s.so" % variant))
+    lib = _refs[variant]
+    mv = np.ascontiguousarray(mv)
+    sol = np.ascontiguousarray(sol, dtype=np.uint8)
+    os.makedirs(os.path.join(workdir, "out"), exist_ok=True)
+    here = os.getcwd()
+    try:
+        os.chdir(workdir)
+        lib.refk_output_frame(LX, LY, LZ, mv.ctypes.data_as(C.c_void_p),
+                              sol.ctypes.data_as(C.c_void_p), time, frame, frame_rate)
+    finally:
+        os.chdir(here)
+    return True

@@ -97,6 +97,7 @@ int cumul_stride[20];
 #include "params.h"
 #include "process.c"
 #include "lbio.c"
+#include "compute.c"
 #include "system_boundary_kernels.c"
 #include "k_stream_collide_stream.c"
 #include "k_collide.c"
@@ -403,5 +404,41 @@ EXPORT int refk_read_raw(const char* path, int LX, int LY, int LZ, unsigned char
   read_solids(l, (char*)path);
   memcpy(out, l->solids_memblock, (size_t)(LX * LY * LZ));
   free(l->solids_memblock); free(l);
+  return 0;
+}
+
+/* ---- the reference's frame output --------------------------------------------
+ * output_frame (src/lbio.c:37-131): the frame statistics of src/compute.c:
+ * 1159-1467, dump_frame_summary (src/lbio.c:140-290), dump_macro_vars (3D
+ * .raw images and .dat files, src/lbio.c:300-420, src/lattice.c:1737-1900)
+ * and write_{rho,u}_txt (src/lbio.c:2864-2973), run on a harness lattice
+ * holding the macro variables mv ([subs][1+D][N], real) and the mask bytes
+ * sol.  Files go to ./out of the current directory (get_out_path). */
+EXPORT int refk_output_frame(int LX, int LY, int LZ, const real* mv, const unsigned char* sol,
+                             int time, int frame, int frame_rate)
+{
+  struct lattice_struct* l = harness_lattice(LX, LY, LZ);
+  const int D = NUM_DIMENSIONS, NN = LX * LY * LZ;
+  int s, c;
+  l->NumDims = D;
+  l->NumSubs = NUM_FLUID_COMPONENTS;
+  l->param.FrameRate = frame_rate > 0 ? frame_rate : 1;
+  memcpy(l->solids_memblock, sol, (size_t)NN);
+  l->vars = (struct vars_struct*)calloc(NUM_FLUID_COMPONENTS, sizeof *l->vars);
+  for (s = 0; s < NUM_FLUID_COMPONENTS; s++) {
+    l->vars[s].macrovars_memblock = (real*)malloc((size_t)NN * (1 + D) * sizeof(real));
+    memcpy(l->vars[s].macrovars_memblock, mv + (size_t)s * (1 + D) * NN,
+           (size_t)NN * (1 + D) * sizeof(real));
+    l->vars[s].macrovars1d = (real**)malloc((1 + D) * sizeof(real*));
+    for (c = 0; c <= D; c++) l->vars[s].macrovars1d[c] = l->vars[s].macrovars_memblock + (size_t)c * NN;
+  }
+  l->time = time;
+  l->frame = frame;
+  output_frame(l);
+  for (s = 0; s < NUM_FLUID_COMPONENTS; s++) {
+    free(l->vars[s].macrovars1d);
+    free(l->vars[s].macrovars_memblock);
+  }
+  free(l->vars); free(l->solids_memblock); free(l);
   return 0;
 }

@@ -27,7 +27,7 @@ TOL = {8: 1e-12, 4: 1e-5}
 
 
 def run_driver(tmp, args):
-    r = subprocess.run([DRIVER] + args, cwd=tmp, capture_output=True, text=True, timeout=300)
+    r = subprocess.run([DRIVER] + args, cwd=tmp, capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stdout + r.stderr
     return r
 
@@ -86,8 +86,8 @@ def test_gpu_driver_2d_pressure_faces(tmp_path):
                            pressure_n_out=(1, 0))
     check_frame(tmp, mv, mask, 2, 3, 8)
     frames, = glob.glob(os.path.join(tmp, "out", "cuda_frames*.dat"))
-    lines = [ln for ln in open(frames) if not ln.startswith("#")]
-    assert [int(ln.split()[0]) for ln in lines] == [0, 10, 20, 30]
+    rows = [ln.split() for ln in open(frames) if ln.split() and ln.split()[0].isdigit()]
+    assert [int(r[0]) for r in rows] == [0, 10, 20, 30]
 
 
 @pytest.mark.parametrize("prec", [8, 4])
@@ -125,3 +125,84 @@ def test_gpu_driver_2d_walsh_mask_rule(tmp_path):
     hp = host.read_params(os.path.join(tmp, "in", "params.in"), 2, 1)
     mv = oracle_last_frame(hp, 2, 8, mask, 30, 10, walsh=1, ns=np.where(mask == 1, 0.6, 0.0))
     check_frame(tmp, mv, mask, 2, 3, 8)
+
+
+def oracle_frames(hp, dims, prec, mask, nframes, fr, **kw):
+    """The oracle's macro variables at frames 0..nframes, starting from the
+    driver's initial state (solid nodes keep their initial values, as on
+    the device)."""
+    rv = (lambda x: x.f) if prec == 4 else (lambda x: x.d)
+    p = po.Params(dims=dims, LX=hp.LX, LY=hp.LY, LZ=hp.LZ,
+                  tau=(rv(hp.tau[0]), rv(hp.tau[1])), rho_A=(rv(hp.rho_A[0]), rv(hp.rho_A[1])),
+                  gaccel=tuple(rv(hp.gforce[s][c]) for s in range(2) for c in range(3)),
+                  rho_in=rv(hp.rho_in), rho_out=rv(hp.rho_out),
+                  bc_ramp_start=hp.bc_ramp_start, bc_ramp_stop=hp.bc_ramp_stop, **kw)
+    dtype = np.float32 if prec == 4 else np.float64
+    rho = host.initial_rho(hp, dims, 1, 0).astype(dtype)
+    z = np.zeros(p.NN)
+    f = po.init_feq(p, rho.astype(np.float64)[None], z[None], z[None], z[None], dtype=dtype)
+    mv = np.zeros((1, 1 + dims, p.NN), dtype=dtype)
+    mv[0, 0] = rho
+    out = [mv.copy()]
+    for k in range(nframes):
+        f, mv = po.run_oracle(p, f, mask, k * fr, fr, fr, mv=mv)
+        out.append(mv.copy())
+    return out
+
+
+@pytest.mark.parametrize("dims,prec", [(3, 8), (2, 4)])
+def test_gpu_driver_frame_files_match_reference_output_frame(tmp_path, dims, prec):
+    """Every file the driver writes per frame against the reference's own
+    output_frame (built by the harness) fed with the oracle's macro variables
+    at the same frames: the same file names; .dat and .txt values within the
+    parity bar; byte images within one level (a value on a rounding edge);
+    summary columns to the printed 7 decimals (FP32 means within the
+    reference's float running sums)."""
+    variant = ("d3q19" if dims == 3 else "d2q9") + ("_f64" if prec == 8 else "_f32")
+    if not po.reference_available(variant):
+        pytest.skip("reference harness not built")
+    tmp = str(tmp_path / "run")
+    os.makedirs(os.path.join(tmp, "in"))
+    LX, LY, LZ = (12, 10, 8) if dims == 3 else (20, 14, 1)
+    N = LX * LY * LZ
+    write_params(os.path.join(tmp, "in", "params.in"),
+                 dict(BASE, LX=LX, LY=LY, LZ=LZ, NumFrames=3, FrameRate=6,
+                      **{"gforce[0][0]": 3e-5, "gforce[0][1]": -1e-5}))
+    rng = np.random.default_rng(51)
+    mask = rng.choice([0, 1, 255], size=N, p=[0.75, 0.2, 0.05]).astype(np.uint8)
+    if dims == 3:
+        host.write_raw_mask(os.path.join(tmp, "in", "%dx%dx%d.raw" % (LX, LY, LZ)), mask)
+    else:
+        mask = np.where(mask == 255, 0, mask).astype(np.uint8)   # a BMP holds 0/1 only
+        host.write_bmp_mask(os.path.join(tmp, "in", "%dx%d.bmp" % (LX, LY)), LX, LY, mask)
+    run_driver(tmp, ["--dims", str(dims), "--precision", str(prec)])
+    hp = host.read_params(os.path.join(tmp, "in", "params.in"), dims, 1)
+    ref = str(tmp_path / "ref")
+    for k, mv in enumerate(oracle_frames(hp, dims, prec, mask, 3, 6)):
+        assert po.reference_output_frame(variant, LX, LY, LZ, mv, mask, 6 * k, k, 6, ref)
+    names = sorted(os.listdir(os.path.join(ref, "out")))
+    assert names == sorted(os.listdir(os.path.join(tmp, "out")))
+    dtype = np.float32 if prec == 4 else np.float64
+    tol = TOL[prec]
+    for name in names:
+        a_path, b_path = os.path.join(ref, "out", name), os.path.join(tmp, "out", name)
+        if name.endswith(".raw"):
+            a = np.fromfile(a_path, np.uint8).astype(int)
+            b = np.fromfile(b_path, np.uint8).astype(int)
+            d = np.minimum(np.abs(a - b), 256 - np.abs(a - b))
+            assert d.max() <= 1 and np.mean(d != 0) < 0.02, name
+        elif "_frames" in name:
+            ra = [ln.split() for ln in open(a_path) if ln.split() and ln.split()[0].isdigit()]
+            rb = [ln.split() for ln in open(b_path) if ln.split() and ln.split()[0].isdigit()]
+            assert len(ra) == len(rb) == 4
+            for x, y in zip(ra, rb):
+                for kk, (u, v) in enumerate(zip(x, y)):
+                    u, v = float(u), float(v)
+                    slack = 1e-5 * abs(u) if kk in (14, 15, 16, 20) else 2e-7
+                    assert abs(u - v) <= slack + (1e-6 if prec == 4 else 0.0), (name, kk, u, v)
+        elif name.endswith(".dat"):
+            assert rel_err(np.fromfile(b_path, dtype), np.fromfile(a_path, dtype)) <= tol, name
+        else:
+            a = np.array(open(a_path).read().split(), dtype=np.float64)
+            b = np.array(open(b_path).read().split(), dtype=np.float64)
+            assert rel_err(b, a) <= tol, name
