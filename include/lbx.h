@@ -248,6 +248,19 @@ typedef struct lbx_frame {
 lbx_status lbx_frame_enqueue(lbx_domain* d, int time);
 lbx_status lbx_frame_wait(lbx_domain* d, lbx_frame* out);
 
+/* PEST point sampling (PEST_OUTPUT_ON, src/latman.c:899-1232): `count`
+ * samples in time order (time[k] non-decreasing, node[k] = y*LX + x as the
+ * reference indexes them).  A step whose time is the next untaken sample's
+ * writes the macro variables and stores, for every sample due then, the
+ * solute's C and the flow's u_x and u_y at its node on the device.  As in
+ * the reference a sample whose time never comes (earlier than the run, or
+ * already passed) leaves it and every later sample untaken.  Needs
+ * nsubs = 2 (the reference reads the solute).  count = 0 clears. */
+lbx_status lbx_pest_set(lbx_domain* d, int count, const int* time, const int* node);
+/* The samples so far (arrays of `count`; NaN where not taken) and the
+ * number taken.  Synchronous. */
+lbx_status lbx_pest_read(lbx_domain* d, double* conc, double* ux, double* uy, int* taken);
+
 /* Device pointers to the populations ([nsubs][Q][N], the dense exchange
  * format; with the compact layout this first writes the current state into
  * it, and the pointer is valid until the next step) and macro variables

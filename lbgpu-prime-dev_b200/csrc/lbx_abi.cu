@@ -449,6 +449,7 @@ void release(lbx_domain* d)
   cudaFree(d->ubuf); cudaFree(d->prof_t); cudaFree(d->prof_b); cudaFree(d->ns);
   lbx_internal_adjoint_free(d);
   lbx_internal_frames_free(d);
+  lbx_internal_pest_free(d);
   if (d->own_stream) cudaStreamDestroy(d->own_stream);
 }
 
@@ -466,10 +467,14 @@ lbx_status do_step(lbx_domain* d, int t, unsigned flags)
   if (((t % 2) != 0) != (want_odd != 0))
     return fail(LBX_ERR_STATE, "step at time %d out of AA order: expected an %s time", t,
                 want_odd ? "odd" : "even");
+  // a due PEST sample needs the macro variables of this step
+  const bool pest = lbx_internal_pest_due(d, t);
+  if (pest) flags |= LBX_WRITE_MV;
   lbx_status st = d->real_size == 8 ? step_t<double>(d, t, flags) : step_t<float>(d, t, flags);
   if (st == LBX_OK) {
     d->parity ^= 1;
     if (d->layout == LBX_LAYOUT_COMPACT) d->dense_stale = true;
+    if (pest) st = lbx_internal_pest_after(d, t);
   }
   return st;
 }
@@ -836,6 +841,7 @@ lbx_status lbx_run(lbx_domain* d, int t0, int nsteps, int frame_rate)
       int pairs = 0;
       for (int u = t; u + 1 <= tend; u += 2) {
         if (frame_rate > 0 && (u % frame_rate == 0 || (u + 1) % frame_rate == 0)) break;
+        if (lbx_internal_pest_due(d, u) || lbx_internal_pest_due(d, u + 1)) break;
         if (pairs > 0 && (step_key(d, u, k) != ko || std::memcmp(k, k_odd, ko) ||
                           step_key(d, u + 1, k) != ke || std::memcmp(k, k_even, ke)))
           break;

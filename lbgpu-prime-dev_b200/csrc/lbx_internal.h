@@ -48,6 +48,7 @@ struct lbx_domain {
   void* fout = nullptr;        // set only while recomputing states (OOP step)
   void* adj = nullptr;         // adjoint checkpoints and objective (lbx_adjoint.cu)
   void* frames = nullptr;      // frame statistics and snapshots (lbx_frames.cu)
+  void* pest = nullptr;        // PEST point samples (lbx_pest.cu)
   int parity = 0;             // 0: natural order (next step odd); 1: swapped
   long long launches = 0;
   // graph replay of frame-free, time-invariant runs: one captured AA pair
@@ -63,3 +64,8 @@ LBX_HIDDEN lbx_status lbx_internal_fail(lbx_status code, const char* msg);
 LBX_HIDDEN lbx_status lbx_internal_step_into(lbx_domain* d, int t, void* src, void* dst);
 LBX_HIDDEN void lbx_internal_adjoint_free(lbx_domain* d);
 LBX_HIDDEN void lbx_internal_frames_free(lbx_domain* d);
+// PEST sampling: whether a sample is due at time t (the step then writes
+// the macro variables), the gather after that step, and the release.
+LBX_HIDDEN bool lbx_internal_pest_due(const lbx_domain* d, int t);
+LBX_HIDDEN lbx_status lbx_internal_pest_after(lbx_domain* d, int t);
+LBX_HIDDEN void lbx_internal_pest_free(lbx_domain* d);

@@ -16,7 +16,10 @@
  * (summary), in 3D the byte images cuda_{rho,u,u_x,u_y,u_z}<size>_frameNNNN.raw
  * (raw), cuda_{rho,u_x,u_y[,u_z]}<size>_frameNNNN.dat (dat) and the text dumps
  * cuda_{rho,ux,uy,uz}<size>_frameNNNN.txt (txt); --frames selects the kinds
- * (default all, as the reference's build writes).
+ * (default all, as the reference's build writes).  With
+ * ./in/{timestep,x_coord,y_coord}_file.in present (and two substances) the
+ * PEST point samples are taken and written at the end to
+ * ./out/{conc_data,vel_data,conc_order}_proc0000.dat.
  *
  * The build-time flags of the reference (NUM_DIMENSIONS, NUM_FLUID_COMPONENTS,
  * DP_ON, ACCURATE/COMPRESSIBLE, KAHAN_SUMMATION, WALSH_NS_ON with
@@ -121,6 +124,8 @@ int main(int argc, char** argv)
   const char* model = "shifted";
   const char* solid_rule = "device";
   int kahan = 0, walsh = 0;
+  int pest_n = -1, pest_kept = 0;
+  int *pest_order = NULL, *pest_time = NULL, *pest_node = NULL;
   const char* frames = "all";
   int device = 0, i, s, time, frame;
   double* ntab = NULL, *stab = NULL;
@@ -207,6 +212,22 @@ int main(int argc, char** argv)
     p.pressure_s_table = stab; p.pressure_s_len = slen;
   }
   LBX(lbx_create(&p, r.mask, &r.dom));
+  /* PEST point samples (PEST_OUTPUT_ON): on when ./in/timestep_file.in exists */
+  pest_n = lbh_pest_count("./in");
+  if (pest_n >= 0 && r.nsubs != 2) {
+    fprintf(stderr, "warning: PEST samples read the solute; a one-substance run skips them\n");
+    pest_n = -1;
+  }
+  if (pest_n >= 0) {
+    pest_order = (int*)malloc((size_t)(pest_n + 1) * sizeof(int));
+    pest_time = (int*)malloc((size_t)(pest_n + 1) * sizeof(int));
+    pest_node = (int*)malloc((size_t)(pest_n + 1) * sizeof(int));
+    pest_kept = lbh_read_pest("./in", r.hp.LX, r.hp.LY, pest_n, pest_order, pest_time,
+                              pest_node, err, sizeof err);
+    if (pest_kept < 0) DIE("%s", err);
+    LBX(lbx_pest_set(r.dom, pest_kept, pest_time, pest_node));
+    printf("PEST: %d samples read, %d in the lattice\n", pest_n, pest_kept);
+  }
   if (walsh) {
     double* ns = (double*)malloc((size_t)r.hp.NumNodes * sizeof(double));
     const int src = r.dims == 3 && r.hp.ns_flag == 1 ? LBH_NS_FILE : LBH_NS_MASK;
@@ -273,6 +294,19 @@ int main(int argc, char** argv)
     printf("ran %d steps of %lld nodes in %.3f s (%.1f MLUPS with frame output)\n",
            r.hp.NumFrames * r.hp.FrameRate, r.hp.NumNodes, secs,
            secs > 0 ? (double)r.hp.NumNodes * r.hp.NumFrames * r.hp.FrameRate / secs * 1e-6 : 0.);
+  }
+  if (pest_n >= 0) {
+    double* v = (double*)malloc((size_t)(3 * pest_kept + 3) * sizeof(double));
+    int taken = 0;
+    LBX(lbx_pest_read(r.dom, v, v + pest_kept, v + 2 * pest_kept, &taken));
+    if (lbh_write_pest("./out", pest_kept, v, v + pest_kept, v + 2 * pest_kept, pest_order,
+                       r.prec))
+      DIE("cannot write the PEST files in ./out");
+    if (taken < pest_kept)
+      fprintf(stderr, "warning: %d of %d PEST samples were not reached\n", pest_kept - taken,
+              pest_kept);
+    free(v);
+    free(pest_order); free(pest_time); free(pest_node);
   }
   LBX(lbx_destroy(r.dom));
   free(r.mask); free(ntab); free(stab);

@@ -649,6 +649,107 @@ int lbh_write_frame(const char* outdir, int dims, int nsubs, int LX, int LY, int
   return 0;
 }
 
+/* ---- PEST samples ----------------------------------------------------------- */
+static FILE* pest_open(const char* dir, const char* name)
+{
+  char path[1024];
+  snprintf(path, sizeof path, "%s/%s", dir, name);
+  return fopen(path, "r");
+}
+
+int lbh_pest_count(const char* dir)
+{
+  FILE* in = pest_open(dir, "timestep_file.in");
+  int v, count = 0, r;
+  if (!in) return -1;
+  r = fscanf(in, "%d", &v);
+  while (!feof(in)) {
+    if (r != 1) { fclose(in); return -1; }   /* a non-integer: the reference loops forever */
+    count++;
+    r = fscanf(in, "%d", &v);
+  }
+  fclose(in);
+  return count;
+}
+
+static int pest_ints(const char* dir, const char* name, int count, int* out, char* err,
+                     int errlen)
+{
+  FILE* in = pest_open(dir, name);
+  int k;
+  if (!in) { snprintf(err, (size_t)errlen, "cannot open %s/%s", dir, name); return -1; }
+  for (k = 0; k < count; k++)
+    if (fscanf(in, "%d", &out[k]) != 1) {
+      fclose(in);
+      snprintf(err, (size_t)errlen, "%s/%s holds fewer than %d integers", dir, name, count);
+      return -1;
+    }
+  fclose(in);
+  return 0;
+}
+
+int lbh_read_pest(const char* dir, int LX, int LY, int count, int* order, int* time,
+                  int* node, char* err, int errlen)
+{
+  int* t = (int*)malloc((size_t)(count > 0 ? count : 1) * sizeof(int));
+  int* x = (int*)malloc((size_t)(count > 0 ? count : 1) * sizeof(int));
+  int* y = (int*)malloc((size_t)(count > 0 ? count : 1) * sizeof(int));
+  int k, kept = -1;
+  if (!t || !x || !y) { snprintf(err, (size_t)errlen, "out of host memory"); goto done; }
+  if (pest_ints(dir, "timestep_file.in", count, t, err, errlen)) goto done;
+  for (k = 1; k < count; k++)
+    if (t[k] < t[k - 1]) {
+      snprintf(err, (size_t)errlen, "PEST sample times not in order (sample %d)", k);
+      goto done;
+    }
+  if (pest_ints(dir, "x_coord_file.in", count, x, err, errlen)) goto done;
+  if (pest_ints(dir, "y_coord_file.in", count, y, err, errlen)) goto done;
+  kept = 0;
+  for (k = 0; k < count; k++) {
+    if (y[k] < 0 || y[k] > LY - 1 || x[k] < 0 || x[k] > LX - 1) continue;
+    order[kept] = k;
+    time[kept] = t[k];
+    node[kept] = y[k] * LX + x[k];
+    kept++;
+  }
+done:
+  free(t); free(x); free(y);
+  return kept;
+}
+
+int lbh_write_pest(const char* outdir, int count, const double* conc, const double* ux,
+                   const double* uy, const int* order, int real_size)
+{
+  char path[1024];
+  FILE* o;
+  int k;
+  snprintf(path, sizeof path, "%s/conc_data_proc%04d.dat", outdir, 0);
+  if (!(o = fopen(path, "w+"))) return -1;
+  for (k = 0; k < count; k++) fprintf(o, "%20.17f\n", conc[k] == conc[k] ? conc[k] : 0.);
+  fclose(o);
+  snprintf(path, sizeof path, "%s/vel_data_proc%04d.dat", outdir, 0);
+  if (!(o = fopen(path, "w+"))) return -1;
+  for (k = 0; k < count; k++) {
+    double v = 0.;
+    if (ux[k] == ux[k] && uy[k] == uy[k]) {
+      if (real_size == 4) {
+        const float fx = (float)ux[k], fy = (float)uy[k];
+        const float s2 = fx * fx + fy * fy;
+        v = sqrt((double)s2);
+      } else {
+        v = sqrt(ux[k] * ux[k] + uy[k] * uy[k]);
+      }
+    }
+    fprintf(o, "%20.17f\n", v);
+  }
+  fclose(o);
+  snprintf(path, sizeof path, "%s/conc_order_proc%04d.dat", outdir, 0);
+  if (!(o = fopen(path, "w+"))) return -1;
+  for (k = 0; k < count; k++) fprintf(o, "%d\n", order[k]);
+  fclose(o);
+  return 0;
+}
+
 int lbh_walsh_ns(double ns_value, int source, const uint8_t* mask, long long N,
                  const char* path, double* ns, char* err, int errlen)
 {

@@ -140,6 +140,28 @@ int lbh_write_frame(const char* outdir, int dims, int nsubs, int LX, int LY, int
                     int time, int frame, int real_size, const void* const* mv,
                     const lbh_frame_stats* st, const uint8_t* mask, unsigned flags);
 
+/* PEST inputs (read_PEST_in_files, src/latman.c:899-1046):
+ * <dir>/timestep_file.in, x_coord_file.in and y_coord_file.in, integers.
+ * lbh_pest_count gives the number of samples by the reference's rule (a
+ * value counts when a read is attempted before end-of-file was seen, so a
+ * last value with no newline after it is not counted); -1 when the file is
+ * missing or holds a non-integer.  lbh_read_pest reads `count` samples,
+ * keeps those with 0 <= x < LX and 0 <= y < LY in file order, and returns
+ * how many: order[k] (the sample's index in the files), time[k] and
+ * node[k] = y*LX + x; -1 with a message for a missing file, too few values
+ * or times that decrease (the reference exits there). */
+int lbh_pest_count(const char* dir);
+int lbh_read_pest(const char* dir, int LX, int LY, int count, int* order, int* time,
+                  int* node, char* err, int errlen);
+
+/* PEST outputs (write_PEST_out_file, src/latman.c:1178-1232):
+ * <outdir>/conc_data_proc0000.dat and vel_data_proc0000.dat ("%20.17f" per
+ * line) and conc_order_proc0000.dat ("%d").  vel = sqrt(u_x^2 + u_y^2)
+ * formed in the run's precision (real_size) as the reference forms it;
+ * samples not taken (NaN) are written as 0.  Returns 0 or -1. */
+int lbh_write_pest(const char* outdir, int count, const double* conc, const double* ux,
+                   const double* uy, const int* order, int real_size);
+
 /* Walsh fraction field ns (N doubles) for a WALSH_NS_ON run.
  * LBH_NS_MASK: ns = the params.in value `ns` where the mask byte is 1, else
  *   0 (process_ns, src/latman.c:48-80: the field the reference's 2D runs

@@ -105,6 +105,9 @@ _SIGNATURES = {
     "lbx_sync": (C.c_int, [C.c_void_p]),
     "lbx_reduce": (C.c_int, [C.c_void_p, C.POINTER(_CReductions)]),
     "lbx_frame_stats_compute": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(_CFrameStats)]),
+    "lbx_pest_set": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
+    "lbx_pest_read": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                C.POINTER(C.c_int)]),
     "lbx_frame_enqueue": (C.c_int, [C.c_void_p, C.c_int]),
     "lbx_frame_wait": (C.c_int, [C.c_void_p, C.POINTER(_CFrame)]),
     "lbx_reduce_mv_static": (C.c_int, [C.c_void_p, C.c_void_p, C.c_longlong, C.c_int,
@@ -329,6 +332,22 @@ class Domain:
         st = _CFrameStats()
         _check(_lib.lbx_frame_stats_compute(self._h, subs, C.byref(st)))
         return st.as_dict()
+
+    def pest_set(self, times, nodes):
+        """lbx_pest_set: PEST samples (time-ordered) at dense node indices."""
+        t = np.ascontiguousarray(times, dtype=np.int32)
+        n = np.ascontiguousarray(nodes, dtype=np.int32)
+        assert t.size == n.size
+        _check(_lib.lbx_pest_set(self._h, int(t.size), t.ctypes.data, n.ctypes.data))
+        self._pest_n = int(t.size)
+
+    def pest_read(self) -> dict:
+        """lbx_pest_read: C, u_x, u_y per sample (NaN where not taken)."""
+        n = getattr(self, "_pest_n", 0)
+        a = [np.zeros(max(n, 1)) for _ in range(3)]
+        taken = C.c_int()
+        _check(_lib.lbx_pest_read(self._h, *[x.ctypes.data for x in a], C.byref(taken)))
+        return dict(conc=a[0][:n], ux=a[1][:n], uy=a[2][:n], taken=taken.value)
 
     def frame_enqueue(self, time: int):
         _check(_lib.lbx_frame_enqueue(self._h, time))

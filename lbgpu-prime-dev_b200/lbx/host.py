@@ -94,6 +94,11 @@ def load():
                                         C.c_int, C.c_int, C.c_int, C.c_int,
                                         C.POINTER(C.c_void_p), C.POINTER(FrameStats),
                                         C.c_void_p, C.c_uint]
+        lib.lbh_pest_count.argtypes = [C.c_char_p]
+        lib.lbh_read_pest.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_void_p,
+                                      C.c_void_p, C.c_void_p, C.c_char_p, C.c_int]
+        lib.lbh_write_pest.argtypes = [C.c_char_p, C.c_int, C.c_void_p, C.c_void_p,
+                                       C.c_void_p, C.c_void_p, C.c_int]
         lib.lbh_walsh_ns.argtypes = [C.c_double, C.c_int, C.c_void_p, C.c_longlong,
                                      C.c_char_p, C.c_void_p, C.c_char_p, C.c_int]
         _lib = lib
@@ -189,6 +194,34 @@ def write_frame(outdir: str, dims: int, LX: int, LY: int, LZ: int, time: int, fr
     if load().lbh_write_frame(outdir.encode(), dims, nsubs, LX, LY, LZ, time, frame,
                               mv.dtype.itemsize, ptrs, st, m.ctypes.data, flags):
         raise HostError("cannot write the frame files in " + outdir)
+
+
+def pest_count(dir_: str) -> int:
+    """lbh_pest_count: samples in dir/timestep_file.in (-1: none)."""
+    return int(load().lbh_pest_count(dir_.encode()))
+
+
+def read_pest(dir_: str, LX: int, LY: int):
+    """lbh_read_pest: (order, time, node) of the kept samples."""
+    n = pest_count(dir_)
+    if n < 0:
+        raise HostError("no PEST sample times in " + dir_)
+    a = [np.zeros(max(n, 1), np.int32) for _ in range(3)]
+    err = C.create_string_buffer(512)
+    kept = load().lbh_read_pest(dir_.encode(), LX, LY, n, a[0].ctypes.data, a[1].ctypes.data,
+                                a[2].ctypes.data, err, 512)
+    if kept < 0:
+        raise HostError(err.value.decode())
+    return tuple(x[:kept] for x in a)
+
+
+def write_pest(outdir: str, conc, ux, uy, order, real_size: int):
+    """lbh_write_pest: the three PEST output files."""
+    arrs = [np.ascontiguousarray(x, dtype=np.float64) for x in (conc, ux, uy)]
+    o = np.ascontiguousarray(order, dtype=np.int32)
+    if load().lbh_write_pest(outdir.encode(), len(o), *[x.ctypes.data for x in arrs],
+                             o.ctypes.data, real_size):
+        raise HostError("cannot write the PEST files in " + outdir)
 
 
 def write_bmp_mask(path: str, LX: int, LY: int, mask: np.ndarray):

@@ -631,12 +631,14 @@ static void apply_bcs3(const ctx_t* c, real_t* f, const uint8_t* sol, int t,
   }
 }
 
+/* t0 even: f in natural order; t0 odd: f as the odd step at t0 left it
+ * (swapped slots), so a run may stop after any step and continue. */
 int SFX(orc_run)(const orc_params* p, REAL* f, const uint8_t* solids,
                  REAL* mv, int t0, int nsteps, int frame_rate, int nthreads)
 {
   ctx_t c;
   int t;
-  if (t0 % 2 != 0 || p->LX < 1 || p->LY < 1 || p->LZ < 1) return -1;
+  if (t0 < 0 || p->LX < 1 || p->LY < 1 || p->LZ < 1) return -1;
   if (p->dims == 2 && p->LZ != 1) return -1;
   make_ctx(&c, p);
   for (t = t0 + 1; t <= t0 + nsteps; t++) {

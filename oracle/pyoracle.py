@@ -411,3 +411,77 @@ def reference_output_frame(variant: str, LX: int, LY: int, LZ: int, mv: np.ndarr
     finally:
         os.chdir(here)
     return True
+
+
+def reference_pest(variant: str, p: Params, f: np.ndarray, solids: np.ndarray, t0: int,
+                   nsteps: int, workdir: str, frame_rate: int = 0,
+                   mv: Optional[np.ndarray] = None):
+    """The reference's PEST point sampling (src/latman.c:899-1232) around its
+    own kernels: reads workdir/in/{timestep,x_coord,y_coord}_file.in, runs
+    the steps, writes workdir/out/{conc_data,vel_data,conc_order}_proc0000.dat.
+    Returns (f, mv, kept samples), or None without the harness variant."""
+    if not reference_available(variant):
+        return None
+    if variant not in _refs:
+        run_reference(variant, p, f.copy(), solids, t0, 0)     # loads the library
+    lib = _refs[variant]
+    os.makedirs(os.path.join(workdir, "out"), exist_ok=True)
+    here = os.getcwd()
+    try:
+        os.chdir(workdir)
+        kept = lib.refk_pest_begin(p.LX, p.LY, p.LZ)
+        if kept < 0:
+            raise ValueError("PEST input files missing in " + workdir)
+        f, mv = run_reference(variant, p, f, solids, t0, nsteps, frame_rate, mv)
+        lib.refk_pest_end()
+    finally:
+        os.chdir(here)
+    return f, mv, kept
+
+
+def pest_samples(p: Params, f: np.ndarray, solids: np.ndarray, t0: int, nsteps: int,
+                 times, nodes, mv: Optional[np.ndarray] = None):
+    """PEST point sampling restated (src/latman.c:1048-1176): samples in
+    order; at each step t, while the next sample's time is t, take the
+    solute's C and the flow's u_x, u_y at its node (written by that step).
+    A sample whose time never comes blocks the ones after it, as in the
+    reference.  Returns (f, mv, C, ux, uy, taken) with NaN for samples not
+    taken."""
+    times = list(times)
+    nodes = list(nodes)
+    n = len(times)
+    c = np.full(n, np.nan)
+    ux = np.full(n, np.nan)
+    uy = np.full(n, np.nan)
+    k = 0
+    for t in range(t0 + 1, t0 + nsteps + 1):
+        f, mv = run_oracle(p, f, solids, t - 1, 1, 1, mv=mv)
+        while k < n and times[k] == t:
+            c[k] = mv[1, 0, nodes[k]]
+            ux[k] = mv[0, 1, nodes[k]]
+            uy[k] = mv[0, 2, nodes[k]]
+            k += 1
+    return f, mv, c, ux, uy, k
+
+
+def reference_pest_inputs(variant: str, LX: int, LY: int, LZ: int, workdir: str):
+    """The reference's read_PEST_in_files on workdir/in: (order, time, x, y)
+    of the kept samples, or None without the harness variant."""
+    if not reference_available(variant):
+        return None
+    if variant not in _refs:
+        _refs[variant] = C.CDLL(os.path.join(REF_DIR, "librefk_%s.so" % variant))
+    lib = _refs[variant]
+    here = os.getcwd()
+    try:
+        os.chdir(workdir)
+        kept = lib.refk_pest_begin(LX, LY, LZ)
+        if kept < 0:
+            return None
+        arrs = [np.zeros(max(kept, 1), np.int32) for _ in range(4)]
+        lib.refk_pest_samples(*[a.ctypes.data_as(C.c_void_p) for a in arrs])
+        os.makedirs("out", exist_ok=True)
+        lib.refk_pest_end()
+    finally:
+        os.chdir(here)
+    return tuple(a[:kept] for a in arrs)

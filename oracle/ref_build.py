@@ -34,8 +34,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_ref")
 DEFAULT_SRC = "/root/reference/src"
 
-# name -> flags.h overrides.  PEST output is always off: with it on and no
-# PEST input files the reference dereferences a never-allocated buffer.
+# name -> flags.h overrides.  PEST output is off except in the *_pest
+# variants: with it on and no PEST input files the reference dereferences a
+# never-allocated buffer.
 VARIANTS = {
     "d2q9_f64": dict(NUM_DIMENSIONS=2, NUM_FLUID_COMPONENTS=1, DP_ON=1),
     "d2q9_f32": dict(NUM_DIMENSIONS=2, NUM_FLUID_COMPONENTS=1, DP_ON=0),
@@ -71,6 +72,11 @@ VARIANTS = {
                       COMPUTE_ON_SOLIDS=1, WALSH_NS_ON=1),
     "d3q19sw_f64": dict(NUM_DIMENSIONS=3, NUM_FLUID_COMPONENTS=2, DP_ON=1,
                         COMPUTE_ON_SOLIDS=1, WALSH_NS_ON=1),
+    # PEST point sampling on (the tests supply its input files)
+    "d2q9s_pest_f64": dict(NUM_DIMENSIONS=2, NUM_FLUID_COMPONENTS=2, DP_ON=1,
+                           PEST_OUTPUT_ON=1),
+    "d3q19s_pest_f32": dict(NUM_DIMENSIONS=3, NUM_FLUID_COMPONENTS=2, DP_ON=0,
+                            PEST_OUTPUT_ON=1),
 }
 
 def variant_flags(src: str, overrides: dict) -> str:

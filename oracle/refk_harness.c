@@ -98,6 +98,21 @@ int cumul_stride[20];
 #include "process.c"
 #include "lbio.c"
 #include "compute.c"
+#if PEST_OUTPUT_ON
+/* PEST point sampling lives in src/latman.c, whose other functions set up
+ * the device; their CUDA calls compile to no-ops here (never run), and a
+ * copy to a __constant__ symbol becomes a copy to the host global. */
+#define cudaMalloc(p, n) 0
+#define cudaFree(p) 0
+#define cudaFreeHost(p) 0
+#define cudaMemcpyToSymbol(sym, src, n, ...) (memcpy(&(sym), (src), (n)), 0)
+#define cudaMemcpyFromSymbol(dst, sym, n, ...) (memcpy((dst), &(sym), (n)), 0)
+/* globals of src/lbgpu_prime.cu:17-24 that src/latman.c names */
+int f_mem_size, mv_mem_size, solids_mem_size;
+real *f_mem_d, *mv_mem_d, *ns_mem_d;
+unsigned char* solids_mem_d;
+#include "latman.c"
+#endif
 #include "system_boundary_kernels.c"
 #include "k_stream_collide_stream.c"
 #include "k_collide.c"
@@ -328,6 +343,11 @@ EXPORT void refk_set_ns(real* ns) { g_ns = ns; }
 
 EXPORT int refk_walsh(void) { return WALSH_NS_ON ? 1 : 0; }
 
+#if PEST_OUTPUT_ON
+/* The lattice of an open PEST sampling (refk_pest_begin .. refk_pest_end). */
+static struct lattice_struct* g_pest;
+#endif
+
 EXPORT int refk_run(const refk_params* p, real* f, const unsigned char* solids,
                     real* mv, int t0, int nsteps, int frame_rate)
 {
@@ -339,6 +359,10 @@ EXPORT int refk_run(const refk_params* p, real* f, const unsigned char* solids,
 #if INAMURO_SIGMA_COMPONENT
     time_c = t;
 #endif
+#if PEST_OUTPUT_ON
+    /* before and after each kernel, src/lbgpu_prime.cu:515, :532, :739, :754 */
+    if (g_pest) { g_pest->time = t; PEST_gpu_switch(&g_pest, mv, 0, NULL); }
+#endif
     if (NUM_DIMENSIONS == 2) bcs(p, t, !(t % 2 == 1), f, sol);
     is_end_of_frame_mem_c = (frame_rate > 0 && t % frame_rate == 0);
     if (t % 2 == 1)
@@ -346,9 +370,81 @@ EXPORT int refk_run(const refk_params* p, real* f, const unsigned char* solids,
     else
       launch_grid(k_collide, p->LX, p->LY, p->LZ, f, mv, sol);
     is_end_of_frame_mem_c = 0;
+#if PEST_OUTPUT_ON
+    if (g_pest) write_PEST_out_data(&g_pest, mv, 0, NULL);
+#endif
   }
   return 0;
 }
+
+EXPORT int refk_pest(void) { return PEST_OUTPUT_ON ? 1 : 0; }
+
+#if PEST_OUTPUT_ON
+/* read_PEST_in_files (src/latman.c:899-1046) on ./in of the current
+ * directory, for a lattice of the given extents whose macro variables the
+ * sampling copies into; refk_run then samples as the reference's main does,
+ * and refk_pest_end writes ./out/{conc_data,vel_data,conc_order}_proc0000.dat
+ * (write_PEST_out_file, src/latman.c:1178-1232).  One entry past the kept
+ * samples is set to time -1: the reference's sampling loop reads the entry
+ * after the last kept sample, which holds stale data there.  Returns the
+ * number of kept samples, or -1 when an input file is missing. */
+EXPORT int refk_pest_begin(int LX, int LY, int LZ)
+{
+  struct lattice_struct* l = (struct lattice_struct*)calloc(1, sizeof *l);
+  int s, c;
+  const int D = NUM_DIMENSIONS, NN = LX * LY * LZ;
+  l->param.LX = LX; l->param.LY = LY; l->param.LZ = LZ;
+  l->NumNodes = NN;
+  l->NumDims = D;
+  l->NumSubs = NUM_FLUID_COMPONENTS;
+  l->process.id = 0; l->process.num_procs = 1;
+  l->vars = (struct vars_struct*)calloc(NUM_FLUID_COMPONENTS, sizeof *l->vars);
+  for (s = 0; s < NUM_FLUID_COMPONENTS; s++) {
+    l->vars[s].macrovars_memblock = (real*)calloc((size_t)NN * (1 + D), sizeof(real));
+    l->vars[s].macrovars1d = (real**)malloc((1 + D) * sizeof(real*));
+    for (c = 0; c <= D; c++) l->vars[s].macrovars1d[c] = l->vars[s].macrovars_memblock + (size_t)c * NN;
+  }
+  read_PEST_in_files(&l, 0, NULL);
+  if (!l->concentration_data) return -1;
+  l->concentration_data = (struct conc_data_struct*)realloc(
+      l->concentration_data, (size_t)(l->conc_array_size + 1) * sizeof *l->concentration_data);
+  memset(&l->concentration_data[l->conc_array_size], 0, sizeof *l->concentration_data);
+  l->concentration_data[l->conc_array_size].timestep = -1;
+  g_pest = l;
+  return l->conc_array_size;
+}
+
+/* The kept samples of the open sampling: original index, time, x, y. */
+EXPORT int refk_pest_samples(int* order, int* time, int* x, int* y)
+{
+  int k;
+  if (!g_pest) return -1;
+  for (k = 0; k < g_pest->conc_array_size; k++) {
+    order[k] = g_pest->concentration_data[k].countervar;
+    time[k] = g_pest->concentration_data[k].timestep;
+    x[k] = g_pest->concentration_data[k].x_coord;
+    y[k] = g_pest->concentration_data[k].y_coord;
+  }
+  return g_pest->conc_array_size;
+}
+
+EXPORT int refk_pest_end(void)
+{
+  struct lattice_struct* l = g_pest;
+  int s;
+  if (!l) return -1;
+  write_PEST_out_file(&l, 0, NULL);
+  for (s = 0; s < NUM_FLUID_COMPONENTS; s++) {
+    free(l->vars[s].macrovars1d);
+    free(l->vars[s].macrovars_memblock);
+  }
+  free(l->vars);
+  free(l->concentration_data);
+  free(l);
+  g_pest = NULL;
+  return 0;
+}
+#endif
 
 /* ---- host-side input readers of the reference ------------------------------
  * read_params (src/params.h:40-660), spy_bmp (src/lbio.c:3073-3363) and

@@ -86,7 +86,16 @@ def test_oracle_conserves_mass_periodic():
     assert abs(f[0][:, sol != 1].sum() - m0) < 1e-12
 
 
-def test_oracle_rejects_odd_start():
-    p = po.Params(dims=3, LX=4, LY=4, LZ=4)
+def test_oracle_continues_from_an_odd_time():
+    """A run stopped after an odd step continues from the swapped state:
+    5 + 3 steps equal 8 steps bit for bit; a negative start is rejected."""
+    p = po.Params(dims=3, LX=6, LY=5, LZ=4, gaccel=(1e-4, 0, 0, 0, 0, 0))
+    rng = np.random.default_rng(2)
+    f0 = rng.standard_normal((1, 19, p.NN)) * 1e-3
+    sol = (rng.random(p.NN) < 0.2).astype(np.uint8)
+    fa, mva = po.run_oracle(p, f0.copy(), sol, 0, 8, 1)
+    fb, mvb = po.run_oracle(p, f0.copy(), sol, 0, 5, 1)
+    fb, mvb = po.run_oracle(p, fb, sol, 5, 3, 1, mv=mvb)
+    assert np.array_equal(fa, fb) and np.array_equal(mva, mvb)
     with pytest.raises(ValueError):
-        po.run_oracle(p, np.zeros((1, 19, 64)), np.zeros(64, np.uint8), 1, 2)
+        po.run_oracle(p, f0.copy(), sol, -1, 2)
