@@ -298,11 +298,6 @@ FaceOps<T> face3_table(const lbx_domain* d, int t)
   return ops;
 }
 
-int count_faces3(const lbx_domain* d)
-{
-  return (d->faces3_active && face3_table<double>(d, 1).n > 0) ? 1 : 0;
-}
-
 template <typename T>
 void launch_faces3(lbx_domain* d, int t, bool second)
 {
@@ -320,20 +315,6 @@ void launch_faces3(lbx_domain* d, int t, bool second)
     face_plane<T, false><<<grid, block, 0, d->stream>>>(f, d->solids, nullptr, p.LX, p.LY, p.LZ,
                                                          stride, second ? 1 : 0, ops);
   d->launches++;
-}
-
-// Kernels one step launches (faces, the step, the breakthrough reduction).
-long long launches_per_step(const lbx_domain* d, bool solute_on)
-{
-  long long n = 1 + (d->p.nsubs == 2 && solute_on ? 1 : 0) + count_faces3(d);
-  if (d->faces_active && !d->faces_fused) {
-    for (int s = 0; s < d->p.nsubs; ++s)
-      n += (d->p.pressure_n_in[s] != 0) + (d->p.pressure_n_out[s] != 0) +
-           (d->p.pressure_s_in[s] != 0) + (d->p.pressure_s_out[s] != 0);
-    if (d->p.nsubs == 2) n += (d->p.zeroconcgrad_n != 0) + (d->p.zeroconcgrad_s != 0);
-  }
-  if (d->btc_vals) n += 1;
-  return n;
 }
 
 template <typename T>
@@ -558,6 +539,7 @@ lbx_status replay_pairs(lbx_domain* d, int t, int pairs)
     if (st == LBX_OK)
       st = d->real_size == 8 ? step_t<double>(d, t + 1, 0) : step_t<float>(d, t + 1, 0);
     cudaError_t e = cudaStreamEndCapture(d->stream, &g);
+    d->graph_launches = d->launches - before;
     d->launches = before;
     if (st != LBX_OK) { if (g) cudaGraphDestroy(g); return st; }
     if (e != cudaSuccess) return fail(LBX_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
@@ -569,8 +551,7 @@ lbx_status replay_pairs(lbx_domain* d, int t, int pairs)
     d->graph_key_len = klen;
   }
   // the graph holds every kernel of both steps (faces and records included)
-  auto on = [&](int tt) { return tt >= d->p.sigma_t_on && tt <= d->p.sigma_t_off; };
-  const long long per_pair = launches_per_step(d, on(t)) + launches_per_step(d, on(t + 1));
+  const long long per_pair = d->graph_launches;
   for (int r = 0; r < pairs; ++r) {
     CK(cudaGraphLaunch(d->graph, d->stream));
     d->launches += per_pair;

@@ -56,6 +56,7 @@ struct lbx_domain {
   cudaStream_t graph_stream = nullptr;   // stream the pair was captured on
   unsigned char graph_key[2 * 640];      // keys of the odd and the even step
   size_t graph_key_len = 0;
+  long long graph_launches = 0;          // kernels one replay of the graph runs
 };
 
 // Hidden helpers of the library's translation units (not exported).

@@ -487,15 +487,15 @@ constexpr int compact_min_blocks()
 // bits (Q * P < 2^32), so slot selects and address arithmetic stay 32-bit.
 // OOP: write the step's result to C.s.fout instead of in place (used to
 // recompute stored forward states for the adjoint).
+// The update of fluid node m (compact index) by one block thread; the
+// odd step's slot table is indexed by threadIdx.x, so a block's threads
+// handle distinct nodes.
 template <typename T, int Q, int NS, int MODEL, bool ODD, int PART, bool IDX32, bool OOP>
-__global__ void __launch_bounds__(256, (compact_min_blocks<T, PART>()))
-aa_step_compact(CompactArgs<T> C)
+__device__ __forceinline__ void compact_node(const CompactArgs<T>& C, const int m)
 {
   using Idx = typename std::conditional<IDX32, unsigned, size_t>::type;
   constexpr int D = (Q == 9) ? 2 : 3;
   const StepArgs<T>& A = C.s;
-  const int m = blockIdx.x * blockDim.x + threadIdx.x;
-  if (m >= C.F) return;
   const Idx F = (Idx)C.P;   // plane stride
   const int LX = A.LX, LY = A.LY;
   const int plane = LX * LY;
@@ -600,6 +600,15 @@ aa_step_compact(CompactArgs<T> C)
       for (int a = 0; a < Q; ++a) fo[a * F + m2] = d[a];
     }
   }
+}
+
+template <typename T, int Q, int NS, int MODEL, bool ODD, int PART, bool IDX32, bool OOP>
+__global__ void __launch_bounds__(256, (compact_min_blocks<T, PART>()))
+aa_step_compact(CompactArgs<T> C)
+{
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= C.F) return;
+  compact_node<T, Q, NS, MODEL, ODD, PART, IDX32, OOP>(C, m);
 }
 
 // Dense <-> compact exchange of all substances' populations.
