@@ -99,6 +99,14 @@ typedef struct lbx_params {
                                every node is updated and streaming ignores
                                the solids.  Dense layout; no face
                                boundaries, batches or adjoint runs.        */
+  /* Zou-He velocity on the z faces (3D; the reference's CPU rule,
+   * src/bcs.c:764-862): the unknowns of the top (k = LZ-1) or bottom (k = 0)
+   * plane from rho = (known sums) / (1 +- u_z) and J = rho u_z with zero
+   * tangential velocity; u_z = uz_in on the *_in faces, uz_out on the *_out
+   * faces (|u_z| < 1).  Ordered after the pressure faces of the same face
+   * and substance (the last configured operation on a face decides). */
+  int velocity_t_in[2], velocity_t_out[2], velocity_b_in[2], velocity_b_out[2];
+  double uz_in, uz_out;
 } lbx_params;
 
 /* Device storage of the populations.  DENSE keeps the reference's

@@ -11,6 +11,7 @@
 #include "lbx_internal.h"
 #include "lbx_kernels.cuh"
 
+#include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
@@ -271,6 +272,10 @@ void for_each_face3(const lbx_domain* d, int t, F&& run)
     if (p.pressure_t_out[s]) run(1, FACE_PRESSURE, s, dr(false));
     if (p.pressure_b_in[s]) run(0, FACE_PRESSURE, s, dr(true));
     if (p.pressure_b_out[s]) run(0, FACE_PRESSURE, s, dr(false));
+    if (p.velocity_t_in[s]) run(1, FACE_VELOCITY, s, (T)p.uz_in);
+    if (p.velocity_t_out[s]) run(1, FACE_VELOCITY, s, (T)p.uz_out);
+    if (p.velocity_b_in[s]) run(0, FACE_VELOCITY, s, (T)p.uz_in);
+    if (p.velocity_b_out[s]) run(0, FACE_VELOCITY, s, (T)p.uz_out);
     if (s == 1 && p.nsubs == 2) {
       if (p.constcon_t_in) run(1, FACE_CONSTCON, s, T(0));
       if (p.constcon_b_in) run(0, FACE_CONSTCON, s, T(0));
@@ -280,21 +285,41 @@ void for_each_face3(const lbx_domain* d, int t, F&& run)
   }
 }
 
-// The face operations of step t that have an effect (the last configured
-// one on each face and substance), in one table.
+// The face operations of step t grouped by (face, substance), each group in
+// the configured order.
 template <typename T>
 FaceOps<T> face3_table(const lbx_domain* d, int t)
 {
+  struct Op { int kind; T drho, shift; const T* profile; };
+  std::vector<Op> group[4];
+  int gtop[4] = {0, 0, 0, 0}, gsubs[4] = {0, 0, 0, 0}, ng = 0;
+  for_each_face3<T>(d, t, [&](int top, int kind, int s, T drho) {
+    int g = 0;
+    while (g < ng && !(gtop[g] == top && gsubs[g] == s)) ++g;
+    if (g == ng) { gtop[g] = top; gsubs[g] = s; ++ng; }
+    const bool shifted = d->p.accurate && !(s == 1 && d->p.nsubs == 2);
+    Op op;
+    op.kind = kind;
+    op.drho = drho;
+    op.shift = kind == FACE_VELOCITY && shifted ? (T)d->p.rho_A[s] : T(0);
+    op.profile = kind == FACE_CONSTCON ? (const T*)(top ? d->prof_t : d->prof_b) : nullptr;
+    group[g].push_back(op);
+  });
   FaceOps<T> ops;
   std::memset(&ops, 0, sizeof ops);
   ops.conc = (T)d->p.rho_sigma_in;
-  for_each_face3<T>(d, t, [&](int top, int kind, int s, T drho) {
-    int q = 0;
-    while (q < ops.n && !(ops.top[q] == top && ops.subs[q] == s)) ++q;
-    if (q == ops.n) ++ops.n;
-    ops.top[q] = top; ops.kind[q] = kind; ops.subs[q] = s; ops.drho[q] = drho;
-    ops.profile[q] = kind == FACE_CONSTCON ? (const T*)(top ? d->prof_t : d->prof_b) : nullptr;
-  });
+  int q = 0;
+  for (int g = 0; g < ng; ++g) {
+    ops.top[g] = gtop[g]; ops.subs[g] = gsubs[g];
+    ops.first[g] = q;
+    ops.count[g] = (int)group[g].size();
+    for (const Op& op : group[g]) {
+      ops.kind[q] = op.kind; ops.drho[q] = op.drho; ops.shift[q] = op.shift;
+      ops.profile[q] = op.profile;
+      ++q;
+    }
+  }
+  ops.ngroups = ng;
   return ops;
 }
 
@@ -305,8 +330,8 @@ void launch_faces3(lbx_domain* d, int t, bool second)
   const bool compact = d->layout == LBX_LAYOUT_COMPACT;
   const long long stride = compact ? d->P : d->N;
   const FaceOps<T> ops = face3_table<T>(d, t);
-  if (ops.n == 0) return;
-  dim3 block(128), grid((p.LX + 127) / 128, p.LY, ops.n);
+  if (ops.ngroups == 0) return;
+  dim3 block(128), grid((p.LX + 127) / 128, p.LY, ops.ngroups);
   T* f = (T*)(compact ? d->fc : d->f);
   if (compact)
     face_plane<T, true><<<grid, block, 0, d->stream>>>(f, nullptr, d->fidx, p.LX, p.LY, p.LZ,
@@ -372,10 +397,16 @@ lbx_status check_params(const lbx_params* p)
   faces |= p->nsubs == 2 && (p->zeroconcgrad_n || p->zeroconcgrad_s);
   if (faces && p->dims != 2)
     return fail(LBX_ERR_INVALID, "north/south face boundaries exist for 2D runs only");
-  bool faces3 = false;
-  for (int s = 0; s < p->nsubs; ++s)
+  bool faces3 = false, vel3 = false;
+  for (int s = 0; s < p->nsubs; ++s) {
     faces3 |= p->pressure_t_in[s] || p->pressure_b_in[s] || p->pressure_t_out[s] ||
               p->pressure_b_out[s];
+    vel3 |= p->velocity_t_in[s] || p->velocity_b_in[s] || p->velocity_t_out[s] ||
+            p->velocity_b_out[s];
+  }
+  faces3 |= vel3;
+  if (vel3 && !(std::fabs(p->uz_in) < 1. && std::fabs(p->uz_out) < 1.))
+    return fail(LBX_ERR_INVALID, "velocity faces need |uz_in|, |uz_out| < 1");
   faces3 |= p->nsubs == 2 && (p->constcon_t_in || p->constcon_b_in || p->zeroconcgrad_t ||
                               p->zeroconcgrad_b);
   if (faces3 && p->dims != 3)
@@ -620,7 +651,8 @@ lbx_status lbx_create(const lbx_params* p, const uint8_t* solids, lbx_domain** o
   d->faces_fused = d->faces_active && faces_fusable(*p, solids);
   for (int s = 0; s < p->nsubs; ++s)
     d->faces3_active |= p->pressure_t_in[s] || p->pressure_b_in[s] || p->pressure_t_out[s] ||
-                        p->pressure_b_out[s];
+                        p->pressure_b_out[s] || p->velocity_t_in[s] || p->velocity_b_in[s] ||
+                        p->velocity_t_out[s] || p->velocity_b_out[s];
   d->faces3_active |= p->nsubs == 2 && (p->constcon_t_in || p->constcon_b_in ||
                                         p->zeroconcgrad_t || p->zeroconcgrad_b);
   {

@@ -442,9 +442,14 @@ lbx_status check_adjoint(const lbx_domain* d)
   if (!p.accurate || p.compressible)
     return afail(LBX_ERR_INVALID, "the adjoint covers the shifted incompressible model");
   if (d->faces_active) return afail(LBX_ERR_INVALID, "the adjoint has no 2D face boundaries");
+  if ((p.constcon_t_in && p.zeroconcgrad_t) || (p.constcon_b_in && p.zeroconcgrad_b))
+    return afail(LBX_ERR_INVALID, "the adjoint takes one solute operation per face");
   for (int s = 0; s < p.nsubs; ++s)
     if (p.pressure_t_in[s] || p.pressure_b_in[s] || p.pressure_t_out[s] || p.pressure_b_out[s])
       return afail(LBX_ERR_INVALID, "the adjoint has no pressure faces");
+    else if (p.velocity_t_in[s] || p.velocity_b_in[s] || p.velocity_t_out[s] ||
+             p.velocity_b_out[s])
+      return afail(LBX_ERR_INVALID, "the adjoint has no velocity faces");
   return LBX_OK;
 }
 
@@ -498,9 +503,8 @@ void launch_adj(lbx_domain* d, bool odd, bool solute, const AdjArgs<T>& A)
   d->launches++;
 }
 
-// Adjoint of the solute face operations of a step: per face the last
-// configured one (zero gradient over constant concentration), as the
-// forward's face launch applies them.
+// Adjoint of the solute face operations of a step: at most one per face
+// (check_adjoint rejects a face with both).
 template <typename T>
 void launch_adj_faces(lbx_domain* d, int t, T* L, double* dprof_t, double* dprof_b)
 {

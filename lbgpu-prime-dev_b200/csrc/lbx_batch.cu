@@ -501,7 +501,9 @@ lbx_status lbx_batch_create(int nsamples, const lbx_params* params, const uint8_
     if (p.precision != 4 && p.precision != 8) return bfail(LBX_ERR_INVALID, "bad precision");
     if (!p.accurate && !p.compressible) return bfail(LBX_ERR_INVALID, "accurate=0 needs compressible=1");
     if (!(p.tau[0] > 0.5)) return bfail(LBX_ERR_INVALID, "sample %d: tau must exceed 0.5", s);
-    if (p.pressure_n_in[0] || p.pressure_s_in[0] || p.pressure_n_out[0] || p.pressure_s_out[0])
+    if (p.pressure_n_in[0] || p.pressure_s_in[0] || p.pressure_n_out[0] || p.pressure_s_out[0] ||
+        p.pressure_t_in[0] || p.pressure_b_in[0] || p.pressure_t_out[0] || p.pressure_b_out[0] ||
+        p.velocity_t_in[0] || p.velocity_b_in[0] || p.velocity_t_out[0] || p.velocity_b_out[0])
       return bfail(LBX_ERR_INVALID, "sample %d: batches have no face boundaries", s);
     if ((long long)p.LX * p.LY * p.LZ >= (1LL << 31)) return bfail(LBX_ERR_INVALID, "sample too large");
     if (!solids[s]) return bfail(LBX_ERR_INVALID, "sample %d: solids is NULL", s);

@@ -129,7 +129,8 @@ enum Model { SHIFTED_INC = 0, PLAIN_COMP = 1, SHIFTED_COMP = 2 };
 // Face action per substance (2D): what the last active boundary on that
 // face does; boundaries on one face all rewrite the same three unknowns from
 // the same knowns, so the last one in the reference's order wins.
-enum FaceKind { FACE_NONE = 0, FACE_PRESSURE = 1, FACE_ZEROGRAD = 2, FACE_CONSTCON = 3 };
+enum FaceKind { FACE_NONE = 0, FACE_PRESSURE = 1, FACE_ZEROGRAD = 2, FACE_CONSTCON = 3,
+                FACE_VELOCITY = 4 };
 
 template <typename T>
 struct SubsConst {
@@ -750,10 +751,24 @@ __device__ __forceinline__ int face3_unknown(bool top, int q)
   return top ? D3B + 2 * q : D3T + 2 * q;   // B,BW,BE,BS,BN / T,TE,TW,TN,TS
 }
 
+// Velocity (the reference's CPU rule, src/bcs.c:764-862): rho =
+// (S0 + 2 S_out + rA) / (1 + u) on the top, / (1 - u) on the bottom, formed
+// in double as the reference's `1.` makes it in FP32 builds, and J = rho u;
+// `drho` carries u and `shift` rA (rho_A for shifted populations, else 0).
 template <typename T>
-__device__ __forceinline__ void face3_apply(T (&d)[19], bool top, int kind, T drho, T conc)
+__device__ __forceinline__ T face3_velocity_J(T S0, T Sout, T u, T shift, bool top)
 {
-  if (kind == FACE_PRESSURE) {
+  const double s = __dadd_rn(__dadd_rn((double)S0, __dmul_rn(2., (double)Sout)), (double)shift);
+  const double den = top ? __dadd_rn(1., (double)u) : __dsub_rn(1., (double)u);
+  const T rho = (T)(s / den);
+  return mul_(rho, u);
+}
+
+template <typename T>
+__device__ __forceinline__ void face3_apply(T (&d)[19], bool top, int kind, T drho, T conc,
+                                            T shift)
+{
+  if (kind == FACE_PRESSURE || kind == FACE_VELOCITY) {
     T S0 = d[DC];
 #pragma unroll
     for (int a = 1; a < 9; ++a) S0 = add_(S0, d[a]);
@@ -761,7 +776,8 @@ __device__ __forceinline__ void face3_apply(T (&d)[19], bool top, int kind, T dr
     const T Ny = mul_(T(0.5), sub_(add_(add_(d[DN], d[DNE]), d[DNW]), add_(add_(d[DS], d[DSW]), d[DSE])));
     if (top) {
       const T Sp = add_(add_(add_(add_(d[D3T], d[D3TE]), d[D3TW]), d[D3TN]), d[D3TS]);
-      const T J = sub_(add_(S0, mul_(T(2), Sp)), drho);
+      const T J = kind == FACE_VELOCITY ? face3_velocity_J<T>(S0, Sp, drho, shift, true)
+                                        : sub_(add_(S0, mul_(T(2), Sp)), drho);
       const T J3 = J / T(3), J6 = J / T(6);
       d[D3B] = sub_(d[D3T], J3);
       d[D3BW] = add_(sub_(d[D3TE], J6), Nx);
@@ -770,7 +786,8 @@ __device__ __forceinline__ void face3_apply(T (&d)[19], bool top, int kind, T dr
       d[D3BN] = sub_(sub_(d[D3TS], J6), Ny);
     } else {
       const T Sm = add_(add_(add_(add_(d[D3B], d[D3BW]), d[D3BE]), d[D3BS]), d[D3BN]);
-      const T J = sub_(drho, add_(S0, mul_(T(2), Sm)));
+      const T J = kind == FACE_VELOCITY ? face3_velocity_J<T>(S0, Sm, drho, shift, false)
+                                        : sub_(drho, add_(S0, mul_(T(2), Sm)));
       const T J3 = J / T(3), J6 = J / T(6);
       d[D3T] = add_(d[D3B], J3);
       d[D3TE] = sub_(add_(d[D3BW], J6), Nx);
@@ -803,21 +820,30 @@ __device__ __forceinline__ void face3_apply(T (&d)[19], bool top, int kind, T dr
   }
 }
 
-// The face operations of one step that have an effect: on each (face,
-// substance) pair every operation reads only the known slots and rewrites
-// all five unknowns, so the last configured one decides the result, and for
-// LZ >= 3 the pairs touch disjoint slots.  They run as one launch
-// (blockIdx.z = operation) with the result of running them in order.
+// The face operations of one step, grouped by (face, substance) in their
+// configured order.  For LZ >= 3 different groups touch disjoint slots, so
+// the groups run side by side in one launch (blockIdx.z = group).  Within a
+// group the operations run in order in each thread: an operation reads the
+// known slots and rewrites the five unknowns, and at a face node with
+// solids above and below a known slot of the node is also the slot its
+// unknown is deposited in (the own-slot fallback on both sides), so a later
+// operation can read an earlier one's result.  Every slot involved belongs
+// to the thread's own node, so no other thread sees the intermediate.
+constexpr int kFaceOpsMax = 24;   // 2 substances x 2 faces x 4 pressure/velocity + 4 solute ops
+
 template <typename T>
 struct FaceOps {
-  int n;
-  int top[4], kind[4], subs[4];
-  T drho[4];
-  const T* profile[4];   // constant concentration per node, or NULL
-  T conc;                // constant concentration otherwise
+  int ngroups;
+  int first[4], count[4];          // each group's operations: [first, first + count)
+  int top[4], subs[4];             // each group's face and substance
+  int kind[kFaceOpsMax];
+  T drho[kFaceOpsMax];             // pressure: rho_bc - rA; velocity: u_z
+  T shift[kFaceOpsMax];            // velocity: rA
+  const T* profile[kFaceOpsMax];   // constant concentration per node, or NULL
+  T conc;                          // constant concentration otherwise
 };
 
-// One thread per (i, j) of one operation.  `_1` form (second == 0, before
+// One thread per (i, j) of one group.  `_1` form (second == 0, before
 // an odd step): loads what the odd step will pull and deposits the unknowns
 // where it will pull them from (slot a of the upstream node, or of the node
 // itself behind a solid, as set_f1d_d does); `_2` form (before an even
@@ -830,10 +856,9 @@ __global__ void face_plane(T* f, const uint8_t* solids, const int* fidx, int LX,
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= LX) return;
   const int j = blockIdx.y;
-  const int op = blockIdx.z;
-  const int top = ops.top[op];
-  const int kind = ops.kind[op];
-  T* const fs = f + (long long)ops.subs[op] * 19 * stride;
+  const int g = blockIdx.z;
+  const int top = ops.top[g];
+  T* const fs = f + (long long)ops.subs[g] * 19 * stride;
   const int k = top ? LZ - 1 : 0;
   const int plane = LX * LY;
   const int n = i + LX * j + plane * k;
@@ -850,31 +875,37 @@ __global__ void face_plane(T* f, const uint8_t* solids, const int* fidx, int LX,
     if (COMPACT) return fidx[q];
     return solids[q] == 1 ? -1 : q;
   };
-  // only the populations the rule reads: the knowns (cz != the unknowns'),
-  // or for the zero gradient the five opposite the unknowns
+  // the group's operations in order; each loads only the populations its
+  // rule reads: the knowns (cz != the unknowns'), or for the zero gradient
+  // the five opposite the unknowns
   const int cz_unknown = top ? -1 : 1;
-  T d[19];
+  const int q_end = ops.first[g] + ops.count[g];
+  for (int q0 = ops.first[g]; q0 < q_end; ++q0) {
+    const int kind = ops.kind[q0];
+    T d[19];
 #pragma unroll
-  for (int a = 0; a < 19; ++a) {
-    const bool need = kind == FACE_ZEROGRAD ? cz(a) == -cz_unknown : cz(a) != cz_unknown;
-    if (!need) { d[a] = T(0); continue; }
-    if (second) {
-      d[a] = fs[opp(a) * stride + self];
-    } else {
-      const int up = upstream(a);
-      d[a] = (up < 0) ? fs[opp(a) * stride + self] : fs[a * stride + up];
+    for (int a = 0; a < 19; ++a) {
+      const bool need = kind == FACE_ZEROGRAD ? cz(a) == -cz_unknown : cz(a) != cz_unknown;
+      if (!need) { d[a] = T(0); continue; }
+      if (second) {
+        d[a] = fs[opp(a) * stride + self];
+      } else {
+        const int up = upstream(a);
+        d[a] = (up < 0) ? fs[opp(a) * stride + self] : fs[a * stride + up];
+      }
     }
-  }
-  const T* prof = ops.profile[op];
-  face3_apply<T>(d, top != 0, kind, ops.drho[op], prof ? prof[i + LX * j] : ops.conc);
+    const T* prof = ops.profile[q0];
+    face3_apply<T>(d, top != 0, kind, ops.drho[q0], prof ? prof[i + LX * j] : ops.conc,
+                   ops.shift[q0]);
 #pragma unroll
-  for (int q = 0; q < 5; ++q) {
-    const int a = face3_unknown(top != 0, q);
-    if (second) {
-      fs[opp(a) * stride + self] = d[a];
-    } else {
-      const int up = upstream(a);
-      fs[a * stride + (up < 0 ? self : up)] = d[a];
+    for (int q = 0; q < 5; ++q) {
+      const int a = face3_unknown(top != 0, q);
+      if (second) {
+        fs[opp(a) * stride + self] = d[a];
+      } else {
+        const int up = upstream(a);
+        fs[a * stride + (up < 0 ? self : up)] = d[a];
+      }
     }
   }
 }

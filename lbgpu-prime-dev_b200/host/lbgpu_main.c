@@ -5,7 +5,7 @@
  *
  *   lbgpu_b200 [name] [--dims 2|3] [--subs 1|2] [--precision 4|8]
  *              [--model shifted|plain|shifted-compressible] [--device N]
- *              [--solid-rule device|nonzero] [--kahan] [--walsh]
+ *              [--solid-rule device|nonzero] [--kahan] [--walsh] [--zfaces]
  *              [--frames summary,raw,dat,txt|all|none]
  *
  * Reads ./in/params.in (./in_<name>/params.in with a name, src/latman.c:
@@ -28,7 +28,11 @@
  * fraction field from the mask and the params.in value `ns` (the field the
  * reference's 2D runs upload); a 3D run with ns_flag 1 reads
  * ./in/ns<LX>x<LY>x<LZ>.raw (byte / 255) instead, as read_ns does (the
- * reference's own 3D runs leave the uploaded field unset).
+ * reference's own 3D runs leave the uploaded field unset).  --zfaces applies
+ * the z-face boundaries of params.in in 3D (pressure_{t,b}_{in,out},
+ * velocity_{t,b}_{in,out} with uz_in / uz_out, constcon_{t,b}_in and
+ * zeroconcgrad_{t,b} for the solute), which the reference's device code
+ * does not implement; without it a 3D run is periodic, as the reference's.
  */
 #include <stdio.h>
 #include <stdlib.h>
@@ -123,7 +127,7 @@ int main(int argc, char** argv)
   const char* name = NULL;
   const char* model = "shifted";
   const char* solid_rule = "device";
-  int kahan = 0, walsh = 0;
+  int kahan = 0, walsh = 0, zfaces = 0;
   int pest_n = -1, pest_kept = 0;
   int *pest_order = NULL, *pest_time = NULL, *pest_node = NULL;
   const char* frames = "all";
@@ -141,6 +145,7 @@ int main(int argc, char** argv)
     else if (!strcmp(argv[i], "--solid-rule") && i + 1 < argc) solid_rule = argv[++i];
     else if (!strcmp(argv[i], "--kahan")) kahan = 1;
     else if (!strcmp(argv[i], "--walsh")) walsh = 1;
+    else if (!strcmp(argv[i], "--zfaces")) zfaces = 1;
     else if (!strcmp(argv[i], "--frames") && i + 1 < argc) frames = argv[++i];
     else if (argv[i][0] != '-') name = argv[i];
     else DIE("unknown option %s", argv[i]);
@@ -193,6 +198,27 @@ int main(int argc, char** argv)
     for (s = 0; s < 2; s++) p.pressure_n_in[1] = p.pressure_s_in[1] = p.pressure_n_out[1] = p.pressure_s_out[1] = 0;
   if (r.dims == 3) {   /* the reference applies faces in 2D only (src/lbgpu_prime.cu:489-496) */
     for (s = 0; s < 2; s++) p.pressure_n_in[s] = p.pressure_s_in[s] = p.pressure_n_out[s] = p.pressure_s_out[s] = 0;
+    if (zfaces) {       /* the z faces of params.in, which the reference's device ignores */
+      for (s = 0; s < r.nsubs; s++) {
+        p.pressure_t_in[s] = r.hp.pressure_t_in[s];
+        p.pressure_b_in[s] = r.hp.pressure_b_in[s];
+        p.pressure_t_out[s] = r.hp.pressure_t_out[s];
+        p.pressure_b_out[s] = r.hp.pressure_b_out[s];
+        p.velocity_t_in[s] = r.hp.velocity_t_in[s];
+        p.velocity_b_in[s] = r.hp.velocity_b_in[s];
+        p.velocity_t_out[s] = r.hp.velocity_t_out[s];
+        p.velocity_b_out[s] = r.hp.velocity_b_out[s];
+      }
+      p.uz_in = rv(&r.hp.uz_in, r.prec);
+      p.uz_out = rv(&r.hp.uz_out, r.prec);
+      if (r.nsubs == 2) {
+        p.constcon_t_in = r.hp.constcon[0];    /* constcon_t_in, constcon_b_in */
+        p.constcon_b_in = r.hp.constcon[1];
+        p.zeroconcgrad_t = r.hp.zeroconcgrad_t;
+        p.zeroconcgrad_b = r.hp.zeroconcgrad_b;
+        p.rho_sigma_in = rv(&r.hp.rho_sigma_in, r.prec);
+      }
+    }
   }
   p.sink = rv(&r.hp.sink, r.prec);
   p.sigma_t_on = r.hp.sigma_t_on; p.sigma_t_off = r.hp.sigma_t_off;

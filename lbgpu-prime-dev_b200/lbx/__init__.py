@@ -50,6 +50,8 @@ class _CParams(C.Structure):
         ("rho_sigma_in", C.c_double),
         ("kahan", C.c_int),
         ("walsh", C.c_int),
+        ("velocity_t_in", _I2), ("velocity_t_out", _I2), ("velocity_b_in", _I2),
+        ("velocity_b_out", _I2), ("uz_in", C.c_double), ("uz_out", C.c_double),
     ]
 
 
@@ -222,6 +224,13 @@ class Params:
     rho_sigma_in: float = 1.0
     kahan: int = 0
     walsh: int = 0          # partial bounce-back by a per-node fraction (set_ns)
+    # Zou-He velocity on the z faces (u_z = uz_in on *_in, uz_out on *_out)
+    velocity_t_in: Sequence[int] = (0, 0)
+    velocity_t_out: Sequence[int] = (0, 0)
+    velocity_b_in: Sequence[int] = (0, 0)
+    velocity_b_out: Sequence[int] = (0, 0)
+    uz_in: float = 0.0
+    uz_out: float = 0.0
 
     @property
     def Q(self) -> int:

@@ -530,7 +530,12 @@ static const int UNK_BOT[5] = {DT, DTE, DTW, DTN, DTS};
  * with Nx, Ny half the in-plane x / y momentum.  In shifted form the rho_A
  * weights cancel from every difference, and the balance uses rho_bc - rho_A
  * (`drho`, formed in double). */
-static void zou_he_3d(real_t* d, int top, real_t drho)
+/* Velocity form (vel != 0, the reference's CPU rule, src/bcs.c:764-862):
+ * rho = (S0 + 2 S_out + rA) / (1 + u) at the top, / (1 - u) at the bottom,
+ * with the `1.` of the reference (a double in FP32 builds too), J = rho u;
+ * rA = rho_A puts the shifted sums back to full densities (the rho_A
+ * weights of the summed directions add to 1), 0 for unshifted populations. */
+static void zou_he_3d(real_t* d, int top, real_t drho, int vel, real_t u, real_t rA)
 {
   real_t S0 = d[DC] + d[DE] + d[DW] + d[DN] + d[DS] + d[DNE] + d[DSW] + d[DNW] + d[DSE];
   real_t Nx = 0.5 * ((d[DE] + d[DNE] + d[DSE]) - (d[DW] + d[DSW] + d[DNW]));
@@ -538,7 +543,12 @@ static void zou_he_3d(real_t* d, int top, real_t drho)
   real_t J;
   if (top) {
     real_t Sp = d[DT] + d[DTE] + d[DTW] + d[DTN] + d[DTS];
-    J = (S0 + 2. * Sp) - drho;
+    if (vel) {
+      real_t rho = ((S0 + 2. * Sp) + rA) / (1. + u);
+      J = rho * u;
+    } else {
+      J = (S0 + 2. * Sp) - drho;
+    }
     d[DB] = d[DT] - J / 3.;
     d[DBW] = d[DTE] - J / 6. + Nx;
     d[DBE] = d[DTW] - J / 6. - Nx;
@@ -546,7 +556,12 @@ static void zou_he_3d(real_t* d, int top, real_t drho)
     d[DBN] = d[DTS] - J / 6. - Ny;
   } else {
     real_t Sm = d[DB] + d[DBW] + d[DBE] + d[DBS] + d[DBN];
-    J = drho - (S0 + 2. * Sm);
+    if (vel) {
+      real_t rho = ((S0 + 2. * Sm) + rA) / (1. - u);
+      J = rho * u;
+    } else {
+      J = drho - (S0 + 2. * Sm);
+    }
     d[DT] = d[DB] + J / 3.;
     d[DTE] = d[DBW] + J / 6. - Nx;
     d[DTW] = d[DBE] + J / 6. + Nx;
@@ -555,8 +570,10 @@ static void zou_he_3d(real_t* d, int top, real_t drho)
   }
 }
 
-enum { F3_PRESSURE = 1, F3_ZEROGRAD = 2, F3_CONSTCON = 3 };
+enum { F3_PRESSURE = 1, F3_ZEROGRAD = 2, F3_CONSTCON = 3, F3_VELOCITY = 4 };
 
+/* drho: pressure faces' rho_bc - rA; for velocity faces the velocity u_z,
+ * with conc carrying rA */
 static void face3(const ctx_t* c, real_t* fs, const uint8_t* sol, int top,
                   int kind, int second, real_t drho, real_t conc,
                   const double* profile)
@@ -571,7 +588,9 @@ static void face3(const ctx_t* c, real_t* fs, const uint8_t* sol, int top,
       if (is_solid(sol, node_of(p, i, j, k))) continue;
       face3_load(c, fs, sol, second, i, j, k, d);
       if (kind == F3_PRESSURE) {
-        zou_he_3d(d, top, drho);
+        zou_he_3d(d, top, drho, 0, 0, 0);
+      } else if (kind == F3_VELOCITY) {
+        zou_he_3d(d, top, 0, 1, drho, conc);
       } else {
         /* unknowns set to w_a X: zero gradient takes X from the outgoing
          * populations opposite the unknowns (the 2D rule of
@@ -596,7 +615,8 @@ static void face3(const ctx_t* c, real_t* fs, const uint8_t* sol, int top,
 }
 
 /* Order: pressure t_in, t_out, b_in, b_out per substance (as n/s in 2D),
- * then the solute's constant-concentration and zero-gradient faces. */
+ * velocity t_in, t_out, b_in, b_out, then the solute's
+ * constant-concentration and zero-gradient faces. */
 static void apply_bcs3(const ctx_t* c, real_t* f, const uint8_t* sol, int t,
                        int second)
 {
@@ -618,6 +638,14 @@ static void apply_bcs3(const ctx_t* c, real_t* f, const uint8_t* sol, int t,
     if (p->pressure_b_out[s])
       face3(c, fs, sol, 0, F3_PRESSURE, second,
             (real_t)((double)face_rho(c, s, t, 0, 0, 0, 0) - rA), 0, 0);
+    if (p->velocity_t_in[s])
+      face3(c, fs, sol, 1, F3_VELOCITY, second, (real_t)p->uz_in, (real_t)rA, 0);
+    if (p->velocity_t_out[s])
+      face3(c, fs, sol, 1, F3_VELOCITY, second, (real_t)p->uz_out, (real_t)rA, 0);
+    if (p->velocity_b_in[s])
+      face3(c, fs, sol, 0, F3_VELOCITY, second, (real_t)p->uz_in, (real_t)rA, 0);
+    if (p->velocity_b_out[s])
+      face3(c, fs, sol, 0, F3_VELOCITY, second, (real_t)p->uz_out, (real_t)rA, 0);
     if (s == 1 && p->nsubs == 2) {
       if (p->constcon_t_in)
         face3(c, fs, sol, 1, F3_CONSTCON, second, 0, (real_t)p->rho_sigma_in,

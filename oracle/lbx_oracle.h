@@ -46,6 +46,11 @@ typedef struct {
    * :2812, :2936) */
   int walsh;
   const double* ns;
+  /* Zou-He velocity on the z faces (the reference's CPU formula,
+   * src/bcs.c:764-862): top / bottom plane, u_z = uz_in for the *_in faces
+   * and uz_out for the *_out faces, per substance */
+  int velocity_t_in[2], velocity_t_out[2], velocity_b_in[2], velocity_b_out[2];
+  double uz_in, uz_out;
 } orc_params;
 
 int orc_run_f64(const orc_params*, double* f, const uint8_t* solids,

@@ -68,6 +68,12 @@ class Params:
     kahan: int = 0
     walsh: int = 0
     ns: Optional[np.ndarray] = None     # per-node Walsh fraction (walsh == 1)
+    velocity_t_in: tuple = (0, 0)
+    velocity_t_out: tuple = (0, 0)
+    velocity_b_in: tuple = (0, 0)
+    velocity_b_out: tuple = (0, 0)
+    uz_in: float = 0.0
+    uz_out: float = 0.0
 
     @property
     def Q(self) -> int:
@@ -107,6 +113,12 @@ class _OrcParams(C.Structure):
         ("kahan", C.c_int),
         ("walsh", C.c_int),
         ("ns", C.POINTER(C.c_double)),
+        ("velocity_t_in", C.c_int * 2),
+        ("velocity_t_out", C.c_int * 2),
+        ("velocity_b_in", C.c_int * 2),
+        ("velocity_b_out", C.c_int * 2),
+        ("uz_in", C.c_double),
+        ("uz_out", C.c_double),
     ]
 
 

@@ -206,3 +206,22 @@ def test_gpu_driver_frame_files_match_reference_output_frame(tmp_path, dims, pre
             a = np.array(open(a_path).read().split(), dtype=np.float64)
             b = np.array(open(b_path).read().split(), dtype=np.float64)
             assert rel_err(b, a) <= tol, name
+
+
+def test_gpu_driver_zfaces_velocity_inflow(tmp_path):
+    """--zfaces in 3D: the z-face boundaries of params.in (here Zou-He
+    velocity inflow on the top plane, pressure outflow on the bottom)."""
+    tmp = str(tmp_path)
+    os.makedirs(os.path.join(tmp, "in"))
+    LX, LY, LZ = 18, 16, 20
+    write_params(os.path.join(tmp, "in", "params.in"),
+                 dict(BASE, LX=LX, LY=LY, LZ=LZ, uz_in=-0.01, rho_out=1.0,
+                      **{"velocity_t_in[0]": 1, "pressure_b_out[0]": 1}))
+    mask = geometry.sphere_pack(LX, LY, LZ, radius=3, porosity=0.6, seed=17)
+    host.write_raw_mask(os.path.join(tmp, "in", "%dx%dx%d.raw" % (LX, LY, LZ)), mask)
+    run_driver(tmp, ["--dims", "3", "--zfaces", "--frames", "dat"])
+    hp = host.read_params(os.path.join(tmp, "in", "params.in"), 3, 1)
+    assert hp.velocity_t_in[0] == 1 and hp.pressure_b_out[0] == 1
+    mv = oracle_last_frame(hp, 3, 8, mask, 30, 10, velocity_t_in=(1, 0), uz_in=hp.uz_in.d,
+                           pressure_b_out=(1, 0))
+    check_frame(tmp, mv, mask, 3, 3, 8)

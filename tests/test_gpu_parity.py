@@ -39,7 +39,8 @@ def to_lbx(p: po.Params, dtype, layout="auto") -> lbx.Params:
         "rho_out", "pfadd", "pfmul", "bc_ramp_start", "bc_ramp_stop", "pressure_n_table",
         "pressure_s_table", "pressure_t_in", "pressure_b_in", "pressure_t_out",
         "pressure_b_out", "constcon_t_in", "constcon_b_in", "zeroconcgrad_t",
-        "zeroconcgrad_b", "rho_sigma_in", "kahan")}
+        "zeroconcgrad_b", "rho_sigma_in", "kahan", "velocity_t_in", "velocity_t_out",
+        "velocity_b_in", "velocity_b_out", "uz_in", "uz_out")}
     return lbx.Params(precision=np.dtype(dtype).itemsize,
                       layout=LAYOUTS.get(layout, lbx.LBX_LAYOUT_AUTO), **kw)
 

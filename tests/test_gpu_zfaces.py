@@ -29,6 +29,15 @@ CASES = {
     # the mirrored set: flow down from the top
     "inlet_top": dict(pressure_t_in=(1, 0), pressure_b_out=(1, 0), constcon_t_in=1,
                       zeroconcgrad_b=1),
+    # Zou-He velocity inflow at the top, pressure outflow at the bottom
+    "velocity_top_in": dict(velocity_t_in=(1, 0), uz_in=-0.01, pressure_b_out=(1, 0),
+                            constcon_t_in=1, zeroconcgrad_b=1),
+    # velocity on both faces, the solute's too; a pressure face overridden
+    # by the velocity face configured after it on the same face
+    "velocity_both": dict(velocity_t_in=(1, 1), velocity_b_out=(1, 0), uz_in=-0.006,
+                          uz_out=-0.004, pressure_t_in=(1, 0), zeroconcgrad_b=1),
+    "velocity_bottom_in": dict(velocity_b_in=(1, 0), velocity_t_out=(1, 0), uz_in=0.008,
+                               uz_out=0.007, constcon_b_in=1, zeroconcgrad_t=1),
 }
 
 
@@ -112,7 +121,9 @@ def test_gpu_breakthrough_record_through_graph_replay():
 
 def test_z_faces_rejected_in_2d_and_thin_lattices():
     bad = [lbx.Params(dims=2, LX=8, LY=8, LZ=1, pressure_t_in=(1, 0)),
-           lbx.Params(dims=3, LX=8, LY=8, LZ=2, pressure_b_in=(1, 0))]
+           lbx.Params(dims=3, LX=8, LY=8, LZ=2, pressure_b_in=(1, 0)),
+           lbx.Params(dims=2, LX=8, LY=8, LZ=1, velocity_t_in=(1, 0), uz_in=-0.01),
+           lbx.Params(dims=3, LX=8, LY=8, LZ=8, velocity_b_out=(1, 0), uz_out=1.0)]
     for lp in bad:
         with pytest.raises(lbx.LbxError):
             lbx.Domain(lp, np.zeros(lp.NN, np.uint8))
@@ -154,3 +165,28 @@ def test_gpu_flow_only_record_has_ux():
     _, _, _, ux_o = po.run_oracle_btc(p, f0.copy(), sol, 0, 20, 4)
     assert np.isnan(c).all()
     assert np.abs(ux - ux_o).max() <= 1e-12 * np.abs(ux_o).max()
+
+
+@pytest.mark.parametrize("model,prec", [((1, 0), 8), ((1, 1), 8), ((1, 0), 4)])
+def test_gpu_velocity_face_imposes_the_momentum(model, prec):
+    """Every fluid node of a velocity face leaves the step with momentum
+    J = rho u_z(bc) and zero tangential momentum (mv holds u = J / den + tau g
+    with den = rho_A for shifted incompressible populations, rho otherwise;
+    no force here)."""
+    acc, comp = model
+    LX, LY, LZ = 24, 20, 32
+    lp = lbx.Params(dims=3, LX=LX, LY=LY, LZ=LZ, precision=prec, accurate=acc,
+                    compressible=comp, tau=(0.8, 1.0), velocity_t_in=(1, 0), uz_in=-0.02,
+                    pressure_b_out=(1, 0), rho_out=1.0)
+    sol = geometry.sphere_pack(LX, LY, LZ, radius=3, porosity=0.6, seed=12)
+    with lbx.Domain(lp, sol) as d:
+        d.init_equilibrium(0, 1.0, 0.0, 0.0, 0.0)
+        d.run(0, 60, 60)
+        d.sync()
+        mv = d.download_mv()[0].astype(np.float64).reshape(4, LZ, LY, LX)
+    top = sol.reshape(LZ, LY, LX)[-1] != 1
+    rho, ux, uy, uz = (mv[c, -1][top] for c in range(4))
+    den = np.ones_like(rho) if comp == 0 else rho
+    tol = 1e-12 if prec == 8 else 2e-6
+    assert np.allclose(uz * den, rho * -0.02, rtol=tol, atol=0)
+    assert np.max(np.abs(ux)) < 0.05 and np.max(np.abs(uy)) < 0.05
