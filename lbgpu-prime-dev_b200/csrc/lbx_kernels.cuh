@@ -475,13 +475,14 @@ struct CompactArgs {
 };
 
 // Resident 256-thread blocks asked of the compiler: six (40 registers) for
-// the FP32 flow kernels, where that measured fastest; for the others the
-// cap closest above their natural register count (FP32 solute 85, FP64 flow
-// 85, FP64 solute 128), since a lower cap spills.
+// the FP32 kernels, where that measured fastest (the solute kernel spills
+// 12-16 bytes there and still runs 4% faster than at three blocks, its
+// natural 85 registers); for FP64 the cap closest above the natural
+// register count (flow 85, solute 128), since a lower cap spills more.
 template <typename T, int PART>
 constexpr int compact_min_blocks()
 {
-  return sizeof(T) == 4 ? (PART == PART_SOLUTE ? 3 : 6) : (PART == PART_SOLUTE ? 2 : 3);
+  return sizeof(T) == 4 ? 6 : (PART == PART_SOLUTE ? 2 : 3);
 }
 
 // IDX32: population offsets within one substance's [Q][P] block fit in 32
