@@ -51,6 +51,15 @@ __attribute__((visibility("hidden"))) lbx_status lbx_internal_fail(lbx_status co
   return code;
 }
 
+// Drops the cached step graphs (their launch arguments no longer hold).
+__attribute__((visibility("hidden"))) void lbx_internal_drop_graphs(lbx_domain* d)
+{
+  if (d->graph) cudaGraphExecDestroy(d->graph);
+  if (d->graph_multi) cudaGraphExecDestroy(d->graph_multi);
+  d->graph = nullptr;
+  d->graph_multi = nullptr;
+}
+
 namespace {
 
 #define CK(call)                                                              \
@@ -452,8 +461,7 @@ bool faces_fusable(const lbx_params& p, const uint8_t* sol)
 
 void release(lbx_domain* d)
 {
-  if (d->graph) cudaGraphExecDestroy(d->graph);
-  d->graph = nullptr;
+  lbx_internal_drop_graphs(d);
   cudaFree(d->fc); cudaFree(d->fidx); cudaFree(d->fnode);
   cudaFree(d->f); cudaFree(d->mv); cudaFree(d->solids); cudaFree(d->cls);
   cudaFree(d->nbm); cudaFree(d->red);
@@ -553,6 +561,38 @@ size_t step_key(const lbx_domain* d, int t, unsigned char* out)
 // Replay `pairs` AA pairs starting at odd time t from one captured pair.
 // Only called when every step of the stretch has the launch arguments of
 // the first pair (checked by the caller) and the stream is capturable.
+// Captures `npairs` repetitions of the pair (t, t+1) into one graph.
+lbx_status capture_pairs(lbx_domain* d, int t, int npairs, cudaGraphExec_t* out,
+                         long long* nlaunch)
+{
+  cudaGraph_t g = nullptr;
+  CK(cudaStreamBeginCapture(d->stream, cudaStreamCaptureModeThreadLocal));
+  const long long before = d->launches;
+  lbx_status st = LBX_OK;
+  for (int r = 0; r < npairs && st == LBX_OK; ++r) {
+    st = d->real_size == 8 ? step_t<double>(d, t, 0) : step_t<float>(d, t, 0);
+    if (st == LBX_OK)
+      st = d->real_size == 8 ? step_t<double>(d, t + 1, 0) : step_t<float>(d, t + 1, 0);
+  }
+  cudaError_t e = cudaStreamEndCapture(d->stream, &g);
+  *nlaunch = d->launches - before;
+  d->launches = before;
+  if (st != LBX_OK) { if (g) cudaGraphDestroy(g); return st; }
+  if (e != cudaSuccess) return fail(LBX_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
+  e = cudaGraphInstantiate(out, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) {
+    *out = nullptr;
+    return fail(LBX_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
+  }
+  return LBX_OK;
+}
+
+// `pairs` AA pairs with the launch arguments of the pair at t, replayed from
+// graphs of one pair and of kGraphPairs pairs (fewer graph launches, and
+// the kernels of a multi-pair graph follow each other without the host).
+constexpr int kGraphPairs = 8;
+
 lbx_status replay_pairs(lbx_domain* d, int t, int pairs)
 {
   alignas(16) unsigned char key[2 * kKey];
@@ -562,30 +602,24 @@ lbx_status replay_pairs(lbx_domain* d, int t, int pairs)
   const size_t klen = k1 + k2;
   if (!d->graph || d->graph_stream != d->stream || d->graph_key_len != klen ||
       std::memcmp(d->graph_key, key, klen) != 0) {
-    if (d->graph) { cudaGraphExecDestroy(d->graph); d->graph = nullptr; }
-    cudaGraph_t g = nullptr;
-    CK(cudaStreamBeginCapture(d->stream, cudaStreamCaptureModeThreadLocal));
-    const long long before = d->launches;
-    lbx_status st = d->real_size == 8 ? step_t<double>(d, t, 0) : step_t<float>(d, t, 0);
-    if (st == LBX_OK)
-      st = d->real_size == 8 ? step_t<double>(d, t + 1, 0) : step_t<float>(d, t + 1, 0);
-    cudaError_t e = cudaStreamEndCapture(d->stream, &g);
-    d->graph_launches = d->launches - before;
-    d->launches = before;
-    if (st != LBX_OK) { if (g) cudaGraphDestroy(g); return st; }
-    if (e != cudaSuccess) return fail(LBX_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
-    e = cudaGraphInstantiate(&d->graph, g, 0);
-    cudaGraphDestroy(g);
-    if (e != cudaSuccess) { d->graph = nullptr; return fail(LBX_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e)); }
+    lbx_internal_drop_graphs(d);
+    if (lbx_status st = capture_pairs(d, t, 1, &d->graph, &d->graph_launches)) return st;
     d->graph_stream = d->stream;
     std::memcpy(d->graph_key, key, klen);
     d->graph_key_len = klen;
   }
-  // the graph holds every kernel of both steps (faces and records included)
-  const long long per_pair = d->graph_launches;
-  for (int r = 0; r < pairs; ++r) {
+  if (pairs >= kGraphPairs && !d->graph_multi) {
+    long long n = 0;
+    if (lbx_status st = capture_pairs(d, t, kGraphPairs, &d->graph_multi, &n)) return st;
+  }
+  // the graphs hold every kernel of their steps (faces and records included)
+  for (int r = 0; r < pairs / kGraphPairs; ++r) {
+    CK(cudaGraphLaunch(d->graph_multi, d->stream));
+    d->launches += kGraphPairs * d->graph_launches;
+  }
+  for (int r = 0; r < pairs % kGraphPairs; ++r) {
     CK(cudaGraphLaunch(d->graph, d->stream));
-    d->launches += per_pair;
+    d->launches += d->graph_launches;
   }
   if (d->layout == LBX_LAYOUT_COMPACT) d->dense_stale = true;
   return LBX_OK;
@@ -953,7 +987,7 @@ lbx_status lbx_btc_stop(lbx_domain* d)
   if (!d) return fail(LBX_ERR_INVALID, "domain is NULL");
   if (d->btc_vals) {
     CK(cudaStreamSynchronize(d->stream));
-    if (d->graph) { cudaGraphExecDestroy(d->graph); d->graph = nullptr; }
+    lbx_internal_drop_graphs(d);
   }
   cudaFree(d->btc_vals); cudaFree(d->btc_rec); cudaFree(d->btc_slot);
   d->btc_vals = nullptr; d->btc_rec = nullptr; d->btc_slot = nullptr;
@@ -987,7 +1021,7 @@ lbx_status lbx_btc_start(lbx_domain* d, int plane, int capacity)
   CK(cudaMalloc(&d->btc_slot, sizeof(int)));
   CK(cudaMemsetAsync(d->btc_slot, 0, sizeof(int), d->stream));
   // the step arguments changed: a captured pair no longer matches
-  if (d->graph) { CK(cudaStreamSynchronize(d->stream)); cudaGraphExecDestroy(d->graph); d->graph = nullptr; }
+  if (d->graph) { CK(cudaStreamSynchronize(d->stream)); lbx_internal_drop_graphs(d); }
   return LBX_OK;
 }
 
@@ -1019,7 +1053,7 @@ lbx_status lbx_set_face_profile(lbx_domain* d, int top, const double* conc)
   if (!d) return fail(LBX_ERR_INVALID, "domain is NULL");
   void*& dst = top ? d->prof_t : d->prof_b;
   CK(cudaStreamSynchronize(d->stream));
-  if (d->graph) { cudaGraphExecDestroy(d->graph); d->graph = nullptr; }
+  lbx_internal_drop_graphs(d);
   if (!conc) { cudaFree(dst); dst = nullptr; return LBX_OK; }
   const size_t n = (size_t)d->p.LX * d->p.LY;
   if (!dst) CK(cudaMalloc(&dst, n * d->real_size));

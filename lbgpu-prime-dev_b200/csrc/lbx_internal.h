@@ -53,6 +53,7 @@ struct lbx_domain {
   long long launches = 0;
   // graph replay of frame-free, time-invariant runs: one captured AA pair
   cudaGraphExec_t graph = nullptr;
+  cudaGraphExec_t graph_multi = nullptr;   // the same pair repeated (replay_pairs)
   cudaStream_t graph_stream = nullptr;   // stream the pair was captured on
   unsigned char graph_key[2 * 640];      // keys of the odd and the even step
   size_t graph_key_len = 0;
@@ -65,6 +66,7 @@ LBX_HIDDEN lbx_status lbx_internal_fail(lbx_status code, const char* msg);
 LBX_HIDDEN lbx_status lbx_internal_step_into(lbx_domain* d, int t, void* src, void* dst);
 LBX_HIDDEN void lbx_internal_adjoint_free(lbx_domain* d);
 LBX_HIDDEN void lbx_internal_frames_free(lbx_domain* d);
+LBX_HIDDEN void lbx_internal_drop_graphs(lbx_domain* d);
 // PEST sampling: whether a sample is due at time t (the step then writes
 // the macro variables), the gather after that step, and the release.
 LBX_HIDDEN bool lbx_internal_pest_due(const lbx_domain* d, int t);

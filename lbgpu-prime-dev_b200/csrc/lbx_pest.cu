@@ -137,7 +137,7 @@ lbx_status lbx_pest_set(lbx_domain* d, int count, const int* time, const int* no
                  cudaGetErrorString(e));
   }
   d->pest = P;
-  if (d->graph) { cudaGraphExecDestroy(d->graph); d->graph = nullptr; }
+  lbx_internal_drop_graphs(d);
   return LBX_OK;
 }
 
