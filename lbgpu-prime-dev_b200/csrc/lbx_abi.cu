@@ -171,6 +171,7 @@ void launch_part(lbx_domain* d, const StepArgs<T>& A, bool odd)
     C.s = A;
     C.fidx = d->fidx;
     C.fnode = d->fnode;
+    C.frm = d->frm;
     C.F = (int)d->fluid;
     C.P = (int)d->P;
     C.div_plane = make_fastdiv((unsigned)(A.LX * A.LY));
@@ -462,7 +463,7 @@ bool faces_fusable(const lbx_params& p, const uint8_t* sol)
 void release(lbx_domain* d)
 {
   lbx_internal_drop_graphs(d);
-  cudaFree(d->fc); cudaFree(d->fidx); cudaFree(d->fnode);
+  cudaFree(d->fc); cudaFree(d->fidx); cudaFree(d->fnode); cudaFree(d->frm);
   cudaFree(d->f); cudaFree(d->mv); cudaFree(d->solids); cudaFree(d->cls);
   cudaFree(d->nbm); cudaFree(d->red);
   cudaFree(d->btc_vals); cudaFree(d->btc_rec); cudaFree(d->btc_slot);
@@ -602,15 +603,17 @@ lbx_status replay_pairs(lbx_domain* d, int t, int pairs)
   const size_t klen = k1 + k2;
   if (!d->graph || d->graph_stream != d->stream || d->graph_key_len != klen ||
       std::memcmp(d->graph_key, key, klen) != 0) {
+    // both graphs at once, so a later, longer stretch does not pay a capture
     lbx_internal_drop_graphs(d);
     if (lbx_status st = capture_pairs(d, t, 1, &d->graph, &d->graph_launches)) return st;
+    long long n = 0;
+    if (lbx_status st = capture_pairs(d, t, kGraphPairs, &d->graph_multi, &n)) {
+      lbx_internal_drop_graphs(d);
+      return st;
+    }
     d->graph_stream = d->stream;
     std::memcpy(d->graph_key, key, klen);
     d->graph_key_len = klen;
-  }
-  if (pairs >= kGraphPairs && !d->graph_multi) {
-    long long n = 0;
-    if (lbx_status st = capture_pairs(d, t, kGraphPairs, &d->graph_multi, &n)) return st;
   }
   // the graphs hold every kernel of their steps (faces and records included)
   for (int r = 0; r < pairs / kGraphPairs; ++r) {
@@ -731,6 +734,25 @@ lbx_status lbx_create(const lbx_params* p, const uint8_t* solids, lbx_domain** o
     CKD(cudaMalloc(&d->fnode, fnode.size() * sizeof(int)));
     CKD(cudaMemcpy(d->fidx, fidx.data(), d->N * sizeof(int), cudaMemcpyHostToDevice));
     CKD(cudaMemcpy(d->fnode, fnode.data(), fnode.size() * sizeof(int), cudaMemcpyHostToDevice));
+    {
+      // the fluid bitmask in 32-node words, each with the number of fluid
+      // nodes before it: the compact index of fluid node n is the word's
+      // rank plus the fluid bits below n
+      const long long W = (d->N + 31) / 32;
+      std::vector<uint2> frm((size_t)W);
+      unsigned rank = 0;
+      for (long long w = 0; w < W; ++w) {
+        unsigned bits = 0;
+        for (int b = 0; b < 32; ++b) {
+          const long long n = w * 32 + b;
+          if (n < d->N && solids[n] != 1) bits |= 1u << b;
+        }
+        frm[(size_t)w] = make_uint2(rank, bits);
+        rank += (unsigned)__builtin_popcount(bits);
+      }
+      CKD(cudaMalloc(&d->frm, (size_t)W * sizeof(uint2)));
+      CKD(cudaMemcpy(d->frm, frm.data(), (size_t)W * sizeof(uint2), cudaMemcpyHostToDevice));
+    }
     CKD(cudaMemsetAsync(d->fc, 0, std::max<size_t>(1, (size_t)p->nsubs * d->Q * d->P * d->real_size), d->stream));
   }
   if (p->nsubs == 2) {
