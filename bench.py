@@ -21,6 +21,7 @@ from __future__ import annotations
 import argparse
 import json
 import os
+import platform
 import re
 import subprocess
 import sys
@@ -198,6 +199,52 @@ def reference_arm(args, rank: int, world: int):
     return 0
 
 
+def cpu_table() -> int:
+    """The CPU side on the host cores, beside the GPU numbers: the oracle
+    port (C restatement, all cores) and the reference's own kernels
+    (oracle/_ref, all cores and one core) on the 256^2 D2Q9 pressure-driven
+    case and a 128^3 crop of the benchmark lattice (FP64 and FP32).  One
+    JSON line per case and implementation; bounded samples (a few seconds
+    each)."""
+    import pyoracle as po
+    from lbx import geometry
+    cores = os.cpu_count() or 1
+    cases = []
+    m2 = geometry.transpose_2d(geometry.disc_pack(256, 256, radius=8, porosity=0.6, seed=1),
+                               256, 256)
+    p2 = po.Params(dims=2, LX=256, LY=256, LZ=1, tau=(1.0, 1.0), pressure_s_in=(1, 0),
+                   pressure_n_out=(1, 0), rho_in=1.001, rho_out=1.0)
+    cases.append(("D2Q9 256^2 FP64, Zou-He pressure", p2, m2, np.float64, "d2q9_f64", 40))
+    m3 = geometry.sphere_pack(128, 128, 128, radius=6, porosity=0.4, seed=1234)
+    for dt, v in ((np.float64, "d3q19_f64"), (np.float32, "d3q19_f32")):
+        p3 = po.Params(dims=3, LX=128, LY=128, LZ=128, tau=(TAU, 1.0),
+                       gaccel=(GX, 0, 0, 0, 0, 0))
+        cases.append(("D3Q19 128^3 %s, benchmark lattice crop" % ("FP64" if dt == np.float64
+                                                                   else "FP32"),
+                      p3, m3, dt, v, 6))
+    for name, p, mask, dt, variant, steps in cases:
+        runs = [("port", cores)]
+        if po.reference_available(variant):
+            runs += [("reference", cores), ("reference", 1)]
+        for kind, nt in runs:
+            f = np.zeros((p.nsubs, p.Q, p.NN), dt)
+            if kind == "port":
+                po.run_oracle(p, f, mask, 0, 2, threads=nt)
+                t0 = time.perf_counter()
+                po.run_oracle(p, f, mask, 2, steps, threads=nt)
+            else:
+                po.run_reference(variant, p, f, mask, 0, 0)
+                po._refs[variant].refk_set_threads(nt)
+                po.run_reference(variant, p, f, mask, 0, 2)
+                t0 = time.perf_counter()
+                po.run_reference(variant, p, f, mask, 2, steps)
+            dt_s = time.perf_counter() - t0
+            print(json.dumps({"cpu_table": name, "kind": kind, "threads": nt,
+                              "mlups": round(p.NN * steps / dt_s / 1e6, 3), "steps": steps,
+                              "cpu": platform.processor() or platform.machine()}))
+    return 0
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -205,6 +252,9 @@ def main(argv=None) -> int:
     ap.add_argument("--warmup", type=int, default=4)
     ap.add_argument("--impl", default="lbx", choices=["lbx", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-table", action="store_true",
+                    help="print the host-core timings of the oracle port and of the "
+                         "reference's kernels on the 2D case and a 128^3 crop, then exit")
     ap.add_argument("--edge", type=int, default=256,
                     help="lattice edge; 256 is the benchmark workload, smaller "
                          "edges are for profiling captures only")
@@ -214,6 +264,8 @@ def main(argv=None) -> int:
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.cpu_table:
+        return cpu_table()
     if args.impl == "reference":
         return reference_arm(args, rank, world)
 
