@@ -188,11 +188,109 @@ enum StepPart { PART_ALL = 0, PART_FLOW = 1, PART_SOLUTE = 2 };
 // incoming one, f_a <- f_a (1 - ns) + ns f_opp(a).  The factor 1 - ns is a
 // double (the reference writes `1.`), so those products round once from
 // double in FP32 as well.
+// FP32 collision by opposite pairs (a, a+1) (same weight, opposite c): the
+// moments come from pair sums and differences, the symmetric part of each
+// pair's equilibrium (w rho / tau + w rq (4.5 (c.u)^2 - 1.5 u^2) / tau, or
+// the solute's w C / tau) is formed once and the antisymmetric part
+// (3 c.u times the same weight) is added to one population and subtracted
+// from the other, and the three divisions of u by the density become one
+// reciprocal: about a third fewer instructions than the per-direction form.
+// A step run for seconds draws the B200's 1000 W cap and its SM clock falls
+// to ~1.6 GHz, where the odd step's instruction count shows; sustained 256^3
+// FP32 steps run 3% faster this way (0.196 vs 0.203 ms; a short burst at
+// full clock gains under 1%).  The sums round in another order, which moves
+// FP32 results by a few ulps; FP64, Kahan sums and Walsh runs keep the
+// reference's operation order.
+template <int Q, int MODEL>
+__device__ __forceinline__ float collide_pairs(const StepArgs<float>& A, int s, bool solute,
+                                               int sinks, float (&d)[Q], float (&u)[3],
+                                               long long n)
+{
+  constexpr int D = (Q == 9) ? 2 : 3;
+  constexpr int NP = (Q - 1) / 2;
+  const SubsConst<float>& c = A.sc[s];
+  float rho = d[0];
+  float dif[NP];
+#pragma unroll
+  for (int p = 0; p < NP; ++p) {
+    rho += d[2 * p + 1] + d[2 * p + 2];
+    dif[p] = d[2 * p + 1] - d[2 * p + 2];
+  }
+  if (solute) {
+    if (sinks == 2) rho *= A.sink1;
+    rho *= A.sink1;
+  } else {
+    float m0 = 0.f, m1 = 0.f, m2 = 0.f;
+#pragma unroll
+    for (int p = 0; p < NP; ++p) {
+      const int a = 2 * p + 1;
+      if (cx(a) > 0) m0 += dif[p]; else if (cx(a) < 0) m0 -= dif[p];
+      if (cy(a) > 0) m1 += dif[p]; else if (cy(a) < 0) m1 -= dif[p];
+      if (D == 3) { if (cz(a) > 0) m2 += dif[p]; else if (cz(a) < 0) m2 -= dif[p]; }
+    }
+    const float den = (MODEL == SHIFTED_INC) ? c.rhoA
+                    : (MODEL == PLAIN_COMP) ? rho : (c.rhoA + rho);
+    const float inv = 1.f / den;
+    u[0] = m0 * inv + c.tg[0];
+    u[1] = m1 * inv + c.tg[1];
+    u[2] = (D == 3) ? m2 * inv + c.tg[2] : 0.f;
+  }
+  if (A.write_mv) {
+    float* m = A.mv + (long long)s * (1 + D) * A.N;
+    m[n] = (!solute && MODEL != PLAIN_COMP) ? rho + c.rhoA : rho;
+    m[A.N + n] = u[0];
+    m[2 * A.N + n] = u[1];
+    if (D == 3) m[3 * A.N + n] = u[2];
+  }
+  auto cdotu = [&](int a) -> float {
+    float r = 0.f;
+    if (cx(a) > 0) r += u[0]; else if (cx(a) < 0) r -= u[0];
+    if (cy(a) > 0) r += u[1]; else if (cy(a) < 0) r -= u[1];
+    if (D == 3) { if (cz(a) > 0) r += u[2]; else if (cz(a) < 0) r -= u[2]; }
+    return r;
+  };
+  if (solute) {
+    const float ci = rho * c.itau;
+    d[0] = fmaf(d[0], c.omc, wgt<float, Q>(0) * ci);
+#pragma unroll
+    for (int p = 0; p < NP; ++p) {
+      const int a = 2 * p + 1;
+      const float base = wgt<float, Q>(a) * ci;
+      const float anti = (3.f * base) * cdotu(a);
+      d[a] = fmaf(d[a], c.omc, base + anti);
+      d[a + 1] = fmaf(d[a + 1], c.omc, base - anti);
+    }
+  } else {
+    const float usq = u[0] * u[0] + u[1] * u[1] + (D == 3 ? u[2] * u[2] : 0.f);
+    const float rq = (MODEL == SHIFTED_INC) ? c.rhoA
+                   : (MODEL == PLAIN_COMP) ? rho : (c.rhoA + rho);
+    const float ri = rho * c.itau, qi = rq * c.itau;
+    const float k = -1.5f * usq;
+    d[0] = fmaf(d[0], c.omc, fmaf(wgt<float, Q>(0) * qi, k, wgt<float, Q>(0) * ri));
+#pragma unroll
+    for (int p = 0; p < NP; ++p) {
+      const int a = 2 * p + 1;
+      const float cu = cdotu(a);
+      const float wq = wgt<float, Q>(a) * qi;
+      const float sym = fmaf(wq, fmaf(4.5f * cu, cu, k), wgt<float, Q>(a) * ri);
+      const float anti = (3.f * wq) * cu;
+      d[a] = fmaf(d[a], c.omc, sym + anti);
+      d[a + 1] = fmaf(d[a + 1], c.omc, sym - anti);
+    }
+  }
+  return rho;
+}
+
 template <typename T, int Q, int MODEL, bool WALSH = false>
 __device__ __forceinline__ T collide(const StepArgs<T>& A, int s, bool solute,
                                         int sinks, T (&d)[Q], T (&u)[3],
                                         long long n)
 {
+  if constexpr (sizeof(T) == 4 && !WALSH) {
+    if (!A.kahan)
+      return collide_pairs<Q, MODEL>(A, s, solute, sinks, reinterpret_cast<float (&)[Q]>(d),
+                                     reinterpret_cast<float (&)[3]>(u), n);
+  }
   constexpr int D = (Q == 9) ? 2 : 3;
   const SubsConst<T>& c = A.sc[s];
   T nsv = T(0), pre[WALSH ? Q : 1];
