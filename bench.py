@@ -199,6 +199,23 @@ def reference_arm(args, rank: int, world: int):
     return 0
 
 
+def max_over_ranks(dist, value: float, device) -> float:
+    """The maximum of `value` over the ranks of the process group (the
+    slowest replica sets the whole job's time); `value` itself without one."""
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_mlups(world: int, nodes: int, steps: int, seconds: float) -> float:
+    """Whole-job MLUPS of `world` replicas that each advanced `nodes` nodes
+    by `steps` steps in `seconds` (the slowest replica's time)."""
+    return world * nodes * steps / seconds / 1e6
+
+
 def cpu_table() -> int:
     """The CPU side on the host cores, beside the GPU numbers: the oracle
     port (C restatement, all cores) and the reference's own kernels
@@ -314,14 +331,12 @@ def main(argv=None) -> int:
     ms = ev0.elapsed_time(ev1)
     launches = dom.launch_count() - launches0
     clocks = sampler.stop()
+    ms = max_over_ranks(dist, ms, "cuda")
     if dist:
-        tms = torch.tensor([ms], device="cuda")
-        dist.all_reduce(tms, op=dist.ReduceOp.MAX)
-        ms = float(tms.item())
         dist.barrier()
     ms_step = ms / args.steps
-    value = world * NN * args.steps / (ms / 1e3) / 1e6
-    mflups = world * fluid * args.steps / (ms / 1e3) / 1e6
+    value = job_mlups(world, NN, args.steps, ms / 1e3)
+    mflups = job_mlups(world, fluid, args.steps, ms / 1e3)
 
     # per-kind launch durations (odd = stream-collide-stream, even = collide)
     per_kind = {}
@@ -376,11 +391,8 @@ def main(argv=None) -> int:
     lbx._check(lib.lbx_download_mv(h, 0, mv_host[0].data_ptr(), mv_host[1].data_ptr(),
                                    mv_host[2].data_ptr(), mv_host[3].data_ptr()))
     e2e_s = time.perf_counter() - t0
-    if dist:
-        te2 = torch.tensor([e2e_s], device="cuda")
-        dist.all_reduce(te2, op=dist.ReduceOp.MAX)
-        e2e_s = float(te2.item())
-    e2e = {"value": round(world * NN * args.steps / e2e_s / 1e6, 3), "unit": "MLUPS",
+    e2e_s = max_over_ranks(dist, e2e_s, "cuda")
+    e2e = {"value": round(job_mlups(world, NN, args.steps, e2e_s), 3), "unit": "MLUPS",
            "h2d_bytes_per_step": int(Q * NN * REAL / args.steps),
            "d2h_bytes_per_step": int(4 * NN * REAL / args.steps),
            "note": "upload of all populations from pinned host memory, K steps, "
