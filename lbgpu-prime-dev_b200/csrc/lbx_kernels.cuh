@@ -661,7 +661,8 @@ __device__ __forceinline__ void compact_node(const CompactArgs<T>& C, const int 
     // pulled d_opp(a) from (the AA pattern's in-place pairing), so the
     // push reads them here instead of repeating the 18 index lookups;
     // one column per thread, no barrier needed
-    __shared__ unsigned sslot[ODD ? Q : 1][256];
+    // (offsets in the kernel's index type: 64-bit above 2^32 slots)
+    __shared__ Idx sslot[ODD ? Q : 1][256];
     T d[Q];
     if (ODD) {
       // pull: d_a = f[a][idx(n - c_a)], or own f[opp a] behind a solid; the
@@ -670,7 +671,7 @@ __device__ __forceinline__ void compact_node(const CompactArgs<T>& C, const int 
       for (int a = 0; a < Q; ++a) {
         const int up = (a == 0) ? m : nb_pull(opp(a));
         const Idx src = (up >= 0) ? (Idx)a * F + (Idx)up : (Idx)opp(a) * F + (Idx)m;
-        sslot[a][threadIdx.x] = (unsigned)src;
+        sslot[a][threadIdx.x] = src;
         d[a] = fs[src];
       }
     } else {
@@ -700,7 +701,7 @@ __device__ __forceinline__ void compact_node(const CompactArgs<T>& C, const int 
       xm = opaque(xm); xp = opaque(xp); ym = opaque(ym); yp = opaque(yp);
       if (D == 3) { zm = opaque(zm); zp = opaque(zp); }
 #pragma unroll
-      for (int a = 0; a < Q; ++a) fo[(Idx)sslot[opp(a)][threadIdx.x]] = d[a];
+      for (int a = 0; a < Q; ++a) fo[sslot[opp(a)][threadIdx.x]] = d[a];
     } else {
       const int m2 = opaque(m);   // do not keep the load addresses live
 #pragma unroll
