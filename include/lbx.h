@@ -179,7 +179,11 @@ lbx_status lbx_step_pair(lbx_domain* d, int time, unsigned flags);
 
 /* Steps t0+1 .. t0+nsteps (t0 even), writing macro variables at every time
  * that is a multiple of frame_rate (frame_rate <= 0: never) -- the
- * is_end_of_frame rule of src/lattice.c:2094-2097.  Asynchronous. */
+ * is_end_of_frame rule of src/lattice.c:2094-2097.  Stretches of
+ * frame-free steps with unchanged launch arguments are replayed from CUDA
+ * graphs (one AA pair, or eight pairs per graph launch; captured on first
+ * use and kept while the arguments and the stream stay the same).
+ * Asynchronous. */
 lbx_status lbx_run(lbx_domain* d, int t0, int nsteps, int frame_rate);
 
 /* Run the domain's work on the caller's CUDA stream (a cudaStream_t passed

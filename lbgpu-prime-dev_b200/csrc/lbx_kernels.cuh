@@ -126,9 +126,11 @@ enum : uint8_t {
 // Collision models: the reference's ACCURATE / COMPRESSIBLE flag pairs.
 enum Model { SHIFTED_INC = 0, PLAIN_COMP = 1, SHIFTED_COMP = 2 };
 
-// Face action per substance (2D): what the last active boundary on that
-// face does; boundaries on one face all rewrite the same three unknowns from
-// the same knowns, so the last one in the reference's order wins.
+// Face action per substance.  2D fused faces: what the last active boundary
+// on that face does (boundaries on one face all rewrite the same three
+// unknowns from the same knowns, and fusing requires fluid upstream nodes,
+// so the last one in the reference's order decides); 3D z faces apply every
+// configured operation in order (FaceOps).
 enum FaceKind { FACE_NONE = 0, FACE_PRESSURE = 1, FACE_ZEROGRAD = 2, FACE_CONSTCON = 3,
                 FACE_VELOCITY = 4 };
 
@@ -560,7 +562,9 @@ aa_step(StepArgs<T> A)
 // order, so a warp's accesses in every direction plane cover only fluid
 // data (with 60% solids a dense layout fetches ~2x the useful bytes at
 // sector granularity).  fidx[n] maps a dense node to its compact index
-// (-1: solid); fnode[m] maps back.  One thread per fluid node.
+// (-1: solid; the face kernels use it), fnode[m] maps back, and frm holds
+// the fluid bitmask with word ranks the odd step finds neighbours in.  One
+// thread per fluid node.
 template <typename T>
 struct CompactArgs {
   StepArgs<T> s;          // f = compact populations; N = dense node count
