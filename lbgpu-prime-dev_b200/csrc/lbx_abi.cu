@@ -171,7 +171,7 @@ void launch_part(lbx_domain* d, const StepArgs<T>& A, bool odd)
     C.s = A;
     C.fidx = d->fidx;
     C.fnode = d->fnode;
-    C.frm = d->frm;
+    C.frm = d->frm + 1;   // past the front guard word
     C.F = (int)d->fluid;
     C.P = (int)d->P;
     C.div_plane = make_fastdiv((unsigned)(A.LX * A.LY));
@@ -737,21 +737,26 @@ lbx_status lbx_create(const lbx_params* p, const uint8_t* solids, lbx_domain** o
     {
       // the fluid bitmask in 32-node words, each with the number of fluid
       // nodes before it: the compact index of fluid node n is the word's
-      // rank plus the fluid bits below n
+      // rank plus the fluid bits below n.  A guard word with no fluid bits
+      // on either side (ranks 0 and F) lets the odd step read the words
+      // around node 0 and node N - 1 without bounds checks.
       const long long W = (d->N + 31) / 32;
-      std::vector<uint2> frm((size_t)W);
+      std::vector<uint2> frm((size_t)W + 2);
       unsigned rank = 0;
+      frm[0] = make_uint2(0u, 0u);
       for (long long w = 0; w < W; ++w) {
         unsigned bits = 0;
         for (int b = 0; b < 32; ++b) {
           const long long n = w * 32 + b;
           if (n < d->N && solids[n] != 1) bits |= 1u << b;
         }
-        frm[(size_t)w] = make_uint2(rank, bits);
+        frm[(size_t)w + 1] = make_uint2(rank, bits);
         rank += (unsigned)__builtin_popcount(bits);
       }
-      CKD(cudaMalloc(&d->frm, (size_t)W * sizeof(uint2)));
-      CKD(cudaMemcpy(d->frm, frm.data(), (size_t)W * sizeof(uint2), cudaMemcpyHostToDevice));
+      frm[(size_t)W + 1] = make_uint2(rank, 0u);
+      CKD(cudaMalloc(&d->frm, ((size_t)W + 2) * sizeof(uint2)));
+      CKD(cudaMemcpy(d->frm, frm.data(), ((size_t)W + 2) * sizeof(uint2),
+                     cudaMemcpyHostToDevice));
     }
     CKD(cudaMemsetAsync(d->fc, 0, std::max<size_t>(1, (size_t)p->nsubs * d->Q * d->P * d->real_size), d->stream));
   }

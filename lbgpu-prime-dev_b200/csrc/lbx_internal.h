@@ -17,7 +17,7 @@ struct lbx_domain {
   void* fc = nullptr;         // [nsubs][Q][P] compact layout
   int* fidx = nullptr;        // [N] dense -> compact (-1 solid)
   int* fnode = nullptr;       // [F] compact -> dense
-  uint2* frm = nullptr;       // [ceil(N/32)] fluid bitmask with word ranks (odd-step lookups)
+  uint2* frm = nullptr;       // [ceil(N/32) + 2] fluid bitmask with word ranks, guard word each end
   long long P = 0;            // compact plane stride: fluid rounded up to 32
   int layout = LBX_LAYOUT_DENSE;
   bool dense_stale = false;   // compact state newer than the dense array
