@@ -335,3 +335,28 @@ def test_gpu_compact_thin_wide_lattice(dtype):
     fo, mvo = _oracle(p, f0, sol, 12, 6)
     assert_close(f, mv, fo, mvo, sol, dtype,
                  fp64_truth(p, f0, sol, 12, 6) if dtype == np.float32 else None)
+
+
+@pytest.mark.parametrize("nsubs", [1, 2])
+@pytest.mark.parametrize("dims,shape", [(3, (1, 5, 7)), (3, (2, 9, 5)), (3, (3, 11, 3)),
+                                        (2, (1, 37, 1)), (2, (2, 19, 1))])
+def test_gpu_compact_narrow_x_extents(dims, shape, nsubs):
+    """Lattices one to three nodes wide in x with nodes 0 and N - 1 fluid:
+    every node sits on an x edge (the odd step's wrapped x neighbours) and
+    the neighbour lookups read the first and last words of the fluid-rank
+    table.  FP64, compact layout, against the oracle."""
+    LX, LY, LZ = shape
+    p = po.Params(dims=dims, LX=LX, LY=LY, LZ=LZ, nsubs=nsubs, tau=(0.9, 0.7),
+                  sink=1e-3 if nsubs == 2 else 0.0, sigma_t_on=2, sigma_t_off=1000,
+                  gaccel=(2e-5, -1e-5, 3e-6 if dims == 3 else 0.0, 0, 0, 0))
+    rng = np.random.default_rng(LX * 100 + LY + nsubs)
+    sol = (rng.random(p.NN) < 0.3).astype(np.uint8)
+    sol[0] = sol[-1] = 0
+    Q = 19 if dims == 3 else 9
+    f0 = rng.standard_normal((nsubs, Q, p.NN)) * 1e-4
+    if nsubs == 2:
+        f0[1] = np.abs(f0[1]) * 10
+    f, mv, info = run_gpu(p, f0, sol, 12, 6, np.float64, "compact")
+    assert info["layout"] == "compact"
+    fo, mvo = _oracle(p, f0, sol, 12, 6)
+    assert_close(f, mv, fo, mvo, sol, np.float64)
