@@ -798,11 +798,17 @@ lbx_status lbx_upload_f(lbx_domain* d, int subs, const void* f_host)
   if (lbx_status st = check_subs(d, subs)) return st;
   if (!f_host) return fail(LBX_ERR_INVALID, "f_host is NULL");
   const size_t bytes = (size_t)d->Q * d->N * d->real_size;
-  if (d->dense_stale) { if (lbx_status st = exchange(d, false)) return st; }
+  // the other substance's dense copy must be current before the gather; a
+  // single substance is overwritten whole, so its stale copy is not brought
+  // back first
+  if (d->dense_stale && d->p.nsubs > 1) {
+    if (lbx_status st = exchange(d, false)) return st;
+  }
   CK(cudaMemcpyAsync((char*)d->f + subs * bytes, f_host, bytes, cudaMemcpyHostToDevice,
                      d->stream));
   if (lbx_status st = exchange(d, true)) return st;
   CK(cudaStreamSynchronize(d->stream));
+  d->dense_stale = false;   // the compact state was just gathered from it
   d->parity = 0;
   return LBX_OK;
 }

@@ -360,3 +360,43 @@ def test_gpu_compact_narrow_x_extents(dims, shape, nsubs):
     assert info["layout"] == "compact"
     fo, mvo = _oracle(p, f0, sol, 12, 6)
     assert_close(f, mv, fo, mvo, sol, np.float64)
+
+
+@pytest.mark.parametrize("nsubs", [1, 2])
+def test_gpu_upload_into_a_stepped_domain(nsubs):
+    """Uploading populations after steps replaces them: all of one
+    substance equals a fresh domain bit for bit; one substance of two keeps
+    the other's stepped state (the oracle, stepped and replaced the same
+    way).  Compact layout, FP64."""
+    p = po.Params(dims=3, LX=18, LY=14, LZ=12, nsubs=nsubs, tau=(0.9, 0.7),
+                  sink=1e-3 if nsubs == 2 else 0.0, sigma_t_on=2, sigma_t_off=1000,
+                  gaccel=(2e-5, 0, 0, 0, 0, 0))
+    sol = geometry.sphere_pack(18, 14, 12, radius=3, porosity=0.5, seed=5)
+    rng = np.random.default_rng(8)
+    f0 = rng.standard_normal((nsubs, 19, p.NN)) * 1e-4
+    f1 = rng.standard_normal((nsubs, 19, p.NN)) * 1e-4
+    if nsubs == 2:
+        f0[1] = np.abs(f0[1]) * 10
+        f1[1] = np.abs(f1[1]) * 10
+    lp = to_lbx(p, np.float64, "compact")
+    with lbx.Domain(lp, sol) as d:
+        d.upload_f(f0)
+        d.run(0, 6, 6)
+        if nsubs == 1:
+            d.upload_f(f1)
+        else:
+            d.upload_f(f1[1], subs=1)
+        d.run(6, 6, 6)
+        d.sync()
+        f = d.download_f()
+    if nsubs == 1:
+        with lbx.Domain(lp, sol) as d:
+            d.upload_f(f1)
+            d.run(0, 6, 6)
+            d.sync()
+            np.testing.assert_array_equal(f, d.download_f())
+    else:
+        fo, _ = po.run_oracle(p, f0.copy(), sol, 0, 6, 6)
+        fo[1] = f1[1]
+        fo, _ = po.run_oracle(p, fo, sol, 6, 6, 6)
+        assert rel_err(f, fo) < 1e-12
