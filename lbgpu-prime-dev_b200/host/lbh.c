@@ -194,6 +194,7 @@ int lbh_read_bmp_mask(const char* path, int LX, int LY, uint8_t* out, char* err,
   row = 3 * w;
   pad = (4 - row % 4) % 4;
   line = (unsigned char*)malloc((size_t)(row + pad));
+  if (!line) { fclose(in); seterr(err, errlen, "out of host memory reading", path); return -1; }
   /* pixel data follows the 54-byte header; rows bottom-up as stored */
   for (j = 0; j < h; j++) {
     size_t got = fread(line, 1, (size_t)(row + pad), in);
@@ -227,6 +228,7 @@ int lbh_write_bmp_mask(const char* path, int LX, int LY, const uint8_t* mask)
   unsigned char hdr[54];
   int row = 3 * LX, pad = (4 - row % 4) % 4, i, j;
   unsigned char* line = (unsigned char*)calloc(1, (size_t)(row + pad));
+  if (!line) return -1;
   memset(hdr, 0, sizeof hdr);
   hdr[0] = 'B'; hdr[1] = 'M';
   put32(hdr + 2, 54u + (unsigned)(row + pad) * (unsigned)LY);
