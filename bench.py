@@ -131,9 +131,10 @@ def make_mask():
     return geometry.sphere_pack(N_EDGE, N_EDGE, N_EDGE, RADIUS, POROSITY, SEED)
 
 
-def cpu_baseline(mask, steps: int = 4) -> dict:
-    """The reference's kernels on the host cores (bounded sample), else the
-    oracle port."""
+def cpu_baseline(mask, seconds: float = 10.0, max_steps: int = 64) -> dict:
+    """The reference's kernels on the host cores, else the oracle port: AA
+    step pairs of the full lattice until `seconds` have passed (bounded by
+    `max_steps`)."""
     import pyoracle as po
     p = po.Params(dims=3, LX=N_EDGE, LY=N_EDGE, LZ=N_EDGE, tau=(TAU, 1.0),
                   gaccel=(GX, 0, 0, 0, 0, 0))
@@ -143,18 +144,22 @@ def cpu_baseline(mask, steps: int = 4) -> dict:
         kind = "reference"
         po.run_reference("d3q19_f32", p, f, mask, 0, 0)   # load the library
         po._refs["d3q19_f32"].refk_set_threads(cores)
-        t0 = time.perf_counter()
-        po.run_reference("d3q19_f32", p, f, mask, 0, steps)
-        dt = time.perf_counter() - t0
+        pair = lambda t: po.run_reference("d3q19_f32", p, f, mask, t, 2)
     else:
         kind = "port"
-        t0 = time.perf_counter()
-        po.run_oracle(p, f, mask, 0, steps, threads=cores)
+        pair = lambda t: po.run_oracle(p, f, mask, t, 2, threads=cores)
+    steps = 0
+    t0 = time.perf_counter()
+    while True:
+        pair(steps)
+        steps += 2
         dt = time.perf_counter() - t0
+        if dt >= seconds or steps >= max_steps:
+            break
     return {"value": round(p.NN * steps / dt / 1e6, 3), "unit": "MLUPS", "cores": cores,
             "kind": kind,
-            "sample": "%d lattice steps of the full %d^3 workload, FP32, %s threads"
-                      % (steps, N_EDGE, cores)}
+            "sample": "%d lattice steps (%.1f s) of the full %d^3 workload, FP32, %s threads"
+                      % (steps, dt, N_EDGE, cores)}
 
 
 def reference_arm(args, rank: int, world: int):
