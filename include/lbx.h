@@ -211,9 +211,12 @@ lbx_status lbx_reduce(lbx_domain* d, lbx_reductions* out);
  * default stream) and the call waits for it.  Scratch lives in a fixed array
  * inside the library (384 KiB, held on every GPU that loads the library
  * until exit), so N is limited to 67,108,864 nodes (LBX_ERR_INVALID beyond).
- * The first call on a device looks up that array's device address; make it
- * before any stream capture.  Calls share the array: calls that overlap on
- * the GPU race.  Allocates nothing: no cudaMalloc, cudaFree or allocating
+ * The first call in a CUDA context (the device's primary context, or a
+ * driver-API context the caller made current) looks up that array's device
+ * address and keeps it for the context; make it before any stream capture.
+ * A cudaDeviceReset between calls is not supported: the kept address would
+ * outlive the context it belongs to.  Calls share the array: calls that
+ * overlap on the GPU race.  Allocates nothing: no cudaMalloc, cudaFree or allocating
  * library call. */
 lbx_status lbx_reduce_mv_static(const void* mv, const uint8_t* solids,
                                 long long N, int dims, int nsubs, int precision,
@@ -249,7 +252,9 @@ lbx_status lbx_frame_stats_compute(lbx_domain* d, int subs, lbx_frame_stats* out
  * stay valid until the second lbx_frame_enqueue after the wait.  At most
  * two frames are outstanding (LBX_ERR_STATE beyond); lbx_frame_wait with
  * none outstanding is LBX_ERR_STATE.  The first enqueue allocates two
- * device and two host buffers of the macro variables' size. */
+ * device and three host buffers of the macro variables' size (the third
+ * keeps a returned frame's view alive through the next enqueue when two
+ * frames were outstanding at its wait). */
 typedef struct lbx_frame {
   int time;
   int nsubs;

@@ -149,8 +149,12 @@ __global__ void frame_final(const FramePart* __restrict__ part, int nparts, int 
 // a scratch statistics slot for lbx_frame_stats_compute.
 struct Frames {
   size_t bytes = 0;                       // the macro variables of every substance
-  void* snap[2] = {nullptr, nullptr};     // device snapshots
-  void* host[2] = {nullptr, nullptr};     // page-locked host copies
+  void* snap[2] = {nullptr, nullptr};     // device snapshots, by queued % 2
+  // page-locked host copies, by queued % 3: a frame's buffer is reused by the
+  // third enqueue after its own, which needs its successor waited first, so
+  // a returned frame's buffer outlives the first enqueue after its wait even
+  // when two frames were outstanding
+  void* host[3] = {nullptr, nullptr, nullptr};
   lbx_frame_stats* st_dev = nullptr;      // [3][2]: slots 0, 1 and scratch 2
   lbx_frame_stats* st_host = nullptr;     // [3][2] page-locked
   FramePart* part = nullptr;              // [kBlocks]
@@ -158,6 +162,7 @@ struct Frames {
   cudaEvent_t taken[2] = {nullptr, nullptr};   // snapshot and statistics queued
   cudaEvent_t landed[2] = {nullptr, nullptr};  // host copies complete
   int time[2] = {0, 0};
+  int hslot[2] = {0, 0};                  // host buffer of the frame in each slot
   long long queued = 0, waited = 0;       // frames enqueued / returned
 };
 
@@ -209,10 +214,10 @@ void lbx_internal_frames_free(lbx_domain* d)
   if (F->copy) cudaStreamSynchronize(F->copy);
   for (int k = 0; k < 2; ++k) {
     cudaFree(F->snap[k]);
-    cudaFreeHost(F->host[k]);
     if (F->taken[k]) cudaEventDestroy(F->taken[k]);
     if (F->landed[k]) cudaEventDestroy(F->landed[k]);
   }
+  for (int k = 0; k < 3; ++k) cudaFreeHost(F->host[k]);
   cudaFree(F->st_dev);
   cudaFreeHost(F->st_host);
   cudaFree(F->part);
@@ -250,25 +255,30 @@ lbx_status lbx_frame_enqueue(lbx_domain* d, int time)
     FCK(cudaStreamCreateWithFlags(&F->copy, cudaStreamNonBlocking));
     for (int k = 0; k < 2; ++k) {
       FCK(cudaMalloc(&F->snap[k], bytes));
-      FCK(cudaHostAlloc(&F->host[k], bytes, cudaHostAllocDefault));
       FCK(cudaEventCreateWithFlags(&F->taken[k], cudaEventDisableTiming));
       FCK(cudaEventCreateWithFlags(&F->landed[k], cudaEventDisableTiming));
     }
+    for (int k = 0; k < 3; ++k) FCK(cudaHostAlloc(&F->host[k], bytes, cudaHostAllocDefault));
   }
   if (lbx_status st = alloc_stats(F)) return st;
   const int k = (int)(F->queued & 1);
-  // The slot's previous frame was returned by lbx_frame_wait, which waited
-  // for its host copy, so its snapshot and host buffers are free.
+  const int h = (int)(F->queued % 3);
+  // The slot's previous frame (queued - 2) was returned by lbx_frame_wait,
+  // which waited for its host copy, so its snapshot is free.  Host buffer h
+  // last held frame queued - 3, returned before frame queued - 2 was, and
+  // the caller was told that its view ends at the second enqueue after its
+  // wait, which this one is at the earliest.
   for (int s = 0; s < d->p.nsubs; ++s)
     if (lbx_status st = queue_stats(d, F, s, F->st_dev + 2 * k + s)) return st;
   FCK(cudaMemcpyAsync(F->snap[k], d->mv, bytes, cudaMemcpyDeviceToDevice, d->stream));
   FCK(cudaEventRecord(F->taken[k], d->stream));
   FCK(cudaStreamWaitEvent(F->copy, F->taken[k], 0));
-  FCK(cudaMemcpyAsync(F->host[k], F->snap[k], bytes, cudaMemcpyDeviceToHost, F->copy));
+  FCK(cudaMemcpyAsync(F->host[h], F->snap[k], bytes, cudaMemcpyDeviceToHost, F->copy));
   FCK(cudaMemcpyAsync(F->st_host + 2 * k, F->st_dev + 2 * k, 2 * sizeof(lbx_frame_stats),
                       cudaMemcpyDeviceToHost, F->copy));
   FCK(cudaEventRecord(F->landed[k], F->copy));
   F->time[k] = time;
+  F->hslot[k] = h;
   F->queued++;
   return LBX_OK;
 }
@@ -285,7 +295,7 @@ lbx_status lbx_frame_wait(lbx_domain* d, lbx_frame* out)
   out->nsubs = d->p.nsubs;
   const size_t per = (size_t)(1 + d->D) * d->N * d->real_size;
   for (int s = 0; s < d->p.nsubs; ++s) {
-    out->mv[s] = (const char*)F->host[k] + s * per;
+    out->mv[s] = (const char*)F->host[F->hslot[k]] + s * per;
     out->stats[s] = F->st_host[2 * k + s];
   }
   F->waited++;

@@ -12,14 +12,17 @@
 // each, 384 KiB): every GPU that loads this library holds it until the
 // process exits.  Host code
 // must not pass the array's name to a kernel -- on the host that name is
-// only a stand-in, not a device address -- so the first call on each device
-// looks the address up with cudaGetSymbolAddress and keeps it.
+// only a stand-in, not a device address -- so the first call in each CUDA
+// context looks the address up with cudaGetSymbolAddress and keeps it,
+// keyed on that context (a driver-API context on a device has its own copy
+// of the array, at its own address).
 #include "lbx.h"
 #include "lbx_kernels.cuh"
 
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 
 namespace {
@@ -28,14 +31,27 @@ constexpr int kThreads = 256;
 constexpr int kNodesPerBlock = kThreads * 64;          // 16384 nodes per partial
 constexpr int kMaxPartials = 4096;                     // => at most 67,108,864 nodes
 constexpr long long kMaxNodes = (long long)kNodesPerBlock * kMaxPartials;
-constexpr int kMaxDevices = 64;
+constexpr int kMaxContexts = 64;
 
 using lbx::RedPartial;
 
 // Partials of one call, then the final sum in slot kMaxPartials.
 static __device__ __align__(256) RedPartial g_red_scratch[kMaxPartials + 1];
 
-RedPartial* g_scratch_addr[kMaxDevices];              // per device, set on first use
+// The array's device address per CUDA context, filled on first use in that
+// context; guarded by g_addr_mu (two host threads may make their first calls
+// at once).
+struct ScratchAddr {
+  void* ctx;
+  RedPartial* addr;
+};
+ScratchAddr g_addr[kMaxContexts];
+int g_naddr = 0;
+std::mutex g_addr_mu;
+
+// cuCtxGetCurrent, fetched through the runtime so that the library does not
+// link the driver library itself.
+typedef int (*CtxGetCurrentFn)(void**);
 
 }  // namespace
 
@@ -151,19 +167,40 @@ extern "C" lbx_status lbx_reduce_mv_static(const void* mv, const uint8_t* solids
     return sfail(LBX_ERR_INVALID,
                  "N = %lld exceeds the %lld nodes the static scratch (%d partials of %d "
                  "nodes) covers", N, kMaxNodes, kMaxPartials, kNodesPerBlock);
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) return sfail(LBX_ERR_CUDA, "cudaGetDevice: %s", cudaGetErrorString(e));
-  if (dev < 0 || dev >= kMaxDevices) return sfail(LBX_ERR_INVALID, "device %d out of range", dev);
-  if (!g_scratch_addr[dev]) {
-    // set-up, once per device, with that device current
+  // set-up, once per context, with the caller's device current
+  cudaError_t e;
+  static CtxGetCurrentFn ctx_current = [] {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      fn = nullptr;
+    return (CtxGetCurrentFn)fn;
+  }();
+  if (!ctx_current) return sfail(LBX_ERR_CUDA, "cuCtxGetCurrent is not available");
+  void* ctx = nullptr;
+  if (ctx_current(&ctx) != 0) return sfail(LBX_ERR_CUDA, "cuCtxGetCurrent failed");
+  if (!ctx) {
+    // no context bound to this thread yet: the runtime binds the current
+    // device's primary context on its first call that needs one
     RedPartial* p = nullptr;
     e = cudaGetSymbolAddress((void**)&p, g_red_scratch);
-    if (e != cudaSuccess || !p)
+    if (e != cudaSuccess)
       return sfail(LBX_ERR_CUDA, "cudaGetSymbolAddress: %s", cudaGetErrorString(e));
-    g_scratch_addr[dev] = p;
+    if (ctx_current(&ctx) != 0 || !ctx) return sfail(LBX_ERR_CUDA, "no current CUDA context");
   }
-  RedPartial* scratch = g_scratch_addr[dev];
+  RedPartial* scratch = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(g_addr_mu);
+    for (int i = 0; i < g_naddr; ++i)
+      if (g_addr[i].ctx == ctx) scratch = g_addr[i].addr;
+    if (!scratch) {
+      e = cudaGetSymbolAddress((void**)&scratch, g_red_scratch);
+      if (e != cudaSuccess || !scratch)
+        return sfail(LBX_ERR_CUDA, "cudaGetSymbolAddress: %s", cudaGetErrorString(e));
+      if (g_naddr < kMaxContexts) g_addr[g_naddr++] = ScratchAddr{ctx, scratch};
+    }
+  }
   cudaStream_t st = (cudaStream_t)stream;
   const int nparts = (int)((N + kNodesPerBlock - 1) / kNodesPerBlock);
   if (precision == 8) {

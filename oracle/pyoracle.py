@@ -23,6 +23,16 @@ ORACLE_SO = os.path.join(HERE, "liblbx_oracle.so")
 REF_DIR = os.path.join(HERE, "_ref")
 
 
+def reference_root() -> str:
+    """The reference project's checkout (present only where the reference-side
+    checker is built): $LBX_REFERENCE_ROOT, else a directory named
+    `reference` beside this repository."""
+    env = os.environ.get("LBX_REFERENCE_ROOT")
+    if env:
+        return env
+    return os.path.normpath(os.path.join(HERE, "..", "..", "reference"))
+
+
 @dataclass
 class Params:
     """Run parameters, named as in the reference's params.in."""

@@ -32,7 +32,18 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_ref")
-DEFAULT_SRC = "/root/reference/src"
+
+
+def reference_root() -> str:
+    """The reference project's checkout: $LBX_REFERENCE_ROOT, else a directory
+    named `reference` beside this repository."""
+    env = os.environ.get("LBX_REFERENCE_ROOT")
+    if env:
+        return env
+    return os.path.normpath(os.path.join(HERE, "..", "..", "reference"))
+
+
+DEFAULT_SRC = os.path.join(reference_root(), "src")
 
 # name -> flags.h overrides.  PEST output is off except in the *_pest
 # variants: with it on and no PEST input files the reference dereferences a

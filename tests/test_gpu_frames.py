@@ -78,3 +78,31 @@ def test_gpu_frame_pipeline_returns_each_frame_state():
         for c in range(4):
             assert rel_err(g["mv"][0, c][fluid], mv[0, c][fluid]) <= 1e-5, (k, c)
         check_stats(g["stats"][0], po.frame_stats(g["mv"][0], sol, 3))
+
+
+def test_gpu_frame_view_survives_the_next_enqueue():
+    """A frame returned with copy=False while a second frame is outstanding
+    keeps its values through the next enqueue (the header promises them
+    until the second enqueue after the wait)."""
+    n = 32
+    lp = lbx.Params(dims=3, LX=n, LY=n, LZ=n, precision=4, tau=(0.8, 1.0),
+                    gaccel=(1e-5, 0, 0, 0, 0, 0))
+    sol = geometry.sphere_pack(n, n, n, radius=4, porosity=0.5, seed=9)
+    f0 = (np.random.default_rng(5).standard_normal((1, 19, lp.NN)) * 1e-4).astype(np.float32)
+    fr = 4
+    with lbx.Domain(lp, sol) as d:
+        d.upload_f(f0)
+        d.run(0, fr, fr)
+        d.frame_enqueue(fr)                       # A
+        d.run(fr, fr, fr)
+        d.frame_enqueue(2 * fr)                   # B: two outstanding
+        a = d.frame_wait(copy=False)
+        a_copy = a["mv"].copy()
+        d.run(2 * fr, fr, fr)
+        d.frame_enqueue(3 * fr)                   # C: the first enqueue after A's wait
+        b = d.frame_wait(copy=True)
+        c = d.frame_wait(copy=False)              # C's host copy has landed
+        assert (a["time"], b["time"], c["time"]) == (fr, 2 * fr, 3 * fr)
+        assert np.array_equal(a["mv"], a_copy)
+        assert not np.array_equal(b["mv"], a_copy)
+        assert not np.array_equal(c["mv"], a_copy)

@@ -14,7 +14,7 @@ import pyoracle as po
 from lbx import host
 from _host_files import write_params
 
-REF_IN = "/root/reference/in"
+REF_IN = os.path.join(po.reference_root(), "in")
 
 
 VALUES = {

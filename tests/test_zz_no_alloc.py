@@ -70,9 +70,14 @@ def test_static_reduce_matches_allocating_reduce(dims, nsubs, precision, shape):
         sol_dev = torch.from_numpy(sol).cuda()
         torch.cuda.synchronize()
         r = lbx._CReductions()
+        free0 = torch.cuda.mem_get_info()[0]
         rc = fn(mv_dev.data_ptr(), sol_dev.data_ptr(), N, dims, nsubs, precision,
                 stream, C.byref(r))
         assert rc == lbx.LBX_OK, lbx._lib.lbx_last_error()
+        if call == 1:
+            # the first call may load the library's module onto the device;
+            # after that a call takes no device memory
+            assert torch.cuda.mem_get_info()[0] == free0
         _close(_as_dict(r), want)
 
 
