@@ -260,31 +260,27 @@ int lbh_write_raw_mask(const char* path, long long N, const uint8_t* mask)
 }
 
 /* ---- initial density (src/latman.c:1319-1632, serial build) -------------- */
+/* Only the uniform (0) and cube (2) cases are compiled in the reference; its
+ * random (1) and sphere (3) cases sit inside #if 0, so init_problem prints
+ * "Unhandled case" and exits for them (src/latman.c:1340-1376, :1507-1630),
+ * and so does this function return -1. */
 int lbh_initial_rho(const lbh_params* p, int dims, int nsubs, int subs, double* rho)
 {
   long long n;
   const int LX = p->LX, LY = p->LY;
+  if (p->initial_condition != 0 && p->initial_condition != 2) return -1;
   for (n = 0; n < p->NumNodes; n++) {
     const int i = (int)(n % LX), j = (int)((n / LX) % LY), k = (int)(n / ((long long)LX * LY));
     const int in_box = i >= p->x1 && i <= p->x2 && j >= p->y1 && j <= p->y2 &&
                        (dims == 2 || (k >= p->z1 && k <= p->z2));
-    const long long dx = i - p->x0, dy = j - p->y0, dz = k - p->z0;
-    const int in_ball = dx * dx + dy * dy + dz * dz <= (long long)p->r0 * p->r0;
-    switch (p->initial_condition) {
-      case 0:
-        rho[n] = (nsubs == 2 && subs == 1) ? p->rho_A[1].d : p->rho_A[subs].d;
-        break;
-      case 2:
-        if (nsubs == 1) rho[n] = in_box ? p->rho_B[0].d : p->rho_A[0].d;
-        else if (subs == 0) rho[n] = p->rho_A[0].d;
-        else rho[n] = in_box ? p->rho_sigma.d : 0.;
-        break;
-      case 3:
-        rho[n] = in_ball ? p->rho_A[subs].d : p->rho_B[subs].d;
-        break;
-      default:
-        return -1;
-    }
+    if (p->initial_condition == 0)
+      rho[n] = p->rho_A[subs].d;
+    else if (nsubs == 1)
+      rho[n] = in_box ? p->rho_B[0].d : p->rho_A[0].d;
+    else if (subs == 0)
+      rho[n] = p->rho_A[0].d;
+    else
+      rho[n] = in_box ? p->rho_sigma.d : 0.;
   }
   return 0;
 }

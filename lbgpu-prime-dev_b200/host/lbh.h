@@ -178,9 +178,10 @@ int lbh_walsh_ns(double ns_value, int source, const uint8_t* mask, long long N,
 int lbh_write_bmp_mask(const char* path, int LX, int LY, const uint8_t* mask);
 int lbh_write_raw_mask(const char* path, long long N, const uint8_t* mask);
 
-/* Initial density of substance `subs` per initial_condition 0 (uniform),
- * 2 (cube) or 3 (sphere) of init_problem (src/latman.c:1319-1632).
- * rho: N doubles.  Returns 0, or -1 for an unsupported condition. */
+/* Initial density of substance `subs` per initial_condition 0 (uniform) or
+ * 2 (cube) of init_problem (src/latman.c:1319-1632).  rho: N doubles.
+ * Returns 0, or -1 for any other condition (the reference compiles only
+ * these two and exits on the others). */
 int lbh_initial_rho(const lbh_params* p, int dims, int nsubs, int subs,
                     double* rho);
 

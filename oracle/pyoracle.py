@@ -507,3 +507,72 @@ def reference_pest_inputs(variant: str, LX: int, LY: int, LZ: int, workdir: str)
     finally:
         os.chdir(here)
     return tuple(a[:kept] for a in arrs)
+
+
+class _RefInit(C.Structure):
+    _fields_ = [("initial_condition", C.c_int), ("rho_A", C.c_double * 2),
+                ("rho_B", C.c_double * 2), ("rho_sigma", C.c_double),
+                ("x1", C.c_int), ("x2", C.c_int), ("y1", C.c_int), ("y2", C.c_int),
+                ("z1", C.c_int), ("z2", C.c_int)]
+
+
+def reference_init_problem(variant: str, LX: int, LY: int, LZ: int, initial_condition: int,
+                           rho_A=(1.0, 0.0), rho_B=(1.0, 0.0), rho_sigma: float = 0.0,
+                           box=(0, -1, 0, -1, 0, -1)):
+    """The reference's init_problem (src/latman.c:1270-2063) through the
+    harness: (f [subs][Q][N], mv [subs][1+D][N]) in the variant's precision,
+    or None without the harness.  Only initial_condition 0 and 2 exist in the
+    reference (it exits on any other value); others raise ValueError here."""
+    if not reference_available(variant):
+        return None
+    if variant not in _refs:
+        _refs[variant] = C.CDLL(os.path.join(REF_DIR, "librefk_%s.so" % variant))
+    lib = _refs[variant]
+    lib.refk_real_size.restype = C.c_int
+    dims, nsubs = lib.refk_num_dims(), lib.refk_num_subs()
+    Q = 9 if dims == 2 else 19
+    dt = np.float64 if lib.refk_real_size() == 8 else np.float32
+    NN = LX * LY * LZ
+    f = np.zeros((nsubs, Q, NN), dt)
+    mv = np.zeros((nsubs, 1 + dims, NN), dt)
+    ip = _RefInit(initial_condition, (C.c_double * 2)(*rho_A), (C.c_double * 2)(*rho_B),
+                  rho_sigma, *box)
+    lib.refk_init_problem.restype = C.c_int
+    rc = lib.refk_init_problem(LX, LY, LZ, C.byref(ip), f.ctypes.data_as(C.c_void_p),
+                               mv.ctypes.data_as(C.c_void_p))
+    if rc != 0:
+        raise ValueError("initial_condition %d: the reference exits" % initial_condition)
+    return f, mv
+
+
+def reference_init_from_params(variant: str, path: str):
+    """The reference's start-up path on a params.in: read_params
+    (src/params.h:40-660) then init_problem (src/latman.c:1270-2063), through
+    the harness.  (f [subs][Q][N], mv [subs][1+D][N]) in the variant's
+    precision, or None without the harness; ValueError for an
+    initial_condition the reference exits on."""
+    if not reference_available(variant):
+        return None
+    if variant not in _refs:
+        _refs[variant] = C.CDLL(os.path.join(REF_DIR, "librefk_%s.so" % variant))
+    lib = _refs[variant]
+    lib.refk_real_size.restype = C.c_int
+    # the extents as this variant's read_params leaves them (a 2D build sets LZ = 1)
+    iout = (C.c_int * 10)()
+    dout = (C.c_double * 8)()
+    lib.refk_read_params(path.encode(), iout, dout)
+    rp = {"LX": iout[0], "LY": iout[1], "LZ": iout[2], "initial_condition": iout[5]}
+    dims, nsubs = lib.refk_num_dims(), lib.refk_num_subs()
+    Q = 9 if dims == 2 else 19
+    dt = np.float64 if lib.refk_real_size() == 8 else np.float32
+    NN = rp["LX"] * rp["LY"] * rp["LZ"]
+    f = np.zeros((nsubs, Q, NN), dt)
+    mv = np.zeros((nsubs, 1 + dims, NN), dt)
+    lib.refk_init_from_params.restype = C.c_int
+    rc = lib.refk_init_from_params(path.encode(), NN, f.ctypes.data_as(C.c_void_p),
+                                   mv.ctypes.data_as(C.c_void_p))
+    if rc == -1:
+        raise ValueError("initial_condition %d: the reference exits" % rp["initial_condition"])
+    if rc != 0:
+        raise ValueError("refk_init_from_params failed (%d)" % rc)
+    return f, mv

@@ -98,10 +98,10 @@ int cumul_stride[20];
 #include "process.c"
 #include "lbio.c"
 #include "compute.c"
-#if PEST_OUTPUT_ON
-/* PEST point sampling lives in src/latman.c, whose other functions set up
- * the device; their CUDA calls compile to no-ops here (never run), and a
- * copy to a __constant__ symbol becomes a copy to the host global. */
+/* init_problem and the PEST point sampling live in src/latman.c, whose
+ * other functions set up the device; their CUDA calls compile to no-ops here
+ * (never run), and a copy to a __constant__ symbol becomes a copy to the host
+ * global. */
 #define cudaMalloc(p, n) 0
 #define cudaFree(p) 0
 #define cudaFreeHost(p) 0
@@ -112,7 +112,6 @@ int f_mem_size, mv_mem_size, solids_mem_size;
 real *f_mem_d, *mv_mem_d, *ns_mem_d;
 unsigned char* solids_mem_d;
 #include "latman.c"
-#endif
 #include "system_boundary_kernels.c"
 #include "k_stream_collide_stream.c"
 #include "k_collide.c"
@@ -534,6 +533,91 @@ EXPORT int refk_output_frame(int LX, int LY, int LZ, const real* mv, const unsig
   for (s = 0; s < NUM_FLUID_COMPONENTS; s++) {
     free(l->vars[s].macrovars1d);
     free(l->vars[s].macrovars_memblock);
+  }
+  free(l->vars); free(l->solids_memblock); free(l);
+  return 0;
+}
+
+/* ---- the reference's initial state -------------------------------------------
+ * init_problem (src/latman.c:1270-2063) on a harness lattice: the density of
+ * every node per initial_condition (0 uniform, 2 cube; the others exit, as
+ * in the reference), u = 0, and f = feq (shifted for the flow lattice of an
+ * ACCURATE build).  f ([subs][Q][N]) and mv ([subs][1+D][N]) are written. */
+typedef struct {
+  int initial_condition;
+  double rho_A[2], rho_B[2], rho_sigma;
+  int x1, x2, y1, y2, z1, z2;
+} refk_init;
+
+EXPORT int refk_init_problem(int LX, int LY, int LZ, const refk_init* ip, real* f, real* mv)
+{
+  struct lattice_struct* l = harness_lattice(LX, LY, LZ);
+  const int D = NUM_DIMENSIONS, Qd = 2 * D * D + 1, NN = LX * LY * LZ;
+  int s, a, c;
+  if (ip->initial_condition != 0 && ip->initial_condition != 2) return -1;
+  l->NumDims = D;
+  l->NumSubs = NUM_FLUID_COMPONENTS;
+  l->NumVelDirs = Qd;
+  l->param.initial_condition = ip->initial_condition;
+  for (s = 0; s < NUM_FLUID_COMPONENTS; s++) {   /* the arrays hold one entry per substance */
+    l->param.rho_A[s] = (real)ip->rho_A[s];
+    l->param.rho_B[s] = (real)ip->rho_B[s];
+  }
+#if INAMURO_SIGMA_COMPONENT
+  l->param.rho_sigma = (real)ip->rho_sigma;
+#endif
+  l->param.x1 = ip->x1; l->param.x2 = ip->x2;
+  l->param.y1 = ip->y1; l->param.y2 = ip->y2;
+  l->param.z1 = ip->z1; l->param.z2 = ip->z2;
+  l->vars = (struct vars_struct*)calloc(NUM_FLUID_COMPONENTS, sizeof *l->vars);
+  for (s = 0; s < NUM_FLUID_COMPONENTS; s++) {
+    l->vars[s].f1d = (real**)malloc((size_t)Qd * sizeof(real*));
+    for (a = 0; a < Qd; a++) l->vars[s].f1d[a] = f + ((size_t)s * Qd + a) * NN;
+    l->vars[s].macrovars1d = (real**)malloc((size_t)(1 + D) * sizeof(real*));
+    for (c = 0; c <= D; c++) l->vars[s].macrovars1d[c] = mv + ((size_t)s * (1 + D) + c) * NN;
+  }
+  init_problem(l);
+  for (s = 0; s < NUM_FLUID_COMPONENTS; s++) {
+    free(l->vars[s].f1d);
+    free(l->vars[s].macrovars1d);
+  }
+  free(l->vars); free(l->solids_memblock); free(l);
+  return 0;
+}
+
+/* read_params (src/params.h:40-660, derived values and defaults included)
+ * on `path`, then init_problem: the reference's whole start-up path.  The
+ * caller sizes f ([subs][Q][N]) and mv ([subs][1+D][N]) from the file's
+ * extents; `cap` is the N they hold (-2 if the file's lattice is larger;
+ * -1 for an initial_condition the reference exits on). */
+EXPORT int refk_init_from_params(const char* path, int cap, real* f, real* mv)
+{
+  struct lattice_struct* l = harness_lattice(1, 1, 1);
+  const int D = NUM_DIMENSIONS, Qd = 2 * D * D + 1;
+  int s, a, c, NN;
+  read_params(l, (char*)path);
+  NN = l->param.LX * l->param.LY * l->param.LZ;
+  if (NN > cap) { free(l->solids_memblock); free(l); return -2; }
+  if (l->param.initial_condition != 0 && l->param.initial_condition != 2) {
+    free(l->solids_memblock); free(l); return -1;
+  }
+  free(l->solids_memblock);
+  l->solids_memblock = (unsigned char*)calloc((size_t)NN, 1);
+  l->NumNodes = NN;
+  l->NumDims = D;
+  l->NumSubs = NUM_FLUID_COMPONENTS;
+  l->NumVelDirs = Qd;
+  l->vars = (struct vars_struct*)calloc(NUM_FLUID_COMPONENTS, sizeof *l->vars);
+  for (s = 0; s < NUM_FLUID_COMPONENTS; s++) {
+    l->vars[s].f1d = (real**)malloc((size_t)Qd * sizeof(real*));
+    for (a = 0; a < Qd; a++) l->vars[s].f1d[a] = f + ((size_t)s * Qd + a) * NN;
+    l->vars[s].macrovars1d = (real**)malloc((size_t)(1 + D) * sizeof(real*));
+    for (c = 0; c <= D; c++) l->vars[s].macrovars1d[c] = mv + ((size_t)s * (1 + D) + c) * NN;
+  }
+  init_problem(l);
+  for (s = 0; s < NUM_FLUID_COMPONENTS; s++) {
+    free(l->vars[s].f1d);
+    free(l->vars[s].macrovars1d);
   }
   free(l->vars); free(l->solids_memblock); free(l);
   return 0;

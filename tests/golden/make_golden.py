@@ -7,6 +7,7 @@ reference tree is available); the fixtures are committed so the tests need
 neither the reference nor the harness.
 
     python tests/golden/make_golden.py [name ...]
+    python tests/golden/make_golden.py init [name ...]   (the start-up path)
 """
 import os
 import sys
@@ -124,5 +125,62 @@ def main(only=None):
             print(name + tag, variant, f.dtype, steps, "steps")
 
 
+# ---- the start-up path ---------------------------------------------------------
+# The reference's read_params + init_problem on params.in files that differ in
+# initial_condition (0 uniform, 2 cube), dimensions, substances and model, with
+# explicit and defaulted cube bounds.  Written to tests/golden/init/.
+INIT_DIR = os.path.join(HERE, "init")
+
+
+def init_cases():
+    base2 = {"LX": 12, "LY": 10, "LZ": 1}
+    base3 = {"LX": 10, "LY": 9, "LZ": 8}
+    box2 = {"x1": 3, "x2": 8, "y1": 2, "y2": 5}
+    box3 = {"x1": 2, "x2": 6, "y1": 1, "y2": 4, "z1": 1, "z2": 5}
+    dflt = {"x1": -1, "x2": -1, "y1": -1, "y2": -1, "z1": -1, "z2": -1,
+            "rel_x1": 0.25, "rel_x2": -1.0, "rel_y1": -1.0, "rel_y2": 0.6,
+            "rel_z1": -1.0, "rel_z2": -1.0}
+    ic0 = {"initial_condition": 0}
+    ic2 = {"initial_condition": 2}
+    rho = {"rho_A[0]": 1.003, "rho_B[0]": 1.05}
+    return [
+        ("d2q9_ic0_f64", "d2q9_f64", dict(base2, **ic0, **rho)),
+        ("d2q9_ic2_f64", "d2q9_f64", dict(base2, **ic2, **rho, **box2)),
+        ("d2q9p_ic2_f64", "d2q9p_f64", dict(base2, **ic2, **rho, **dflt)),
+        ("d2q9s_ic0_f64", "d2q9s_f64", dict(base2, **ic0, **rho)),
+        ("d2q9s_ic2_f64", "d2q9s_f64", dict(base2, **ic2, **rho, **box2, rho_sigma=0.8)),
+        ("d3q19_ic2_f64", "d3q19_f64", dict(base3, **ic2, **rho, **box3)),
+        ("d3q19p_ic2_f64", "d3q19p_f64", dict(base3, **ic2, **rho, **dflt)),
+        ("d3q19c_ic2_f64", "d3q19c_f64", dict(base3, **ic2, **rho, **box3)),
+        ("d3q19s_ic0_f64", "d3q19s_f64", dict(base3, **ic0, **rho)),
+        ("d3q19s_ic2_f64", "d3q19s_f64", dict(base3, **ic2, **rho, **box3, rho_sigma=0.6)),
+        ("d3q19_ic2_f32", "d3q19_f32", dict(base3, **ic2, **rho, **box3)),
+        ("d3q19s_ic2_f32", "d3q19s_f32", dict(base3, **ic2, **rho, **box3, rho_sigma=0.6)),
+    ]
+
+
+def make_init(only=None):
+    sys.path.insert(0, os.path.join(ROOT, "lbgpu-prime-dev_b200"))
+    sys.path.insert(0, os.path.dirname(HERE))
+    import tempfile
+    from _host_files import write_params
+    os.makedirs(INIT_DIR, exist_ok=True)
+    for name, variant, values in init_cases():
+        if only and name not in only:
+            continue
+        with tempfile.TemporaryDirectory() as tmp:
+            path = os.path.join(tmp, "params.in")
+            write_params(path, values)
+            text = open(path).read()
+            f, mv = po.reference_init_from_params(variant, path)
+        np.savez_compressed(os.path.join(INIT_DIR, name + ".npz"), params_in=np.array(text),
+                            variant=variant, f=f, mv=mv)
+        print(name, variant, f.shape, f.dtype)
+
+
 if __name__ == "__main__":
-    main(sys.argv[1:] or None)
+    args = sys.argv[1:]
+    if args and args[0] == "init":
+        make_init(args[1:] or None)
+    else:
+        main(args or None)
