@@ -68,13 +68,18 @@ def load_peaks() -> dict:
     return {"hbm_gbs": 6650.0, "source": "fallback"}
 
 
-def load_traffic() -> float | None:
-    """DRAM bytes per launch of the step kernel from the committed ncu summary."""
+def load_traffic() -> dict:
+    """DRAM bytes per launch of the step kernels (mean of the pair, odd,
+    even) from the committed ncu summary of a 256^3 capture."""
     path = os.path.join(ROOT, "profiles", "aa_step_d3q19_f32_256cube.md")
+    out = {"pair": None, "odd": None, "even": None}
     if not os.path.exists(path):
-        return None
-    m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", open(path).read())
-    return float(m.group(1)) if m else None
+        return out
+    text = open(path).read()
+    for key, label in (("pair", "traffic"), ("odd", "traffic_odd"), ("even", "traffic_even")):
+        m = re.search(r"^%s_bytes_per_launch:\s*([0-9.eE+]+)" % label, text, re.M)
+        out[key] = float(m.group(1)) if m else None
+    return out
 
 
 class ClockSampler:
@@ -204,6 +209,56 @@ def reference_arm(args, rank: int, world: int):
     return 0
 
 
+def precision_leg(mask, local: int, steps: int) -> dict:
+    """The rest of the headline metric on the same lattice: FP32 shifted
+    populations against the plain FP64 model (ACCURATE 0, COMPRESSIBLE 1 in
+    the reference, src/lattice.c:2880-2919) at the permeability error FP32
+    costs.  Three runs of `steps` steps from rest (equilibrium at rho = 1):
+    FP32 shifted and FP64 plain timed with CUDA events (seconds long, so the
+    GPU sits at its sustained, power-capped clock; the FP32 run's clocks are
+    sampled), and FP64 shifted as the reference result for the permeability
+    k = nu <u_x> / g_x (superficial mean, FP64 device sums)."""
+    import torch
+    import lbx
+    nu = (TAU - 0.5) / 3.0
+    out = {}
+    for name, prec, acc, comp in (("fp32_shifted", 4, 1, 0), ("fp64_plain", 8, 0, 1),
+                                  ("fp64_shifted", 8, 1, 0)):
+        p = lbx.Params(dims=3, LX=N_EDGE, LY=N_EDGE, LZ=N_EDGE, precision=prec, accurate=acc,
+                       compressible=comp, tau=(TAU, 1.0), gaccel=(GX, 0, 0, 0, 0, 0),
+                       device=local)
+        stream = torch.cuda.Stream()
+        with lbx.Domain(p, mask) as dom:
+            dom.set_stream(stream.cuda_stream)
+            dom.init_equilibrium(0, 1.0, 0.0, 0.0, 0.0)
+            dom.run(0, 8, 0)                           # warm-up (graph capture)
+            dom.init_equilibrium(0, 1.0, 0.0, 0.0, 0.0)
+            torch.cuda.synchronize()
+            sampler = ClockSampler(local) if name == "fp32_shifted" else None
+            if sampler:
+                sampler.start()
+                time.sleep(0.3)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            dom.run(0, steps - 1, 0)
+            dom.step(steps, write_mv=True)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1)
+            clocks = sampler.stop() if sampler else None
+            r = dom.reduce()
+        k = nu * (r["u_sum"][0] / mask.size) / GX      # solid nodes hold u = 0
+        out[name] = {"mlups": round(mask.size * steps / (ms / 1e3) / 1e6, 3),
+                     "ms_per_step": round(ms / steps, 5), "permeability": k}
+        if clocks:
+            out[name]["clocks"] = clocks
+    k64 = out["fp64_shifted"]["permeability"]
+    for v in out.values():
+        v["perm_rel_err_vs_fp64_shifted"] = abs(v["permeability"] - k64) / abs(k64)
+    return out
+
+
 def max_over_ranks(dist, value: float, device) -> float:
     """The maximum of `value` over the ranks of the process group (the
     slowest replica sets the whole job's time); `value` itself without one."""
@@ -274,6 +329,8 @@ def main(argv=None) -> int:
     ap.add_argument("--warmup", type=int, default=4)
     ap.add_argument("--impl", default="lbx", choices=["lbx", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--precision-steps", type=int, default=6000,
+                    help="steps of each run of the FP32-vs-FP64 leg (0: skip it)")
     ap.add_argument("--cpu-table", action="store_true",
                     help="print the host-core timings of the oracle port and of the "
                          "reference's kernels on the 2D case and a 128^3 crop, then exit")
@@ -365,12 +422,16 @@ def main(argv=None) -> int:
         per_kind[kind] = float(np.median(durs))
 
     peaks = load_peaks()
+    traffic = load_traffic()
     alg_bytes = fluid * BYTES_PER_FLUID_UPDATE + NN * FLAG_BYTES_PER_NODE
     achieved = alg_bytes / (ms_step / 1e3) / 1e9
     roofline = {
         "bound": "hbm", "achieved": round(achieved, 1), "peak": peaks["hbm_gbs"],
         "unit": "GB/s", "frac": round(achieved / peaks["hbm_gbs"], 4),
-        "traffic": load_traffic(),
+        "traffic": traffic["pair"],
+        "traffic_by_kind": {"odd": traffic["odd"], "even": traffic["even"]},
+        "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum at 256^3, "
+                          "steady state (profiles/aa_step_d3q19_f32_256cube.md)",
         "peak_source": peaks["source"],
         "kernel": "%s<float,19,1,SHIFTED_INC> (odd and even alternate)"
                   % ("aa_step_compact" if layout == "compact" else "aa_step"),
@@ -412,6 +473,26 @@ def main(argv=None) -> int:
         "roofline": roofline, "clocks": clocks, "e2e": e2e,
         "gpu_launches": launches,
     }
+    if args.precision_steps > 0:
+        prec = precision_leg(mask, local, args.precision_steps)
+        f32, plain = prec["fp32_shifted"], prec["fp64_plain"]
+        line["sustained"] = {
+            "value": f32["mlups"], "unit": "MLUPS", "ms_per_step": f32["ms_per_step"],
+            "steps": args.precision_steps, "clocks": f32.get("clocks"),
+            "note": "FP32 shifted, one lattice, %d steps from rest in one CUDA-event "
+                    "window (seconds long: the power-capped clock)" % args.precision_steps}
+        line["fp64_plain"] = {
+            "value": plain["mlups"], "unit": "MLUPS", "ms_per_step": plain["ms_per_step"],
+            "steps": args.precision_steps,
+            "model": "ACCURATE 0, COMPRESSIBLE 1 (plain compressible BGK), FP64"}
+        line["fp32_over_fp64_plain"] = round(f32["mlups"] / plain["mlups"], 4)
+        line["perm_rel_err"] = f32["perm_rel_err_vs_fp64_shifted"]
+        line["precision"] = {
+            k: {kk: vv for kk, vv in v.items() if kk != "clocks"} for k, v in prec.items()}
+        line["precision"]["note"] = (
+            "permeability k = nu <u_x> / g_x after %d steps from rest; perm_rel_err = "
+            "|k(FP32 shifted) - k(FP64 shifted)| / k(FP64 shifted), the same kernels"
+            % args.precision_steps)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(mask)
     dom.close()

@@ -35,8 +35,16 @@
  *
  * Threads: plain pthreads over node ranges (no OpenMP runtime needed).
  *
- * Compiled twice (REAL = double, and float with -DLBX_ORACLE_F32) by
- * oracle/Makefile into one .so.
+ * Compiled three times by oracle/Makefile into one .so: REAL = double,
+ * float (-DLBX_ORACLE_F32), and double _Complex (-DLBX_ORACLE_CPLX) for
+ * complex-step differentiation (Squire & Trapp, SIAM Review 40, 1998):
+ * with tau, g and the inlet profile given imaginary parts i h v, every
+ * result's imaginary part is h times its directional derivative along v,
+ * exact to rounding because no difference of nearby values is taken.  That
+ * forward-mode (tangent) derivative of the FP64 discrete model is the
+ * independent check of the product's discrete adjoint.  The arithmetic here
+ * is analytic in those parameters (sums, products and divisions; no branch
+ * depends on a value), which the method needs.
  */
 #include <pthread.h>
 #include <stdint.h>
@@ -48,12 +56,25 @@
 #ifdef LBX_ORACLE_F32
 #define REAL float
 #define SFX(name) name##_f32
+#elif defined(LBX_ORACLE_CPLX)
+#define REAL double _Complex
+#define SFX(name) name##_cs
 #else
 #define REAL double
 #define SFX(name) name##_f64
 #endif
 
 typedef REAL real_t;
+
+/* Plane-record sums: FP64 in the real builds; complex in the complex-step
+ * build, whose imaginary parts carry the derivative. */
+#ifdef LBX_ORACLE_CPLX
+typedef double _Complex acc_t;
+#define ACC(x) (x)
+#else
+typedef double acc_t;
+#define ACC(x) ((double)(x))
+#endif
 
 /* Direction order of the reference (src/lbgpu_prime.h:82-84). */
 static const int CX[19] = { 0, 1,-1, 0, 0, 1,-1,-1, 1, 0, 0, 1,-1,-1, 1, 0, 0, 0, 0};
@@ -91,11 +112,20 @@ static void make_ctx(ctx_t* c, const orc_params* p)
     for (; a < 19; a++) c->w[a] = (c->D == 2) ? (real_t)0. : W2;
   }
   for (s = 0; s < 2; s++) {
+#ifdef LBX_ORACLE_CPLX
+    c->tau[s] = p->tau[s] + I * p->d_tau[s];
+    c->inv_tau[s] = 1. / c->tau[s];
+#else
     c->tau[s] = (real_t)p->tau[s];
     c->inv_tau[s] = 1. / (real_t)p->tau[s];   /* src/latman.c:232-235 */
+#endif
     c->rho_A[s] = (real_t)p->rho_A[s];
   }
+#ifdef LBX_ORACLE_CPLX
+  for (a = 0; a < 6; a++) c->g[a] = p->gaccel[a] + I * p->d_gaccel[a];
+#else
   for (a = 0; a < 6; a++) c->g[a] = (real_t)p->gaccel[a];
+#endif
   c->sink = (real_t)p->sink;
 }
 
@@ -576,7 +606,7 @@ enum { F3_PRESSURE = 1, F3_ZEROGRAD = 2, F3_CONSTCON = 3, F3_VELOCITY = 4 };
  * with conc carrying rA */
 static void face3(const ctx_t* c, real_t* fs, const uint8_t* sol, int top,
                   int kind, int second, real_t drho, real_t conc,
-                  const double* profile)
+                  const double* profile, const double* dprofile)
 {
   const orc_params* p = c->p;
   const int k = top ? p->LZ - 1 : 0;
@@ -606,7 +636,14 @@ static void face3(const ctx_t* c, real_t* fs, const uint8_t* sol, int top,
           int a;
           for (a = 0; a < 19; a++)
             if (CZ[a] != (top ? -1 : 1)) known += d[a];
-          X = ((profile ? (real_t)profile[i + (long)p->LX * j] : conc) - known) / wsum;
+          real_t cin = conc;
+          if (profile) cin = (real_t)profile[i + (long)p->LX * j];
+#ifdef LBX_ORACLE_CPLX
+          if (profile && dprofile) cin += I * dprofile[i + (long)p->LX * j];
+#else
+          (void)dprofile;
+#endif
+          X = (cin - known) / wsum;
         }
         for (q = 0; q < 5; q++) d[unk[q]] = c->w[unk[q]] * X;
       }
@@ -628,33 +665,33 @@ static void apply_bcs3(const ctx_t* c, real_t* f, const uint8_t* sol, int t,
     const double rA = shifted ? (double)c->rho_A[s] : 0.;
     if (p->pressure_t_in[s])
       face3(c, fs, sol, 1, F3_PRESSURE, second,
-            (real_t)((double)face_rho(c, s, t, 1, 1, 0, 0) - rA), 0, 0);
+            (real_t)((double)face_rho(c, s, t, 1, 1, 0, 0) - rA), 0, 0, 0);
     if (p->pressure_t_out[s])
       face3(c, fs, sol, 1, F3_PRESSURE, second,
-            (real_t)((double)face_rho(c, s, t, 0, 0, 0, 0) - rA), 0, 0);
+            (real_t)((double)face_rho(c, s, t, 0, 0, 0, 0) - rA), 0, 0, 0);
     if (p->pressure_b_in[s])
       face3(c, fs, sol, 0, F3_PRESSURE, second,
-            (real_t)((double)face_rho(c, s, t, 1, 1, 0, 0) - rA), 0, 0);
+            (real_t)((double)face_rho(c, s, t, 1, 1, 0, 0) - rA), 0, 0, 0);
     if (p->pressure_b_out[s])
       face3(c, fs, sol, 0, F3_PRESSURE, second,
-            (real_t)((double)face_rho(c, s, t, 0, 0, 0, 0) - rA), 0, 0);
+            (real_t)((double)face_rho(c, s, t, 0, 0, 0, 0) - rA), 0, 0, 0);
     if (p->velocity_t_in[s])
-      face3(c, fs, sol, 1, F3_VELOCITY, second, (real_t)p->uz_in, (real_t)rA, 0);
+      face3(c, fs, sol, 1, F3_VELOCITY, second, (real_t)p->uz_in, (real_t)rA, 0, 0);
     if (p->velocity_t_out[s])
-      face3(c, fs, sol, 1, F3_VELOCITY, second, (real_t)p->uz_out, (real_t)rA, 0);
+      face3(c, fs, sol, 1, F3_VELOCITY, second, (real_t)p->uz_out, (real_t)rA, 0, 0);
     if (p->velocity_b_in[s])
-      face3(c, fs, sol, 0, F3_VELOCITY, second, (real_t)p->uz_in, (real_t)rA, 0);
+      face3(c, fs, sol, 0, F3_VELOCITY, second, (real_t)p->uz_in, (real_t)rA, 0, 0);
     if (p->velocity_b_out[s])
-      face3(c, fs, sol, 0, F3_VELOCITY, second, (real_t)p->uz_out, (real_t)rA, 0);
+      face3(c, fs, sol, 0, F3_VELOCITY, second, (real_t)p->uz_out, (real_t)rA, 0, 0);
     if (s == 1 && p->nsubs == 2) {
       if (p->constcon_t_in)
         face3(c, fs, sol, 1, F3_CONSTCON, second, 0, (real_t)p->rho_sigma_in,
-              p->constcon_profile_t);
+              p->constcon_profile_t, p->d_profile_t);
       if (p->constcon_b_in)
         face3(c, fs, sol, 0, F3_CONSTCON, second, 0, (real_t)p->rho_sigma_in,
-              p->constcon_profile_b);
-      if (p->zeroconcgrad_t) face3(c, fs, sol, 1, F3_ZEROGRAD, second, 0, 0, 0);
-      if (p->zeroconcgrad_b) face3(c, fs, sol, 0, F3_ZEROGRAD, second, 0, 0, 0);
+              p->constcon_profile_b, p->d_profile_b);
+      if (p->zeroconcgrad_t) face3(c, fs, sol, 1, F3_ZEROGRAD, second, 0, 0, 0, 0);
+      if (p->zeroconcgrad_b) face3(c, fs, sol, 0, F3_ZEROGRAD, second, 0, 0, 0, 0);
     }
   }
 }
@@ -704,18 +741,27 @@ int SFX(orc_run_btc)(const orc_params* p, REAL* f, const uint8_t* solids,
     int wmv = frame_rate > 0 && t % frame_rate == 0;
     int odd = (t % 2) == 1;
     REAL* m = wmv ? mv : scratch;
-    double sc = 0, su = 0;
+    acc_t sc = 0, su = 0;
     if (p->dims == 2) apply_bcs(&c, f, solids, t, !odd);
     else apply_bcs3(&c, f, solids, t, !odd);
     half_step(&c, f, solids, m, t, 1, odd, nthreads);
     for (q = 0; q < per; q++)
       if (!is_solid(solids, base + q)) {
-        su += (double)m[c.NN + base + q];                      /* subs 0, u_x */
-        if (p->nsubs == 2) sc += (double)m[(long)(1 + c.D) * c.NN + base + q];
+        su += ACC(m[c.NN + base + q]);                      /* subs 0, u_x */
+        if (p->nsubs == 2) sc += ACC(m[(long)(1 + c.D) * c.NN + base + q]);
       }
-    btc_ux[t - t0 - 1] = cnt ? su / (double)cnt : 0. / 0.;
-    btc[t - t0 - 1] = (p->nsubs == 2 && t >= p->sigma_t_on && t <= p->sigma_t_off && cnt)
-                          ? sc / (double)cnt : 0. / 0.;
+    {
+      const acc_t ux = cnt ? su / (double)cnt : 0. / 0.;
+      const acc_t cc = (p->nsubs == 2 && t >= p->sigma_t_on && t <= p->sigma_t_off && cnt)
+                           ? sc / (double)cnt : 0. / 0.;
+#ifdef LBX_ORACLE_CPLX
+      btc_ux[2 * (t - t0 - 1)] = creal(ux); btc_ux[2 * (t - t0 - 1) + 1] = cimag(ux);
+      btc[2 * (t - t0 - 1)] = creal(cc); btc[2 * (t - t0 - 1) + 1] = cimag(cc);
+#else
+      btc_ux[t - t0 - 1] = ux;
+      btc[t - t0 - 1] = cc;
+#endif
+    }
   }
   free(scratch);
   return 0;

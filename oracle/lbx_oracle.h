@@ -51,6 +51,13 @@ typedef struct {
    * and uz_out for the *_out faces, per substance */
   int velocity_t_in[2], velocity_t_out[2], velocity_b_in[2], velocity_b_out[2];
   double uz_in, uz_out;
+  /* Complex-step build only (orc_*_cs): imaginary parts added to tau,
+   * gaccel and the constant-concentration profiles, so that the imaginary
+   * part of every result is h times its derivative along that direction
+   * (h the size of these parts).  Ignored by the real builds. */
+  double d_tau[2], d_gaccel[6];
+  const double* d_profile_t;
+  const double* d_profile_b;
 } orc_params;
 
 int orc_run_f64(const orc_params*, double* f, const uint8_t* solids,
@@ -69,4 +76,18 @@ int orc_init_feq_f64(const orc_params*, const double* rho, const double* ux,
                      const double* uy, const double* uz, double* f);
 int orc_init_feq_f32(const orc_params*, const float* rho, const float* ux,
                      const float* uy, const float* uz, float* f);
+#ifdef LBX_ORACLE_CPLX
+#include <complex.h>
+/* The forward run in complex arithmetic (complex-step differentiation): f
+ * and mv complex; btc and btc_ux hold 2*nsteps doubles, (real, imaginary)
+ * per step. */
+int orc_run_btc_cs(const orc_params*, double _Complex* f, const uint8_t* solids,
+                   double _Complex* mv, int t0, int nsteps, int frame_rate,
+                   int nthreads, int plane, double* btc, double* btc_ux);
+int orc_run_cs(const orc_params*, double _Complex* f, const uint8_t* solids,
+               double _Complex* mv, int t0, int nsteps, int frame_rate, int nthreads);
+int orc_init_feq_cs(const orc_params*, const double _Complex* rho,
+                    const double _Complex* ux, const double _Complex* uy,
+                    const double _Complex* uz, double _Complex* f);
+#endif
 #endif

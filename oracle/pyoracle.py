@@ -84,6 +84,12 @@ class Params:
     velocity_b_out: tuple = (0, 0)
     uz_in: float = 0.0
     uz_out: float = 0.0
+    # complex-step runs only: imaginary parts of tau, gaccel and the inlet
+    # profiles (h times a direction)
+    d_tau: tuple = (0.0, 0.0)
+    d_gaccel: tuple = (0.0,) * 6
+    d_profile_t: Optional[np.ndarray] = None
+    d_profile_b: Optional[np.ndarray] = None
 
     @property
     def Q(self) -> int:
@@ -129,6 +135,10 @@ class _OrcParams(C.Structure):
         ("velocity_b_out", C.c_int * 2),
         ("uz_in", C.c_double),
         ("uz_out", C.c_double),
+        ("d_tau", _D2),
+        ("d_gaccel", _D6),
+        ("d_profile_t", C.POINTER(C.c_double)),
+        ("d_profile_b", C.POINTER(C.c_double)),
     ]
 
 
@@ -150,7 +160,7 @@ class _RefParams(C.Structure):
 
 def _fill(st, p: Params, keep):
     for name, _ in st._fields_:
-        if name.startswith("constcon_profile") or name == "ns":
+        if name.startswith("constcon_profile") or name.startswith("d_profile") or name == "ns":
             v = getattr(p, name)
             if v is not None and np.size(v) > 0:
                 arr = np.ascontiguousarray(v, dtype=np.float64).reshape(-1)
@@ -198,6 +208,10 @@ def _lib():
             fn = getattr(lib, "orc_init_feq_" + sfx)
             fn.argtypes = [C.POINTER(_OrcParams)] + [C.POINTER(ct)] * 4 + [C.POINTER(ct)]
             fn.restype = C.c_int
+        lib.orc_run_btc_cs.argtypes = [C.POINTER(_OrcParams), C.c_void_p, C.c_void_p,
+                                       C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int,
+                                       C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        lib.orc_run_btc_cs.restype = C.c_int
         _oracle = lib
     return _oracle
 
@@ -576,3 +590,53 @@ def reference_init_from_params(variant: str, path: str):
     if rc != 0:
         raise ValueError("refk_init_from_params failed (%d)" % rc)
     return f, mv
+
+
+def run_oracle_btc_cs(p: Params, f: np.ndarray, solids: np.ndarray, t0: int, nsteps: int,
+                      plane: int, threads: int = 0):
+    """run_oracle_btc in complex arithmetic (the complex-step build): f is
+    complex128 and advanced in place; p.d_tau, p.d_gaccel and
+    p.d_profile_b/t give tau, gaccel and the inlet profiles imaginary parts.
+    Returns (f, btc, btc_ux) with complex plane records."""
+    assert f.dtype == np.complex128 and f.flags.c_contiguous
+    assert f.size == p.nsubs * p.Q * p.NN
+    sol = np.ascontiguousarray(solids, dtype=np.uint8).reshape(-1)
+    mv = np.zeros((p.nsubs, 1 + p.dims, p.NN), np.complex128)
+    btc = np.zeros(2 * nsteps)
+    bux = np.zeros(2 * nsteps)
+    keep = []
+    st = _OrcParams()
+    _fill(st, p, keep)
+    nt = threads or min(os.cpu_count() or 1, 64)
+    rc = _lib().orc_run_btc_cs(C.byref(st), f.ctypes.data, sol.ctypes.data, mv.ctypes.data,
+                               t0, nsteps, 0, nt, plane,
+                               btc.ctypes.data_as(C.POINTER(C.c_double)),
+                               bux.ctypes.data_as(C.POINTER(C.c_double)))
+    if rc != 0:
+        raise ValueError("orc_run_btc_cs rejected the parameters")
+    return f, btc[0::2] + 1j * btc[1::2], bux[0::2] + 1j * bux[1::2]
+
+
+def tangent_objective(p: Params, f0: np.ndarray, solids: np.ndarray, nsteps: int,
+                      plane: int, t_first: int, t_last: int, w_c: float, w_ux: float,
+                      d_tau=(0.0, 0.0), d_gaccel=(0.0,) * 6, d_profile_b=None,
+                      h: float = 1e-30):
+    """The plane objective J = w_c mean_t <C>_plane + w_ux mean_t <u_x>_plane
+    over the steps t_first..t_last of a run of `nsteps` steps from f0 (even
+    time 0), and its forward-mode derivative dJ/dp . v along the direction
+    v = (d_tau, d_gaccel, d_profile_b), by complex step with step h.
+    Returns (J, dJ)."""
+    import dataclasses
+    q = dataclasses.replace(p)
+    q.d_tau = tuple(h * x for x in d_tau)
+    q.d_gaccel = tuple(h * x for x in d_gaccel)
+    q.d_profile_b = None if d_profile_b is None else h * np.asarray(d_profile_b, np.float64)
+    f = np.ascontiguousarray(f0, dtype=np.complex128).copy()
+    _, btc, bux = run_oracle_btc_cs(q, f, solids, 0, nsteps, plane)
+    win = slice(t_first - 1, t_last)
+    J = 0j
+    if w_c:
+        J += w_c * np.mean(btc[win])
+    if w_ux:
+        J += w_ux * np.mean(bux[win])
+    return float(J.real), float(J.imag / h)

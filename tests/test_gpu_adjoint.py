@@ -1,9 +1,11 @@
 """Discrete adjoint (GPU): gradients of plane objectives against central
-finite differences of the FP64 forward solve."""
+finite differences of the FP64 forward solve and against the forward-mode
+(tangent) derivative of the same FP64 model."""
 import numpy as np
 import pytest
 
 import lbx
+import pyoracle as po
 from lbx import geometry
 
 pytestmark = pytest.mark.gpu
@@ -80,6 +82,53 @@ def test_gpu_adjoint_fp64_matches_finite_differences(objective):
         if scale < 1e-14 * abs(J):          # no dependence (e.g. u_x on tau_s)
             continue
         assert abs(adj - fd) <= 1e-6 * scale, (objective, name, adj, fd)
+
+
+def _oracle_case(kw, mask, prof):
+    """The oracle's parameters and initial state for the same run."""
+    p = po.Params(dims=3, LX=kw["LX"], LY=kw["LY"], LZ=kw["LZ"], nsubs=kw["nsubs"],
+                  tau=tuple(kw["tau"]), gaccel=tuple(kw["gaccel"]),
+                  sigma_t_on=kw["sigma_t_on"], sigma_t_off=kw["sigma_t_off"],
+                  constcon_b_in=kw.get("constcon_b_in", 0),
+                  zeroconcgrad_t=kw.get("zeroconcgrad_t", 0),
+                  rho_sigma_in=kw.get("rho_sigma_in", 1.0),
+                  constcon_profile_b=prof if kw["nsubs"] == 2 else None)
+    ns = kw["nsubs"]
+    rho = np.stack([np.ones(p.NN)] + [np.zeros(p.NN)] * (ns - 1))
+    z = np.zeros((ns, p.NN))
+    return p, po.init_feq(p, rho, z, z, z)
+
+
+@pytest.mark.parametrize("objective", sorted(OBJS))
+def test_gpu_adjoint_fp64_matches_tangent(objective):
+    """adjoint . v against the forward-mode derivative along v of the same
+    FP64 discrete model (the oracle run in complex arithmetic, exact to
+    rounding), for g_x, tau, tau_s, a random inlet-profile direction and a
+    random direction over all of them at once."""
+    kw, mask, prof = _setup()
+    obj = OBJS[objective]
+    J, g = _J(kw, mask, prof, 8, STEPS, 7, obj, grads=True)
+    p, f0 = _oracle_case(kw, mask, prof)
+    rng = np.random.default_rng(17)
+    v = rng.standard_normal(prof.size)
+    a = rng.standard_normal(3)
+    dirs = {
+        "gx": (dict(d_gaccel=(1, 0, 0, 0, 0, 0)), g["d_gaccel"][0]),
+        "tau": (dict(d_tau=(1, 0)), g["d_tau"]),
+        "tau_s": (dict(d_tau=(0, 1)), g["d_tau_s"]),
+        "profile": (dict(d_profile_b=v), float(g["d_profile_b"] @ v)),
+        "all": (dict(d_gaccel=(a[0], 0, 0, 0, 0, 0), d_tau=(a[1], a[2]), d_profile_b=v),
+                a[0] * g["d_gaccel"][0] + a[1] * g["d_tau"] + a[2] * g["d_tau_s"]
+                + float(g["d_profile_b"] @ v)),
+    }
+    for name, (kwd, adj) in dirs.items():
+        Jt, tan = po.tangent_objective(p, f0, mask, STEPS, *obj, **kwd)
+        assert Jt == pytest.approx(J, rel=1e-12, abs=0)
+        # directions the objective does not depend on (u_x on the solute's
+        # parameters) give exactly 0 in the tangent; the adjoint's sums of
+        # exact zeros stay 0 there too
+        tol = 1e-10 * max(abs(tan), abs(adj)) + 1e-15 * abs(J)
+        assert abs(adj - tan) <= tol, (objective, name, adj, tan)
 
 
 @pytest.mark.parametrize("objective", sorted(OBJS))
