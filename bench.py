@@ -259,6 +259,46 @@ def precision_leg(mask, local: int, steps: int) -> dict:
     return out
 
 
+def adjoint_leg(local: int, steps: int, K: int = 100, window: int = 500) -> dict:
+    """The discrete adjoint's cost against a plain forward solve on the
+    128^3 flow + solute configuration (sphere pack r = 4 to porosity 0.45,
+    tau 0.8 / tau_s 0.75, gx 1e-5, C from a 128 x 128 inlet profile on the
+    bottom plane): `steps` steps, checkpoints every K, objective = mean
+    outlet C over the last `window` steps, gradients w.r.t. g, tau, tau_s
+    and the profile.  CUDA-event times; the gradient run is the second on
+    its domain (checkpoints and workspace allocated), as in an optimisation
+    loop."""
+    import torch
+    from lbx import Domain, configs
+    torch.cuda.set_device(local)
+    s = torch.cuda.Stream()
+    p, mask, prof = configs.cfg5_params(4, 128)
+    with Domain(p, mask) as dom:
+        dom.set_stream(s.cuda_stream)
+        dom.set_face_profile(False, prof)
+        for rep in range(2):
+            dom.init_equilibrium(0, 1.0, 0.0, 0.0, 0.0)
+            dom.init_equilibrium(1, 0.0, 0.0, 0.0, 0.0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(s)
+            dom.run(0, steps if rep else 20, 0)
+            e1.record(s)
+            s.synchronize()
+        t_plain = e0.elapsed_time(e1) / 1e3
+    w = min(window, steps)
+    obj = (p.LZ - 1, steps - w + 1, steps, 1.0, 0.0)
+    J, g, t_fwd, t_bwd = configs._cfg5_objective(p, mask, prof, steps, K, obj, True, s)
+    return {"value": round((t_fwd + t_bwd) / t_plain, 4), "unit": "x plain forward",
+            "J": J, "d_gx": g["d_gaccel"][0], "d_tau": g["d_tau"], "d_tau_s": g["d_tau_s"],
+            "profile_grad_norm": float(np.linalg.norm(g["d_profile_b"])),
+            "seconds_plain_forward": round(t_plain, 5),
+            "seconds_forward_with_checkpoints": round(t_fwd, 5),
+            "seconds_backward": round(t_bwd, 5),
+            "workload": "D3Q19 flow + solute 128^3, FP32 (FP64 gradient sums), %d steps, "
+                        "checkpoints every %d, objective mean outlet C over the last %d "
+                        "steps" % (steps, K, w)}
+
+
 def max_over_ranks(dist, value: float, device) -> float:
     """The maximum of `value` over the ranks of the process group (the
     slowest replica sets the whole job's time); `value` itself without one."""
@@ -331,6 +371,8 @@ def main(argv=None) -> int:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--precision-steps", type=int, default=6000,
                     help="steps of each run of the FP32-vs-FP64 leg (0: skip it)")
+    ap.add_argument("--adjoint-steps", type=int, default=4000,
+                    help="steps of the adjoint cost leg (0: skip it)")
     ap.add_argument("--cpu-table", action="store_true",
                     help="print the host-core timings of the oracle port and of the "
                          "reference's kernels on the 2D case and a 128^3 crop, then exit")
@@ -493,6 +535,8 @@ def main(argv=None) -> int:
             "permeability k = nu <u_x> / g_x after %d steps from rest; perm_rel_err = "
             "|k(FP32 shifted) - k(FP64 shifted)| / k(FP64 shifted), the same kernels"
             % args.precision_steps)
+    if args.adjoint_steps > 0:
+        line["adjoint"] = adjoint_leg(local, args.adjoint_steps)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(mask)
     dom.close()

@@ -100,6 +100,22 @@ T face_rho(const lbx_domain* d, int s, int t, int in_kind, bool is_in,
   return rho;
 }
 
+// A step with the solute off still runs the solute's face operations: the
+// reference launches its face kernels whatever sigma_t_on/off say
+// (src/bcs.c:503-541, :1453-1491), and their deposits change the idle
+// solute's slots.  The fused face paths apply the rules only to the
+// substances a step updates, so such steps take the stand-alone face kernels.
+bool solute_faces_idle(const lbx_domain* d, int t)
+{
+  const lbx_params& p = d->p;
+  if (p.nsubs != 2 || (t >= p.sigma_t_on && t <= p.sigma_t_off)) return false;
+  return p.zeroconcgrad_n || p.zeroconcgrad_s || p.pressure_n_in[1] || p.pressure_n_out[1] ||
+         p.pressure_s_in[1] || p.pressure_s_out[1] || p.constcon_t_in || p.constcon_b_in ||
+         p.zeroconcgrad_t || p.zeroconcgrad_b || p.pressure_t_in[1] || p.pressure_t_out[1] ||
+         p.pressure_b_in[1] || p.pressure_b_out[1] || p.velocity_t_in[1] ||
+         p.velocity_t_out[1] || p.velocity_b_in[1] || p.velocity_b_out[1];
+}
+
 template <typename T>
 void fill_args(const lbx_domain* d, int t, unsigned flags, StepArgs<T>& A)
 {
@@ -138,7 +154,7 @@ void fill_args(const lbx_domain* d, int t, unsigned flags, StepArgs<T>& A)
     A.btc_lo = d->btc_lo;
     A.btc_hi = d->btc_hi;
   }
-  if (d->faces_fused) {
+  if (d->faces_fused && !solute_faces_idle(d, t)) {
     for (int s = 0; s < p.nsubs; ++s) {
       // last active boundary on each face wins (see FaceKind)
       if (s == 1 && p.nsubs == 2 && p.zeroconcgrad_n) A.face_n[s] = FACE_ZEROGRAD;
@@ -163,22 +179,69 @@ StepArgs<T> make_args(const lbx_domain* d, int t, unsigned flags)
   return A;
 }
 
+// The compact kernels' arguments for one step.
+template <typename T>
+CompactArgs<T> make_compact(const lbx_domain* d, const StepArgs<T>& A)
+{
+  CompactArgs<T> C;
+  std::memset(&C, 0, sizeof C);
+  C.s = A;
+  C.fidx = d->fidx;
+  C.fnode = d->fnode;
+  C.frm = d->frm + 1;   // past the front guard word
+  C.F = (int)d->fluid;
+  C.P = (int)d->P;
+  C.div_plane = make_fastdiv((unsigned)(A.LX * A.LY));
+  C.div_lx = make_fastdiv((unsigned)A.LX);
+  C.faces = d->faces_fused ? 1 : 0;
+  C.m_base = 0;
+  C.m_skip = 0x7fffffff;
+  C.m_jump = 0;
+  C.m_end = C.F;
+  return C;
+}
+
+// The fluid nodes of the two z-face planes (compact [0, lo_end) and
+// [hi_start, F)) with their face operations applied in registers, every
+// substance in one launch (flow, then solute, per node).  The interior
+// between them runs in the ordinary step launches, so the face code's
+// registers do not weigh on the bulk of the nodes.
+template <typename T, int Q, int NS, int MODEL>
+void launch_face_nodes(lbx_domain* d, const StepArgs<T>& A, bool odd, const Face3Fused<T>& f3)
+{
+  if constexpr (Q == 19) {
+    CompactArgs<T> C = make_compact<T>(d, A);
+    C.f3 = f3;
+    C.m_base = 0;
+    C.m_skip = f3.lo_end;
+    C.m_jump = f3.hi_start - f3.lo_end;
+    const long long count = (long long)f3.lo_end + (d->fluid - f3.hi_start);
+    const unsigned blocks = (unsigned)((count + 255) / 256);
+    if (blocks == 0) return;
+    const bool idx32 = (unsigned long long)Q * (unsigned long long)d->P < (1ull << 32);
+    auto go = [&](auto odd_c, auto idx_c) {
+      aa_step_compact<T, Q, NS, MODEL, decltype(odd_c)::value, PART_ALL, decltype(idx_c)::value,
+                      false, true><<<blocks, 256, 0, d->stream>>>(C);
+    };
+    using TT = std::true_type;
+    using FF = std::false_type;
+    if (idx32) { if (odd) go(TT{}, TT{}); else go(FF{}, TT{}); }
+    else { if (odd) go(TT{}, FF{}); else go(FF{}, FF{}); }
+    d->launches++;
+  }
+}
+
 template <typename T, int Q, int NS, int MODEL, int PART>
-void launch_part(lbx_domain* d, const StepArgs<T>& A, bool odd)
+void launch_part(lbx_domain* d, const StepArgs<T>& A, bool odd, const Face3Fused<T>* f3)
 {
   if (d->layout == LBX_LAYOUT_COMPACT) {
-    CompactArgs<T> C;
-    C.s = A;
-    C.fidx = d->fidx;
-    C.fnode = d->fnode;
-    C.frm = d->frm + 1;   // past the front guard word
-    C.F = (int)d->fluid;
-    C.P = (int)d->P;
-    C.div_plane = make_fastdiv((unsigned)(A.LX * A.LY));
-    C.div_lx = make_fastdiv((unsigned)A.LX);
-    C.faces = d->faces_fused ? 1 : 0;
-    const unsigned blocks = (unsigned)((d->fluid + 255) / 256);
-    if (blocks == 0) return;
+    CompactArgs<T> C = make_compact<T>(d, A);
+    if (f3) {   // the interior only; launch_face_nodes takes the two planes
+      C.m_base = f3->lo_end;
+      C.m_end = f3->hi_start;
+    }
+    const unsigned blocks = (unsigned)((C.m_end - C.m_base + 255) / 256);
+    if (C.m_end <= C.m_base) return;
     const bool idx32 = (unsigned long long)Q * (unsigned long long)d->P < (1ull << 32);
     auto go = [&](auto odd_c, auto idx_c, auto oop_c) {
       aa_step_compact<T, Q, NS, MODEL, decltype(odd_c)::value, PART, decltype(idx_c)::value,
@@ -211,24 +274,26 @@ void launch_part(lbx_domain* d, const StepArgs<T>& A, bool odd)
 // One step: a single launch for the flow alone; flow then solute for two
 // substances (the solute launch only while the solute is active).
 template <typename T, int Q, int NS, int MODEL>
-void launch_aa(lbx_domain* d, const StepArgs<T>& A, bool odd)
+void launch_aa(lbx_domain* d, const StepArgs<T>& A, bool odd, const Face3Fused<T>* f3)
 {
   if constexpr (NS == 1) {
-    launch_part<T, Q, NS, MODEL, PART_ALL>(d, A, odd);
+    launch_part<T, Q, NS, MODEL, PART_ALL>(d, A, odd, f3);
   } else {
-    launch_part<T, Q, NS, MODEL, PART_FLOW>(d, A, odd);
-    if (A.solute_on) launch_part<T, Q, NS, MODEL, PART_SOLUTE>(d, A, odd);
+    launch_part<T, Q, NS, MODEL, PART_FLOW>(d, A, odd, f3);
+    if (A.solute_on) launch_part<T, Q, NS, MODEL, PART_SOLUTE>(d, A, odd, f3);
   }
+  if (f3) launch_face_nodes<T, Q, NS, MODEL>(d, A, odd, *f3);
 }
 
 template <typename T, int Q, int NS>
-void launch_model(lbx_domain* d, const StepArgs<T>& A, bool odd)
+void launch_model(lbx_domain* d, const StepArgs<T>& A, bool odd,
+                  const Face3Fused<T>* f3 = nullptr)
 {
   const int model = d->p.accurate ? (d->p.compressible ? SHIFTED_COMP : SHIFTED_INC)
                                   : PLAIN_COMP;
-  if (model == SHIFTED_INC) launch_aa<T, Q, NS, SHIFTED_INC>(d, A, odd);
-  else if (model == PLAIN_COMP) launch_aa<T, Q, NS, PLAIN_COMP>(d, A, odd);
-  else launch_aa<T, Q, NS, SHIFTED_COMP>(d, A, odd);
+  if (model == SHIFTED_INC) launch_aa<T, Q, NS, SHIFTED_INC>(d, A, odd, f3);
+  else if (model == PLAIN_COMP) launch_aa<T, Q, NS, PLAIN_COMP>(d, A, odd, f3);
+  else launch_aa<T, Q, NS, SHIFTED_COMP>(d, A, odd, f3);
 }
 
 // The stand-alone face kernels, in the order of bcs_1 / bcs_2.
@@ -333,6 +398,28 @@ FaceOps<T> face3_table(const lbx_domain* d, int t)
   return ops;
 }
 
+// The same operations for the step kernels (FACES3): per substance and face.
+template <typename T>
+Face3Fused<T> face3_fused(const lbx_domain* d, int t)
+{
+  Face3Fused<T> f;
+  std::memset(&f, 0, sizeof f);
+  f.lo_end = (int)d->plane_fluid[0];
+  f.hi_start = (int)(d->fluid - d->plane_fluid[d->p.LZ - 1]);
+  f.conc = (T)d->p.rho_sigma_in;
+  for_each_face3<T>(d, t, [&](int top, int kind, int s, T drho) {
+    int& n = f.nops[s][top];
+    const bool shifted = d->p.accurate && !(s == 1 && d->p.nsubs == 2);
+    f.kind[s][top][n] = kind;
+    f.drho[s][top][n] = drho;
+    f.shift[s][top][n] = kind == FACE_VELOCITY && shifted ? (T)d->p.rho_A[s] : T(0);
+    f.profile[s][top][n] = kind == FACE_CONSTCON ? (const T*)(top ? d->prof_t : d->prof_b)
+                                                 : nullptr;
+    ++n;
+  });
+  return f;
+}
+
 template <typename T>
 void launch_faces3(lbx_domain* d, int t, bool second)
 {
@@ -356,22 +443,32 @@ template <typename T>
 lbx_status step_t(lbx_domain* d, int t, unsigned flags)
 {
   const bool odd = (t % 2) != 0;
-  if (d->faces_active && !d->faces_fused) launch_faces_exact<T>(d, t, !odd);
-  if (d->faces3_active) launch_faces3<T>(d, t, !odd);
+  const bool idle = solute_faces_idle(d, t);
+  if (d->faces_active && (!d->faces_fused || idle)) launch_faces_exact<T>(d, t, !odd);
+  // z faces inside the compact step kernel where that is exact (before an
+  // even step always, before an odd step with fluid upstream planes); never
+  // while recomputing stored states, which keep the stand-alone deposits
+  const bool f3_fused = d->faces3_active && d->layout == LBX_LAYOUT_COMPACT && !d->fout &&
+                        (!odd || d->faces3_fuse_odd) && !idle;
+  if (d->faces3_active && !f3_fused) launch_faces3<T>(d, t, !odd);
+  Face3Fused<T> f3;
+  if (f3_fused) f3 = face3_fused<T>(d, t);
   StepArgs<T> A = make_args<T>(d, t, flags);
   if (d->Q == 9) {
     if (d->p.nsubs == 1) launch_model<T, 9, 1>(d, A, odd);
     else launch_model<T, 9, 2>(d, A, odd);
   } else {
-    if (d->p.nsubs == 1) launch_model<T, 19, 1>(d, A, odd);
-    else launch_model<T, 19, 2>(d, A, odd);
+    if (d->p.nsubs == 1) launch_model<T, 19, 1>(d, A, odd, f3_fused ? &f3 : nullptr);
+    else launch_model<T, 19, 2>(d, A, odd, f3_fused ? &f3 : nullptr);
   }
   if (d->btc_vals) {
     const bool compact = d->layout == LBX_LAYOUT_COMPACT;
-    btc_reduce<<<1, kBtcThreads, 0, d->stream>>>(
-        d->btc_vals, d->btc_hi - d->btc_lo, compact ? nullptr : d->solids + d->btc_lo,
+    const int count = d->btc_hi - d->btc_lo;
+    const int nb = std::max(1, std::min(kBtcMaxBlocks, (count + 1023) / 1024));
+    btc_reduce<<<nb, kBtcThreads, 0, d->stream>>>(
+        d->btc_vals, count, compact ? nullptr : d->solids + d->btc_lo,
         (double)d->plane_fluid[d->btc_plane], d->p.nsubs == 2 && A.solute_on, d->btc_rec,
-        d->btc_slot, d->btc_cap);
+        d->btc_slot, d->btc_cap, d->btc_part, d->btc_ticket);
     d->launches++;
   }
   CK(cudaGetLastError());
@@ -460,6 +557,37 @@ bool faces_fusable(const lbx_params& p, const uint8_t* sol)
   return true;
 }
 
+// The z faces' deposits before an odd step land only in slots their own
+// face node pulls when every upstream node n - c_a of every unknown
+// direction a of every fluid node of a configured face is fluid: the
+// planes across the periodic z wrap, shifted by the unknowns' in-plane c.
+bool faces3_fusable_odd(const lbx_params& p, const uint8_t* sol)
+{
+  bool top = false, bot = false;
+  for (int s = 0; s < p.nsubs; ++s) {
+    top |= p.pressure_t_in[s] || p.pressure_t_out[s] || p.velocity_t_in[s] || p.velocity_t_out[s];
+    bot |= p.pressure_b_in[s] || p.pressure_b_out[s] || p.velocity_b_in[s] || p.velocity_b_out[s];
+  }
+  if (p.nsubs == 2) {
+    top |= p.constcon_t_in || p.zeroconcgrad_t;
+    bot |= p.constcon_b_in || p.zeroconcgrad_b;
+  }
+  auto solid = [&](int i, int j, int k) {
+    i = (i + p.LX) % p.LX; j = (j + p.LY) % p.LY; k = (k + p.LZ) % p.LZ;
+    return sol[(long long)i + (long long)p.LX * ((long long)j + (long long)p.LY * k)] == 1;
+  };
+  // in-plane parts of the unknowns (cz = +1 at the bottom, -1 at the top):
+  // (0,0), (+-1,0), (0,+-1)
+  const int ux[5] = {0, 1, -1, 0, 0}, uy[5] = {0, 0, 0, 1, -1};
+  for (int j = 0; j < p.LY; ++j)
+    for (int i = 0; i < p.LX; ++i)
+      for (int q = 0; q < 5; ++q) {
+        if (bot && !solid(i, j, 0) && solid(i - ux[q], j - uy[q], -1)) return false;
+        if (top && !solid(i, j, p.LZ - 1) && solid(i - ux[q], j - uy[q], p.LZ)) return false;
+      }
+  return true;
+}
+
 void release(lbx_domain* d)
 {
   lbx_internal_drop_graphs(d);
@@ -467,6 +595,7 @@ void release(lbx_domain* d)
   cudaFree(d->f); cudaFree(d->mv); cudaFree(d->solids); cudaFree(d->cls);
   cudaFree(d->nbm); cudaFree(d->red);
   cudaFree(d->btc_vals); cudaFree(d->btc_rec); cudaFree(d->btc_slot);
+  cudaFree(d->btc_part); cudaFree(d->btc_ticket);
   cudaFree(d->ubuf); cudaFree(d->prof_t); cudaFree(d->prof_b); cudaFree(d->ns);
   lbx_internal_adjoint_free(d);
   lbx_internal_frames_free(d);
@@ -692,6 +821,7 @@ lbx_status lbx_create(const lbx_params* p, const uint8_t* solids, lbx_domain** o
                         p->velocity_t_out[s] || p->velocity_b_out[s];
   d->faces3_active |= p->nsubs == 2 && (p->constcon_t_in || p->constcon_b_in ||
                                         p->zeroconcgrad_t || p->zeroconcgrad_b);
+  d->faces3_fuse_odd = d->faces3_active && faces3_fusable_odd(*p, solids);
   {
     const int planes = p->dims == 2 ? p->LY : p->LZ;
     const long long per = d->N / planes;
@@ -1023,7 +1153,9 @@ lbx_status lbx_btc_stop(lbx_domain* d)
     lbx_internal_drop_graphs(d);
   }
   cudaFree(d->btc_vals); cudaFree(d->btc_rec); cudaFree(d->btc_slot);
+  cudaFree(d->btc_part); cudaFree(d->btc_ticket);
   d->btc_vals = nullptr; d->btc_rec = nullptr; d->btc_slot = nullptr;
+  d->btc_part = nullptr; d->btc_ticket = nullptr;
   d->btc_cap = 0;
   return LBX_OK;
 }
@@ -1052,7 +1184,10 @@ lbx_status lbx_btc_start(lbx_domain* d, int plane, int capacity)
   CK(cudaMalloc(&d->btc_vals, 2 * std::max<long long>(1, hi - lo) * sizeof(double)));
   CK(cudaMalloc(&d->btc_rec, (size_t)capacity * 2 * sizeof(double)));
   CK(cudaMalloc(&d->btc_slot, sizeof(int)));
+  CK(cudaMalloc(&d->btc_part, 2 * kBtcMaxBlocks * sizeof(double)));
+  CK(cudaMalloc(&d->btc_ticket, sizeof(unsigned)));
   CK(cudaMemsetAsync(d->btc_slot, 0, sizeof(int), d->stream));
+  CK(cudaMemsetAsync(d->btc_ticket, 0, sizeof(unsigned), d->stream));
   // the step arguments changed: a captured pair no longer matches
   if (d->graph) { CK(cudaStreamSynchronize(d->stream)); lbx_internal_drop_graphs(d); }
   return LBX_OK;

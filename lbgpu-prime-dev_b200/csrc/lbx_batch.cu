@@ -15,8 +15,8 @@
 //               between steps (the AA pattern needs the odd step complete
 //               before the even one);
 //   SEQUENTIAL  one launch per sample per step (the per-sample baseline).
-// lbx_batch_autotune times each mode and block size on a few steps and
-// keeps the fastest.
+// lbx_batch_autotune times FUSED at each block size and PERSISTENT with the
+// full and half resident grid on a few steps and keeps the fastest.
 #include "lbx.h"
 #include "lbx_internal.h"
 #include "lbx_kernels.cuh"
@@ -53,10 +53,11 @@ template <typename T>
 struct SampleDesc {
   int LX, LY, LZ, plane;
   long long N;          // dense nodes
-  long long dbase;      // first dense node of the sample in fidx / solids
+  long long dbase;      // first dense node of the sample in the solids array
   long long mvbase;     // first macro-variable element: [1+D][N]
   int cbase;            // first compact index (a multiple of kAlign)
   int F;                // fluid nodes
+  long long frm_base;   // the sample's word 0 in the rank table
   FastDiv div_plane, div_lx;
   SubsConst<T> sc;
 };
@@ -65,7 +66,8 @@ template <typename T>
 struct BatchArgs {
   T* f;                         // [Q][Ftot]
   T* mv;                        // per sample [1+D][N]
-  const int* fidx;              // per sample [N]: global compact index, -1 solid
+  const uint2* frm;             // per sample, ceil(N/32) words: (global compact index
+                                // of the word's first fluid node, fluid bits)
   const int* fnode;             // [Ftot]: dense index inside the sample, -1 padding
   const SampleDesc<T>* samples;
   const int* blk_sample;        // [nblocks]
@@ -76,83 +78,46 @@ struct BatchArgs {
   int kahan;                    // compensated density sums
 };
 
-// One block of the batch: the compact AA step of aa_step_compact, with the
-// sample's extents and constants.
+// One block of the batch: the single-lattice compact update (compact_node,
+// with its rank-table neighbour lookups and pull-slot table) on the block's
+// sample: its extents, constants and rank table, whose word ranks are
+// global compact indices, so the neighbours it finds are slots of the
+// shared population array.
 template <typename T, int Q, int MODEL, bool ODD, bool IDX32>
 __device__ __forceinline__ void batch_block(const BatchArgs<T>& A, int b)
 {
-  using Idx = typename std::conditional<IDX32, unsigned, size_t>::type;
-  constexpr int D = (Q == 9) ? 2 : 3;
   const int s = A.blk_sample[b];
   const SampleDesc<T>& S = A.samples[s];
   const int m = b * blockDim.x + threadIdx.x;            // global compact index
   if (m - S.cbase >= S.F) return;                        // padding after the sample
-  const Idx F = (Idx)A.Ftot;
-  const int n = A.fnode[m];
-  if (n < 0) return;
-  const int LX = S.LX, LY = S.LY, plane = S.plane;
-  StepArgs<T> L;
+  CompactArgs<T> C;
+  StepArgs<T>& L = C.s;
+  L.f = A.f;
   L.mv = A.mv + S.mvbase;
+  L.LX = S.LX; L.LY = S.LY; L.LZ = S.LZ;
   L.N = S.N;
   L.sc[0] = S.sc;
   L.write_mv = A.write_mv;
   L.kahan = A.kahan;
-  int xm = 0, xp = 0, ym = 0, yp = 0, zm = 0, zp = 0;
-  if (ODD) {
-    const int k = fast_div(n, S.div_plane);
-    const int r = n - k * plane;
-    const int j = fast_div(r, S.div_lx);
-    const int i = r - j * LX;
-    xm = (i == 0) ? LX - 1 : -1; xp = (i == LX - 1) ? 1 - LX : 1;
-    ym = (j == 0) ? plane - LX : -LX; yp = (j == LY - 1) ? LX - plane : LX;
-    if (D == 3) {
-      const int tot = plane * S.LZ;
-      zm = (k == 0) ? tot - plane : -plane;
-      zp = (k == S.LZ - 1) ? plane - tot : plane;
-    }
-  }
-  auto off = [&](int a) -> int {
-    return (cx(a) < 0 ? xm : (cx(a) > 0 ? xp : 0)) + (cy(a) < 0 ? ym : (cy(a) > 0 ? yp : 0))
-         + (cz(a) < 0 ? zm : (cz(a) > 0 ? zp : 0));
-  };
-  const int* const fidx_n = A.fidx + S.dbase + n;
-  auto nb_pull = [&](int a) -> int { return fidx_n[off(a)]; };
-  auto nb_push = [&](int a) -> int { return ld_reload(fidx_n + off(a)); };
-  T* const fs = A.f;
-  T d[Q];
-  T u[3] = {T(0), T(0), T(0)};
-  if (ODD) {
-#pragma unroll
-    for (int a = 0; a < Q; ++a) {
-      const int up = (a == 0) ? m : nb_pull(opp(a));
-      const Idx src = (up >= 0) ? (Idx)a * F + (Idx)up : (Idx)opp(a) * F + (Idx)m;
-      d[a] = fs[src];
-    }
-  } else {
-#pragma unroll
-    for (int a = 0; a < Q; ++a) d[a] = fs[opp(a) * F + m];
-  }
-  collide<T, Q, MODEL>(L, 0, false, ODD ? 1 : 2, d, u, n);
-  if (ODD) {
-    xm = opaque(xm); xp = opaque(xp); ym = opaque(ym); yp = opaque(yp);
-    if (D == 3) { zm = opaque(zm); zp = opaque(zp); }
-#pragma unroll
-    for (int a = 0; a < Q; ++a) {
-      const int dn = (a == 0) ? m : nb_push(a);
-      const Idx dst = (dn >= 0) ? (Idx)opp(a) * F + (Idx)dn : (Idx)a * F + (Idx)m;
-      fs[dst] = d[a];
-    }
-  } else {
-    const int m2 = opaque(m);
-#pragma unroll
-    for (int a = 0; a < Q; ++a) fs[a * F + m2] = d[a];
-  }
+  L.solute_on = 0;
+  L.btc = nullptr;
+  L.ubuf = nullptr;
+  L.fout = nullptr;
+  L.ns = nullptr;
+  C.fnode = A.fnode;
+  C.frm = A.frm + S.frm_base;
+  C.F = S.cbase + S.F;
+  C.P = (int)A.Ftot;
+  C.div_plane = S.div_plane;
+  C.div_lx = S.div_lx;
+  C.faces = 0;
+  compact_node<T, Q, 1, MODEL, ODD, PART_ALL, IDX32, false>(C, m);
 }
 
-// Up to 256 threads per block; five resident blocks of 256 (48 registers)
-// in FP32, three in FP64.
+// Up to 256 threads per block, resident blocks as for the single-lattice
+// compact kernels.
 template <typename T, int Q, int MODEL, bool ODD, bool IDX32>
-__global__ void __launch_bounds__(256, (sizeof(T) == 4 ? 5 : 3))
+__global__ void __launch_bounds__(256, (compact_min_blocks<T, PART_ALL>()))
 aa_step_batch(BatchArgs<T> A)
 {
   batch_block<T, Q, MODEL, ODD, IDX32>(A, A.block0 + blockIdx.x);
@@ -200,13 +165,13 @@ __global__ void batch_scatter(T* fdense, const T* fc, const int* fnode, long lon
 struct lbx_batch {
   int nsamples = 0, dims = 0, Q = 0, precision = 0, model = 0, kahan = 0;
   std::vector<lbx_params> params;         // per sample (as given)
-  std::vector<long long> N, dbase, fbase_dense, mvbase;
+  std::vector<long long> N, dbase, fbase_dense, mvbase, frm_base;
   std::vector<int> cbase, F, order;
   long long Ntot = 0, Ftot = 0;
   void* fc = nullptr;         // [Q][Ftot]
   void* fdense = nullptr;     // per sample [Q][N]: the exchange format
   void* mv = nullptr;
-  int* fidx = nullptr;
+  uint2* frm = nullptr;       // per-sample rank tables (BatchArgs::frm)
   int* fnode = nullptr;
   uint8_t* solids = nullptr;
   void* samples = nullptr;    // SampleDesc<T>[nsamples]
@@ -222,7 +187,8 @@ struct lbx_batch {
   cudaGraphExec_t graph = nullptr;
   cudaStream_t graph_stream = nullptr;
   int graph_bs = -1;
-  int coop_grid = 0;
+  int coop_grid = 0;           // resident blocks of the persistent kernel
+  int coop_div = 1;            // persistent grid = coop_grid / coop_div (autotuned)
 };
 
 namespace {
@@ -235,7 +201,7 @@ BatchArgs<T> batch_args(lbx_batch* b, int write_mv)
 {
   BatchArgs<T> A;
   std::memset(&A, 0, sizeof A);
-  A.f = (T*)b->fc; A.mv = (T*)b->mv; A.fidx = b->fidx; A.fnode = b->fnode;
+  A.f = (T*)b->fc; A.mv = (T*)b->mv; A.frm = b->frm; A.fnode = b->fnode;
   A.samples = (const SampleDesc<T>*)b->samples;
   A.blk_sample = b->blk_sample[b->bs_index];
   A.Ftot = b->Ftot; A.nblocks = b->nblocks[b->bs_index];
@@ -295,7 +261,7 @@ lbx_status launch_persistent(lbx_batch* b, int steps, bool odd_first)
       return bfail(LBX_ERR_CUDA, "persistent mode unavailable (%s)", cudaGetErrorString(e));
     b->coop_grid = sms * per_sm;
   }
-  const int grid = std::min(b->coop_grid, std::max(1, A.nblocks));
+  const int grid = std::min(std::max(1, b->coop_grid / b->coop_div), std::max(1, A.nblocks));
   int odd0 = odd_first ? 1 : 0;
   void* args[] = {&A, &steps, &odd0};
   cudaError_t e = cudaLaunchCooperativeKernel(
@@ -351,7 +317,7 @@ void fill_desc(lbx_batch* b, std::vector<unsigned char>& out)
     std::memset(&x, 0, sizeof x);
     x.LX = p.LX; x.LY = p.LY; x.LZ = p.LZ; x.plane = p.LX * p.LY;
     x.N = b->N[s]; x.dbase = b->dbase[s]; x.mvbase = b->mvbase[s];
-    x.cbase = b->cbase[s]; x.F = b->F[s];
+    x.cbase = b->cbase[s]; x.F = b->F[s]; x.frm_base = b->frm_base[s];
     x.div_plane = make_fastdiv((unsigned)(p.LX * p.LY));
     x.div_lx = make_fastdiv((unsigned)p.LX);
     const T tau = (T)p.tau[0];
@@ -366,7 +332,7 @@ void fill_desc(lbx_batch* b, std::vector<unsigned char>& out)
 void release(lbx_batch* b)
 {
   if (b->graph) cudaGraphExecDestroy(b->graph);
-  cudaFree(b->fc); cudaFree(b->fdense); cudaFree(b->mv); cudaFree(b->fidx);
+  cudaFree(b->fc); cudaFree(b->fdense); cudaFree(b->mv); cudaFree(b->frm);
   cudaFree(b->fnode); cudaFree(b->solids); cudaFree(b->samples); cudaFree(b->red);
   for (int i = 0; i < kNumBlockSizes; ++i) cudaFree(b->blk_sample[i]);
   if (b->own_stream) cudaStreamDestroy(b->own_stream);
@@ -544,15 +510,35 @@ lbx_status lbx_batch_create(int nsamples, const lbx_params* params, const uint8_
   b->Ftot = c;
   if (c >= (1LL << 31)) { delete b; return bfail(LBX_ERR_INVALID, "batch holds >= 2^31 fluid nodes"); }
 
-  std::vector<int> fidx(b->Ntot), fnode(std::max<long long>(b->Ftot, 1), -1);
+  // per sample: the dense index of each fluid node, and a rank table of
+  // ceil(N/32) words (global compact index of the word's first fluid node,
+  // fluid bits), with a guard word in front and behind
+  std::vector<int> fnode(std::max<long long>(b->Ftot, 1), -1);
   std::vector<uint8_t> sol(b->Ntot);
+  b->frm_base.resize(nsamples);
+  long long words = 0;
+  for (int s = 0; s < nsamples; ++s) {
+    b->frm_base[s] = words + 1;
+    words += (b->N[s] + 31) / 32 + 2;
+  }
+  std::vector<uint2> frm((size_t)words);
   for (int s = 0; s < nsamples; ++s) {
     int m = b->cbase[s];
-    for (long long n = 0; n < b->N[s]; ++n) {
-      sol[b->dbase[s] + n] = solids[s][n];
-      if (solids[s][n] == 1) fidx[b->dbase[s] + n] = -1;
-      else { fidx[b->dbase[s] + n] = m; fnode[m++] = (int)n; }
+    const long long W = (b->N[s] + 31) / 32;
+    uint2* tab = frm.data() + b->frm_base[s];
+    tab[-1] = make_uint2((unsigned)m, 0u);
+    for (long long w = 0; w < W; ++w) {
+      unsigned bits = 0;
+      tab[w].x = (unsigned)m;
+      for (int q = 0; q < 32; ++q) {
+        const long long n = w * 32 + q;
+        if (n >= b->N[s]) break;
+        sol[b->dbase[s] + n] = solids[s][n];
+        if (solids[s][n] != 1) { bits |= 1u << q; fnode[m++] = (int)n; }
+      }
+      tab[w].y = bits;
     }
+    tab[W] = make_uint2((unsigned)m, 0u);
   }
   auto bail = [&](lbx_status st) { release(b); delete b; return st; };
   cudaError_t e;
@@ -563,11 +549,11 @@ lbx_status lbx_batch_create(int nsamples, const lbx_params* params, const uint8_
   BCKD(cudaMalloc(&b->fc, std::max<size_t>(1, (size_t)b->Q * b->Ftot * rs)));
   BCKD(cudaMalloc(&b->fdense, (size_t)b->Q * b->Ntot * rs));
   BCKD(cudaMalloc(&b->mv, (size_t)(1 + b->dims) * b->Ntot * rs));
-  BCKD(cudaMalloc(&b->fidx, (size_t)b->Ntot * sizeof(int)));
+  BCKD(cudaMalloc(&b->frm, frm.size() * sizeof(uint2)));
   BCKD(cudaMalloc(&b->fnode, fnode.size() * sizeof(int)));
   BCKD(cudaMalloc(&b->solids, (size_t)b->Ntot));
   BCKD(cudaMalloc(&b->red, 2 * 148 * sizeof(RedPartial)));
-  BCKD(cudaMemcpy(b->fidx, fidx.data(), fidx.size() * sizeof(int), cudaMemcpyHostToDevice));
+  BCKD(cudaMemcpy(b->frm, frm.data(), frm.size() * sizeof(uint2), cudaMemcpyHostToDevice));
   BCKD(cudaMemcpy(b->fnode, fnode.data(), fnode.size() * sizeof(int), cudaMemcpyHostToDevice));
   BCKD(cudaMemcpy(b->solids, sol.data(), sol.size(), cudaMemcpyHostToDevice));
   BCKD(cudaMemset(b->fc, 0, std::max<size_t>(1, (size_t)b->Q * b->Ftot * rs)));
@@ -710,26 +696,31 @@ lbx_status lbx_batch_autotune(lbx_batch* b, int steps, int* mode_out, int* block
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
   float best = 1e30f;
-  int best_mode = LBX_BATCH_FUSED, best_bs = 1;
-  const int modes[2] = {LBX_BATCH_FUSED, LBX_BATCH_PERSISTENT};
+  int best_mode = LBX_BATCH_FUSED, best_bs = 1, best_div = 1;
+  // candidates: FUSED at each block size; PERSISTENT (256-thread blocks) with
+  // the resident grid, or half of it (fewer blocks contending for the grid
+  // barrier, more sample blocks walked by each)
+  struct Cand { int mode, bs, div; };
+  const Cand cands[] = {{LBX_BATCH_FUSED, 0, 1}, {LBX_BATCH_FUSED, 1, 1},
+                        {LBX_BATCH_PERSISTENT, 1, 1}, {LBX_BATCH_PERSISTENT, 1, 2}};
   lbx_status st = LBX_OK;
-  for (int mi = 0; mi < 2 && st == LBX_OK; ++mi) {
-    for (int bi = 0; bi < kNumBlockSizes && st == LBX_OK; ++bi) {
-      if (modes[mi] == LBX_BATCH_PERSISTENT && bi != 1) continue;
-      b->bs_index = bi;
-      st = run_steps(b, 0, 2, 0, modes[mi]);            // warm-up (and graph capture)
-      if (st != LBX_OK) { st = LBX_OK; continue; }      // mode unavailable: skip it
-      cudaEventRecord(e0, b->stream);
-      st = run_steps(b, 2, steps, 0, modes[mi]);
-      cudaEventRecord(e1, b->stream);
-      cudaEventSynchronize(e1);
-      float ms = 0;
-      cudaEventElapsedTime(&ms, e0, e1);
-      if (st == LBX_OK && ms < best) { best = ms; best_mode = modes[mi]; best_bs = bi; }
-    }
+  for (const Cand& c : cands) {
+    if (st != LBX_OK) break;
+    b->bs_index = c.bs;
+    b->coop_div = c.div;
+    st = run_steps(b, 0, 2, 0, c.mode);              // warm-up (and graph capture)
+    if (st != LBX_OK) { st = LBX_OK; continue; }      // mode unavailable: skip it
+    cudaEventRecord(e0, b->stream);
+    st = run_steps(b, 2, steps, 0, c.mode);
+    cudaEventRecord(e1, b->stream);
+    cudaEventSynchronize(e1);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (st == LBX_OK && ms < best) { best = ms; best_mode = c.mode; best_bs = c.bs; best_div = c.div; }
   }
   b->mode = best_mode;
   b->bs_index = best_bs;
+  b->coop_div = best_div;
   b->parity = 0;
   cudaMemcpyAsync(b->fc, save, bytes, cudaMemcpyDeviceToDevice, b->stream);
   cudaStreamSynchronize(b->stream);

@@ -34,6 +34,7 @@ struct lbx_domain {
   bool faces_active = false;  // any 2D face boundary configured
   bool faces_fused = false;   // fused into the step kernels
   bool faces3_active = false; // any 3D z-face boundary configured
+  bool faces3_fuse_odd = false;  // z faces exact inside odd compact steps (fluid upstream)
   std::vector<long long> plane_fluid;  // fluid nodes per plane (k in 3D, j in 2D)
   void* ubuf = nullptr;        // [3][P or N] flow velocity for the solute launch
   void* prof_t = nullptr;      // [LX*LY] constant-concentration profiles (real)
@@ -43,6 +44,8 @@ struct lbx_domain {
   double* btc_vals = nullptr;  // [2][plane nodes]: C and u_x this step
   double* btc_rec = nullptr;   // [btc_cap][2] means
   int* btc_slot = nullptr;     // steps recorded
+  double* btc_part = nullptr;  // [kBtcMaxBlocks][2] block partials of one step
+  unsigned* btc_ticket = nullptr;  // blocks done this step (reset by the last)
   int btc_cap = 0;
   int btc_lo = 0, btc_hi = 0;  // node (dense) or slot (compact) range
   int btc_plane = 0;

@@ -565,6 +565,32 @@ aa_step(StepArgs<T> A)
 // (-1: solid; the face kernels use it), fnode[m] maps back, and frm holds
 // the fluid bitmask with word ranks the odd step finds neighbours in.  One
 // thread per fluid node.
+// The z-face operations of one step applied inside the compact step kernel
+// (the FACES3 instantiations) instead of by the stand-alone face_plane
+// kernel.  Exact wherever that kernel's deposit is read only by the face
+// node itself: always before an even step (it works on the node's own
+// slots), and before an odd step when every upstream node of every unknown
+// direction of every fluid face node is fluid (the host checks; otherwise
+// face_plane runs).  The bottom plane's fluid nodes are the compact indices
+// [0, lo_end), the top plane's [hi_start, F).  Per substance and face, the
+// operations in their configured order.
+constexpr int kFace3PerGroup = 6;   // pressure in/out, velocity in/out, constcon, zero gradient
+
+template <typename T>
+struct Face3Fused {
+  int lo_end, hi_start;
+  int nops[2][2];                        // [substance][top]
+  int kind[2][2][kFace3PerGroup];
+  T drho[2][2][kFace3PerGroup];          // pressure: rho_bc - rA; velocity: u_z
+  T shift[2][2][kFace3PerGroup];         // velocity: rA
+  const T* profile[2][2][kFace3PerGroup];  // constant concentration per (i, j), or NULL
+  T conc;
+};
+
+template <typename T>
+__device__ __forceinline__ void face3_apply(T (&d)[19], bool top, int kind, T drho, T conc,
+                                            T shift);
+
 template <typename T>
 struct CompactArgs {
   StepArgs<T> s;          // f = compact populations; N = dense node count
@@ -576,6 +602,11 @@ struct CompactArgs {
   int P;                  // plane stride of fc: F rounded up to 32 (aligned warps)
   FastDiv div_plane, div_lx;   // n / (LX*LY), r / LX
   int faces;              // 2D: fused face boundaries configured
+  Face3Fused<T> f3;       // 3D: read by the FACES3 kernels only
+  // the compact indices a launch covers: thread t takes m = t + m_base,
+  // moved on by m_jump once it reaches m_skip, up to m_end (the whole range
+  // [0, F), the interior between the z-face planes, or the two planes)
+  int m_base, m_skip, m_jump, m_end;
 };
 
 // Resident 256-thread blocks asked of the compiler: six (40 registers) for
@@ -596,7 +627,8 @@ constexpr int compact_min_blocks()
 // The update of fluid node m (compact index) by one block thread; the
 // odd step's slot table is indexed by threadIdx.x, so a block's threads
 // handle distinct nodes.
-template <typename T, int Q, int NS, int MODEL, bool ODD, int PART, bool IDX32, bool OOP>
+template <typename T, int Q, int NS, int MODEL, bool ODD, int PART, bool IDX32, bool OOP,
+          bool FACES3 = false>
 __device__ __forceinline__ void compact_node(const CompactArgs<T>& C, const int m)
 {
   using Idx = typename std::conditional<IDX32, unsigned, size_t>::type;
@@ -737,6 +769,24 @@ __device__ __forceinline__ void compact_node(const CompactArgs<T>& C, const int 
 #pragma unroll
       for (int a = 0; a < Q; ++a) d[a] = fs[opp(a) * F + m];
     }
+    if constexpr (FACES3 && Q == 19) {
+      // z faces: the stand-alone face_plane rules on the loaded populations
+      const bool bot = m < C.f3.lo_end, top = m >= C.f3.hi_start;
+      if (bot || top) {
+        const int tp = top ? 1 : 0;
+        const int cnt = C.f3.nops[s][tp];
+        for (int q = 0; q < cnt; ++q) {
+          T conc = C.f3.conc;
+          const T* prof = C.f3.profile[s][tp][q];
+          if (prof) {
+            const int nd = (ODD || A.write_mv) ? n : C.fnode[m];
+            conc = prof[nd - (top ? (A.LZ - 1) * plane : 0)];
+          }
+          face3_apply<T>(reinterpret_cast<T (&)[19]>(d), top, C.f3.kind[s][tp][q],
+                         C.f3.drho[s][tp][q], conc, C.f3.shift[s][tp][q]);
+        }
+      }
+    }
     if (faces && (j == 0 || j == LY - 1)) {
       T (&d9)[9] = reinterpret_cast<T (&)[9]>(d);
       const bool shifted = (MODEL != PLAIN_COMP) && !solute;
@@ -769,13 +819,15 @@ __device__ __forceinline__ void compact_node(const CompactArgs<T>& C, const int 
   }
 }
 
-template <typename T, int Q, int NS, int MODEL, bool ODD, int PART, bool IDX32, bool OOP>
+template <typename T, int Q, int NS, int MODEL, bool ODD, int PART, bool IDX32, bool OOP,
+          bool FACES3 = false>
 __global__ void __launch_bounds__(256, (compact_min_blocks<T, PART>()))
 aa_step_compact(CompactArgs<T> C)
 {
-  const int m = blockIdx.x * blockDim.x + threadIdx.x;
-  if (m >= C.F) return;
-  compact_node<T, Q, NS, MODEL, ODD, PART, IDX32, OOP>(C, m);
+  int m = blockIdx.x * blockDim.x + threadIdx.x + C.m_base;
+  if (m >= C.m_skip) m += C.m_jump;
+  if (m >= C.m_end) return;
+  compact_node<T, Q, NS, MODEL, ODD, PART, IDX32, OOP, FACES3>(C, m);
 }
 
 // Dense <-> compact exchange of all substances' populations.
@@ -1077,41 +1129,63 @@ __global__ void face_plane(T* f, const uint8_t* solids, const int* fidx, int LX,
 }
 
 // ---- plane record ---------------------------------------------------------------
-// One block: the means over the plane's fluid nodes of the recorded C
-// (channel 0, when the solute was active) and u_x (channel 1) into
-// rec[2 * slot + channel] (skipping solid nodes of a dense plane), then the
-// slot advances.  The sum order is fixed, so the record is reproducible.
-constexpr int kBtcThreads = 1024;
+// The means over the plane's fluid nodes of the recorded C (channel 0, when
+// the solute was active) and u_x (channel 1) into rec[2 * slot + channel]
+// (skipping solid nodes of a dense plane), then the slot advances.  Each
+// block sums a fixed chunk of the plane; the block that finishes last (a
+// ticket taken with an atomic counter, no waiting) adds the block partials
+// in block order, so the record is reproducible, and resets the counter for
+// the next step.
+constexpr int kBtcThreads = 256;
+constexpr int kBtcMaxBlocks = 64;
 
 static __global__ void __launch_bounds__(kBtcThreads)
 btc_reduce(const double* vals, int count, const uint8_t* plane_solids, double fluid,
-           int on_c, double* rec, int* slot, int capacity)
+           int on_c, double* rec, int* slot, int capacity, double* part, unsigned* ticket)
 {
-  __shared__ double part[2][kBtcThreads];
+  __shared__ double sh[2][kBtcThreads];
+  __shared__ int last;
+  const int per = (count + gridDim.x - 1) / gridDim.x;
+  const int q0 = blockIdx.x * per;
+  const int q1 = min(count, q0 + per);
   double sc = 0.0, su = 0.0;
-  for (int q = threadIdx.x; q < count; q += kBtcThreads)
+  for (int q = q0 + threadIdx.x; q < q1; q += kBtcThreads)
     if (!plane_solids || plane_solids[q] != 1) {
       if (on_c) sc += vals[q];
       su += vals[count + q];
     }
-  part[0][threadIdx.x] = sc;
-  part[1][threadIdx.x] = su;
+  sh[0][threadIdx.x] = sc;
+  sh[1][threadIdx.x] = su;
   __syncthreads();
   for (int w = kBtcThreads / 2; w > 0; w >>= 1) {
     if (threadIdx.x < w) {
-      part[0][threadIdx.x] += part[0][threadIdx.x + w];
-      part[1][threadIdx.x] += part[1][threadIdx.x + w];
+      sh[0][threadIdx.x] += sh[0][threadIdx.x + w];
+      sh[1][threadIdx.x] += sh[1][threadIdx.x + w];
     }
     __syncthreads();
   }
   if (threadIdx.x == 0) {
+    part[2 * blockIdx.x] = sh[0][0];
+    part[2 * blockIdx.x + 1] = sh[1][0];
+    __threadfence();
+    last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (last && threadIdx.x == 0) {
+    __threadfence();
+    double c = 0.0, u = 0.0;
+    for (int b = 0; b < (int)gridDim.x; ++b) {
+      c += __ldcg(part + 2 * b);
+      u += __ldcg(part + 2 * b + 1);
+    }
     const int k = *slot;
     const double nan = __longlong_as_double(0x7ff8000000000000LL);
     if (k < capacity) {
-      rec[2 * k] = (on_c && fluid > 0.0) ? part[0][0] / fluid : nan;
-      rec[2 * k + 1] = fluid > 0.0 ? part[1][0] / fluid : nan;
+      rec[2 * k] = (on_c && fluid > 0.0) ? c / fluid : nan;
+      rec[2 * k + 1] = fluid > 0.0 ? u / fluid : nan;
     }
     *slot = k + 1;
+    *ticket = 0u;
   }
 }
 

@@ -79,6 +79,12 @@ def cases():
         out.append((name, p, dt, 16, 4))
     p = po.Params(dims=2, LX=12, LY=10, LZ=1, tau=(0.9, 0.75), gaccel=g2, walsh=1)
     out.append(("d2q9w_f64", p, np.float64, 18, 6))
+    # the solute switched on at t = 7 and off after t = 14 with zero-gradient
+    # faces: the reference runs its face kernels on the idle solute too
+    p = po.Params(dims=2, LX=12, LY=10, LZ=1, tau=(0.9, 0.75), gaccel=g2,
+                  **dict(bc, nsubs=2, sink=1e-3, zeroconcgrad_n=1, zeroconcgrad_s=1,
+                         sigma_t_on=7, sigma_t_off=14))
+    out.append(("d2q9s_bc_gate_f64", p, np.float64, 18, 6))
     return out
 
 

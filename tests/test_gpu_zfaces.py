@@ -190,3 +190,37 @@ def test_gpu_velocity_face_imposes_the_momentum(model, prec):
     tol = 1e-12 if prec == 8 else 2e-6
     assert np.allclose(uz * den, rho * -0.02, rtol=tol, atol=0)
     assert np.max(np.abs(ux)) < 0.05 and np.max(np.abs(uy)) < 0.05
+
+
+@pytest.mark.parametrize("case", ["inlet_bottom", "velocity_top_in", "velocity_both"])
+def test_gpu_z_faces_fused_equal_standalone(case):
+    """With fluid planes across the z wrap the compact layout applies the z
+    faces inside a step launch over the two face planes (no stand-alone
+    face-plane kernel); the dense layout keeps the stand-alone face kernels.
+    FP64 results are bit-identical."""
+    p, sol, f0 = _flow_solute(18, 16, 12, 0.6, 13, **CASES[case])
+    m3 = sol.reshape(12, 16, 18)
+    m3[0] = 0
+    m3[-1] = 0
+    sol = m3.reshape(-1)
+    if case == "inlet_bottom":
+        p.constcon_profile_b = np.random.default_rng(2).uniform(0, 1, p.LX * p.LY)
+    out = {}
+    for layout in ("dense", "compact"):
+        with lbx.Domain(to_lbx(p, np.float64, layout), sol) as d:
+            if p.constcon_profile_b is not None:
+                d.set_face_profile(False, p.constcon_profile_b)
+            d.upload_f(f0)
+            n0 = d.launch_count()
+            for t in range(1, 31):
+                d.step(t, write_mv=(t == 30))
+            launches = d.launch_count() - n0
+            d.sync()
+            out[layout] = (d.download_f(), d.download_mv(), launches)
+    assert np.array_equal(out["dense"][0], out["compact"][0])
+    assert np.array_equal(out["dense"][1], out["compact"][1])
+    # dense: face plane + flow + solute per step; compact: flow and solute
+    # over the interior, then the two face planes (every substance)
+    assert out["compact"][2] == 3 * 30 and out["dense"][2] == 3 * 30
+    fo, mvo = po.run_oracle(p, f0.copy(), sol, 0, 30, 30)
+    assert_close(out["compact"][0], out["compact"][1], fo, mvo, sol, np.float64)
