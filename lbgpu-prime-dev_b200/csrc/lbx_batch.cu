@@ -69,8 +69,7 @@ struct BatchArgs {
   const uint2* frm;             // per sample, ceil(N/32) words: (global compact index
                                 // of the word's first fluid node, fluid bits)
   const int* fnode;             // [Ftot]: dense index inside the sample, -1 padding
-  const SampleDesc<T>* samples;
-  const int* blk_sample;        // [nblocks]
+  const SampleDesc<T>* blkdesc; // [nblocks]: the descriptor of each block's sample
   long long Ftot;
   int nblocks;                  // blocks of the current block size
   int block0;                   // first block (SEQUENTIAL mode)
@@ -83,13 +82,19 @@ struct BatchArgs {
 // sample: its extents, constants and rank table, whose word ranks are
 // global compact indices, so the neighbours it finds are slots of the
 // shared population array.
+// The block's sample descriptor is stored per block, so it is one load
+// that depends only on the block index.  An even step also updates the
+// padding slots after a sample, in place like any node's own slots: no real
+// node ever reads them, so whatever values they take never reach a sample,
+// and the step's population loads need not wait for the descriptor.  An odd
+// step (whose neighbour lookups need a real node) and a step writing the
+// macro variables skip the padding.
 template <typename T, int Q, int MODEL, bool ODD, bool IDX32>
 __device__ __forceinline__ void batch_block(const BatchArgs<T>& A, int b)
 {
-  const int s = A.blk_sample[b];
-  const SampleDesc<T>& S = A.samples[s];
+  const SampleDesc<T>& S = A.blkdesc[b];
   const int m = b * blockDim.x + threadIdx.x;            // global compact index
-  if (m - S.cbase >= S.F) return;                        // padding after the sample
+  if ((ODD || A.write_mv) && m - S.cbase >= S.F) return;   // padding after the sample
   CompactArgs<T> C;
   StepArgs<T>& L = C.s;
   L.f = A.f;
@@ -174,8 +179,7 @@ struct lbx_batch {
   uint2* frm = nullptr;       // per-sample rank tables (BatchArgs::frm)
   int* fnode = nullptr;
   uint8_t* solids = nullptr;
-  void* samples = nullptr;    // SampleDesc<T>[nsamples]
-  int* blk_sample[2] = {nullptr, nullptr};   // block sizes 128, 256
+  void* blkdesc[2] = {nullptr, nullptr};   // SampleDesc<real> per block, block sizes 128, 256
   int nblocks[2] = {0, 0};
   void* red = nullptr;
   cudaStream_t stream = nullptr, own_stream = nullptr;
@@ -202,8 +206,7 @@ BatchArgs<T> batch_args(lbx_batch* b, int write_mv)
   BatchArgs<T> A;
   std::memset(&A, 0, sizeof A);
   A.f = (T*)b->fc; A.mv = (T*)b->mv; A.frm = b->frm; A.fnode = b->fnode;
-  A.samples = (const SampleDesc<T>*)b->samples;
-  A.blk_sample = b->blk_sample[b->bs_index];
+  A.blkdesc = (const SampleDesc<T>*)b->blkdesc[b->bs_index];
   A.Ftot = b->Ftot; A.nblocks = b->nblocks[b->bs_index];
   A.write_mv = write_mv;
   A.kahan = b->kahan;
@@ -246,7 +249,7 @@ lbx_status launch_persistent(lbx_batch* b, int steps, bool odd_first)
 {
   BatchArgs<T> A = batch_args<T, Q, MODEL>(b, 0);
   // the persistent kernel is compiled for 256-thread blocks
-  A.blk_sample = b->blk_sample[1];
+  A.blkdesc = (const SampleDesc<T>*)b->blkdesc[1];
   A.nblocks = b->nblocks[1];
   const bool idx32 = (unsigned long long)Q * (unsigned long long)b->Ftot < (1ull << 32);
   if (b->coop_grid == 0) {
@@ -333,8 +336,8 @@ void release(lbx_batch* b)
 {
   if (b->graph) cudaGraphExecDestroy(b->graph);
   cudaFree(b->fc); cudaFree(b->fdense); cudaFree(b->mv); cudaFree(b->frm);
-  cudaFree(b->fnode); cudaFree(b->solids); cudaFree(b->samples); cudaFree(b->red);
-  for (int i = 0; i < kNumBlockSizes; ++i) cudaFree(b->blk_sample[i]);
+  cudaFree(b->fnode); cudaFree(b->solids); cudaFree(b->red);
+  for (int i = 0; i < kNumBlockSizes; ++i) cudaFree(b->blkdesc[i]);
   if (b->own_stream) cudaStreamDestroy(b->own_stream);
 }
 
@@ -559,25 +562,23 @@ lbx_status lbx_batch_create(int nsamples, const lbx_params* params, const uint8_
   BCKD(cudaMemset(b->fc, 0, std::max<size_t>(1, (size_t)b->Q * b->Ftot * rs)));
   BCKD(cudaMemset(b->fdense, 0, (size_t)b->Q * b->Ntot * rs));
   BCKD(cudaMemset(b->mv, 0, (size_t)(1 + b->dims) * b->Ntot * rs));
-  {
-    std::vector<unsigned char> desc;
-    if (b->precision == 8) fill_desc<double>(b, desc); else fill_desc<float>(b, desc);
-    BCKD(cudaMalloc(&b->samples, desc.size()));
-    BCKD(cudaMemcpy(b->samples, desc.data(), desc.size(), cudaMemcpyHostToDevice));
-  }
+  std::vector<unsigned char> desc;   // per sample
+  if (b->precision == 8) fill_desc<double>(b, desc); else fill_desc<float>(b, desc);
+  const size_t dsz = desc.size() / (size_t)nsamples;
   for (int i = 0; i < kNumBlockSizes; ++i) {
-    // every block of a sample's padded range belongs to that sample, so a
-    // padding thread finds m - cbase >= F and exits
+    // every block of a sample's padded range belongs to that sample and
+    // holds a copy of its descriptor; a padding thread finds m - cbase >= F
     const int bs = kBlockSizes[i];
     const int nb = (int)(b->Ftot / bs);
-    std::vector<int> tab(std::max(nb, 1), 0);
+    std::vector<unsigned char> tab((size_t)std::max(nb, 1) * dsz, 0);
     for (int s : b->order) {
       const long long len = (b->F[s] + kAlign - 1) / kAlign * kAlign;
-      for (long long q = b->cbase[s] / bs; q < (b->cbase[s] + len) / bs; ++q) tab[q] = s;
+      for (long long q = b->cbase[s] / bs; q < (b->cbase[s] + len) / bs; ++q)
+        std::memcpy(tab.data() + (size_t)q * dsz, desc.data() + (size_t)s * dsz, dsz);
     }
     b->nblocks[i] = nb;
-    BCKD(cudaMalloc(&b->blk_sample[i], tab.size() * sizeof(int)));
-    BCKD(cudaMemcpy(b->blk_sample[i], tab.data(), tab.size() * sizeof(int), cudaMemcpyHostToDevice));
+    BCKD(cudaMalloc(&b->blkdesc[i], tab.size()));
+    BCKD(cudaMemcpy(b->blkdesc[i], tab.data(), tab.size(), cudaMemcpyHostToDevice));
   }
 #undef BCKD
   *out = b;

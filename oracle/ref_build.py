@@ -4,6 +4,10 @@ Test infrastructure only.  Nothing in the product path imports or links this.
 
 The artefacts, written only into ``oracle/_ref/``, are
 
+* ``refgpu_<variant>`` -- the same kernels compiled by nvcc for sm_100a and
+  launched on the GPU as the reference's serial main launches them
+  (``oracle/refgpu_harness.cu``), for GPU-against-GPU parity and a timing of
+  the reference's kernels on the same device.
 * ``librefk_<variant>.so`` -- the reference's CUDA kernel sources
   (``src/k_stream_collide_stream.c``, ``src/k_collide.c``,
   ``src/system_boundary_kernels.c`` and the device helpers in
@@ -129,6 +133,26 @@ def build(src: str, only=None) -> None:
             "-o", os.path.join(OUT, "librefk_%s.so" % name), "-lm"])
 
 
+# The reference's CUDA step kernels, compiled for sm_100a by nvcc into
+# oracle/_ref/refgpu_<variant> through oracle/refgpu_harness.cu.
+GPU_VARIANTS = ["d3q19_f32", "d3q19_f64"]
+
+
+def build_gpu(src: str, only=None) -> None:
+    os.makedirs(OUT, exist_ok=True)
+    for name in GPU_VARIANTS:
+        if only and name not in only:
+            continue
+        vdir = os.path.join(OUT, name)
+        os.makedirs(vdir, exist_ok=True)
+        fl = os.path.join(vdir, "flags.h")
+        with open(fl, "w") as fh:
+            fh.write(variant_flags(src, VARIANTS[name]))
+        sh(["nvcc", "-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-w",
+            "-include", fl, "-I", src, os.path.join(HERE, "refgpu_harness.cu"),
+            "-o", os.path.join(OUT, "refgpu_%s" % name)])
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--src", default=DEFAULT_SRC)
@@ -138,6 +162,7 @@ def main(argv=None) -> int:
         print("reference tree not present; oracle/_ref not rebuilt")
         return 0
     build(a.src, a.only)
+    build_gpu(a.src, a.only)
     return 0
 
 
