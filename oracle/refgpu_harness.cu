@@ -70,7 +70,7 @@ static void refgpu_const(const V& sym, const void* src, size_t n)
 
 int main(int argc, char** argv)
 {
-  if (argc < 16) {
+  if (argc < 15) {
     fprintf(stderr, "usage: refgpu LX LY LZ BX BY BZ tau gx gy gz steps mask f_in f_out [time]\n");
     return 1;
   }
