@@ -7,6 +7,14 @@
 // samples and a block finds its sample from a per-block table.  Samples are
 // laid out largest first, so the tail of every step is made of small blocks.
 //
+// Sample descriptors (extents, constants, table addresses) live in a pool in
+// constant memory, written once when the batch is created: a block finds its
+// sample by a block-uniform search of the samples' first blocks and reads
+// the descriptor from the constant bank where the update uses it, so the
+// per-sample values cost the thread no registers, as the single-lattice
+// kernels' arguments do.  A batch whose descriptors do not fit the pool's
+// free space reads them from a per-block table in global memory instead.
+//
 // Modes (lbx_batch_run):
 //   FUSED       one launch per lattice step covering every sample; runs of
 //               steps are replayed from a captured CUDA graph;
@@ -27,6 +35,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <numeric>
 #include <type_traits>
 #include <vector>
@@ -50,16 +59,28 @@ lbx_status bfail(lbx_status code, const char* fmt, ...)
 }
 
 template <typename T>
-struct SampleDesc {
-  int LX, LY, LZ, plane;
+struct alignas(16) SampleDesc {
+  const uint2* frm;     // the sample's rank table, word 0 (device)
+  T* mv;                // the sample's macro variables [1+D][N] (device)
   long long N;          // dense nodes
-  long long dbase;      // first dense node of the sample in the solids array
-  long long mvbase;     // first macro-variable element: [1+D][N]
+  int LX, LY, LZ;
   int cbase;            // first compact index (a multiple of kAlign)
   int F;                // fluid nodes
-  long long frm_base;   // the sample's word 0 in the rank table
   FastDiv div_plane, div_lx;
   SubsConst<T> sc;
+};
+
+// The descriptor pool (one per device, as constant memory is).  A batch's
+// range holds its descriptors in layout order, then for each block size the
+// first block of each sample in layout order and the end of the last.
+constexpr int kPoolBytes = 63 * 1024;
+__constant__ __align__(16) unsigned char g_pool[kPoolBytes];
+
+struct PoolRef {
+  int desc;             // byte offset of the descriptors in g_pool
+  int starts;           // byte offset of the first-block table in g_pool
+  int s_lo, s_hi;       // samples (layout positions) this launch covers
+  int block0;           // the launch's first block in the batch
 };
 
 template <typename T>
@@ -70,9 +91,10 @@ struct BatchArgs {
                                 // of the word's first fluid node, fluid bits)
   const int* fnode;             // [Ftot]: dense index inside the sample, -1 padding
   const SampleDesc<T>* blkdesc; // [nblocks]: the descriptor of each block's sample
+                                // (global-memory path)
   long long Ftot;
   int nblocks;                  // blocks of the current block size
-  int block0;                   // first block (SEQUENTIAL mode)
+  int block0;                   // first block (SEQUENTIAL mode, global-memory path)
   int write_mv;
   int kahan;                    // compensated density sums
 };
@@ -82,23 +104,21 @@ struct BatchArgs {
 // sample: its extents, constants and rank table, whose word ranks are
 // global compact indices, so the neighbours it finds are slots of the
 // shared population array.
-// The block's sample descriptor is stored per block, so it is one load
-// that depends only on the block index.  An even step also updates the
+// An even step also updates the
 // padding slots after a sample, in place like any node's own slots: no real
 // node ever reads them, so whatever values they take never reach a sample,
 // and the step's population loads need not wait for the descriptor.  An odd
 // step (whose neighbour lookups need a real node) and a step writing the
 // macro variables skip the padding.
 template <typename T, int Q, int MODEL, bool ODD, bool IDX32>
-__device__ __forceinline__ void batch_block(const BatchArgs<T>& A, int b)
+__device__ __forceinline__ void batch_node(const SampleDesc<T>& S, const BatchArgs<T>& A,
+                                           const int m)
 {
-  const SampleDesc<T>& S = A.blkdesc[b];
-  const int m = b * blockDim.x + threadIdx.x;            // global compact index
   if ((ODD || A.write_mv) && m - S.cbase >= S.F) return;   // padding after the sample
   CompactArgs<T> C;
   StepArgs<T>& L = C.s;
   L.f = A.f;
-  L.mv = A.mv + S.mvbase;
+  L.mv = S.mv;
   L.LX = S.LX; L.LY = S.LY; L.LZ = S.LZ;
   L.N = S.N;
   L.sc[0] = S.sc;
@@ -110,13 +130,21 @@ __device__ __forceinline__ void batch_block(const BatchArgs<T>& A, int b)
   L.fout = nullptr;
   L.ns = nullptr;
   C.fnode = A.fnode;
-  C.frm = A.frm + S.frm_base;
+  C.frm = S.frm;
   C.F = S.cbase + S.F;
   C.P = (int)A.Ftot;
   C.div_plane = S.div_plane;
   C.div_lx = S.div_lx;
   C.faces = 0;
   compact_node<T, Q, 1, MODEL, ODD, PART_ALL, IDX32, false>(C, m);
+}
+
+// Global-memory path: the block's descriptor from the per-block table, one
+// load that depends only on the block index.
+template <typename T, int Q, int MODEL, bool ODD, bool IDX32>
+__device__ __forceinline__ void batch_block(const BatchArgs<T>& A, int b)
+{
+  batch_node<T, Q, MODEL, ODD, IDX32>(A.blkdesc[b], A, b * blockDim.x + threadIdx.x);
 }
 
 // Up to 256 threads per block, resident blocks as for the single-lattice
@@ -126,6 +154,24 @@ __global__ void __launch_bounds__(256, (compact_min_blocks<T, PART_ALL>()))
 aa_step_batch(BatchArgs<T> A)
 {
   batch_block<T, Q, MODEL, ODD, IDX32>(A, A.block0 + blockIdx.x);
+}
+
+// Pool path: the block's sample is the last of samples s_lo..s_hi whose
+// first block is at most the block's (a sample with no fluid node shares its
+// first block with the next one and is never chosen).
+template <typename T, int Q, int MODEL, bool ODD, bool IDX32>
+__global__ void __launch_bounds__(256, (compact_min_blocks<T, PART_ALL>()))
+aa_step_batch_pool(BatchArgs<T> A, PoolRef R)
+{
+  const int* starts = reinterpret_cast<const int*>(g_pool + R.starts);
+  const int bl = R.block0 + blockIdx.x;
+  int lo = R.s_lo, hi = R.s_hi;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (starts[mid] <= bl) lo = mid; else hi = mid - 1;
+  }
+  const SampleDesc<T>* desc = reinterpret_cast<const SampleDesc<T>*>(g_pool + R.desc);
+  batch_node<T, Q, MODEL, ODD, IDX32>(desc[lo], A, bl * blockDim.x + threadIdx.x);
 }
 
 // Persistent: a resident grid walks all blocks of the batch for `steps`
@@ -180,6 +226,11 @@ struct lbx_batch {
   int* fnode = nullptr;
   uint8_t* solids = nullptr;
   void* blkdesc[2] = {nullptr, nullptr};   // SampleDesc<real> per block, block sizes 128, 256
+  int device = 0;
+  int pool_off = -1;          // the batch's range in g_pool (bytes), -1: none
+  int pool_len = 0;
+  int pool_desc = 0;          // offsets in g_pool: descriptors, first-block tables
+  int pool_starts[2] = {0, 0};
   int nblocks[2] = {0, 0};
   void* red = nullptr;
   cudaStream_t stream = nullptr, own_stream = nullptr;
@@ -219,7 +270,17 @@ lbx_status launch_step(lbx_batch* b, bool odd, int write_mv, int mode)
   BatchArgs<T> A = batch_args<T, Q, MODEL>(b, write_mv);
   const int bs = kBlockSizes[b->bs_index];
   const bool idx32 = (unsigned long long)Q * (unsigned long long)b->Ftot < (1ull << 32);
-  auto go = [&](unsigned nb) {
+  auto go_pool = [&](unsigned nb, const PoolRef& R) {
+    if (idx32) {
+      if (odd) aa_step_batch_pool<T, Q, MODEL, true, true><<<nb, bs, 0, b->stream>>>(A, R);
+      else aa_step_batch_pool<T, Q, MODEL, false, true><<<nb, bs, 0, b->stream>>>(A, R);
+    } else {
+      if (odd) aa_step_batch_pool<T, Q, MODEL, true, false><<<nb, bs, 0, b->stream>>>(A, R);
+      else aa_step_batch_pool<T, Q, MODEL, false, false><<<nb, bs, 0, b->stream>>>(A, R);
+    }
+    b->launches++;
+  };
+  auto go_global = [&](unsigned nb) {
     if (idx32) {
       if (odd) aa_step_batch<T, Q, MODEL, true, true><<<nb, bs, 0, b->stream>>>(A);
       else aa_step_batch<T, Q, MODEL, false, true><<<nb, bs, 0, b->stream>>>(A);
@@ -229,15 +290,33 @@ lbx_status launch_step(lbx_batch* b, bool odd, int write_mv, int mode)
     }
     b->launches++;
   };
+  const bool pool = b->pool_off >= 0;
+  PoolRef R;
+  R.desc = b->pool_desc;
+  R.starts = b->pool_starts[b->bs_index];
   if (mode == LBX_BATCH_SEQUENTIAL) {
-    for (int s : b->order) {
+    for (int i = 0; i < b->nsamples; ++i) {
+      const int s = b->order[i];
       if (b->F[s] == 0) continue;
-      A.block0 = b->cbase[s] / bs;
-      go((unsigned)((b->F[s] + bs - 1) / bs));
+      const unsigned nb = (unsigned)((b->F[s] + bs - 1) / bs);
+      if (pool) {
+        R.s_lo = R.s_hi = i;
+        R.block0 = b->cbase[s] / bs;
+        go_pool(nb, R);
+      } else {
+        A.block0 = b->cbase[s] / bs;
+        go_global(nb);
+      }
     }
-  } else {
-    if (A.nblocks == 0) return LBX_OK;
-    go((unsigned)A.nblocks);
+  } else if (A.nblocks > 0) {
+    if (pool) {
+      R.s_lo = 0;
+      R.s_hi = b->nsamples - 1;
+      R.block0 = 0;
+      go_pool((unsigned)A.nblocks, R);
+    } else {
+      go_global((unsigned)A.nblocks);
+    }
   }
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return bfail(LBX_ERR_CUDA, "batch step: %s", cudaGetErrorString(e));
@@ -318,9 +397,11 @@ void fill_desc(lbx_batch* b, std::vector<unsigned char>& out)
     const lbx_params& p = b->params[s];
     SampleDesc<T>& x = d[s];
     std::memset(&x, 0, sizeof x);
-    x.LX = p.LX; x.LY = p.LY; x.LZ = p.LZ; x.plane = p.LX * p.LY;
-    x.N = b->N[s]; x.dbase = b->dbase[s]; x.mvbase = b->mvbase[s];
-    x.cbase = b->cbase[s]; x.F = b->F[s]; x.frm_base = b->frm_base[s];
+    x.LX = p.LX; x.LY = p.LY; x.LZ = p.LZ;
+    x.N = b->N[s];
+    x.cbase = b->cbase[s]; x.F = b->F[s];
+    x.frm = b->frm + b->frm_base[s];
+    x.mv = (T*)b->mv + b->mvbase[s];
     x.div_plane = make_fastdiv((unsigned)(p.LX * p.LY));
     x.div_lx = make_fastdiv((unsigned)p.LX);
     const T tau = (T)p.tau[0];
@@ -332,6 +413,70 @@ void fill_desc(lbx_batch* b, std::vector<unsigned char>& out)
   std::memcpy(out.data(), d.data(), out.size());
 }
 
+// g_pool's ranges in use on each device: (offset, length), sorted.
+constexpr int kPoolDevices = 64;
+std::mutex g_pool_mu;
+std::vector<std::pair<int, int>> g_pool_used[kPoolDevices];
+
+// First fit of `len` bytes (a multiple of 16) on `dev`; -1 when none is free.
+int pool_claim(int dev, int len)
+{
+  if (dev < 0 || dev >= kPoolDevices || len <= 0 || len > kPoolBytes) return -1;
+  std::lock_guard<std::mutex> lock(g_pool_mu);
+  std::vector<std::pair<int, int>>& used = g_pool_used[dev];
+  int at = 0;
+  size_t i = 0;
+  for (; i < used.size(); ++i) {
+    if (used[i].first - at >= len) break;
+    at = used[i].first + used[i].second;
+  }
+  if (i == used.size() && kPoolBytes - at < len) return -1;
+  used.insert(used.begin() + (long)i, std::make_pair(at, len));
+  return at;
+}
+
+void pool_release(int dev, int off)
+{
+  if (off < 0 || dev < 0 || dev >= kPoolDevices) return;
+  std::lock_guard<std::mutex> lock(g_pool_mu);
+  std::vector<std::pair<int, int>>& used = g_pool_used[dev];
+  for (size_t i = 0; i < used.size(); ++i)
+    if (used[i].first == off) { used.erase(used.begin() + (long)i); return; }
+}
+
+// The batch's pool range: descriptors in layout order, then the first-block
+// tables of both block sizes.  Leaves pool_off at -1 (the global-memory
+// path) when the pool has no room.
+template <typename T>
+cudaError_t pool_fill(lbx_batch* b, const std::vector<unsigned char>& desc)
+{
+  const int n = b->nsamples;
+  const long long dbytes = (long long)n * (long long)sizeof(SampleDesc<T>);
+  const long long sbytes = ((long long)(n + 1) * 4 + 15) / 16 * 16;
+  const long long len = dbytes + kNumBlockSizes * sbytes;
+  if (len > kPoolBytes) return cudaSuccess;
+  const int off = pool_claim(b->device, (int)len);
+  if (off < 0) return cudaSuccess;
+  std::vector<unsigned char> img((size_t)len, 0);
+  for (int i = 0; i < n; ++i)
+    std::memcpy(img.data() + (size_t)i * sizeof(SampleDesc<T>),
+                desc.data() + (size_t)b->order[i] * sizeof(SampleDesc<T>), sizeof(SampleDesc<T>));
+  for (int k = 0; k < kNumBlockSizes; ++k) {
+    const int bs = kBlockSizes[k];
+    int* st = (int*)(img.data() + dbytes + k * sbytes);
+    for (int i = 0; i < n; ++i) st[i] = b->cbase[b->order[i]] / bs;
+    st[n] = (int)(b->Ftot / bs);
+  }
+  cudaError_t e = cudaMemcpyToSymbol(g_pool, img.data(), (size_t)len, (size_t)off,
+                                     cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) { pool_release(b->device, off); return e; }
+  b->pool_off = off;
+  b->pool_len = (int)len;
+  b->pool_desc = off;
+  for (int k = 0; k < kNumBlockSizes; ++k) b->pool_starts[k] = (int)(off + dbytes + k * sbytes);
+  return cudaSuccess;
+}
+
 void release(lbx_batch* b)
 {
   if (b->graph) cudaGraphExecDestroy(b->graph);
@@ -339,6 +484,8 @@ void release(lbx_batch* b)
   cudaFree(b->fnode); cudaFree(b->solids); cudaFree(b->red);
   for (int i = 0; i < kNumBlockSizes; ++i) cudaFree(b->blkdesc[i]);
   if (b->own_stream) cudaStreamDestroy(b->own_stream);
+  pool_release(b->device, b->pool_off);
+  b->pool_off = -1;
 }
 
 lbx_status exchange(lbx_batch* b, int s, bool to_compact)
@@ -479,6 +626,7 @@ lbx_status lbx_batch_create(int nsamples, const lbx_params* params, const uint8_
   }
   BCK(cudaSetDevice(p0.device));
   lbx_batch* b = new lbx_batch();
+  b->device = p0.device;
   b->nsamples = nsamples;
   b->dims = p0.dims;
   b->Q = p0.dims == 2 ? 9 : 19;
@@ -565,6 +713,7 @@ lbx_status lbx_batch_create(int nsamples, const lbx_params* params, const uint8_
   std::vector<unsigned char> desc;   // per sample
   if (b->precision == 8) fill_desc<double>(b, desc); else fill_desc<float>(b, desc);
   const size_t dsz = desc.size() / (size_t)nsamples;
+  BCKD(b->precision == 8 ? pool_fill<double>(b, desc) : pool_fill<float>(b, desc));
   for (int i = 0; i < kNumBlockSizes; ++i) {
     // every block of a sample's padded range belongs to that sample and
     // holds a copy of its descriptor; a padding thread finds m - cbase >= F

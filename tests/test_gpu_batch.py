@@ -64,3 +64,60 @@ def test_batch_autotune_keeps_state_and_picks_a_mode():
         b.run(0, 10, 10)
         r = b.reduce(0)
         assert r["fluid_nodes"] == int((masks[0] != 1).sum())
+
+
+def _check_against_oracle(params, masks, f0, out, steps, tol=1e-12):
+    for i, p in enumerate(params):
+        q = po.Params(dims=3, LX=p.LX, LY=p.LY, LZ=p.LZ, tau=tuple(p.tau),
+                      gaccel=tuple(p.gaccel))
+        fo, mvo = po.run_oracle(q, f0[i].reshape(1, 19, -1).copy(), masks[i], 0, steps, steps,
+                                threads=1)
+        assert rel_err(out[i][0], fo[0]) <= tol, (i, rel_err(out[i][0], fo[0]))
+        fl = masks[i] != 1
+        if fl.any():
+            assert rel_err(out[i][1][0], mvo[0, 0], fl) <= tol, i
+
+
+def _run_batch(b, params, f0, steps, mode="fused"):
+    for i in range(len(params)):
+        b.upload_f(i, f0[i])
+    b.run(0, steps, steps, mode=mode)
+    b.sync()
+    return [(b.download_f(i), b.download_mv(i)) for i in range(len(params))]
+
+
+@pytest.mark.parametrize("mode", ["fused", "sequential"])
+def test_batch_beyond_the_descriptor_pool(mode):
+    """600 FP64 samples: their descriptors (112 bytes each) do not fit the
+    constant-memory pool (63 KB), so the batch reads them from its per-block
+    table in global memory.  Every sample still evolves as the oracle's run
+    of it alone, empty and all-fluid samples included."""
+    params, masks = make_samples(600, seed=21, prec=8, sizes=(3, 8))
+    masks[5][:] = 1                       # a sample without fluid nodes
+    masks[9][:] = 0                       # an all-fluid sample
+    rng = np.random.default_rng(4)
+    f0 = [rng.standard_normal((19, p.NN)) * 1e-4 for p in params]
+    with Batch(params, masks) as b:
+        out = _run_batch(b, params, f0, 11, mode)
+    _check_against_oracle(params, masks, f0, out, 11)
+
+
+def test_batches_alive_together_keep_their_own_descriptors():
+    """Batches alive at the same time hold disjoint ranges of the descriptor
+    pool; a destroyed batch's range goes to the next batch that fits it, and
+    the batch created in between keeps its own."""
+    pa, ma = make_samples(5, seed=31, prec=8)
+    pb, mb = make_samples(4, seed=32, prec=8)
+    pc, mc = make_samples(3, seed=33, prec=8)
+    rng = np.random.default_rng(5)
+    fa, fb, fc = ([rng.standard_normal((19, p.NN)) * 1e-4 for p in ps] for ps in (pa, pb, pc))
+    ba = Batch(pa, ma)
+    with Batch(pb, mb) as bb:
+        out_a = _run_batch(ba, pa, fa, 13)
+        ba.close()
+        with Batch(pc, mc) as bc:
+            out_b = _run_batch(bb, pb, fb, 13)
+            out_c = _run_batch(bc, pc, fc, 13)
+    _check_against_oracle(pa, ma, fa, out_a, 13)
+    _check_against_oracle(pb, mb, fb, out_b, 13)
+    _check_against_oracle(pc, mc, fc, out_c, 13)

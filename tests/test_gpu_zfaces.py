@@ -192,6 +192,39 @@ def test_gpu_velocity_face_imposes_the_momentum(model, prec):
     assert np.max(np.abs(ux)) < 0.05 and np.max(np.abs(uy)) < 0.05
 
 
+@pytest.mark.parametrize("layout", ["dense", "compact"])
+@pytest.mark.parametrize("prec", [8, 4])
+def test_gpu_pressure_faces_impose_the_density(layout, prec):
+    """Every fluid node of a Zou-He pressure face leaves an even step with
+    the imposed density: the rule sets the unknowns so that the node's
+    populations sum to rho_in (bottom) / rho_out (top), and the even step
+    collides those populations in place, so its rho is that sum (the shifted
+    sums plus rho_A).  After an odd step the node holds populations pulled
+    from its neighbours, whose sum is not pinned.  Checked in a developed run
+    of the flow + solute lattice, both z faces, solid neighbours included."""
+    LX, LY, LZ = 24, 20, 32
+    lp = lbx.Params(dims=3, LX=LX, LY=LY, LZ=LZ, nsubs=2, precision=prec, tau=(0.9, 0.7),
+                    pressure_b_in=(1, 0), pressure_t_out=(1, 0), rho_in=1.0012,
+                    rho_out=0.9995, constcon_b_in=1, zeroconcgrad_t=1, rho_sigma_in=1.0,
+                    layout=lbx.LBX_LAYOUT_DENSE if layout == "dense" else lbx.LBX_LAYOUT_COMPACT)
+    sol = geometry.sphere_pack(LX, LY, LZ, radius=3, porosity=0.6, seed=14)
+    with lbx.Domain(lp, sol) as d:
+        d.init_equilibrium(0, 1.0, 0.0, 0.0, 0.0)
+        d.init_equilibrium(1, 0.0, 0.0, 0.0, 0.0)
+        d.run(0, 200, 200)             # ends on an even (in-place) step
+        d.sync()
+        mv = d.download_mv()[0].astype(np.float64).reshape(4, LZ, LY, LX)
+    tol = 1e-12 if prec == 8 else 2e-6
+    for k, rho_bc in ((0, 1.0012), (LZ - 1, 0.9995)):
+        fluid = sol.reshape(LZ, LY, LX)[k] != 1
+        rho = mv[0, k][fluid]
+        assert fluid.any()
+        assert np.abs(rho - rho_bc).max() <= tol * rho_bc, (k, np.abs(rho - rho_bc).max())
+    # the flow is developed: the interior density lies between the two
+    inner = mv[0, LZ // 2][sol.reshape(LZ, LY, LX)[LZ // 2] != 1]
+    assert 0.9995 < inner.mean() < 1.0012
+
+
 @pytest.mark.parametrize("case", ["inlet_bottom", "velocity_top_in", "velocity_both"])
 def test_gpu_z_faces_fused_equal_standalone(case):
     """With fluid planes across the z wrap the compact layout applies the z
