@@ -192,6 +192,21 @@ lbx_status lbx_run(lbx_domain* d, int t0, int nsteps, int frame_rate);
  * own work and time them with its own events. */
 lbx_status lbx_set_stream(lbx_domain* d, void* stream);
 
+/* How lbx_run advances a stretch of frame-free AA pairs whose launch
+ * arguments do not change (no extension of the reference's interface: the
+ * reference launches every step, src/lbgpu_prime.cu:517-527, :741-750).
+ *   LBX_RUN_AUTO   (default) the tiled path where it applies and the lattice
+ *                  is small enough for it to pay, else STEPS;
+ *   LBX_RUN_STEPS  one launch per step, replayed from captured CUDA graphs;
+ *   LBX_RUN_TILED  the tiled path wherever it applies: 2D, one substance, no
+ *                  Walsh run, no plane record, faces absent or fused.  One
+ *                  cooperative launch runs rounds of K steps (K = 4 in FP64,
+ *                  6 in FP32) on tiles held in shared memory with halos K
+ *                  deep; FP64 results are bit-identical to STEPS.
+ * LBX_ERR_INVALID for another mode. */
+enum { LBX_RUN_AUTO = 0, LBX_RUN_STEPS = 1, LBX_RUN_TILED = 2 };
+lbx_status lbx_set_run_mode(lbx_domain* d, int mode);
+
 /* Wait for all queued work of the domain; reports asynchronous errors. */
 lbx_status lbx_sync(lbx_domain* d);
 

@@ -62,7 +62,19 @@ struct lbx_domain {
   unsigned char graph_key[2 * 640];      // keys of the odd and the even step
   size_t graph_key_len = 0;
   long long graph_launches = 0;          // kernels one replay of the graph runs
+  // temporal blocking of small 2D lattices (lbx_tiled.cu)
+  int run_mode = LBX_RUN_AUTO;
+  void* tiled_scratch = nullptr;         // a second population array for its rounds
+  int* tiled_flags = nullptr;            // per-tile round counters, then a status word
+  int4* tiled_plan = nullptr;            // per tile: x, y, height
+  int* tiled_nbrs = nullptr;             // per tile: the tiles its halo reads
+  int tiled_ntiles = 0;
+  bool tiled_local = false;              // tiles wait for their neighbours only
+  int tiled_base = 0;                    // counter value the next launch starts from
+  int tiled_grid = 0;                    // resident blocks of the tiled kernel (-1: none)
 };
+
+namespace lbx { template <typename T> struct StepArgs; }
 
 // Hidden helpers of the library's translation units (not exported).
 #define LBX_HIDDEN __attribute__((visibility("hidden")))
@@ -76,3 +88,13 @@ LBX_HIDDEN void lbx_internal_drop_graphs(lbx_domain* d);
 LBX_HIDDEN bool lbx_internal_pest_due(const lbx_domain* d, int t);
 LBX_HIDDEN lbx_status lbx_internal_pest_after(lbx_domain* d, int t);
 LBX_HIDDEN void lbx_internal_pest_free(lbx_domain* d);
+// Temporal blocking: steps one round advances, and `rounds` (even) rounds
+// with the launch arguments A of every step, from the state after an even
+// step.
+LBX_HIDDEN int lbx_internal_tiled_steps_per_round(const lbx_domain* d);
+template <typename T>
+LBX_HIDDEN lbx_status lbx_internal_tiled_run(lbx_domain* d, const lbx::StepArgs<T>& A, int rounds);
+LBX_HIDDEN void lbx_internal_tiled_free(lbx_domain* d);
+// LBX_OK, or the error of a tiled launch whose bounded wait ran out (then
+// cleared); synchronous.
+LBX_HIDDEN lbx_status lbx_internal_tiled_status(lbx_domain* d);

@@ -283,7 +283,10 @@ __device__ __forceinline__ float collide_pairs(const StepArgs<float>& A, int s, 
   return rho;
 }
 
-template <typename T, int Q, int MODEL, bool WALSH = false>
+// UNIT_DEN: the caller knows the divisor of the momentum is exactly 1
+// (the shifted incompressible model with rho_A = 1), and m / 1 == m in
+// IEEE arithmetic, so the divisions are left out with the same results.
+template <typename T, int Q, int MODEL, bool WALSH = false, bool UNIT_DEN = false>
 __device__ __forceinline__ T collide(const StepArgs<T>& A, int s, bool solute,
                                         int sinks, T (&d)[Q], T (&u)[3],
                                         long long n)
@@ -341,6 +344,10 @@ __device__ __forceinline__ T collide(const StepArgs<T>& A, int s, bool solute,
       u[1] = (T)__dadd_rn((double)(m1 / den), __dmul_rn(ot, A.wg[s * 3 + 1]));
       u[2] = (D == 3) ? (T)__dadd_rn((double)(m2 / den), __dmul_rn(ot, A.wg[s * 3 + 2]))
                       : T(0);
+    } else if (UNIT_DEN) {
+      u[0] = add_(m0, c.tg[0]);
+      u[1] = add_(m1, c.tg[1]);
+      u[2] = (D == 3) ? add_(m2, c.tg[2]) : T(0);
     } else {
       u[0] = add_(m0 / den, c.tg[0]);
       u[1] = add_(m1 / den, c.tg[1]);

@@ -21,6 +21,7 @@ LIB_PATH = os.path.join(os.path.dirname(_HERE), "lib", "liblbx.so")
 LBX_OK, LBX_ERR_INVALID, LBX_ERR_CUDA, LBX_ERR_NOMEM, LBX_ERR_STATE, LBX_ERR_NUMERIC = range(6)
 LBX_WRITE_MV = 1
 LBX_LAYOUT_AUTO, LBX_LAYOUT_DENSE, LBX_LAYOUT_COMPACT = 0, 1, 2
+LBX_RUN_AUTO, LBX_RUN_STEPS, LBX_RUN_TILED = 0, 1, 2
 
 _D2 = C.c_double * 2
 _D6 = C.c_double * 6
@@ -104,6 +105,7 @@ _SIGNATURES = {
     "lbx_step_pair": (C.c_int, [C.c_void_p, C.c_int, C.c_uint]),
     "lbx_run": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int]),
     "lbx_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "lbx_set_run_mode": (C.c_int, [C.c_void_p, C.c_int]),
     "lbx_sync": (C.c_int, [C.c_void_p]),
     "lbx_reduce": (C.c_int, [C.c_void_p, C.POINTER(_CReductions)]),
     "lbx_frame_stats_compute": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(_CFrameStats)]),
@@ -401,6 +403,17 @@ class Domain:
         """Queue work on a caller's cudaStream_t (an integer handle); 0 or
         None is the CUDA default stream."""
         _check(_lib.lbx_set_stream(self._h, stream_handle))
+
+    RUN_MODES = {"auto": LBX_RUN_AUTO, "steps": LBX_RUN_STEPS, "tiled": LBX_RUN_TILED}
+
+    def set_run_mode(self, mode: str):
+        """How run() advances stretches of AA pairs with unchanging launch
+        arguments: "auto" (default), "steps" (a launch per step, replayed
+        from CUDA graphs) or "tiled" (temporal blocking in shared memory,
+        2D one-substance lattices; see lbx_set_run_mode in lbx.h)."""
+        if mode not in self.RUN_MODES:
+            raise ValueError("run mode must be one of %s" % sorted(self.RUN_MODES))
+        _check(_lib.lbx_set_run_mode(self._h, self.RUN_MODES[mode]))
 
     def sync(self):
         _check(_lib.lbx_sync(self._h))
