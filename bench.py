@@ -259,6 +259,102 @@ def precision_leg(mask, local: int, steps: int) -> dict:
     return out
 
 
+def small_2d_leg(local: int, steps: int) -> dict:
+    """The 2D case (256^2 D2Q9 FP64 between Zou-He pressure faces, discs of
+    porosity 0.6, from rest): `steps` steps in one CUDA-event window, run
+    as the library runs it (LBX_RUN_AUTO: the tiled path, rounds of steps on
+    tiles in shared memory) and one launch per step (LBX_RUN_STEPS, graph
+    replay), and the speed-up between them."""
+    import torch
+    import lbx
+    from lbx import configs
+    out = {}
+    for mode in ("auto", "steps"):
+        lp, mask = configs.cfg1_params(8)
+        lp.device = local
+        stream = torch.cuda.Stream()
+        with lbx.Domain(lp, mask) as dom:
+            dom.set_run_mode(mode)
+            dom.set_stream(stream.cuda_stream)
+            dom.init_equilibrium(0, 1.0, 0.0, 0.0)
+            dom.run(0, 40, 0)                          # warm-up (plans, graphs)
+            dom.init_equilibrium(0, 1.0, 0.0, 0.0)
+            torch.cuda.synchronize()
+            n0 = dom.launch_count()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            dom.run(0, steps, 0)
+            e1.record(stream)
+            dom.sync()
+            ms = e0.elapsed_time(e1)
+            out[mode] = {"mlups": round(mask.size * steps / (ms / 1e3) / 1e6, 3),
+                         "us_per_step": round(1e3 * ms / steps, 4),
+                         "launches": dom.launch_count() - n0}
+    out["tiled_over_steps"] = round(out["auto"]["mlups"] / out["steps"]["mlups"], 4)
+    out["workload"] = "256^2 D2Q9 FP64, pressure_s_in / pressure_n_out, %d steps" % steps
+    return out
+
+
+def batch_leg(local: int, nsamples: int, steps: int) -> dict:
+    """Many small lattices at once: 512 D3Q19 FP32 sphere packs with edges
+    32..96 (172.8M nodes, 87.0M fluid) stepped as one batch (one launch per
+    step, graph-replayed), timed over `steps` steps with CUDA events; the
+    roofline counts 152 B per fluid node update plus the rank-table bit per
+    node, as the headline does.  Also the per-kind launch times and the
+    per-sample launches of SEQUENTIAL mode."""
+    import torch
+    from lbx.batch import Batch
+    from lbx.configs import cfg4_samples
+    params, masks = cfg4_samples(nsamples)
+    for p in params:
+        p.device = local
+    nodes = sum(m.size for m in masks)
+    fluid = sum(int(np.count_nonzero(m != 1)) for m in masks)
+    peaks = load_peaks()
+    out = {"samples": nsamples, "nodes": nodes, "fluid_nodes": fluid, "steps": steps}
+    with Batch(params, masks) as b:
+        s = torch.cuda.Stream()
+        b.set_stream(s.cuda_stream)
+        for mode in ("fused", "sequential"):
+            for i in range(nsamples):
+                b.init_equilibrium(i, 1.0)
+            b.run(0, 4, 0, mode=mode)                  # warm-up (graph capture)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(s)
+            b.run(4, steps, 0, mode=mode)
+            e1.record(s)
+            s.synchronize()
+            secs = e0.elapsed_time(e1) / 1e3
+            alg = fluid * BYTES_PER_FLUID_UPDATE + nodes * FLAG_BYTES_PER_NODE
+            out[mode] = {"mlups": round(nodes * steps / secs / 1e6, 3),
+                         "mflups": round(fluid * steps / secs / 1e6, 3),
+                         "ms_per_step": round(1e3 * secs / steps, 4),
+                         "frac": round(alg * steps / secs / 1e9 / peaks["hbm_gbs"], 4)}
+        per_kind = {"odd": [], "even": []}
+        t = 4 + steps                                   # even: the next step is odd
+        for rep in range(8):
+            for kind in ("odd", "even"):
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(s)
+                b.run(t, 1, 0, mode="fused")
+                e1.record(s)
+                s.synchronize()
+                if rep >= 2:
+                    per_kind[kind].append(e0.elapsed_time(e1))
+                t += 1
+        alg = fluid * BYTES_PER_FLUID_UPDATE + nodes * FLAG_BYTES_PER_NODE
+        out["by_kind_ms"] = {k: round(float(np.median(v)), 4) for k, v in per_kind.items()}
+        out["by_kind_frac"] = {k: round(alg / (float(np.median(v)) / 1e3) / 1e9 / peaks["hbm_gbs"], 4)
+                               for k, v in per_kind.items()}
+    out["fused_over_sequential"] = round(out["fused"]["mlups"] / out["sequential"]["mlups"], 4)
+    out["workload"] = ("cfg 4: %d D3Q19 FP32 sphere packs, edges 32-96, porosity 0.3-0.7"
+                       % nsamples)
+    return out
+
+
 def adjoint_leg(local: int, steps: int, K: int = 100, window: int = 500) -> dict:
     """The discrete adjoint's cost against a plain forward solve on the
     128^3 flow + solute configuration (sphere pack r = 4 to porosity 0.45,
@@ -373,6 +469,12 @@ def main(argv=None) -> int:
                     help="steps of each run of the FP32-vs-FP64 leg (0: skip it)")
     ap.add_argument("--adjoint-steps", type=int, default=4000,
                     help="steps of the adjoint cost leg (0: skip it)")
+    ap.add_argument("--small-steps", type=int, default=2000,
+                    help="steps of the 256^2 D2Q9 FP64 leg (0: skip it)")
+    ap.add_argument("--batch-samples", type=int, default=512,
+                    help="samples of the batched-lattice leg (0: skip it)")
+    ap.add_argument("--batch-steps", type=int, default=200,
+                    help="timed steps of the batched-lattice leg")
     ap.add_argument("--cpu-table", action="store_true",
                     help="print the host-core timings of the oracle port and of the "
                          "reference's kernels on the 2D case and a 128^3 crop, then exit")
@@ -537,6 +639,10 @@ def main(argv=None) -> int:
             % args.precision_steps)
     if args.adjoint_steps > 0:
         line["adjoint"] = adjoint_leg(local, args.adjoint_steps)
+    if args.small_steps > 0:
+        line["small_2d"] = small_2d_leg(local, args.small_steps)
+    if args.batch_samples > 0:
+        line["batch"] = batch_leg(local, args.batch_samples, args.batch_steps)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(mask)
     dom.close()
