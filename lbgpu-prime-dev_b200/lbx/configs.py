@@ -4,6 +4,7 @@
     python -m lbx.configs cfg2 [--steps 10000]
     python -m lbx.configs cfg3 [--steps 20000]
     python -m lbx.configs cfg5 [--steps 4000]
+    python -m lbx.configs cfg4 [--samples 512] [--steps 200] [--modes fused,...] [--quick]
 
 cfg1: D2Q9 BGK 256x256, FP64, tau = 1.0, non-overlapping discs r = 8 to
       porosity 0.6 (the inlet/outlet rows kept fluid), Zou-He pressure
@@ -367,7 +368,9 @@ def cfg4_samples(nsamples: int = 512, seed: int = 4000):
     return params, masks
 
 
-def run_cfg4(nsamples: int = 512, steps: int = 200, perm_steps: int = 0) -> list:
+def run_cfg4(nsamples: int = 512, steps: int = 200, perm_steps: int = 0,
+             modes=("fused", "persistent", "sequential"), independent: bool = True,
+             autotune: bool = True) -> list:
     import torch
     from .batch import Batch
     params, masks = cfg4_samples(nsamples)
@@ -378,7 +381,7 @@ def run_cfg4(nsamples: int = 512, steps: int = 200, perm_steps: int = 0) -> list
         s = torch.cuda.Stream()
         b.set_stream(s.cuda_stream)
         times = {}
-        for mode in ("fused", "persistent", "sequential"):
+        for mode in modes:
             for i in range(nsamples):
                 b.init_equilibrium(i, 1.0)
             b.run(0, 4, 0, mode=mode)                    # warm-up (graph capture)
@@ -389,16 +392,19 @@ def run_cfg4(nsamples: int = 512, steps: int = 200, perm_steps: int = 0) -> list
             e1.record(s)
             s.synchronize()
             times[mode] = e0.elapsed_time(e1) / 1e3
-        for i in range(nsamples):
-            b.init_equilibrium(i, 1.0)
-        tuned = b.autotune(6)
         for mode, secs in times.items():
-            out.append({"config": "cfg4", "mode": mode, "samples": nsamples, "steps": steps,
-                        "nodes": nodes, "fluid_nodes": fluid,
-                        "mlups": nodes * steps / secs / 1e6,
-                        "mflups": fluid * steps / secs / 1e6, "seconds": secs,
-                        "speedup_vs_sequential": times["sequential"] / secs})
-        out.append({"config": "cfg4", "autotuned": {"mode": tuned[0], "block": tuned[1]}})
+            line = {"config": "cfg4", "mode": mode, "samples": nsamples, "steps": steps,
+                    "nodes": nodes, "fluid_nodes": fluid,
+                    "mlups": nodes * steps / secs / 1e6,
+                    "mflups": fluid * steps / secs / 1e6, "seconds": secs}
+            if "sequential" in times:
+                line["speedup_vs_sequential"] = times["sequential"] / secs
+            out.append(line)
+        if autotune:
+            for i in range(nsamples):
+                b.init_equilibrium(i, 1.0)
+            tuned = b.autotune(6)
+            out.append({"config": "cfg4", "autotuned": {"mode": tuned[0], "block": tuned[1]}})
         if perm_steps:
             for i in range(nsamples):
                 b.init_equilibrium(i, 1.0)
@@ -419,6 +425,8 @@ def run_cfg4(nsamples: int = 512, steps: int = 200, perm_steps: int = 0) -> list
                         "mlups": nodes * perm_steps / secs / 1e6, "seconds": secs,
                         "k_min": float(ks.min()), "k_median": float(np.median(ks)),
                         "k_max": float(ks.max()), "k_first8": [float(x) for x in ks[:8]]})
+    if not independent:
+        return out
     # the same samples as independent lattices, one after another (what a
     # caller without the batch API runs): only the stepping is timed
     secs_ind = 0.0
@@ -523,6 +531,11 @@ def main(argv=None) -> int:
     ap.add_argument("--fd-dirs", type=int, default=2)
     ap.add_argument("--frame-rate", type=int, default=200)
     ap.add_argument("--frame-files", default="summary,raw,dat")
+    ap.add_argument("--modes", default="fused,persistent,sequential",
+                    help="cfg4: batch modes to time, comma-separated")
+    ap.add_argument("--quick", action="store_true",
+                    help="cfg4: skip the autotuner and the independent-lattice comparison "
+                         "(a short run, e.g. under a profiler)")
     a = ap.parse_args(argv)
     if a.config == "cfg1":
         print(json.dumps(run_cfg1(a.steps or 2000)))
@@ -537,7 +550,9 @@ def main(argv=None) -> int:
         for line in run_frames(a.steps or 2000, a.frame_rate, a.edge, a.frame_files):
             print(json.dumps(line))
     elif a.config == "cfg4":
-        for line in run_cfg4(a.samples, a.steps or 200, a.perm_steps):
+        for line in run_cfg4(a.samples, a.steps or 200, a.perm_steps,
+                             modes=tuple(m for m in a.modes.split(",") if m),
+                             independent=not a.quick, autotune=not a.quick):
             print(json.dumps(line))
     else:
         for line in run_cfg2(a.steps or 10000, a.edge):
