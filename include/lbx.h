@@ -407,9 +407,21 @@ lbx_status lbx_batch_init_equilibrium(lbx_batch* b, int sample, const void* rho,
 /* Steps t0+1 .. t0+nsteps of every sample, macro variables at multiples of
  * frame_rate, in `mode` (LBX_BATCH_*). */
 lbx_status lbx_batch_run(lbx_batch* b, int t0, int nsteps, int frame_rate, int mode);
-/* Times FUSED at block sizes 128/256 and PERSISTENT on `steps` trial
- * steps, restores the populations, and keeps the fastest for AUTO. */
+/* Times FUSED at block sizes 128/256 and PERSISTENT at the full and half
+ * resident grid, each in every sample order below, on `steps` trial steps;
+ * restores the populations and keeps the fastest mode, block size and
+ * order (AUTO then uses that mode). */
 lbx_status lbx_batch_autotune(lbx_batch* b, int steps, int* mode, int* block);
+/* Order of the samples in the batch's compact population array (the order
+ * of its thread blocks): largest first (the default; the last blocks of a
+ * step are small ones), interleaved (largest, smallest, second largest,
+ * ...) or as given.  Setting another order rebuilds the batch's tables and
+ * moves the populations; results are the same in every order.  No
+ * counterpart in the reference, which runs one lattice. */
+enum { LBX_BATCH_LAYOUT_LARGEST_FIRST = 0, LBX_BATCH_LAYOUT_INTERLEAVED = 1,
+       LBX_BATCH_LAYOUT_GIVEN = 2 };
+lbx_status lbx_batch_set_layout(lbx_batch* b, int layout);
+lbx_status lbx_batch_get_layout(lbx_batch* b, int* layout);
 lbx_status lbx_batch_set_stream(lbx_batch* b, void* stream);
 lbx_status lbx_batch_sync(lbx_batch* b);
 /* FP64 reductions over one sample's macro variables (as lbx_reduce). */

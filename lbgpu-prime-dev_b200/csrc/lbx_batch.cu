@@ -227,6 +227,8 @@ struct lbx_batch {
   uint8_t* solids = nullptr;
   void* blkdesc[2] = {nullptr, nullptr};   // SampleDesc<real> per block, block sizes 128, 256
   int device = 0;
+  int layout = LBX_BATCH_LAYOUT_LARGEST_FIRST;   // sample order of the compact array
+  long long frm_words = 0;    // rank-table words, guards included
   int pool_off = -1;          // the batch's range in g_pool (bytes), -1: none
   int pool_len = 0;
   int pool_desc = 0;          // offsets in g_pool: descriptors, first-block tables
@@ -596,6 +598,100 @@ lbx_status run_steps(lbx_batch* b, int t0, int nsteps, int frame_rate, int mode)
 
 extern "C" {
 
+namespace {
+
+// The compact layout for the sample order `layout`: each sample's range in
+// the population array, the dense index of every compact slot, the rank
+// tables (whose ranks are global compact indices), the sample descriptors
+// (pool and per-block tables).  `sol`: every sample's solids in sample order.
+// The populations are not moved (lbx_batch_set_layout moves them).
+lbx_status lay_out(lbx_batch* b, int layout, const std::vector<uint8_t>& sol)
+{
+  const int ns = b->nsamples;
+  b->order.resize(ns);
+  std::iota(b->order.begin(), b->order.end(), 0);
+  if (layout != LBX_BATCH_LAYOUT_GIVEN) {
+    // largest first: the last blocks of a step are the small ones
+    std::stable_sort(b->order.begin(), b->order.end(),
+                     [&](int x, int y) { return b->F[x] > b->F[y]; });
+    if (layout == LBX_BATCH_LAYOUT_INTERLEAVED) {
+      // largest, smallest, second largest, second smallest, ...
+      std::vector<int> by_size = b->order;
+      for (int i = 0, lo = 0, hi = ns - 1; i < ns; ++i)
+        b->order[i] = (i & 1) ? by_size[hi--] : by_size[lo++];
+    }
+  }
+  long long c = 0;
+  for (int s : b->order) {
+    b->cbase[s] = (int)c;
+    c += (b->F[s] + kAlign - 1) / kAlign * kAlign;
+  }
+  std::vector<int> fnode(std::max<long long>(b->Ftot, 1), -1);
+  std::vector<uint2> frm((size_t)b->frm_words);
+  for (int s = 0; s < ns; ++s) {
+    int m = b->cbase[s];
+    const long long W = (b->N[s] + 31) / 32;
+    uint2* tab = frm.data() + b->frm_base[s];
+    tab[-1] = make_uint2((unsigned)m, 0u);
+    for (long long w = 0; w < W; ++w) {
+      unsigned bits = 0;
+      tab[w].x = (unsigned)m;
+      for (int q = 0; q < 32; ++q) {
+        const long long n = w * 32 + q;
+        if (n >= b->N[s]) break;
+        if (sol[b->dbase[s] + n] != 1) { bits |= 1u << q; fnode[m++] = (int)n; }
+      }
+      tab[w].y = bits;
+    }
+    tab[W] = make_uint2((unsigned)m, 0u);
+  }
+  BCK(cudaMemcpy(b->frm, frm.data(), frm.size() * sizeof(uint2), cudaMemcpyHostToDevice));
+  BCK(cudaMemcpy(b->fnode, fnode.data(), fnode.size() * sizeof(int), cudaMemcpyHostToDevice));
+  std::vector<unsigned char> desc;   // per sample
+  if (b->precision == 8) fill_desc<double>(b, desc); else fill_desc<float>(b, desc);
+  const size_t dsz = desc.size() / (size_t)ns;
+  pool_release(b->device, b->pool_off);
+  b->pool_off = -1;
+  BCK(b->precision == 8 ? pool_fill<double>(b, desc) : pool_fill<float>(b, desc));
+  for (int i = 0; i < kNumBlockSizes; ++i) {
+    // every block of a sample's padded range belongs to that sample and
+    // holds a copy of its descriptor; a padding thread finds m - cbase >= F
+    const int bs = kBlockSizes[i];
+    const int nb = (int)(b->Ftot / bs);
+    std::vector<unsigned char> tab((size_t)std::max(nb, 1) * dsz, 0);
+    for (int s : b->order) {
+      const long long len = (b->F[s] + kAlign - 1) / kAlign * kAlign;
+      for (long long q = b->cbase[s] / bs; q < (b->cbase[s] + len) / bs; ++q)
+        std::memcpy(tab.data() + (size_t)q * dsz, desc.data() + (size_t)s * dsz, dsz);
+    }
+    b->nblocks[i] = nb;
+    if (!b->blkdesc[i]) BCK(cudaMalloc(&b->blkdesc[i], tab.size()));
+    BCK(cudaMemcpy(b->blkdesc[i], tab.data(), tab.size(), cudaMemcpyHostToDevice));
+  }
+  // captured steps hold the old tables' launch arguments
+  if (b->graph) { cudaGraphExecDestroy(b->graph); b->graph = nullptr; }
+  b->layout = layout;
+  return LBX_OK;
+}
+
+// Another sample order with the state kept: the populations go to the
+// dense exchange array, the tables are rebuilt, the populations come back.
+lbx_status relayout(lbx_batch* b, int layout)
+{
+  if (lbx_status st = sync_dense(b)) return st;
+  std::vector<uint8_t> sol((size_t)b->Ntot);
+  BCK(cudaStreamSynchronize(b->stream));
+  BCK(cudaMemcpy(sol.data(), b->solids, sol.size(), cudaMemcpyDeviceToHost));
+  if (lbx_status st = lay_out(b, layout, sol)) return st;
+  for (int s = 0; s < b->nsamples; ++s)
+    if (lbx_status st = exchange(b, s, true)) return st;
+  BCK(cudaStreamSynchronize(b->stream));
+  b->dense_stale = false;
+  return LBX_OK;
+}
+
+}  // namespace
+
 lbx_status lbx_batch_create(int nsamples, const lbx_params* params, const uint8_t* const* solids,
                             lbx_batch** out)
 {
@@ -643,54 +739,29 @@ lbx_status lbx_batch_create(int nsamples, const lbx_params* params, const uint8_
     for (long long n = 0; n < b->N[s]; ++n) f += solids[s][n] != 1;
     b->F[s] = (int)f;
   }
-  // largest first: the last blocks of a step are the small ones
-  b->order.resize(nsamples);
-  std::iota(b->order.begin(), b->order.end(), 0);
-  std::stable_sort(b->order.begin(), b->order.end(),
-                   [&](int x, int y) { return b->F[x] > b->F[y]; });
-  long long c = 0, dn = 0, mvn = 0;
+  long long dn = 0, mvn = 0, c = 0;
   for (int s = 0; s < nsamples; ++s) {          // dense arrays in sample order
     b->dbase[s] = dn; b->fbase_dense[s] = dn * b->Q; b->mvbase[s] = mvn;
     dn += b->N[s]; mvn += (1 + b->dims) * b->N[s];
-  }
-  for (int s : b->order) {                       // compact ranges largest first
-    b->cbase[s] = (int)c;
     c += (b->F[s] + kAlign - 1) / kAlign * kAlign;
   }
   b->Ntot = dn;
   b->Ftot = c;
   if (c >= (1LL << 31)) { delete b; return bfail(LBX_ERR_INVALID, "batch holds >= 2^31 fluid nodes"); }
 
-  // per sample: the dense index of each fluid node, and a rank table of
-  // ceil(N/32) words (global compact index of the word's first fluid node,
-  // fluid bits), with a guard word in front and behind
-  std::vector<int> fnode(std::max<long long>(b->Ftot, 1), -1);
+  // per sample: a rank table of ceil(N/32) words (global compact index of
+  // the word's first fluid node, fluid bits), with a guard word in front and
+  // behind (filled by lay_out)
   std::vector<uint8_t> sol(b->Ntot);
   b->frm_base.resize(nsamples);
   long long words = 0;
   for (int s = 0; s < nsamples; ++s) {
     b->frm_base[s] = words + 1;
     words += (b->N[s] + 31) / 32 + 2;
+    std::memcpy(sol.data() + b->dbase[s], solids[s], (size_t)b->N[s]);
   }
-  std::vector<uint2> frm((size_t)words);
-  for (int s = 0; s < nsamples; ++s) {
-    int m = b->cbase[s];
-    const long long W = (b->N[s] + 31) / 32;
-    uint2* tab = frm.data() + b->frm_base[s];
-    tab[-1] = make_uint2((unsigned)m, 0u);
-    for (long long w = 0; w < W; ++w) {
-      unsigned bits = 0;
-      tab[w].x = (unsigned)m;
-      for (int q = 0; q < 32; ++q) {
-        const long long n = w * 32 + q;
-        if (n >= b->N[s]) break;
-        sol[b->dbase[s] + n] = solids[s][n];
-        if (solids[s][n] != 1) { bits |= 1u << q; fnode[m++] = (int)n; }
-      }
-      tab[w].y = bits;
-    }
-    tab[W] = make_uint2((unsigned)m, 0u);
-  }
+  b->frm_words = words;
+  b->cbase.assign(nsamples, 0);
   auto bail = [&](lbx_status st) { release(b); delete b; return st; };
   cudaError_t e;
 #define BCKD(call) if ((e = (call)) != cudaSuccess) return bail(bfail(e == cudaErrorMemoryAllocation ? LBX_ERR_NOMEM : LBX_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e)));
@@ -700,35 +771,15 @@ lbx_status lbx_batch_create(int nsamples, const lbx_params* params, const uint8_
   BCKD(cudaMalloc(&b->fc, std::max<size_t>(1, (size_t)b->Q * b->Ftot * rs)));
   BCKD(cudaMalloc(&b->fdense, (size_t)b->Q * b->Ntot * rs));
   BCKD(cudaMalloc(&b->mv, (size_t)(1 + b->dims) * b->Ntot * rs));
-  BCKD(cudaMalloc(&b->frm, frm.size() * sizeof(uint2)));
-  BCKD(cudaMalloc(&b->fnode, fnode.size() * sizeof(int)));
+  BCKD(cudaMalloc(&b->frm, (size_t)b->frm_words * sizeof(uint2)));
+  BCKD(cudaMalloc(&b->fnode, (size_t)std::max<long long>(b->Ftot, 1) * sizeof(int)));
   BCKD(cudaMalloc(&b->solids, (size_t)b->Ntot));
   BCKD(cudaMalloc(&b->red, 2 * 148 * sizeof(RedPartial)));
-  BCKD(cudaMemcpy(b->frm, frm.data(), frm.size() * sizeof(uint2), cudaMemcpyHostToDevice));
-  BCKD(cudaMemcpy(b->fnode, fnode.data(), fnode.size() * sizeof(int), cudaMemcpyHostToDevice));
   BCKD(cudaMemcpy(b->solids, sol.data(), sol.size(), cudaMemcpyHostToDevice));
   BCKD(cudaMemset(b->fc, 0, std::max<size_t>(1, (size_t)b->Q * b->Ftot * rs)));
   BCKD(cudaMemset(b->fdense, 0, (size_t)b->Q * b->Ntot * rs));
   BCKD(cudaMemset(b->mv, 0, (size_t)(1 + b->dims) * b->Ntot * rs));
-  std::vector<unsigned char> desc;   // per sample
-  if (b->precision == 8) fill_desc<double>(b, desc); else fill_desc<float>(b, desc);
-  const size_t dsz = desc.size() / (size_t)nsamples;
-  BCKD(b->precision == 8 ? pool_fill<double>(b, desc) : pool_fill<float>(b, desc));
-  for (int i = 0; i < kNumBlockSizes; ++i) {
-    // every block of a sample's padded range belongs to that sample and
-    // holds a copy of its descriptor; a padding thread finds m - cbase >= F
-    const int bs = kBlockSizes[i];
-    const int nb = (int)(b->Ftot / bs);
-    std::vector<unsigned char> tab((size_t)std::max(nb, 1) * dsz, 0);
-    for (int s : b->order) {
-      const long long len = (b->F[s] + kAlign - 1) / kAlign * kAlign;
-      for (long long q = b->cbase[s] / bs; q < (b->cbase[s] + len) / bs; ++q)
-        std::memcpy(tab.data() + (size_t)q * dsz, desc.data() + (size_t)s * dsz, dsz);
-    }
-    b->nblocks[i] = nb;
-    BCKD(cudaMalloc(&b->blkdesc[i], tab.size()));
-    BCKD(cudaMemcpy(b->blkdesc[i], tab.data(), tab.size(), cudaMemcpyHostToDevice));
-  }
+  if (lbx_status st = lay_out(b, LBX_BATCH_LAYOUT_LARGEST_FIRST, sol)) return bail(st);
 #undef BCKD
   *out = b;
   return LBX_OK;
@@ -839,6 +890,7 @@ lbx_status lbx_batch_autotune(lbx_batch* b, int steps, int* mode_out, int* block
   steps += steps & 1;
   // The trial steps advance the lattice; start from a copy and put it back.
   const size_t bytes = (size_t)b->Q * b->Ftot * (size_t)b->precision;
+  const int layout0 = b->layout;
   void* save = nullptr;
   BCK(cudaMalloc(&save, std::max<size_t>(bytes, 1)));
   BCK(cudaMemcpyAsync(save, b->fc, bytes, cudaMemcpyDeviceToDevice, b->stream));
@@ -846,33 +898,47 @@ lbx_status lbx_batch_autotune(lbx_batch* b, int steps, int* mode_out, int* block
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
   float best = 1e30f;
-  int best_mode = LBX_BATCH_FUSED, best_bs = 1, best_div = 1;
+  int best_mode = LBX_BATCH_FUSED, best_bs = 1, best_div = 1, best_layout = layout0;
   // candidates: FUSED at each block size; PERSISTENT (256-thread blocks) with
   // the resident grid, or half of it (fewer blocks contending for the grid
-  // barrier, more sample blocks walked by each)
+  // barrier, more sample blocks walked by each); each in every sample order,
+  // the current one first
   struct Cand { int mode, bs, div; };
   const Cand cands[] = {{LBX_BATCH_FUSED, 0, 1}, {LBX_BATCH_FUSED, 1, 1},
                         {LBX_BATCH_PERSISTENT, 1, 1}, {LBX_BATCH_PERSISTENT, 1, 2}};
+  const int layouts[3] = {layout0, (layout0 + 1) % 3, (layout0 + 2) % 3};
   lbx_status st = LBX_OK;
-  for (const Cand& c : cands) {
-    if (st != LBX_OK) break;
-    b->bs_index = c.bs;
-    b->coop_div = c.div;
-    st = run_steps(b, 0, 2, 0, c.mode);              // warm-up (and graph capture)
-    if (st != LBX_OK) { st = LBX_OK; continue; }      // mode unavailable: skip it
-    cudaEventRecord(e0, b->stream);
-    st = run_steps(b, 2, steps, 0, c.mode);
-    cudaEventRecord(e1, b->stream);
-    cudaEventSynchronize(e1);
-    float ms = 0;
-    cudaEventElapsedTime(&ms, e0, e1);
-    if (st == LBX_OK && ms < best) { best = ms; best_mode = c.mode; best_bs = c.bs; best_div = c.div; }
+  for (int li = 0; li < 3 && st == LBX_OK; ++li) {
+    if (layouts[li] != b->layout) st = relayout(b, layouts[li]);
+    for (const Cand& c : cands) {
+      if (st != LBX_OK) break;
+      b->bs_index = c.bs;
+      b->coop_div = c.div;
+      st = run_steps(b, 0, 2, 0, c.mode);              // warm-up (and graph capture)
+      if (st != LBX_OK) { st = LBX_OK; b->parity = 0; continue; }   // mode unavailable
+      cudaEventRecord(e0, b->stream);
+      st = run_steps(b, 2, steps, 0, c.mode);
+      cudaEventRecord(e1, b->stream);
+      cudaEventSynchronize(e1);
+      float ms = 0;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (st == LBX_OK && ms < best) {
+        best = ms; best_mode = c.mode; best_bs = c.bs; best_div = c.div; best_layout = b->layout;
+      }
+    }
   }
   b->mode = best_mode;
   b->bs_index = best_bs;
   b->coop_div = best_div;
   b->parity = 0;
-  cudaMemcpyAsync(b->fc, save, bytes, cudaMemcpyDeviceToDevice, b->stream);
+  // the saved populations are in the first order: back to it, restore, then
+  // move them to the chosen order
+  if (st == LBX_OK && b->layout != layout0) st = relayout(b, layout0);
+  if (st == LBX_OK) {
+    cudaMemcpyAsync(b->fc, save, bytes, cudaMemcpyDeviceToDevice, b->stream);
+    b->dense_stale = true;
+    if (best_layout != layout0) st = relayout(b, best_layout);
+  }
   cudaStreamSynchronize(b->stream);
   cudaFree(save);
   cudaEventDestroy(e0);
@@ -880,6 +946,23 @@ lbx_status lbx_batch_autotune(lbx_batch* b, int steps, int* mode_out, int* block
   if (mode_out) *mode_out = best_mode;
   if (block_out) *block_out = kBlockSizes[best_bs];
   return st;
+}
+
+lbx_status lbx_batch_set_layout(lbx_batch* b, int layout)
+{
+  if (!b) return bfail(LBX_ERR_INVALID, "batch is NULL");
+  if (layout != LBX_BATCH_LAYOUT_LARGEST_FIRST && layout != LBX_BATCH_LAYOUT_INTERLEAVED &&
+      layout != LBX_BATCH_LAYOUT_GIVEN)
+    return bfail(LBX_ERR_INVALID, "unknown batch layout %d", layout);
+  if (layout == b->layout) return LBX_OK;
+  return relayout(b, layout);
+}
+
+lbx_status lbx_batch_get_layout(lbx_batch* b, int* layout)
+{
+  if (!b || !layout) return bfail(LBX_ERR_INVALID, "batch and layout must not be NULL");
+  *layout = b->layout;
+  return LBX_OK;
 }
 
 lbx_status lbx_batch_set_stream(lbx_batch* b, void* stream)

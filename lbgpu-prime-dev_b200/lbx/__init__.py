@@ -132,6 +132,8 @@ _SIGNATURES = {
     "lbx_batch_run": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int]),
     "lbx_batch_autotune": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int),
                                      C.POINTER(C.c_int)]),
+    "lbx_batch_set_layout": (C.c_int, [C.c_void_p, C.c_int]),
+    "lbx_batch_get_layout": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
     "lbx_batch_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
     "lbx_batch_sync": (C.c_int, [C.c_void_p]),
     "lbx_batch_reduce": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(_CReductions)]),

@@ -12,6 +12,7 @@ from . import (LbxError, Params, _CParams, _CReductions, _check, load_library)
 LBX_BATCH_AUTO, LBX_BATCH_FUSED, LBX_BATCH_PERSISTENT, LBX_BATCH_SEQUENTIAL = 0, 1, 2, 3
 MODES = {"auto": LBX_BATCH_AUTO, "fused": LBX_BATCH_FUSED,
          "persistent": LBX_BATCH_PERSISTENT, "sequential": LBX_BATCH_SEQUENTIAL}
+LAYOUTS = {"largest_first": 0, "interleaved": 1, "given": 2}
 
 
 class Batch:
@@ -84,6 +85,18 @@ class Batch:
         m, b = C.c_int(), C.c_int()
         _check(self._lib.lbx_batch_autotune(self._h, steps, C.byref(m), C.byref(b)))
         return {v: k for k, v in MODES.items()}[m.value], b.value
+
+    def set_layout(self, layout: str):
+        """Sample order of the compact population array: "largest_first"
+        (default), "interleaved" or "given"; the state is kept."""
+        if layout not in LAYOUTS:
+            raise ValueError("layout must be one of %s" % sorted(LAYOUTS))
+        _check(self._lib.lbx_batch_set_layout(self._h, LAYOUTS[layout]))
+
+    def layout(self) -> str:
+        v = C.c_int()
+        _check(self._lib.lbx_batch_get_layout(self._h, C.byref(v)))
+        return {k: x for x, k in LAYOUTS.items()}[v.value]
 
     def set_stream(self, handle):
         _check(self._lib.lbx_batch_set_stream(self._h, handle))

@@ -121,3 +121,52 @@ def test_batches_alive_together_keep_their_own_descriptors():
     _check_against_oracle(pa, ma, fa, out_a, 13)
     _check_against_oracle(pb, mb, fb, out_b, 13)
     _check_against_oracle(pc, mc, fc, out_c, 13)
+
+
+@pytest.mark.parametrize("prec", [8, 4])
+def test_batch_layouts_give_the_same_results(prec):
+    """The three sample orders of the compact array (largest first,
+    interleaved, as given) give the same populations, and switching the
+    order mid-run keeps the state; FP64 matches the oracle."""
+    params, masks = make_samples(9, seed=41, prec=prec)
+    rng = np.random.default_rng(6)
+    f0 = [(rng.standard_normal((19, p.NN)) * 1e-4).astype(p.dtype) for p in params]
+    out = {}
+    for layout in ("largest_first", "interleaved", "given"):
+        with Batch(params, masks) as b:
+            b.set_layout(layout)
+            assert b.layout() == layout
+            for i in range(len(params)):
+                b.upload_f(i, f0[i])
+            b.run(0, 10, 0, mode="fused")
+            b.set_layout("given" if layout != "given" else "interleaved")
+            b.run(10, 12, 0, mode="fused")
+            b.sync()
+            out[layout] = [b.download_f(i) for i in range(len(params))]
+    for layout in ("interleaved", "given"):
+        for i in range(len(params)):
+            if prec == 8:
+                assert np.array_equal(out[layout][i], out["largest_first"][i]), (layout, i)
+            else:
+                assert rel_err(out[layout][i], out["largest_first"][i]) <= 1e-6, (layout, i)
+    if prec == 8:
+        for i, p in enumerate(params):
+            q = po.Params(dims=3, LX=p.LX, LY=p.LY, LZ=p.LZ, tau=tuple(p.tau),
+                          gaccel=tuple(p.gaccel))
+            fo, _ = po.run_oracle(q, f0[i].reshape(1, 19, -1).copy(), masks[i], 0, 22, 0,
+                                  threads=1)
+            assert rel_err(out["given"][i], fo[0]) <= 1e-12, i
+
+
+def test_batch_autotune_over_layouts_keeps_state():
+    params, masks = make_samples(6, seed=43, prec=4)
+    with Batch(params, masks) as b:
+        for i in range(6):
+            b.init_equilibrium(i, 1.0)
+        b.run(0, 6, 0)
+        before = [b.download_f(i) for i in range(6)]
+        mode, bs = b.autotune(4)
+        assert b.layout() in ("largest_first", "interleaved", "given")
+        after = [b.download_f(i) for i in range(6)]
+        for x, y in zip(before, after):
+            assert np.array_equal(x, y)
