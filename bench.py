@@ -322,12 +322,19 @@ def batch_leg(local: int, nsamples: int, steps: int) -> dict:
             for i in range(nsamples):
                 b.init_equilibrium(i, 1.0)
             b.run(0, 4, 0, mode=mode)                  # warm-up (graph capture)
+            s.synchronize()
+            sampler = ClockSampler(local) if mode == "fused" else None
+            if sampler:
+                sampler.start()
+                time.sleep(0.3)
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record(s)
             b.run(4, steps, 0, mode=mode)
             e1.record(s)
             s.synchronize()
+            if sampler:
+                out["clocks"] = sampler.stop()
             secs = e0.elapsed_time(e1) / 1e3
             alg = fluid * BYTES_PER_FLUID_UPDATE + nodes * FLAG_BYTES_PER_NODE
             out[mode] = {"mlups": round(nodes * steps / secs / 1e6, 3),
