@@ -480,6 +480,28 @@ def cpu_table() -> int:
             print(json.dumps({"cpu_table": name, "kind": kind, "threads": nt,
                               "mlups": round(p.NN * steps / dt_s / 1e6, 3), "steps": steps,
                               "cpu": platform.processor() or platform.machine()}))
+    # the reference's own host loops (stream_collide_stream.c + collide.c):
+    # a different model (unshifted, no face rows), single-threaded as
+    # shipped, built with ACCURATE 0 / COMPRESSIBLE 1; a cost baseline only
+    for name, p, mask, dt, variant, steps in (
+            (cases[0][0], cases[0][1], cases[0][2], np.float64, "d2q9p_f64", 20),
+            (cases[1][0], cases[1][1], cases[1][2], np.float64, "d3q19p_f64", 4),
+            (cases[2][0], cases[2][1], cases[2][2], np.float32, "d3q19p_f32", 4)):
+        if not po.reference_available(variant):
+            continue
+        w = po.init_feq(po.Params(dims=p.dims, LX=p.LX, LY=p.LY, LZ=p.LZ, accurate=0,
+                                  compressible=1),
+                        np.ones((1, p.NN)), np.zeros((1, p.NN)), np.zeros((1, p.NN)),
+                        np.zeros((1, p.NN))).astype(dt)
+        f = np.ascontiguousarray(w)
+        po.reference_cpu_loops(variant, p, f, mask, 0, 2)
+        t0 = time.perf_counter()
+        po.reference_cpu_loops(variant, p, f, mask, 2, steps)
+        dt_s = time.perf_counter() - t0
+        print(json.dumps({"cpu_table": name, "kind": "reference host loops", "threads": 1,
+                          "mlups": round(p.NN * steps / dt_s / 1e6, 3), "steps": steps,
+                          "finite": bool(np.isfinite(f).all()),
+                          "cpu": platform.processor() or platform.machine()}))
     return 0
 
 

@@ -449,6 +449,28 @@ def reference_output_frame(variant: str, LX: int, LY: int, LZ: int, mv: np.ndarr
     return True
 
 
+def reference_cpu_loops(variant: str, p: Params, f: np.ndarray, solids: np.ndarray,
+                        t0: int, nsteps: int) -> np.ndarray:
+    """The reference's own host time loop (src/stream_collide_stream.c,
+    src/collide.c: its CPU model, not the device arithmetic) on f in place,
+    one thread; a cost baseline.  Periodic lattice with body force, one
+    substance; `variant` names the flags it is built with."""
+    if variant not in _refs:
+        _refs[variant] = C.CDLL(os.path.join(REF_DIR, "librefk_%s.so" % variant))
+    lib = _refs[variant]
+    lib.refk_real_size.restype = C.c_int
+    assert f.dtype.itemsize == lib.refk_real_size(), "variant precision mismatch"
+    assert f.flags.c_contiguous and f.size == p.nsubs * p.Q * p.NN
+    sol = np.ascontiguousarray(solids, dtype=np.uint8).reshape(-1)
+    g = (C.c_double * 3)(*[float(x) for x in p.gaccel[:3]])
+    rc = lib.refk_cpu_loops(p.LX, p.LY, p.LZ, C.c_double(p.tau[0]), g,
+                            sol.ctypes.data_as(C.c_void_p), f.ctypes.data_as(C.c_void_p),
+                            int(t0), int(nsteps))
+    if rc != 0:
+        raise RuntimeError("refk_cpu_loops failed")
+    return f
+
+
 def reference_pest(variant: str, p: Params, f: np.ndarray, solids: np.ndarray, t0: int,
                    nsteps: int, workdir: str, frame_rate: int = 0,
                    mv: Optional[np.ndarray] = None):

@@ -115,6 +115,10 @@ unsigned char* solids_mem_d;
 #include "system_boundary_kernels.c"
 #include "k_stream_collide_stream.c"
 #include "k_collide.c"
+/* the reference's own CPU loops (its host-only build), timed as a cost
+ * baseline; src/stream_collide_stream.c:2-240, src/collide.c:9-251 */
+#include "stream_collide_stream.c"
+#include "collide.c"
 
 /* The dynamic shared-memory scratch of one one-thread block (per host
    thread). */
@@ -620,5 +624,45 @@ EXPORT int refk_init_from_params(const char* path, int cap, real* f, real* mv)
     free(l->vars[s].macrovars1d);
   }
   free(l->vars); free(l->solids_memblock); free(l);
+  return 0;
+}
+
+/* The reference's CPU time loop (src/lbgpu_prime.cu:597, :818, the
+ * non-CUDA branches): stream_collide_stream on odd steps, collide on even
+ * ones, on a serial lattice with the given populations ([subs][Q][N]),
+ * solids, tau and body force of substance 0.  A cost baseline: this is the
+ * reference's host model, not the device arithmetic the oracle pins. */
+EXPORT int refk_cpu_loops(int LX, int LY, int LZ, double tau, const double* g,
+                          const unsigned char* solids, real* f, int t0, int nsteps)
+{
+  struct lattice_struct* l = harness_lattice(LX, LY, LZ);
+  const int D = NUM_DIMENSIONS, Qd = 2 * D * D + 1, NN = LX * LY * LZ;
+  int s, a, t;
+  memcpy(l->solids_memblock, solids, (size_t)NN);
+  l->NumDims = D;
+  l->NumSubs = NUM_FLUID_COMPONENTS;
+  l->NumVelDirs = Qd;
+  for (s = 0; s < NUM_FLUID_COMPONENTS; s++) {
+    l->param.tau[s] = (real)tau;
+    for (a = 0; a < 3; a++) l->param.gforce[s][a] = (real)g[a];
+  }
+  real* mv = (real*)calloc((size_t)NUM_FLUID_COMPONENTS * (1 + D) * NN, sizeof(real));
+  l->vars = (struct vars_struct*)calloc(NUM_FLUID_COMPONENTS, sizeof *l->vars);
+  for (s = 0; s < NUM_FLUID_COMPONENTS; s++) {
+    l->vars[s].f1d = (real**)malloc((size_t)Qd * sizeof(real*));
+    for (a = 0; a < Qd; a++) l->vars[s].f1d[a] = f + ((size_t)s * Qd + a) * NN;
+    /* collide stores rho and u of every node (set_rho / set_ux ...) */
+    l->vars[s].macrovars1d = (real**)malloc((size_t)(1 + D) * sizeof(real*));
+    for (a = 0; a <= D; a++) l->vars[s].macrovars1d[a] = mv + ((size_t)s * (1 + D) + a) * NN;
+  }
+  for (t = t0 + 1; t <= t0 + nsteps; t++) {
+    if (t % 2) stream_collide_stream(l);
+    else collide(l);
+  }
+  for (s = 0; s < NUM_FLUID_COMPONENTS; s++) {
+    free(l->vars[s].f1d);
+    free(l->vars[s].macrovars1d);
+  }
+  free(l->vars); free(mv); free(l->solids_memblock); free(l);
   return 0;
 }

@@ -99,3 +99,31 @@ def test_oracle_continues_from_an_odd_time():
     assert np.array_equal(fa, fb) and np.array_equal(mva, mvb)
     with pytest.raises(ValueError):
         po.run_oracle(p, f0.copy(), sol, -1, 2)
+
+
+@pytest.mark.parametrize("variant,dims", [("d2q9p_f64", 2), ("d3q19p_f64", 3)])
+def test_reference_host_loops_run_and_conserve_mass(variant, dims):
+    """The reference's own host time loop (stream_collide_stream.c +
+    collide.c), the CPU cost baseline of bench.py --cpu-table: on a closed
+    periodic lattice with solids and a body force it keeps every value
+    finite and the total mass.  It updates solid nodes as well (unlike the
+    device kernels), so mass moves between fluid and solid nodes and only
+    the sum over all nodes is kept."""
+    if not po.reference_available(variant):
+        pytest.skip("oracle/_ref not built")
+    from lbx import geometry
+    if dims == 2:
+        p = po.Params(dims=2, LX=24, LY=20, LZ=1, accurate=0, compressible=1, tau=(0.9, 1.0),
+                      gaccel=(1e-5, 0, 0, 0, 0, 0))
+        sol = geometry.transpose_2d(geometry.disc_pack(20, 24, radius=3, porosity=0.6, seed=3),
+                                    20, 24)
+    else:
+        p = po.Params(dims=3, LX=12, LY=10, LZ=8, accurate=0, compressible=1, tau=(0.9, 1.0),
+                      gaccel=(1e-5, 0, 0, 0, 0, 0))
+        sol = geometry.sphere_pack(12, 10, 8, radius=2, porosity=0.6, seed=3)
+    n = p.NN
+    f = po.init_feq(p, np.ones((1, n)), np.zeros((1, n)), np.zeros((1, n)), np.zeros((1, n)))
+    m0 = f.sum()
+    po.reference_cpu_loops(variant, p, f, sol, 0, 20)
+    assert np.isfinite(f).all()
+    assert abs(f.sum() - m0) <= 1e-12 * m0
