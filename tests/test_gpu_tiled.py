@@ -150,3 +150,17 @@ def test_tiled_plans_bit_identical_to_steps(shape):
     assert np.isfinite(ft).all()
     assert np.array_equal(ft, fs) and np.array_equal(mvt, mvs)
     assert nt < ns
+
+
+@pytest.mark.parametrize("shape", [(32, 16), (64, 8), (32, 48)])
+def test_tiled_equal_work_edge_shapes(shape):
+    """Lattices the tile columns divide: one tile whose halo wraps onto
+    itself (it waits for its own counter), rows shorter than a tile's
+    height, one column of three tiles."""
+    LX, LY = shape
+    p, sol, f0 = _case(LX, LY, seed=19)
+    ft, mvt, info, nt = _run(p, sol, f0, 52, 52, np.float64, "compact", "tiled")
+    fs, mvs, _, ns = _run(p, sol, f0, 52, 52, np.float64, "compact", "steps")
+    assert info["faces_fused"]
+    assert np.array_equal(ft, fs) and np.array_equal(mvt, mvs)
+    assert nt < ns
