@@ -4,8 +4,9 @@
 // collision model; own extents, mask, tau, rho_A and body force) in one
 // compact population array [a][Ftot].  Each sample's fluid nodes occupy a
 // range starting at a multiple of kAlign, so no thread block straddles two
-// samples and a block finds its sample from a per-block table.  Samples are
-// laid out largest first, so the tail of every step is made of small blocks.
+// samples.  The samples' order in the array is a layout (lbx_batch_set_layout):
+// largest first by default, so the tail of every step is made of small
+// blocks; interleaved or as given on request.
 //
 // Sample descriptors (extents, constants, table addresses) live in a pool in
 // constant memory, written once when the batch is created: a block finds its
@@ -24,7 +25,8 @@
 //               before the even one);
 //   SEQUENTIAL  one launch per sample per step (the per-sample baseline).
 // lbx_batch_autotune times FUSED at each block size and PERSISTENT with the
-// full and half resident grid on a few steps and keeps the fastest.
+// full and half resident grid, in each sample order, on a few steps and
+// keeps the fastest.
 #include "lbx.h"
 #include "lbx_internal.h"
 #include "lbx_kernels.cuh"
