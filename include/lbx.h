@@ -200,8 +200,8 @@ lbx_status lbx_set_stream(lbx_domain* d, void* stream);
  *   LBX_RUN_STEPS  one launch per step, replayed from captured CUDA graphs;
  *   LBX_RUN_TILED  the tiled path wherever it applies: 2D, one substance, no
  *                  Walsh run, no plane record, faces absent or fused.  One
- *                  cooperative launch runs rounds of K steps (K = 4 in FP64,
- *                  6 in FP32) on tiles held in shared memory with halos K
+ *                  cooperative launch runs rounds of K steps (K = 6 in FP64,
+ *                  10 in FP32) on tiles held in shared memory with halos K
  *                  deep; FP64 results are bit-identical to STEPS.
  * LBX_ERR_INVALID for another mode. */
 enum { LBX_RUN_AUTO = 0, LBX_RUN_STEPS = 1, LBX_RUN_TILED = 2 };

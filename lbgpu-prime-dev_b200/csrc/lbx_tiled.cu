@@ -61,10 +61,10 @@ constexpr int kTiledThreads = 512;
 constexpr int kMaxNb = 32;             // tiles one halo may read (one warp polls them)
 constexpr long long kWaitLimit = 1LL << 20;   // polls of one counter (about a second)
 
-// Steps per round: FP64 six (a halo six nodes deep), FP32 eight (its nodes
-// take half the shared memory).
+// Steps per round: FP64 six (a halo six nodes deep), FP32 ten (its nodes
+// take half the shared memory); measured best of 4/6 and 6/8/10.
 template <typename T>
-constexpr int tiled_k() { return sizeof(T) == 8 ? 6 : 8; }
+constexpr int tiled_k() { return sizeof(T) == 8 ? 6 : 10; }
 
 // A tile's node lists (tile-local node indices of fluid nodes, row order),
 // by the node's distance e from the edge of the tile's region:
