@@ -135,7 +135,7 @@ def build(src: str, only=None) -> None:
 
 # The reference's CUDA step kernels, compiled for sm_100a by nvcc into
 # oracle/_ref/refgpu_<variant> through oracle/refgpu_harness.cu.
-GPU_VARIANTS = ["d3q19_f32", "d3q19_f64"]
+GPU_VARIANTS = ["d3q19_f32", "d3q19_f64", "d2q9_f64"]
 
 
 def build_gpu(src: str, only=None) -> None:
