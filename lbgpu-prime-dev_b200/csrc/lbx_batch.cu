@@ -9,9 +9,9 @@
 // blocks; interleaved or as given on request.
 //
 // Sample descriptors (extents, constants, table addresses) live in a pool in
-// constant memory, written once when the batch is created: a block finds its
-// sample by a block-uniform search of the samples' first blocks and reads
-// the descriptor from the constant bank where the update uses it, so the
+// constant memory, written once when the batch is created: a block reads its
+// sample's position from a per-block table (one 4-byte load) and the
+// descriptor from the constant bank where the update uses it, so the
 // per-sample values cost the thread no registers, as the single-lattice
 // kernels' arguments do.  A batch whose descriptors do not fit the pool's
 // free space reads them from a per-block table in global memory instead.
@@ -73,15 +73,12 @@ struct alignas(16) SampleDesc {
 };
 
 // The descriptor pool (one per device, as constant memory is).  A batch's
-// range holds its descriptors in layout order, then for each block size the
-// first block of each sample in layout order and the end of the last.
+// range holds its descriptors in layout order.
 constexpr int kPoolBytes = 63 * 1024;
 __constant__ __align__(16) unsigned char g_pool[kPoolBytes];
 
 struct PoolRef {
   int desc;             // byte offset of the descriptors in g_pool
-  int starts;           // byte offset of the first-block table in g_pool
-  int s_lo, s_hi;       // samples (layout positions) this launch covers
   int block0;           // the launch's first block in the batch
 };
 
@@ -94,6 +91,8 @@ struct BatchArgs {
   const int* fnode;             // [Ftot]: dense index inside the sample, -1 padding
   const SampleDesc<T>* blkdesc; // [nblocks]: the descriptor of each block's sample
                                 // (global-memory path)
+  const int* blkpos;            // [nblocks]: the layout position of each block's
+                                // sample (pool path)
   long long Ftot;
   int nblocks;                  // blocks of the current block size
   int block0;                   // first block (SEQUENTIAL mode, global-memory path)
@@ -158,22 +157,18 @@ aa_step_batch(BatchArgs<T> A)
   batch_block<T, Q, MODEL, ODD, IDX32>(A, A.block0 + blockIdx.x);
 }
 
-// Pool path: the block's sample is the last of samples s_lo..s_hi whose
-// first block is at most the block's (a sample with no fluid node shares its
-// first block with the next one and is never chosen).
+// Pool path: the block's sample position from the per-block table, its
+// descriptor from the pool.  (A binary search of the samples' first blocks
+// in the pool instead cost the odd step 3-6 %: nine dependent constant-cache
+// reads that miss when 512 samples' tables share an SM's constant cache.)
 template <typename T, int Q, int MODEL, bool ODD, bool IDX32>
 __global__ void __launch_bounds__(256, (compact_min_blocks<T, PART_ALL>()))
 aa_step_batch_pool(BatchArgs<T> A, PoolRef R)
 {
-  const int* starts = reinterpret_cast<const int*>(g_pool + R.starts);
   const int bl = R.block0 + blockIdx.x;
-  int lo = R.s_lo, hi = R.s_hi;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (starts[mid] <= bl) lo = mid; else hi = mid - 1;
-  }
+  const int pos = __ldg(A.blkpos + bl);
   const SampleDesc<T>* desc = reinterpret_cast<const SampleDesc<T>*>(g_pool + R.desc);
-  batch_node<T, Q, MODEL, ODD, IDX32>(desc[lo], A, bl * blockDim.x + threadIdx.x);
+  batch_node<T, Q, MODEL, ODD, IDX32>(desc[pos], A, bl * blockDim.x + threadIdx.x);
 }
 
 // Persistent: a resident grid walks all blocks of the batch for `steps`
@@ -228,13 +223,13 @@ struct lbx_batch {
   int* fnode = nullptr;
   uint8_t* solids = nullptr;
   void* blkdesc[2] = {nullptr, nullptr};   // SampleDesc<real> per block, block sizes 128, 256
+  int* blkpos[2] = {nullptr, nullptr};     // sample position per block, block sizes 128, 256
   int device = 0;
   int layout = LBX_BATCH_LAYOUT_LARGEST_FIRST;   // sample order of the compact array
   long long frm_words = 0;    // rank-table words, guards included
   int pool_off = -1;          // the batch's range in g_pool (bytes), -1: none
   int pool_len = 0;
-  int pool_desc = 0;          // offsets in g_pool: descriptors, first-block tables
-  int pool_starts[2] = {0, 0};
+  int pool_desc = 0;          // offset of the descriptors in g_pool
   int nblocks[2] = {0, 0};
   void* red = nullptr;
   cudaStream_t stream = nullptr, own_stream = nullptr;
@@ -262,6 +257,7 @@ BatchArgs<T> batch_args(lbx_batch* b, int write_mv)
   std::memset(&A, 0, sizeof A);
   A.f = (T*)b->fc; A.mv = (T*)b->mv; A.frm = b->frm; A.fnode = b->fnode;
   A.blkdesc = (const SampleDesc<T>*)b->blkdesc[b->bs_index];
+  A.blkpos = b->blkpos[b->bs_index];
   A.Ftot = b->Ftot; A.nblocks = b->nblocks[b->bs_index];
   A.write_mv = write_mv;
   A.kahan = b->kahan;
@@ -297,14 +293,12 @@ lbx_status launch_step(lbx_batch* b, bool odd, int write_mv, int mode)
   const bool pool = b->pool_off >= 0;
   PoolRef R;
   R.desc = b->pool_desc;
-  R.starts = b->pool_starts[b->bs_index];
   if (mode == LBX_BATCH_SEQUENTIAL) {
     for (int i = 0; i < b->nsamples; ++i) {
       const int s = b->order[i];
       if (b->F[s] == 0) continue;
       const unsigned nb = (unsigned)((b->F[s] + bs - 1) / bs);
       if (pool) {
-        R.s_lo = R.s_hi = i;
         R.block0 = b->cbase[s] / bs;
         go_pool(nb, R);
       } else {
@@ -314,8 +308,6 @@ lbx_status launch_step(lbx_batch* b, bool odd, int write_mv, int mode)
     }
   } else if (A.nblocks > 0) {
     if (pool) {
-      R.s_lo = 0;
-      R.s_hi = b->nsamples - 1;
       R.block0 = 0;
       go_pool((unsigned)A.nblocks, R);
     } else {
@@ -448,16 +440,13 @@ void pool_release(int dev, int off)
     if (used[i].first == off) { used.erase(used.begin() + (long)i); return; }
 }
 
-// The batch's pool range: descriptors in layout order, then the first-block
-// tables of both block sizes.  Leaves pool_off at -1 (the global-memory
-// path) when the pool has no room.
+// The batch's pool range: its descriptors in layout order.  Leaves pool_off
+// at -1 (the global-memory path) when the pool has no room.
 template <typename T>
 cudaError_t pool_fill(lbx_batch* b, const std::vector<unsigned char>& desc)
 {
   const int n = b->nsamples;
-  const long long dbytes = (long long)n * (long long)sizeof(SampleDesc<T>);
-  const long long sbytes = ((long long)(n + 1) * 4 + 15) / 16 * 16;
-  const long long len = dbytes + kNumBlockSizes * sbytes;
+  const long long len = ((long long)n * (long long)sizeof(SampleDesc<T>) + 15) / 16 * 16;
   if (len > kPoolBytes) return cudaSuccess;
   const int off = pool_claim(b->device, (int)len);
   if (off < 0) return cudaSuccess;
@@ -465,19 +454,12 @@ cudaError_t pool_fill(lbx_batch* b, const std::vector<unsigned char>& desc)
   for (int i = 0; i < n; ++i)
     std::memcpy(img.data() + (size_t)i * sizeof(SampleDesc<T>),
                 desc.data() + (size_t)b->order[i] * sizeof(SampleDesc<T>), sizeof(SampleDesc<T>));
-  for (int k = 0; k < kNumBlockSizes; ++k) {
-    const int bs = kBlockSizes[k];
-    int* st = (int*)(img.data() + dbytes + k * sbytes);
-    for (int i = 0; i < n; ++i) st[i] = b->cbase[b->order[i]] / bs;
-    st[n] = (int)(b->Ftot / bs);
-  }
   cudaError_t e = cudaMemcpyToSymbol(g_pool, img.data(), (size_t)len, (size_t)off,
                                      cudaMemcpyHostToDevice);
   if (e != cudaSuccess) { pool_release(b->device, off); return e; }
   b->pool_off = off;
   b->pool_len = (int)len;
   b->pool_desc = off;
-  for (int k = 0; k < kNumBlockSizes; ++k) b->pool_starts[k] = (int)(off + dbytes + k * sbytes);
   return cudaSuccess;
 }
 
@@ -486,7 +468,7 @@ void release(lbx_batch* b)
   if (b->graph) cudaGraphExecDestroy(b->graph);
   cudaFree(b->fc); cudaFree(b->fdense); cudaFree(b->mv); cudaFree(b->frm);
   cudaFree(b->fnode); cudaFree(b->solids); cudaFree(b->red);
-  for (int i = 0; i < kNumBlockSizes; ++i) cudaFree(b->blkdesc[i]);
+  for (int i = 0; i < kNumBlockSizes; ++i) { cudaFree(b->blkdesc[i]); cudaFree(b->blkpos[i]); }
   if (b->own_stream) cudaStreamDestroy(b->own_stream);
   pool_release(b->device, b->pool_off);
   b->pool_off = -1;
@@ -669,6 +651,15 @@ lbx_status lay_out(lbx_batch* b, int layout, const std::vector<uint8_t>& sol)
     b->nblocks[i] = nb;
     if (!b->blkdesc[i]) BCK(cudaMalloc(&b->blkdesc[i], tab.size()));
     BCK(cudaMemcpy(b->blkdesc[i], tab.data(), tab.size(), cudaMemcpyHostToDevice));
+    // the sample position of every block (the pool path's lookup)
+    std::vector<int> pos((size_t)std::max(nb, 1), 0);
+    for (int li = 0; li < ns; ++li) {
+      const int s = b->order[li];
+      const long long len = (b->F[s] + kAlign - 1) / kAlign * kAlign;
+      for (long long q = b->cbase[s] / bs; q < (b->cbase[s] + len) / bs; ++q) pos[(size_t)q] = li;
+    }
+    if (!b->blkpos[i]) BCK(cudaMalloc(&b->blkpos[i], pos.size() * sizeof(int)));
+    BCK(cudaMemcpy(b->blkpos[i], pos.data(), pos.size() * sizeof(int), cudaMemcpyHostToDevice));
   }
   // captured steps hold the old tables' launch arguments
   if (b->graph) { cudaGraphExecDestroy(b->graph); b->graph = nullptr; }
