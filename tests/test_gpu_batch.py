@@ -170,3 +170,69 @@ def test_batch_autotune_over_layouts_keeps_state():
         after = [b.download_f(i) for i in range(6)]
         for x, y in zip(before, after):
             assert np.array_equal(x, y)
+
+
+def _samples_2d(n, seed):
+    rng = np.random.default_rng(seed)
+    params, masks = [], []
+    for i in range(n):
+        LX, LY = (int(x) for x in rng.integers(16, 80, size=2))
+        tau = float(rng.uniform(0.6, 1.2))
+        masks.append(geometry.transpose_2d(
+            geometry.disc_pack(LY, LX, radius=3, porosity=float(rng.uniform(0.4, 0.8)),
+                               seed=seed * 100 + i), LY, LX))
+        params.append(lbx.Params(dims=2, LX=LX, LY=LY, LZ=1, precision=8, tau=(tau, 1.0),
+                                 gaccel=(1e-5, -2e-6, 0, 0, 0, 0)))
+    return params, masks
+
+
+@pytest.mark.parametrize("mode", ["fused", "persistent", "sequential"])
+def test_batch_d2q9_matches_oracle(mode):
+    """A batch of D2Q9 FP64 samples (uneven extents, discs): every sample
+    evolves as the oracle's run of it alone."""
+    params, masks = _samples_2d(7, seed=51)
+    rng = np.random.default_rng(2)
+    f0 = [rng.standard_normal((9, p.NN)) * 1e-4 for p in params]
+    with Batch(params, masks) as b:
+        for i in range(len(params)):
+            b.upload_f(i, f0[i])
+        b.run(0, 21, 21, mode=mode)
+        b.sync()
+        out = [(b.download_f(i), b.download_mv(i)) for i in range(len(params))]
+    for i, p in enumerate(params):
+        q = po.Params(dims=2, LX=p.LX, LY=p.LY, LZ=1, tau=tuple(p.tau), gaccel=tuple(p.gaccel))
+        fo, mvo = po.run_oracle(q, f0[i].reshape(1, 9, -1).copy(), masks[i], 0, 21, 21,
+                                threads=1)
+        assert rel_err(out[i][0], fo[0]) <= 1e-12, i
+        fl = masks[i] != 1
+        for c in range(3):
+            assert rel_err(out[i][1][c], mvo[0, c], fl) <= 1e-12, (i, c)
+
+
+@pytest.mark.parametrize("model,kahan", [((0, 1), 0), ((1, 1), 0), ((1, 0), 1)])
+def test_batch_models_match_oracle(model, kahan):
+    """Plain compressible, shifted compressible and Kahan-summed batches
+    (FP64) against the oracle."""
+    acc, comp = model
+    params, masks = make_samples(5, seed=61, prec=8)
+    for p in params:
+        p.accurate, p.compressible, p.kahan = acc, comp, kahan
+    rng = np.random.default_rng(3)
+    w = np.array([1 / 3] + [1 / 18] * 4 + [1 / 36] * 4 + [1 / 18] * 2 + [1 / 36] * 8)
+    f0 = []
+    for p in params:
+        noise = rng.standard_normal((19, p.NN)) * 1e-4
+        f0.append(w[:, None] * (1.0 + noise) if not acc else noise)
+    with Batch(params, masks) as b:
+        for i in range(len(params)):
+            b.upload_f(i, f0[i])
+        b.run(0, 17, 17, mode="fused")
+        b.sync()
+        out = [b.download_f(i) for i in range(len(params))]
+    for i, p in enumerate(params):
+        q = po.Params(dims=3, LX=p.LX, LY=p.LY, LZ=p.LZ, tau=tuple(p.tau),
+                      gaccel=tuple(p.gaccel), accurate=acc, compressible=comp, kahan=kahan)
+        fo, _ = po.run_oracle(q, f0[i].reshape(1, 19, -1).copy(), masks[i], 0, 17, 17,
+                              threads=1)
+        assert np.isfinite(out[i]).all()
+        assert rel_err(out[i], fo[0]) <= 1e-12, i
