@@ -160,9 +160,14 @@ lbx_status lbx_download_mv(lbx_domain* d, int subs, void* rho, void* ux,
                            void* uy, void* uz);
 
 /* Equilibrium initial state on the device from host rho/u ([N] reals each
- * for substance `subs`; uz may be NULL in 2D): the f = feq loop of
+ * for substance `subs`; uz is not read in 2D): the f = feq loop of
  * src/latman.c:1786-1840 (shifted deviations for the flow lattice of an
- * ACCURATE run, full feq otherwise).  Solid nodes are initialised too. */
+ * ACCURATE run, full feq otherwise).  Solid nodes are initialised too.
+ * rho is required; a velocity component passed as NULL is zero (the
+ * reference's init_problem always starts at rest), so the reference's
+ * start moves one plane across the host link instead of Q.  The
+ * substance's macro variables then hold rho and u, as init_problem leaves
+ * them (src/latman.c:1302-1780). */
 lbx_status lbx_init_equilibrium(lbx_domain* d, int subs, const void* rho,
                                 const void* ux, const void* uy,
                                 const void* uz);

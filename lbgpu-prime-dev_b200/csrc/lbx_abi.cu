@@ -1022,28 +1022,30 @@ lbx_status lbx_init_equilibrium(lbx_domain* d, int subs, const void* rho, const 
 {
   if (lbx_status st = check_subs(d, subs)) return st;
   if (d->dense_stale) { if (lbx_status st = exchange(d, false)) return st; }
-  if (!rho || !ux || !uy || (d->D == 3 && !uz))
-    return fail(LBX_ERR_INVALID, "rho/ux/uy (and uz in 3D) are required");
+  if (!rho) return fail(LBX_ERR_INVALID, "rho is required");
+  // the fields land in the substance's macro variables, where the
+  // reference's init_problem leaves them (src/latman.c:1302-1780), and the
+  // populations are formed from there: no staging allocation.  A velocity
+  // component given as NULL is zero, filled on the device (init_problem
+  // always starts at rest, so only rho need cross the host link)
   const size_t plane = (size_t)d->N * d->real_size;
-  void* tmp = nullptr;
-  CK(cudaMalloc(&tmp, 4 * plane));
+  char* t = (char*)d->mv + (size_t)subs * (1 + d->D) * plane;
   const void* src[4] = {rho, ux, uy, uz};
   cudaError_t e = cudaSuccess;
-  for (int c = 0; c < 4 && e == cudaSuccess; ++c)
-    if (src[c]) e = cudaMemcpyAsync((char*)tmp + c * plane, src[c], plane,
-                                    cudaMemcpyHostToDevice, d->stream);
+  for (int c = 0; c <= d->D && e == cudaSuccess; ++c)
+    e = src[c] ? cudaMemcpyAsync(t + c * plane, src[c], plane, cudaMemcpyHostToDevice, d->stream)
+               : cudaMemsetAsync(t + c * plane, 0, plane, d->stream);
   if (e == cudaSuccess) {
     const int shifted = d->p.accurate && subs == 0;
     const unsigned blocks = (unsigned)((d->N + 255) / 256);
-    char* t = (char*)tmp;
     if (d->real_size == 8) {
       double* fs = (double*)d->f + (long long)subs * d->Q * d->N;
-      const double* uzp = uz ? (const double*)(t + 3 * plane) : nullptr;
+      const double* uzp = d->D == 3 ? (const double*)(t + 3 * plane) : nullptr;
       if (d->Q == 9) init_feq<double, 9><<<blocks, 256, 0, d->stream>>>(fs, (double*)t, (double*)(t + plane), (double*)(t + 2 * plane), uzp, d->N, shifted);
       else init_feq<double, 19><<<blocks, 256, 0, d->stream>>>(fs, (double*)t, (double*)(t + plane), (double*)(t + 2 * plane), uzp, d->N, shifted);
     } else {
       float* fs = (float*)d->f + (long long)subs * d->Q * d->N;
-      const float* uzp = uz ? (const float*)(t + 3 * plane) : nullptr;
+      const float* uzp = d->D == 3 ? (const float*)(t + 3 * plane) : nullptr;
       if (d->Q == 9) init_feq<float, 9><<<blocks, 256, 0, d->stream>>>(fs, (float*)t, (float*)(t + plane), (float*)(t + 2 * plane), uzp, d->N, shifted);
       else init_feq<float, 19><<<blocks, 256, 0, d->stream>>>(fs, (float*)t, (float*)(t + plane), (float*)(t + 2 * plane), uzp, d->N, shifted);
     }
@@ -1054,7 +1056,6 @@ lbx_status lbx_init_equilibrium(lbx_domain* d, int subs, const void* rho, const 
     if (exchange(d, true) != LBX_OK) e = cudaErrorUnknown;
   }
   if (e == cudaSuccess) e = cudaStreamSynchronize(d->stream);
-  cudaFree(tmp);
   if (e != cudaSuccess) return fail(LBX_ERR_CUDA, "init_equilibrium: %s", cudaGetErrorString(e));
   d->parity = 0;
   return LBX_OK;

@@ -266,13 +266,13 @@ int main(int argc, char** argv)
   }
 
   /* initial state (init_problem, src/latman.c:1270-1959): rho per
-   * initial_condition, u = 0, f = feq; the same [rho, u] planes are the
-   * macro variables frame 0 reports */
+   * initial_condition, u = 0 (NULL: filled on the device), f = feq; the
+   * domain's macro variables then hold [rho, u], which frame 0 reports */
   {
     const long long N = r.hp.NumNodes;
     const size_t plane = (size_t)N * (size_t)r.prec;
     double* rho = (double*)malloc((size_t)N * sizeof(double));
-    char* b = (char*)calloc(1 + (size_t)r.dims, plane);
+    char* b = (char*)malloc(plane);
     long long n;
     for (s = 0; s < r.nsubs; s++) {
       if (lbh_initial_rho(&r.hp, r.dims, r.nsubs, s, rho))
@@ -281,9 +281,7 @@ int main(int argc, char** argv)
         if (r.prec == 8) ((double*)b)[n] = rho[n];
         else ((float*)b)[n] = (float)rho[n];
       }
-      LBX(lbx_init_equilibrium(r.dom, s, b, b + plane, b + 2 * plane,
-                               r.dims == 3 ? b + 3 * plane : NULL));
-      LBX(lbx_upload_mv(r.dom, s, b));
+      LBX(lbx_init_equilibrium(r.dom, s, b, NULL, NULL, NULL));
     }
     free(rho);
     free(b);

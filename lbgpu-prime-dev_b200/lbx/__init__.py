@@ -379,17 +379,15 @@ class Domain:
         return dict(time=fr.time, mv=mv.copy() if copy else mv,
                     stats=[fr.stats[s].as_dict() for s in range(fr.nsubs)])
 
-    def init_equilibrium(self, subs: int, rho, ux, uy, uz=None):
+    def init_equilibrium(self, subs: int, rho, ux=None, uy=None, uz=None):
+        """f = feq of rho, u (scalars or [N] arrays); a velocity component
+        left None is zero, filled on the device (only rho is copied)."""
         p = self.p
-        arrs = [np.ascontiguousarray(np.broadcast_to(np.asarray(x, dtype=p.dtype), (p.NN,)))
-                for x in (rho, ux, uy)]
-        uzp = None
-        if p.dims == 3:
-            arrs.append(np.ascontiguousarray(np.broadcast_to(
-                np.asarray(0.0 if uz is None else uz, dtype=p.dtype), (p.NN,))))
-            uzp = arrs[3].ctypes.data
-        _check(_lib.lbx_init_equilibrium(self._h, subs, arrs[0].ctypes.data,
-                                         arrs[1].ctypes.data, arrs[2].ctypes.data, uzp))
+        arrs = [None if x is None else
+                np.ascontiguousarray(np.broadcast_to(np.asarray(x, dtype=p.dtype), (p.NN,)))
+                for x in (rho, ux, uy, uz if p.dims == 3 else None)]
+        _check(_lib.lbx_init_equilibrium(self._h, subs, *[
+            None if a is None else a.ctypes.data for a in arrs]))
 
     # -- stepping ----------------------------------------------------------
     def step(self, time: int, write_mv: bool = False):

@@ -5,7 +5,9 @@ src/latman.c:1786-1840) fed with lbh_initial_rho's densities must give,
 bit for bit, the populations the reference's read_params + init_problem
 made of the same params.in (tests/golden/init/, see tests/test_init_pin.py),
 on every node: the reference initialises solid nodes too, and the compact
-layout returns them exactly as set.
+layout returns them exactly as set.  The macro variables then hold what
+init_problem leaves in them (rho, u = 0), whether u is passed as zeros
+(dense runs) or left out and filled on the device (compact runs).
 """
 import numpy as np
 import pytest
@@ -29,7 +31,13 @@ def test_gpu_init_equilibrium_matches_reference_init_problem(name, layout, tmp_p
                     compressible=p.compressible, layout=layout)
     with lbx.Domain(lp, mask) as d:
         for s in range(nsubs):
-            d.init_equilibrium(s, rho[s], 0.0, 0.0, 0.0 if dims == 3 else None)
+            if layout == lbx.LBX_LAYOUT_DENSE:
+                d.init_equilibrium(s, rho[s], 0.0, 0.0, 0.0 if dims == 3 else None)
+            else:
+                d.init_equilibrium(s, rho[s])   # u = 0 filled on the device
         d.sync()
         f = d.download_f()
+        mv = d.download_mv()
     assert same_bits(f, z["f"])
+    # and the macro variables init_problem leaves: rho, and u at rest
+    assert same_bits(mv, z["mv"])

@@ -263,7 +263,39 @@ def test_gpu_init_equilibrium_matches_oracle():
         for s in range(2):
             d.init_equilibrium(s, rho[s], u[0, s], u[1, s], u[2, s])
         f = d.download_f()
+        mv = d.download_mv()
     assert rel_err(f, fo) < 1e-14
+    # the macro variables hold the fields, as init_problem leaves them
+    for s in range(2):
+        assert np.array_equal(mv[s, 0], rho[s])
+        for c in range(3):
+            assert np.array_equal(mv[s, 1 + c], u[c, s])
+
+
+@pytest.mark.parametrize("layout", ["dense", "compact"])
+def test_gpu_init_equilibrium_2d_then_steps(layout):
+    """2D FP32 over solids: the state formed from rho, u equals the oracle's
+    feq, the macro variables hold the fields, and steps from it match the
+    oracle run from the same populations."""
+    p = po.Params(dims=2, LX=40, LY=28, LZ=1, tau=(0.9, 1), gaccel=(1e-5, 0, 0, 0, 0, 0))
+    sol = geometry.transpose_2d(geometry.disc_pack(28, 40, radius=3, porosity=0.6, seed=4),
+                                28, 40)
+    rng = np.random.default_rng(8)
+    rho = (1 + 0.01 * rng.random(p.NN)).astype(np.float32)
+    u = (0.01 * rng.standard_normal((2, p.NN))).astype(np.float32)
+    fo = po.init_feq(p, rho[None], u[0][None], u[1][None], None)
+    with lbx.Domain(to_lbx(p, np.float32, layout), sol) as d:
+        d.init_equilibrium(0, rho, u[0], u[1])
+        f0 = d.download_f()
+        mv = d.download_mv()
+        d.run(0, 20, 20)
+        f = d.download_f()
+    assert rel_err(f0, fo) < 1e-6
+    assert np.array_equal(mv[0, 0], rho) and np.array_equal(mv[0, 1], u[0])
+    assert np.array_equal(mv[0, 2], u[1])
+    fr, _ = _oracle(p, f0.astype(np.float32), sol, 20, 20)
+    fr64, _ = _oracle(p, f0.astype(np.float64), sol, 20, 20)
+    assert rel_err(f, fr64) <= max(1e-5, 1.25 * rel_err(fr, fr64))
 
 
 def test_gpu_rejects_out_of_order_steps():
