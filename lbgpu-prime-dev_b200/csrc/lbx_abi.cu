@@ -1021,8 +1021,13 @@ lbx_status lbx_init_equilibrium(lbx_domain* d, int subs, const void* rho, const 
                                 const void* uy, const void* uz)
 {
   if (lbx_status st = check_subs(d, subs)) return st;
-  if (d->dense_stale) { if (lbx_status st = exchange(d, false)) return st; }
   if (!rho) return fail(LBX_ERR_INVALID, "rho is required");
+  // as in lbx_upload_f: the other substance's dense copy must be current
+  // before the gather; a single substance is overwritten whole, so its
+  // stale copy is not brought back first
+  if (d->dense_stale && d->p.nsubs > 1) {
+    if (lbx_status st = exchange(d, false)) return st;
+  }
   // the fields land in the substance's macro variables, where the
   // reference's init_problem leaves them (src/latman.c:1302-1780), and the
   // populations are formed from there: no staging allocation.  A velocity
@@ -1057,6 +1062,7 @@ lbx_status lbx_init_equilibrium(lbx_domain* d, int subs, const void* rho, const 
   }
   if (e == cudaSuccess) e = cudaStreamSynchronize(d->stream);
   if (e != cudaSuccess) return fail(LBX_ERR_CUDA, "init_equilibrium: %s", cudaGetErrorString(e));
+  d->dense_stale = false;   // the compact state was just gathered from it
   d->parity = 0;
   return LBX_OK;
 }

@@ -342,7 +342,11 @@ def test_gpu_cfg1_full_run_matches_oracle(layout):
     assert info["faces_fused"] and info["layout"] == layout
     p = po.Params(dims=2, LX=256, LY=256, LZ=1, tau=(1.0, 1.0), pressure_s_in=(1, 0),
                   pressure_n_out=(1, 0), rho_in=1.001, rho_out=1.0)
-    fo, mvo = po.run_oracle(p, np.zeros((1, 9, p.NN)), mask, 0, 2000, 2000)
+    # the macro variables init_equilibrium leaves (rho = 1, u = 0), which
+    # the steps never overwrite at solid nodes
+    mv0 = np.zeros((1, 3, p.NN))
+    mv0[0, 0] = 1.0
+    fo, mvo = po.run_oracle(p, np.zeros((1, 9, p.NN)), mask, 0, 2000, 2000, mv=mv0)
     assert_close(f, mv, fo, mvo, mask, np.float64)
     # pressure-driven flow along j, from the rho_in face to the rho_out face
     fl = mask != 1
@@ -431,4 +435,51 @@ def test_gpu_upload_into_a_stepped_domain(nsubs):
         fo, _ = po.run_oracle(p, f0.copy(), sol, 0, 6, 6)
         fo[1] = f1[1]
         fo, _ = po.run_oracle(p, fo, sol, 6, 6, 6)
+        assert rel_err(f, fo) < 1e-12
+
+
+@pytest.mark.parametrize("nsubs", [1, 2])
+def test_gpu_init_into_a_stepped_domain(nsubs):
+    """lbx_init_equilibrium after steps replaces the substance's state: one
+    substance equals a fresh domain's init bit for bit (solid nodes and
+    macro variables included) and steps on identically; one substance of
+    two keeps the other's stepped state (the oracle, stepped and replaced
+    the same way).  Compact layout, FP64."""
+    p = po.Params(dims=3, LX=18, LY=14, LZ=12, nsubs=nsubs, tau=(0.9, 0.7),
+                  sink=1e-3 if nsubs == 2 else 0.0, sigma_t_on=2, sigma_t_off=1000,
+                  gaccel=(2e-5, 0, 0, 0, 0, 0))
+    sol = geometry.sphere_pack(18, 14, 12, radius=3, porosity=0.5, seed=6)
+    rng = np.random.default_rng(9)
+    f0 = rng.standard_normal((nsubs, 19, p.NN)) * 1e-4
+    if nsubs == 2:
+        f0[1] = np.abs(f0[1]) * 10
+    s = nsubs - 1                     # the substance re-initialised
+    rho = (0.01 if s else 1.0) + 0.001 * rng.random(p.NN)
+    lp = to_lbx(p, np.float64, "compact")
+
+    def init(d):
+        d.init_equilibrium(s, rho)    # at rest: u filled on the device
+    with lbx.Domain(lp, sol) as d:
+        d.upload_f(f0)
+        d.run(0, 6, 6)
+        init(d)
+        fi, mvi = d.download_f(), d.download_mv()
+        d.run(0, 6, 6)
+        d.sync()
+        f = d.download_f()
+    if nsubs == 1:
+        with lbx.Domain(lp, sol) as d:
+            init(d)
+            np.testing.assert_array_equal(fi, d.download_f())
+            np.testing.assert_array_equal(mvi, d.download_mv())
+            d.run(0, 6, 6)
+            d.sync()
+            np.testing.assert_array_equal(f, d.download_f())
+    else:
+        fo, _ = po.run_oracle(p, f0.copy(), sol, 0, 6, 6)
+        z = np.zeros((2, p.NN))
+        fo[1] = po.init_feq(p, np.stack([rho, rho]), z, z, z)[1]
+        assert rel_err(fi, fo) < 1e-14
+        assert np.array_equal(mvi[1, 0], rho) and not mvi[1, 1:].any()
+        fo, _ = po.run_oracle(p, fo, sol, 0, 6, 6)
         assert rel_err(f, fo) < 1e-12
