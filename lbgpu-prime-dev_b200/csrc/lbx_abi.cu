@@ -207,7 +207,8 @@ CompactArgs<T> make_compact(const lbx_domain* d, const StepArgs<T>& A)
 // between them runs in the ordinary step launches, so the face code's
 // registers do not weigh on the bulk of the nodes.
 template <typename T, int Q, int NS, int MODEL>
-void launch_face_nodes(lbx_domain* d, const StepArgs<T>& A, bool odd, const Face3Fused<T>& f3)
+void launch_face_nodes(lbx_domain* d, const StepArgs<T>& A, bool odd, const Face3Fused<T>& f3,
+                       cudaStream_t stream)
 {
   if constexpr (Q == 19) {
     CompactArgs<T> C = make_compact<T>(d, A);
@@ -221,7 +222,7 @@ void launch_face_nodes(lbx_domain* d, const StepArgs<T>& A, bool odd, const Face
     const bool idx32 = (unsigned long long)Q * (unsigned long long)d->P < (1ull << 32);
     auto go = [&](auto odd_c, auto idx_c) {
       aa_step_compact<T, Q, NS, MODEL, decltype(odd_c)::value, PART_ALL, decltype(idx_c)::value,
-                      false, true><<<blocks, 256, 0, d->stream>>>(C);
+                      false, true><<<blocks, 256, 0, stream>>>(C);
     };
     using TT = std::true_type;
     using FF = std::false_type;
@@ -272,28 +273,43 @@ void launch_part(lbx_domain* d, const StepArgs<T>& A, bool odd, const Face3Fused
 }
 
 // One step: a single launch for the flow alone; flow then solute for two
-// substances (the solute launch only while the solute is active).
+// substances (the solute launch only while the solute is active).  With
+// the z faces fused, the face planes' nodes run in a launch of their own on
+// the side stream, beside the interior launches: in an AA step every node
+// reads and writes only its own set of population slots, the face launch
+// carries the flow's u to the solute in registers (it reads no handoff
+// value of the interior's), and node-indexed outputs (macro variables,
+// plane-record values) are disjoint, so the two touch no common location.
+// Returns true when the face launch went to the side stream: the caller
+// joins it back into the step's stream (step_t).
 template <typename T, int Q, int NS, int MODEL>
-void launch_aa(lbx_domain* d, const StepArgs<T>& A, bool odd, const Face3Fused<T>* f3)
+bool launch_aa(lbx_domain* d, const StepArgs<T>& A, bool odd, const Face3Fused<T>* f3)
 {
+  const bool beside = f3 && d->side;
+  if (beside) {
+    cudaEventRecord(d->side_fork, d->stream);
+    cudaStreamWaitEvent(d->side, d->side_fork, 0);
+    launch_face_nodes<T, Q, NS, MODEL>(d, A, odd, *f3, d->side);
+  }
   if constexpr (NS == 1) {
     launch_part<T, Q, NS, MODEL, PART_ALL>(d, A, odd, f3);
   } else {
     launch_part<T, Q, NS, MODEL, PART_FLOW>(d, A, odd, f3);
     if (A.solute_on) launch_part<T, Q, NS, MODEL, PART_SOLUTE>(d, A, odd, f3);
   }
-  if (f3) launch_face_nodes<T, Q, NS, MODEL>(d, A, odd, *f3);
+  if (f3 && !beside) launch_face_nodes<T, Q, NS, MODEL>(d, A, odd, *f3, d->stream);
+  return beside;
 }
 
 template <typename T, int Q, int NS>
-void launch_model(lbx_domain* d, const StepArgs<T>& A, bool odd,
+bool launch_model(lbx_domain* d, const StepArgs<T>& A, bool odd,
                   const Face3Fused<T>* f3 = nullptr)
 {
   const int model = d->p.accurate ? (d->p.compressible ? SHIFTED_COMP : SHIFTED_INC)
                                   : PLAIN_COMP;
-  if (model == SHIFTED_INC) launch_aa<T, Q, NS, SHIFTED_INC>(d, A, odd, f3);
-  else if (model == PLAIN_COMP) launch_aa<T, Q, NS, PLAIN_COMP>(d, A, odd, f3);
-  else launch_aa<T, Q, NS, SHIFTED_COMP>(d, A, odd, f3);
+  if (model == SHIFTED_INC) return launch_aa<T, Q, NS, SHIFTED_INC>(d, A, odd, f3);
+  if (model == PLAIN_COMP) return launch_aa<T, Q, NS, PLAIN_COMP>(d, A, odd, f3);
+  return launch_aa<T, Q, NS, SHIFTED_COMP>(d, A, odd, f3);
 }
 
 // The stand-alone face kernels, in the order of bcs_1 / bcs_2.
@@ -454,22 +470,35 @@ lbx_status step_t(lbx_domain* d, int t, unsigned flags)
   Face3Fused<T> f3;
   if (f3_fused) f3 = face3_fused<T>(d, t);
   StepArgs<T> A = make_args<T>(d, t, flags);
+  bool beside = false;   // the face planes' launch is on the side stream
   if (d->Q == 9) {
     if (d->p.nsubs == 1) launch_model<T, 9, 1>(d, A, odd);
     else launch_model<T, 9, 2>(d, A, odd);
   } else {
-    if (d->p.nsubs == 1) launch_model<T, 19, 1>(d, A, odd, f3_fused ? &f3 : nullptr);
-    else launch_model<T, 19, 2>(d, A, odd, f3_fused ? &f3 : nullptr);
+    if (d->p.nsubs == 1) beside = launch_model<T, 19, 1>(d, A, odd, f3_fused ? &f3 : nullptr);
+    else beside = launch_model<T, 19, 2>(d, A, odd, f3_fused ? &f3 : nullptr);
+  }
+  // a record of a face plane reads values only the face launch wrote: its
+  // reduction follows that launch on the side stream, beside the interior
+  const bool record_beside = beside && d->btc_vals &&
+                             (d->btc_hi <= f3.lo_end || d->btc_lo >= f3.hi_start);
+  if (beside && !record_beside) {
+    cudaEventRecord(d->side_join, d->side);
+    cudaStreamWaitEvent(d->stream, d->side_join, 0);
   }
   if (d->btc_vals) {
     const bool compact = d->layout == LBX_LAYOUT_COMPACT;
     const int count = d->btc_hi - d->btc_lo;
     const int nb = std::max(1, std::min(kBtcMaxBlocks, (count + 1023) / 1024));
-    btc_reduce<<<nb, kBtcThreads, 0, d->stream>>>(
+    btc_reduce<<<nb, kBtcThreads, 0, record_beside ? d->side : d->stream>>>(
         d->btc_vals, count, compact ? nullptr : d->solids + d->btc_lo,
         (double)d->plane_fluid[d->btc_plane], d->p.nsubs == 2 && A.solute_on, d->btc_rec,
         d->btc_slot, d->btc_cap, d->btc_part, d->btc_ticket);
     d->launches++;
+  }
+  if (record_beside) {
+    cudaEventRecord(d->side_join, d->side);
+    cudaStreamWaitEvent(d->stream, d->side_join, 0);
   }
   CK(cudaGetLastError());
   return LBX_OK;
@@ -601,6 +630,9 @@ void release(lbx_domain* d)
   lbx_internal_frames_free(d);
   lbx_internal_pest_free(d);
   lbx_internal_tiled_free(d);
+  if (d->side) cudaStreamDestroy(d->side);
+  if (d->side_fork) cudaEventDestroy(d->side_fork);
+  if (d->side_join) cudaEventDestroy(d->side_join);
   if (d->own_stream) cudaStreamDestroy(d->own_stream);
 }
 
@@ -880,6 +912,11 @@ lbx_status lbx_create(const lbx_params* p, const uint8_t* solids, lbx_domain** o
                      "%s: %s", #call, cudaGetErrorString(e)));
   CKD(cudaStreamCreateWithFlags(&d->own_stream, cudaStreamNonBlocking));
   d->stream = d->own_stream;
+  if (d->faces3_active && d->layout == LBX_LAYOUT_COMPACT) {
+    CKD(cudaStreamCreateWithFlags(&d->side, cudaStreamNonBlocking));
+    CKD(cudaEventCreateWithFlags(&d->side_fork, cudaEventDisableTiming));
+    CKD(cudaEventCreateWithFlags(&d->side_join, cudaEventDisableTiming));
+  }
   const size_t fbytes = (size_t)p->nsubs * d->Q * d->N * d->real_size;
   const size_t mvbytes = (size_t)p->nsubs * (1 + d->D) * d->N * d->real_size;
   CKD(cudaMalloc(&d->f, fbytes));

@@ -306,6 +306,82 @@ struct AdjFaceOps {
   double* dprof[2];
 };
 
+// Node (i, j) of the top (TOP, a compile-time constant so that the
+// per-direction arrays are indexed by constants and stay in registers) or
+// bottom plane, compact slot `self`.
+template <typename T, bool TOP>
+__device__ __forceinline__ void adj_face_node(T* Ls, const int* fidx, int LX, int LY, int LZ,
+                                              long long stride, int second, int kind,
+                                              double* dprof, int i, int j, int self)
+{
+  const int k = TOP ? LZ - 1 : 0;
+  const int plane = LX * LY;
+  // Every slot address first, then every value, then every store: written
+  // as read-modify-writes in order, each access waited for the one before
+  // it (the compiler cannot tell the slots apart), a chain of ~19 memory
+  // round trips per thread.  Slots of distinct directions are distinct,
+  // except that a known slot can be the very slot an unknown was deposited
+  // in (solids on both sides: the own-slot fallback of the load and of the
+  // deposit); there the known's old value is the cleared unknown's, 0.
+  constexpr bool tp = TOP;
+  int up[19];
+#pragma unroll
+  for (int a = 1; a < 19; ++a) {
+    if (second) { up[a] = -1; continue; }
+    int ii = i - cx(a), jj = j - cy(a), kk = k - cz(a);
+    ii = ii < 0 ? LX - 1 : (ii == LX ? 0 : ii);
+    jj = jj < 0 ? LY - 1 : (jj == LY ? 0 : jj);
+    kk = kk < 0 ? LZ - 1 : (kk == LZ ? 0 : kk);
+    up[a] = fidx[ii + LX * jj + plane * kk];
+  }
+  up[0] = self;
+  auto rslot = [&](int a) -> long long {   // where the forward loaded d_a
+    if (second) return (long long)opp(a) * stride + self;
+    return up[a] < 0 ? (long long)opp(a) * stride + self : (long long)a * stride + up[a];
+  };
+  auto wslot = [&](int a) -> long long {   // where it stored unknown a
+    if (second) return (long long)opp(a) * stride + self;
+    return (long long)a * stride + (up[a] < 0 ? self : up[a]);
+  };
+  T wsum = wgt<T, 19>(face3_unknown(tp, 0));
+#pragma unroll
+  for (int q = 1; q < 5; ++q) wsum = wsum + wgt<T, 19>(face3_unknown(tp, q));
+  long long ws[5];
+  T lu[5];
+#pragma unroll
+  for (int q = 0; q < 5; ++q) ws[q] = wslot(face3_unknown(tp, q));
+#pragma unroll
+  for (int q = 0; q < 5; ++q) lu[q] = Ls[ws[q]];
+  // the knowns the adjoint of X goes to: the five opposite the unknowns
+  // (zero gradient: in D3Q19 exactly the directions of the other c_z) or
+  // every direction but the unknowns (the rest)
+  const bool zg = kind == FACE_ZEROGRAD;
+  long long rs[19];
+  T lk[19];
+#pragma unroll
+  for (int a = 0; a < 19; ++a) {
+    const bool known = zg ? cz(a) == (tp ? 1 : -1) : cz(a) != (tp ? -1 : 1);
+    rs[a] = known ? rslot(a) : -1;
+  }
+#pragma unroll
+  for (int a = 0; a < 19; ++a) lk[a] = rs[a] >= 0 ? Ls[rs[a]] : T(0);
+  T Ax = T(0);
+#pragma unroll
+  for (int q = 0; q < 5; ++q) Ax += wgt<T, 19>(face3_unknown(tp, q)) * lu[q];
+  const T ax = Ax / wsum;
+#pragma unroll
+  for (int q = 0; q < 5; ++q) Ls[ws[q]] = T(0);
+#pragma unroll
+  for (int a = 0; a < 19; ++a) {
+    if (rs[a] < 0) continue;
+    T old = lk[a];
+#pragma unroll
+    for (int q = 0; q < 5; ++q) old = rs[a] == ws[q] ? T(0) : old;
+    Ls[rs[a]] = zg ? old + ax : old - ax;
+  }
+  if (!zg && dprof) dprof[i + LX * j] += (double)ax;
+}
+
 template <typename T>
 __global__ void adj_face_plane(T* Ls, const int* fidx, int LX, int LY, int LZ,
                                long long stride, int second, AdjFaceOps ops)
@@ -313,53 +389,17 @@ __global__ void adj_face_plane(T* Ls, const int* fidx, int LX, int LY, int LZ,
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= LX) return;
   const int j = blockIdx.y;
-  const int top = ops.top[blockIdx.z];
-  const int kind = ops.kind[blockIdx.z];
-  double* const dprof = ops.dprof[blockIdx.z];
-  const int k = top ? LZ - 1 : 0;
-  const int plane = LX * LY;
-  const int n = i + LX * j + plane * k;
+  // the group's entries by select: indexing the parameter arrays by
+  // blockIdx.z would copy them to local memory
+  const bool g1 = blockIdx.z != 0;
+  const int top = g1 ? ops.top[1] : ops.top[0];
+  const int kind = g1 ? ops.kind[1] : ops.kind[0];
+  double* const dprof = g1 ? ops.dprof[1] : ops.dprof[0];
+  const int n = i + LX * j + LX * LY * (top ? LZ - 1 : 0);
   const int self = fidx[n];
   if (self < 0) return;
-  auto upstream = [&](int a) -> int {
-    int ii = i - cx(a), jj = j - cy(a), kk = k - cz(a);
-    ii = ii < 0 ? LX - 1 : (ii == LX ? 0 : ii);
-    jj = jj < 0 ? LY - 1 : (jj == LY ? 0 : jj);
-    kk = kk < 0 ? LZ - 1 : (kk == LZ ? 0 : kk);
-    return fidx[ii + LX * jj + plane * kk];
-  };
-  auto rslot = [&](int a) -> long long {   // where the forward loaded d_a
-    if (second) return (long long)opp(a) * stride + self;
-    const int up = upstream(a);
-    return up < 0 ? (long long)opp(a) * stride + self : (long long)a * stride + up;
-  };
-  auto wslot = [&](int a) -> long long {   // where it stored unknown a
-    if (second) return (long long)opp(a) * stride + self;
-    const int up = upstream(a);
-    return (long long)a * stride + (up < 0 ? self : up);
-  };
-  const bool tp = top != 0;
-  T wsum = wgt<T, 19>(face3_unknown(tp, 0));
-#pragma unroll
-  for (int q = 1; q < 5; ++q) wsum = wsum + wgt<T, 19>(face3_unknown(tp, q));
-  T Ax = T(0);
-#pragma unroll
-  for (int q = 0; q < 5; ++q) {
-    const int a = face3_unknown(tp, q);
-    const long long s = wslot(a);
-    Ax += wgt<T, 19>(a) * Ls[s];
-    Ls[s] = T(0);
-  }
-  const T ax = Ax / wsum;
-  if (kind == FACE_ZEROGRAD) {
-#pragma unroll
-    for (int q = 0; q < 5; ++q) Ls[rslot(opp(face3_unknown(tp, q)))] += ax;
-  } else {
-#pragma unroll
-    for (int a = 0; a < 19; ++a)
-      if (cz(a) != (tp ? -1 : 1)) Ls[rslot(a)] -= ax;
-    if (dprof) dprof[i + LX * j] += (double)ax;
-  }
+  if (top) adj_face_node<T, true>(Ls, fidx, LX, LY, LZ, stride, second, kind, dprof, i, j, self);
+  else adj_face_node<T, false>(Ls, fidx, LX, LY, LZ, stride, second, kind, dprof, i, j, self);
 }
 
 struct AdjState {

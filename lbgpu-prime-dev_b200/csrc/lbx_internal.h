@@ -29,6 +29,11 @@ struct lbx_domain {
   int red_blocks = 0;
   cudaStream_t stream = nullptr;      // stream all work is queued on
   cudaStream_t own_stream = nullptr;  // the library's stream
+  // with z faces in the compact layout: the face planes' launch runs on
+  // `side` beside the interior launches, forked from and joined back into
+  // `stream` by the two events
+  cudaStream_t side = nullptr;
+  cudaEvent_t side_fork = nullptr, side_join = nullptr;
   std::vector<double> n_table, s_table;
   long long fluid = 0;
   bool faces_active = false;  // any 2D face boundary configured

@@ -1068,6 +1068,60 @@ struct FaceOps {
   T conc;                          // constant concentration otherwise
 };
 
+// The face operations of group g at node (i, j) of the top (TOP) or bottom
+// plane, whose populations are at slots `self` of fs (see face_plane).
+template <typename T, bool COMPACT, bool TOP>
+__device__ __forceinline__ void face_plane_node(T* fs, const uint8_t* solids, const int* fidx,
+                                                int LX, int LY, int LZ, long long stride,
+                                                int second, const FaceOps<T>& ops, int g,
+                                                int i, int j, int self)
+{
+  const int k = TOP ? LZ - 1 : 0;
+  const int plane = LX * LY;
+  // slot of the upstream node n - c_a, -1 if it is solid, for every a
+  // before any population moves: looked up between the stores, each lookup
+  // waited for the store before it (the compiler cannot tell the arrays
+  // apart).  TOP is a compile-time constant so that every index into the
+  // per-direction arrays is one, and they stay in registers.
+  int up[19];
+#pragma unroll
+  for (int a = 0; a < 19; ++a) {
+    if (second || a == 0) { up[a] = self; continue; }
+    int ii = i - cx(a), jj = j - cy(a), kk = k - cz(a);
+    ii = ii < 0 ? LX - 1 : (ii == LX ? 0 : ii);
+    jj = jj < 0 ? LY - 1 : (jj == LY ? 0 : jj);
+    kk = kk < 0 ? LZ - 1 : (kk == LZ ? 0 : kk);
+    const int q = ii + LX * jj + plane * kk;
+    if (COMPACT) up[a] = fidx[q];
+    else up[a] = solids[q] == 1 ? -1 : q;
+  }
+  // the group's operations in order; each loads only the populations its
+  // rule reads: the knowns (cz != the unknowns'), or for the zero gradient
+  // the five opposite the unknowns
+  constexpr int cz_unknown = TOP ? -1 : 1;
+  const int q_end = ops.first[g] + ops.count[g];
+  for (int q0 = ops.first[g]; q0 < q_end; ++q0) {
+    const int kind = ops.kind[q0];
+    T d[19];
+#pragma unroll
+    for (int a = 0; a < 19; ++a) {
+      const bool need = kind == FACE_ZEROGRAD ? cz(a) == -cz_unknown : cz(a) != cz_unknown;
+      if (!need) { d[a] = T(0); continue; }
+      if (second) d[a] = fs[opp(a) * stride + self];
+      else d[a] = (up[a] < 0) ? fs[opp(a) * stride + self] : fs[a * stride + up[a]];
+    }
+    const T* prof = ops.profile[q0];
+    face3_apply<T>(d, TOP, kind, ops.drho[q0], prof ? prof[i + LX * j] : ops.conc,
+                   ops.shift[q0]);
+#pragma unroll
+    for (int q = 0; q < 5; ++q) {
+      const int a = face3_unknown(TOP, q);
+      if (second) fs[opp(a) * stride + self] = d[a];
+      else fs[a * stride + (up[a] < 0 ? self : up[a])] = d[a];
+    }
+  }
+}
+
 // One thread per (i, j) of one group.  `_1` form (second == 0, before
 // an odd step): loads what the odd step will pull and deposits the unknowns
 // where it will pull them from (slot a of the upstream node, or of the node
@@ -1084,55 +1138,12 @@ __global__ void face_plane(T* f, const uint8_t* solids, const int* fidx, int LX,
   const int g = blockIdx.z;
   const int top = ops.top[g];
   T* const fs = f + (long long)ops.subs[g] * 19 * stride;
-  const int k = top ? LZ - 1 : 0;
-  const int plane = LX * LY;
-  const int n = i + LX * j + plane * k;
+  const int n = i + LX * j + LX * LY * (top ? LZ - 1 : 0);
   int self;
   if (COMPACT) { self = fidx[n]; if (self < 0) return; }
   else { if (solids[n] == 1) return; self = n; }
-  // slot of the upstream node n - c_a, -1 if it is solid
-  auto upstream = [&](int a) -> int {
-    int ii = i - cx(a), jj = j - cy(a), kk = k - cz(a);
-    ii = ii < 0 ? LX - 1 : (ii == LX ? 0 : ii);
-    jj = jj < 0 ? LY - 1 : (jj == LY ? 0 : jj);
-    kk = kk < 0 ? LZ - 1 : (kk == LZ ? 0 : kk);
-    const int q = ii + LX * jj + plane * kk;
-    if (COMPACT) return fidx[q];
-    return solids[q] == 1 ? -1 : q;
-  };
-  // the group's operations in order; each loads only the populations its
-  // rule reads: the knowns (cz != the unknowns'), or for the zero gradient
-  // the five opposite the unknowns
-  const int cz_unknown = top ? -1 : 1;
-  const int q_end = ops.first[g] + ops.count[g];
-  for (int q0 = ops.first[g]; q0 < q_end; ++q0) {
-    const int kind = ops.kind[q0];
-    T d[19];
-#pragma unroll
-    for (int a = 0; a < 19; ++a) {
-      const bool need = kind == FACE_ZEROGRAD ? cz(a) == -cz_unknown : cz(a) != cz_unknown;
-      if (!need) { d[a] = T(0); continue; }
-      if (second) {
-        d[a] = fs[opp(a) * stride + self];
-      } else {
-        const int up = upstream(a);
-        d[a] = (up < 0) ? fs[opp(a) * stride + self] : fs[a * stride + up];
-      }
-    }
-    const T* prof = ops.profile[q0];
-    face3_apply<T>(d, top != 0, kind, ops.drho[q0], prof ? prof[i + LX * j] : ops.conc,
-                   ops.shift[q0]);
-#pragma unroll
-    for (int q = 0; q < 5; ++q) {
-      const int a = face3_unknown(top != 0, q);
-      if (second) {
-        fs[opp(a) * stride + self] = d[a];
-      } else {
-        const int up = upstream(a);
-        fs[a * stride + (up < 0 ? self : up)] = d[a];
-      }
-    }
-  }
+  if (top) face_plane_node<T, COMPACT, true>(fs, solids, fidx, LX, LY, LZ, stride, second, ops, g, i, j, self);
+  else face_plane_node<T, COMPACT, false>(fs, solids, fidx, LX, LY, LZ, stride, second, ops, g, i, j, self);
 }
 
 // ---- plane record ---------------------------------------------------------------

@@ -2,7 +2,7 @@
 
     python -m lbx.configs cfg1 [--steps 2000]
     python -m lbx.configs cfg2 [--steps 10000]
-    python -m lbx.configs cfg3 [--steps 20000]
+    python -m lbx.configs cfg3 [--steps 20000] [--edge 192] [--quick]
     python -m lbx.configs cfg5 [--steps 4000]
     python -m lbx.configs cfg4 [--samples 512] [--steps 200] [--modes fused,...] [--quick]
 
@@ -213,10 +213,13 @@ def _cfg3_run(p, mask, steps: int, chunk: int, blob: bool = False):
     return dict(seconds=secs, m0=m0, masses=masses, btc=btc, reduce=r)
 
 
-def run_cfg3(steps: int = 20000, shape=(192, 192, 384), chunk: int = 1000) -> list:
+def run_cfg3(steps: int = 20000, shape=(192, 192, 384), chunk: int = 1000,
+             quick: bool = False) -> list:
+    """quick: the FP32 run between the faces only (no FP64 comparison, no
+    closed box), e.g. under a profiler."""
     out = []
     res = {}
-    for name, prec in (("fp32", 4), ("fp64", 8)):
+    for name, prec in (("fp32", 4),) + ((("fp64", 8),) if not quick else ()):
         p, mask = cfg3_params(prec, shape)
         r = _cfg3_run(p, mask, steps, chunk)
         res[name] = r
@@ -229,6 +232,8 @@ def run_cfg3(steps: int = 20000, shape=(192, 192, 384), chunk: int = 1000) -> li
                     "btc_first_above_0.01": first(0.01), "btc_first_above_0.5": first(0.5),
                     "solute_mass_every_chunk": [[t, m] for t, m in r["masses"]],
                     "flow_mass": r["reduce"]["mass"]})
+    if quick:
+        return out
     b32, b64 = res["fp32"]["btc"], res["fp64"]["btc"]
     m32, m64 = res["fp32"]["masses"][-1][1], res["fp64"]["masses"][-1][1]
     out.append({"config": "cfg3", "compare": "fp32_vs_fp64",
@@ -534,8 +539,9 @@ def main(argv=None) -> int:
     ap.add_argument("--modes", default="fused,persistent,sequential",
                     help="cfg4: batch modes to time, comma-separated")
     ap.add_argument("--quick", action="store_true",
-                    help="cfg4: skip the autotuner and the independent-lattice comparison "
-                         "(a short run, e.g. under a profiler)")
+                    help="cfg4: skip the autotuner and the independent-lattice comparison; "
+                         "cfg3: the FP32 run between the faces only (short runs, e.g. under "
+                         "a profiler)")
     a = ap.parse_args(argv)
     if a.config == "cfg1":
         print(json.dumps(run_cfg1(a.steps or 2000)))
@@ -544,7 +550,9 @@ def main(argv=None) -> int:
                              K=a.checkpoint_every, fd_dirs=a.fd_dirs):
             print(json.dumps(line))
     elif a.config == "cfg3":
-        for line in run_cfg3(a.steps or 20000):
+        # --edge E: an E x E x 2E lattice instead of 192 x 192 x 384
+        shape = (a.edge, a.edge, 2 * a.edge) if a.edge != 256 else (192, 192, 384)
+        for line in run_cfg3(a.steps or 20000, shape, quick=a.quick):
             print(json.dumps(line))
     elif a.config == "frames":
         for line in run_frames(a.steps or 2000, a.frame_rate, a.edge, a.frame_files):
