@@ -75,19 +75,24 @@ def test_gpu_z_faces_solid_wrap_neighbours(layout):
     assert_close(f, mv, fo, mvo, sol, np.float64)
 
 
+@pytest.mark.parametrize("where", ["top", "bottom", "interior"])
 @pytest.mark.parametrize("layout", ["dense", "compact"])
 @pytest.mark.parametrize("dtype", [np.float64, np.float32])
-def test_gpu_breakthrough_record_matches_oracle(dtype, layout):
+def test_gpu_breakthrough_record_matches_oracle(dtype, layout, where):
+    """The record of a face plane (written only by the compact layout's
+    face-plane launch, and reduced beside the interior launches) and of an
+    interior plane (reduced after both)."""
     p, sol, f0 = _flow_solute(20, 18, 16, 0.55, 7, **CASES["inlet_bottom"])
     p.sigma_t_on, p.sigma_t_off = 3, 10 ** 6
+    plane = {"top": p.LZ - 1, "bottom": 0, "interior": p.LZ // 2}[where]
     f0 = f0.astype(dtype)
     steps = 60
     with lbx.Domain(to_lbx(p, dtype, layout), sol) as d:
         d.upload_f(f0)
-        d.btc_start(p.LZ - 1, 100)
+        d.btc_start(plane, 100)
         d.run(0, steps, 0)
         btc, ux = d.btc_read(ux=True)
-    _, _, btc_o, ux_o = po.run_oracle_btc(p, f0.copy(), sol, 0, steps, p.LZ - 1)
+    _, _, btc_o, ux_o = po.run_oracle_btc(p, f0.copy(), sol, 0, steps, plane)
     assert btc.shape == (steps,)
     assert np.isnan(btc[:2]).all() and np.isnan(btc_o[:2]).all()   # solute off at t=1,2
     live = ~np.isnan(btc_o)
