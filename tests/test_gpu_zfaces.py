@@ -262,3 +262,47 @@ def test_gpu_z_faces_fused_equal_standalone(case):
     assert out["compact"][2] == 3 * 30 and out["dense"][2] == 3 * 30
     fo, mvo = po.run_oracle(p, f0.copy(), sol, 0, 30, 30)
     assert_close(out["compact"][0], out["compact"][1], fo, mvo, sol, np.float64)
+
+
+def test_gpu_z_faces_side_stream_on_every_path():
+    """The compact layout's face-plane launch (and the record of a face
+    plane) run on a second stream, forked from and joined back into the
+    step's stream.  Step by step, replayed from captured graphs, and on a
+    caller's stream, FP64 results and the record are bit-identical, and
+    equal to the oracle."""
+    torch = pytest.importorskip("torch")
+    p, sol, f0 = _flow_solute(18, 16, 12, 0.6, 21, **CASES["inlet_bottom"])
+    m3 = sol.reshape(12, 16, 18)
+    m3[0] = 0
+    m3[-1] = 0
+    sol = m3.reshape(-1)
+    steps = 40
+    out = {}
+    for how in ("steps", "graphs", "caller_stream"):
+        with lbx.Domain(to_lbx(p, np.float64, "compact"), sol) as d:
+            s = torch.cuda.Stream() if how == "caller_stream" else None
+            if s is not None:
+                d.set_stream(s.cuda_stream)
+            d.upload_f(f0)
+            d.btc_start(p.LZ - 1, steps)
+            if how == "steps":
+                for t in range(1, steps + 1):
+                    d.step(t, write_mv=(t == steps))
+            else:
+                d.run(0, steps, steps)
+            if s is not None:
+                s.synchronize()
+                d.set_stream(None)
+            d.sync()
+            out[how] = (d.download_f(), d.download_mv(), d.btc_read(ux=True))
+    for how in ("graphs", "caller_stream"):
+        assert np.array_equal(out[how][0], out["steps"][0]), how
+        assert np.array_equal(out[how][1], out["steps"][1]), how
+        for c in range(2):
+            assert np.array_equal(out[how][2][c], out["steps"][2][c], equal_nan=True), how
+    fo, mvo, btc_o, ux_o = po.run_oracle_btc(p, f0.copy(), sol, 0, steps, p.LZ - 1,
+                                             frame_rate=steps)
+    assert_close(out["steps"][0], out["steps"][1], fo, mvo, sol, np.float64)
+    live = ~np.isnan(btc_o)
+    assert np.abs(out["steps"][2][0][live] - btc_o[live]).max() <= \
+        1e-12 * np.abs(btc_o[live]).max()
