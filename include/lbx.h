@@ -194,7 +194,12 @@ lbx_status lbx_run(lbx_domain* d, int t0, int nsteps, int frame_rate);
 /* Run the domain's work on the caller's CUDA stream (a cudaStream_t passed
  * as void*; NULL is the CUDA default stream).  The domain uses a stream of
  * its own until the first call.  Lets a caller order lbx launches with its
- * own work and time them with its own events. */
+ * own work and time them with its own events.  A compact-layout domain
+ * with z faces also queues each step's face-plane launch on a second,
+ * internal stream, forked from this stream by an event and joined back
+ * into it before the step's later work: everything a step does is ordered
+ * after the caller's earlier work on this stream and before its later
+ * work, and a stream capture of lbx calls captures both streams. */
 lbx_status lbx_set_stream(lbx_domain* d, void* stream);
 
 /* How lbx_run advances a stretch of frame-free AA pairs whose launch
