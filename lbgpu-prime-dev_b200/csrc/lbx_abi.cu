@@ -272,8 +272,12 @@ void launch_part(lbx_domain* d, const StepArgs<T>& A, bool odd, const Face3Fused
   d->launches++;
 }
 
-// One step: a single launch for the flow alone; flow then solute for two
-// substances (the solute launch only while the solute is active).  With
+// One step: a single launch for the flow alone; for two substances, an odd
+// step of the compact layout is one launch too (per node the flow, then the
+// solute from the slots the flow's pulls found, its u in registers), and an
+// even step, or a recomputation that keeps each step's u for the adjoint,
+// is a flow launch that hands u to a solute launch (the solute launch only
+// while the solute is active; fused, the even step spilled and ran slower).  With
 // the z faces fused, the face planes' nodes run in a launch of their own on
 // the side stream, beside the interior launches: in an AA step every node
 // reads and writes only its own set of population slots, the face launch
@@ -292,6 +296,8 @@ bool launch_aa(lbx_domain* d, const StepArgs<T>& A, bool odd, const Face3Fused<T
     launch_face_nodes<T, Q, NS, MODEL>(d, A, odd, *f3, d->side);
   }
   if constexpr (NS == 1) {
+    launch_part<T, Q, NS, MODEL, PART_ALL>(d, A, odd, f3);
+  } else if (odd && !A.fout && d->layout == LBX_LAYOUT_COMPACT) {
     launch_part<T, Q, NS, MODEL, PART_ALL>(d, A, odd, f3);
   } else {
     launch_part<T, Q, NS, MODEL, PART_FLOW>(d, A, odd, f3);

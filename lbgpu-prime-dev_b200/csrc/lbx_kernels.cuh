@@ -627,6 +627,17 @@ constexpr int compact_min_blocks()
   return sizeof(T) == 4 ? 6 : (PART == PART_SOLUTE ? 2 : 3);
 }
 
+// The odd step of two substances in one launch (flow, then the solute from
+// the flow's slot table): 64 registers in FP32, where it runs without
+// spills (at six blocks it spilled and ran no faster than the two launches
+// it replaces).
+template <typename T, int PART, int NS, bool FACES3>
+constexpr int compact_step_min_blocks()
+{
+  return (PART == PART_ALL && NS == 2 && !FACES3) ? (sizeof(T) == 4 ? 4 : 2)
+                                                  : compact_min_blocks<T, PART>();
+}
+
 // IDX32: population offsets within one substance's [Q][P] block fit in 32
 // bits (Q * P < 2^32), so slot selects and address arithmetic stay 32-bit.
 // OOP: write the step's result to C.s.fout instead of in place (used to
@@ -737,6 +748,13 @@ __device__ __forceinline__ void compact_node(const CompactArgs<T>& C, const int 
         sslot[a][threadIdx.x] = src;
         d[a] = fs[src];
       };
+      if (PART == PART_ALL && NS == 2 && s > 0) {
+        // the solute's slots are the flow's (the same solids): read them from
+        // the table the flow's pulls filled, this thread's column, instead of
+        // repeating the upstream lookups
+#pragma unroll
+        for (int a = 0; a < Q; ++a) d[a] = fs[sslot[a][threadIdx.x]];
+      } else {
       pull(0, m);
       if (NS == 1) {
         // one lookup per direction: measured faster than the row windows
@@ -771,6 +789,7 @@ __device__ __forceinline__ void compact_node(const CompactArgs<T>& C, const int 
                 pull(a, cx(a) > 0 ? im : (cx(a) < 0 ? ip : i0));
           }
         }
+      }
       }
     } else {
 #pragma unroll
@@ -828,7 +847,7 @@ __device__ __forceinline__ void compact_node(const CompactArgs<T>& C, const int 
 
 template <typename T, int Q, int NS, int MODEL, bool ODD, int PART, bool IDX32, bool OOP,
           bool FACES3 = false>
-__global__ void __launch_bounds__(256, (compact_min_blocks<T, PART>()))
+__global__ void __launch_bounds__(256, (compact_step_min_blocks<T, PART, NS, FACES3>()))
 aa_step_compact(CompactArgs<T> C)
 {
   int m = blockIdx.x * blockDim.x + threadIdx.x + C.m_base;

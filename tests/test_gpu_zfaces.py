@@ -257,9 +257,10 @@ def test_gpu_z_faces_fused_equal_standalone(case):
             out[layout] = (d.download_f(), d.download_mv(), launches)
     assert np.array_equal(out["dense"][0], out["compact"][0])
     assert np.array_equal(out["dense"][1], out["compact"][1])
-    # dense: face plane + flow + solute per step; compact: flow and solute
-    # over the interior, then the two face planes (every substance)
-    assert out["compact"][2] == 3 * 30 and out["dense"][2] == 3 * 30
+    # dense: face plane + flow + solute per step; compact: the two face
+    # planes (every substance) and the interior, flow and solute in one
+    # launch on odd steps, two on even steps
+    assert out["compact"][2] == 2 * 15 + 3 * 15 and out["dense"][2] == 3 * 30
     fo, mvo = po.run_oracle(p, f0.copy(), sol, 0, 30, 30)
     assert_close(out["compact"][0], out["compact"][1], fo, mvo, sol, np.float64)
 
