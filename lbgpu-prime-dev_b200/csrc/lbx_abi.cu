@@ -274,10 +274,11 @@ void launch_part(lbx_domain* d, const StepArgs<T>& A, bool odd, const Face3Fused
 
 // One step: a single launch for the flow alone; for two substances, an odd
 // step of the compact layout is one launch too (per node the flow, then the
-// solute from the slots the flow's pulls found, its u in registers), and an
-// even step, or a recomputation that keeps each step's u for the adjoint,
-// is a flow launch that hands u to a solute launch (the solute launch only
-// while the solute is active; fused, the even step spilled and ran slower).  With
+// solute from the slots the flow's pulls found, its u in registers; written
+// out of place, for the adjoint's recomputation, it also stores u), and an
+// even step is a flow launch that hands u to a solute launch (the solute
+// launch only while the solute is active; fused, the even step spilled and
+// ran slower).  With
 // the z faces fused, the face planes' nodes run in a launch of their own on
 // the side stream, beside the interior launches: in an AA step every node
 // reads and writes only its own set of population slots, the face launch
@@ -297,7 +298,7 @@ bool launch_aa(lbx_domain* d, const StepArgs<T>& A, bool odd, const Face3Fused<T
   }
   if constexpr (NS == 1) {
     launch_part<T, Q, NS, MODEL, PART_ALL>(d, A, odd, f3);
-  } else if (odd && !A.fout && d->layout == LBX_LAYOUT_COMPACT) {
+  } else if (odd && d->layout == LBX_LAYOUT_COMPACT) {
     launch_part<T, Q, NS, MODEL, PART_ALL>(d, A, odd, f3);
   } else {
     launch_part<T, Q, NS, MODEL, PART_FLOW>(d, A, odd, f3);

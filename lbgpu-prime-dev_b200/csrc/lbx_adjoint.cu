@@ -80,7 +80,47 @@ struct AdjArgs {
   T wc, wu;                // this step's seeds: dJ/dC_eff, dJ/du_x per plane node
   double* acc;             // [blocks][5]: per-block sums of dJ/dg_x, dJ/dg_y,
                            // dJ/dg_z, dJ/dtau, dJ/dtau_s over all steps
+  // the solute's z-face adjoint applied in the step kernel (see adj_face_local)
+  int face_on;             // 1: apply it at this step's face-plane nodes
+  int face_lo_end, face_hi_start;   // face planes: compact [0, lo_end), [hi_start, F)
+  int face_kind[2];        // bottom, top: 0, FACE_CONSTCON or FACE_ZEROGRAD
+  double* face_dprof[2];   // bottom, top: constant-concentration profile gradient
 };
+
+// The adjoint of the solute's face operation of a face node, applied to the
+// adjoints the step kernel is about to store at the node's slots (l[a] at
+// the slot it loaded d_a from).  Where the faces fuse into the step (every
+// unknown's upstream node fluid before an odd step; always before an even
+// one), the forward deposited the unknowns in slots the node itself then
+// read, and every slot the adjoint of the face operation touches is one of
+// the node's own: the same arithmetic, in the same order, as adj_face_plane
+// on the stored values, without a launch of its own.  TOP is a compile-time
+// constant so that l stays in registers.
+template <typename T, int Q, bool TOP>
+__device__ __forceinline__ void adj_face_local(T (&l)[Q], int kind, double* dprof, int ij)
+{
+  if constexpr (Q == 19) {
+    T wsum = wgt<T, 19>(face3_unknown(TOP, 0));
+#pragma unroll
+    for (int q = 1; q < 5; ++q) wsum = wsum + wgt<T, 19>(face3_unknown(TOP, q));
+    T Ax = T(0);
+#pragma unroll
+    for (int q = 0; q < 5; ++q) Ax += wgt<T, 19>(face3_unknown(TOP, q)) * l[face3_unknown(TOP, q)];
+    const T ax = Ax / wsum;
+#pragma unroll
+    for (int q = 0; q < 5; ++q) l[face3_unknown(TOP, q)] = T(0);
+    if (kind == FACE_ZEROGRAD) {
+#pragma unroll
+      for (int a = 0; a < 19; ++a)
+        if (cz(a) == (TOP ? 1 : -1)) l[a] = l[a] + ax;
+    } else {
+#pragma unroll
+      for (int a = 0; a < 19; ++a)
+        if (cz(a) != (TOP ? -1 : 1)) l[a] = l[a] - ax;
+      if (dprof) dprof[ij] += (double)ax;
+    }
+  }
+}
 
 // Sum of v over the block, added by one thread to this block's own row of
 // partial sums (out[q], q < NV).  A block index covers the same nodes in
@@ -112,8 +152,8 @@ __device__ __forceinline__ void block_add(double (&v)[NV], double* out)
 // Adjoint of one AA kernel launch on the compact layout: the solute's
 // (WITH_SOLUTE, first, as the forward's solute depends on the flow's u) and
 // then the flow's, handing dJ/du between them in registers.  256 threads per block, every thread reaches the block reduction.
-// Neighbour indices are re-read where used (L1 hits) rather than held, as
-// in the forward kernel; lam' is loaded first and the forward populations
+// The slots come from a shared-memory table filled once per node (as in
+// the forward kernel); lam' is loaded first and the forward populations
 // stream through running sums, so one 19-value array is live at a time.
 // The solute reads the flow's u of the step from the recompute pass.
 // Resident 256-thread blocks: in FP32 four (64 registers) for the flow
@@ -155,16 +195,31 @@ adj_step(AdjArgs<T> A)
     };
     const int* const fidx_n = A.fidx + n;
     int mm = m;   // laundered between phases so slot addresses are not kept live
-    // slot the forward read d_a from / wrote d'_a to
+    // The slot the forward read d_a from (odd step: slot a of the upstream
+    // node n - c_a, or the node's own opp(a) behind a solid), once per node
+    // into this thread's column of a shared-memory table; the slot it wrote
+    // d'_a to is the one it read d_opp(a) from (the AA pairing), so the table
+    // gives both.  Looked up at every use instead (114 index loads per node
+    // over the two phases), the lookups' instructions dominated the kernel.
+    __shared__ Idx slot_tab[ODD ? Q : 1][256];
+    if (ODD) {
+#pragma unroll
+      for (int a = 0; a < Q; ++a) {
+        Idx v = (Idx)opp(a) * F + (Idx)m;
+        if (a != 0) {
+          const int up = fidx_n[off(opp(a))];
+          if (up >= 0) v = (Idx)a * F + (Idx)up;
+        }
+        slot_tab[a][threadIdx.x] = v;
+      }
+    }
     auto src = [&](int a) -> Idx {
-      if (!ODD || a == 0) return (Idx)opp(a) * F + (Idx)mm;
-      const int up = ld_reload(fidx_n + off(opp(a)));
-      return up >= 0 ? (Idx)a * F + (Idx)up : (Idx)opp(a) * F + (Idx)mm;
+      if (!ODD) return (Idx)opp(a) * F + (Idx)mm;
+      return slot_tab[a][threadIdx.x];
     };
     auto dst = [&](int a) -> Idx {
-      if (!ODD || a == 0) return (Idx)a * F + (Idx)mm;
-      const int dn = ld_reload(fidx_n + off(a));
-      return dn >= 0 ? (Idx)opp(a) * F + (Idx)dn : (Idx)a * F + (Idx)mm;
+      if (!ODD) return (Idx)a * F + (Idx)mm;
+      return slot_tab[opp(a)][threadIdx.x];
     };
     auto launder = [&]() {
       xm = opaque(xm); xp = opaque(xp); ym = opaque(ym); yp = opaque(yp);
@@ -217,7 +272,19 @@ adj_step(AdjArgs<T> A)
       const T sB = s1k * B;
       launder();
 #pragma unroll
-      for (int b = 0; b < Q; ++b) Ls[src(b)] = omw * lam[b] + sB;
+      for (int b = 0; b < Q; ++b) lam[b] = omw * lam[b] + sB;
+      if (A.face_on && (m < A.face_lo_end || m >= A.face_hi_start)) {
+        const bool top = m >= A.face_hi_start;
+        const int kind = top ? A.face_kind[1] : A.face_kind[0];
+        if (kind) {
+          const int nn = ODD ? n : A.fnode[m];
+          const int ij = nn - (top ? (A.LZ - 1) * A.LX * A.LY : 0);
+          if (top) adj_face_local<T, Q, true>(lam, kind, A.face_dprof[1], ij);
+          else adj_face_local<T, Q, false>(lam, kind, A.face_dprof[0], ij);
+        }
+      }
+#pragma unroll
+      for (int b = 0; b < Q; ++b) Ls[src(b)] = lam[b];
       const T k3 = T(3) * w * Ce;
       mux = k3 * M0;
       muy = k3 * M1;
@@ -627,9 +694,22 @@ lbx_status backward_t(lbx_domain* d, lbx_gradient* out, double* dprof_b, double*
       A.wu = in_win ? (T)(ob.w_ux / (nwin * nout)) : T(0);
       solute_live = solute_live || (p.nsubs == 2 && A.wc != T(0));
       const bool sol = p.nsubs == 2 && solute_on(p, t) && solute_live;
+      // the adjoint of the solute's face operations inside the step kernel
+      // where the z faces fuse (adj_face_local), else its own launch
+      const bool face_fused = sol && d->Q == 19 && d->faces3_active &&
+                              (!odd || d->faces3_fuse_odd);
+      if (face_fused) {
+        A.face_on = 1;
+        A.face_lo_end = (int)d->plane_fluid[0];
+        A.face_hi_start = (int)(d->fluid - d->plane_fluid[p.LZ - 1]);
+        A.face_kind[0] = p.zeroconcgrad_b ? FACE_ZEROGRAD : (p.constcon_b_in ? FACE_CONSTCON : 0);
+        A.face_kind[1] = p.zeroconcgrad_t ? FACE_ZEROGRAD : (p.constcon_t_in ? FACE_CONSTCON : 0);
+        A.face_dprof[0] = A.face_kind[0] == FACE_CONSTCON ? st->dpb : nullptr;
+        A.face_dprof[1] = A.face_kind[1] == FACE_CONSTCON ? st->dpt : nullptr;
+      }
       if (d->Q == 19) launch_adj<T, 19>(d, odd, sol, A);
       else launch_adj<T, 9>(d, odd, sol, A);
-      if (solute_live) launch_adj_faces<T>(d, t, (T*)L, st->dpt, st->dpb);
+      if (solute_live && !face_fused) launch_adj_faces<T>(d, t, (T*)L, st->dpt, st->dpb);
       ACK(cudaGetLastError());
     }
   }

@@ -822,7 +822,9 @@ __device__ __forceinline__ void compact_node(const CompactArgs<T>& C, const int 
         face_south<T>(A.face_s[s], A.rho_s[s], A.sc[s].rhoA, A.drho_s[s], shifted, d9);
     }
     const T rho = collide<T, Q, MODEL>(A, s, solute, ODD ? 1 : 2, d, u, n);
-    if (PART == PART_FLOW && A.solute_on) {
+    // the flow's u for the solute launch, or, written out of place by the
+    // joint launch (the adjoint's recomputation), kept for the adjoint
+    if ((PART == PART_FLOW || (PART == PART_ALL && NS == 2 && OOP && s == 0)) && A.solute_on) {
 #pragma unroll
       for (int c = 0; c < D; ++c) A.ubuf[c * A.ustride + m] = u[c];
     }
