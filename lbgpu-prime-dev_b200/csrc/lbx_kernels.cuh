@@ -628,9 +628,10 @@ constexpr int compact_min_blocks()
 }
 
 // The odd step of two substances in one launch (flow, then the solute from
-// the flow's slot table): 64 registers in FP32, where it runs without
-// spills (at six blocks it spilled and ran no faster than the two launches
-// it replaces).
+// the flow's slot table): four resident blocks (64 registers) in FP32,
+// where it runs without spills (at six blocks it spilled and ran no faster
+// than the two launches it replaces); two (128) in FP64, which spills 4-12
+// bytes there and 230-250 at three blocks.
 template <typename T, int PART, int NS, bool FACES3>
 constexpr int compact_step_min_blocks()
 {
