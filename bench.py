@@ -296,6 +296,51 @@ def small_2d_leg(local: int, steps: int) -> dict:
     return out
 
 
+def flow_solute_leg(local: int, steps: int) -> dict:
+    """The coupled flow + solute lattice of the breakthrough case: 192 x 192
+    x 384 D3Q19 FP32, spheres r = 5 to porosity 0.35 with the two z-face
+    planes kept fluid, Zou-He density on the bottom (rho_in = 1.0005) and
+    top (rho_out = 1.0) planes, solute C = 1 held at the bottom, zero
+    gradient at the top, the outlet-plane record on: `steps` steps from rest
+    in one CUDA-event window (one frame at the end).  The roofline counts
+    2 x 152 B per fluid node update (both substances)."""
+    import torch
+    import lbx
+    from lbx import configs
+    p, mask = configs.cfg3_params(4)
+    p.device = local
+    fluid = int(np.count_nonzero(mask != 1))
+    stream = torch.cuda.Stream()
+    with lbx.Domain(p, mask) as dom:
+        dom.set_stream(stream.cuda_stream)
+        # the record is started once: starting it drops the captured graphs
+        dom.btc_start(p.LZ - 1, 40 + steps)
+        dom.init_equilibrium(0, 1.0)
+        dom.init_equilibrium(1, 0.0)
+        dom.run(0, 40, 40)                             # warm-up (graphs)
+        dom.init_equilibrium(0, 1.0)                   # back to rest
+        dom.init_equilibrium(1, 0.0)
+        torch.cuda.synchronize()
+        n0 = dom.launch_count()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        dom.run(0, steps, steps)
+        e1.record(stream)
+        dom.sync()
+        ms = e0.elapsed_time(e1)
+        launches = dom.launch_count() - n0
+        outlet_c = float(dom.btc_read()[-1])
+    peaks = load_peaks()
+    gbs = 2 * Q * REAL * 2 * fluid * steps / (ms / 1e3) / 1e9
+    return {"mlups": round(mask.size * steps / (ms / 1e3) / 1e6, 3),
+            "ms_per_step": round(ms / steps, 5), "steps": steps, "launches": launches,
+            "fluid_nodes": fluid, "roofline_frac": round(gbs / peaks["hbm_gbs"], 4),
+            "outlet_c_last": outlet_c,
+            "workload": "192x192x384 D3Q19 flow + solute FP32, Zou-He z faces, C = 1 inlet, "
+                        "outlet record, %d steps from rest" % steps}
+
+
 def batch_leg(local: int, nsamples: int, steps: int) -> dict:
     """Many small lattices at once: 512 D3Q19 FP32 sphere packs with edges
     32..96 (172.8M nodes, 87.0M fluid) stepped as one batch (one launch per
@@ -516,6 +561,8 @@ def main(argv=None) -> int:
                     help="steps of each run of the FP32-vs-FP64 leg (0: skip it)")
     ap.add_argument("--adjoint-steps", type=int, default=4000,
                     help="steps of the adjoint cost leg (0: skip it)")
+    ap.add_argument("--flow-solute-steps", type=int, default=2000,
+                    help="steps of the flow + solute key (192x192x384 with z faces); 0: skip")
     ap.add_argument("--small-steps", type=int, default=2000,
                     help="steps of the 256^2 D2Q9 FP64 leg (0: skip it)")
     ap.add_argument("--batch-samples", type=int, default=512,
@@ -712,6 +759,8 @@ def main(argv=None) -> int:
         line["adjoint"] = adjoint_leg(local, args.adjoint_steps)
     if args.small_steps > 0:
         line["small_2d"] = small_2d_leg(local, args.small_steps)
+    if args.flow_solute_steps > 0:
+        line["flow_solute"] = flow_solute_leg(local, args.flow_solute_steps)
     if args.batch_samples > 0:
         line["batch"] = batch_leg(local, args.batch_samples, args.batch_steps)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
