@@ -156,11 +156,12 @@ __device__ __forceinline__ void block_add(double (&v)[NV], double* out)
 // the forward kernel); lam' is loaded first and the forward populations
 // stream through running sums, so one 19-value array is live at a time.
 // The solute reads the flow's u of the step from the recompute pass.
-// Resident 256-thread blocks: in FP32 four (64 registers) for the flow
-// alone and three (85) with the solute phase; FP64 keeps about its natural
-// register count (lower caps spill).
+// Resident 256-thread blocks: in FP32 four (64 registers), with or without
+// the solute phase: with the slot table neither spills there (cfg5's
+// backward 3 % faster than at three blocks; five blocks spill and lose);
+// FP64 keeps about its natural register count (lower caps spill).
 template <typename T, bool WITH_SOLUTE>
-constexpr int adj_min_blocks() { return sizeof(T) == 4 ? (WITH_SOLUTE ? 3 : 4) : 2; }
+constexpr int adj_min_blocks() { return sizeof(T) == 4 ? 4 : 2; }
 
 template <typename T, int Q, bool ODD, bool WITH_SOLUTE, bool IDX32>
 __global__ void __launch_bounds__(256, (adj_min_blocks<T, WITH_SOLUTE>()))
