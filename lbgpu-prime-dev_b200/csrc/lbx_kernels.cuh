@@ -755,14 +755,14 @@ __device__ __forceinline__ void compact_node(const CompactArgs<T>& C, const int 
         // repeating the upstream lookups
 #pragma unroll
         for (int a = 0; a < Q; ++a) d[a] = fs[sslot[a][threadIdx.x]];
-      } else {
-      pull(0, m);
-      if (NS == 1) {
+      } else if (NS == 1) {
         // one lookup per direction: measured faster than the row windows
         // below for the flow-only kernels (0.214 vs 0.218 ms at 256^3 FP32)
+        pull(0, m);
 #pragma unroll
         for (int a = 1; a < Q; ++a) pull(a, nb_at(n + off(opp(a))));
       } else {
+        pull(0, m);
         // two substances: upstream neighbours n - c_a grouped by their (y, z)
         // row, three per window (the split flow + solute step pair 1.2%
         // faster at 256^3 FP32)
@@ -790,7 +790,6 @@ __device__ __forceinline__ void compact_node(const CompactArgs<T>& C, const int 
                 pull(a, cx(a) > 0 ? im : (cx(a) < 0 ? ip : i0));
           }
         }
-      }
       }
     } else {
 #pragma unroll
