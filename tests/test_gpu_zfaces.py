@@ -268,9 +268,9 @@ def test_gpu_z_faces_fused_equal_standalone(case):
 def test_gpu_z_faces_side_stream_on_every_path():
     """The compact layout's face-plane launch (and the record of a face
     plane) run on a second stream, forked from and joined back into the
-    step's stream.  Step by step, replayed from captured graphs, and on a
-    caller's stream, FP64 results and the record are bit-identical, and
-    equal to the oracle."""
+    step's stream.  Step by step, replayed from captured graphs, on a
+    caller's stream and on the CUDA default stream (direct launches), FP64
+    results and the record are bit-identical, and equal to the oracle."""
     torch = pytest.importorskip("torch")
     p, sol, f0 = _flow_solute(18, 16, 12, 0.6, 21, **CASES["inlet_bottom"])
     m3 = sol.reshape(12, 16, 18)
@@ -279,11 +279,13 @@ def test_gpu_z_faces_side_stream_on_every_path():
     sol = m3.reshape(-1)
     steps = 40
     out = {}
-    for how in ("steps", "graphs", "caller_stream"):
+    for how in ("steps", "graphs", "caller_stream", "default_stream"):
         with lbx.Domain(to_lbx(p, np.float64, "compact"), sol) as d:
             s = torch.cuda.Stream() if how == "caller_stream" else None
             if s is not None:
                 d.set_stream(s.cuda_stream)
+            if how == "default_stream":
+                d.set_stream(None)
             d.upload_f(f0)
             d.btc_start(p.LZ - 1, steps)
             if how == "steps":
@@ -296,7 +298,7 @@ def test_gpu_z_faces_side_stream_on_every_path():
                 d.set_stream(None)
             d.sync()
             out[how] = (d.download_f(), d.download_mv(), d.btc_read(ux=True))
-    for how in ("graphs", "caller_stream"):
+    for how in ("graphs", "caller_stream", "default_stream"):
         assert np.array_equal(out[how][0], out["steps"][0]), how
         assert np.array_equal(out[how][1], out["steps"][1]), how
         for c in range(2):
