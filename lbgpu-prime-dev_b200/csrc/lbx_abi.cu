@@ -278,15 +278,15 @@ void launch_part(lbx_domain* d, const StepArgs<T>& A, bool odd, const Face3Fused
 // out of place, for the adjoint's recomputation, it also stores u), and an
 // even step is a flow launch that hands u to a solute launch (the solute
 // launch only while the solute is active; fused, the even step spilled and
-// ran slower).  With
-// the z faces fused, the face planes' nodes run in a launch of their own on
-// the side stream, beside the interior launches: in an AA step every node
-// reads and writes only its own set of population slots, the face launch
-// carries the flow's u to the solute in registers (it reads no handoff
-// value of the interior's), and node-indexed outputs (macro variables,
-// plane-record values) are disjoint, so the two touch no common location.
-// Returns true when the face launch went to the side stream: the caller
-// joins it back into the step's stream (step_t).
+// ran slower).
+// With the z faces fused, the face planes' nodes run in a launch of their
+// own on the side stream, beside the interior launches: in an AA step every
+// node reads and writes only its own set of population slots, the face
+// launch carries the flow's u to the solute in registers (it reads no
+// handoff value of the interior's), and node-indexed outputs (macro
+// variables, plane-record values) are disjoint, so the two touch no common
+// location.  Returns true when the face launch went to the side stream: the
+// caller joins it back into the step's stream (step_t).
 template <typename T, int Q, int NS, int MODEL>
 bool launch_aa(lbx_domain* d, const StepArgs<T>& A, bool odd, const Face3Fused<T>* f3)
 {
